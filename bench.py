@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Throughput of the STEAM field step on B200: Mvoxels/s at 2048^2 x 256 FP32.
+
+Workload: the finest size class of the 2048 x 2048 x 256 domain (dx = dz =
+100 m, k = 200 m; alpha = 1.8, C1 = 0.1, H = 1/3, Hz = 5/9, spheroscale 1 km,
+seed 0) taken through one cascade class -- world-keyed Philox noise, extremal
+Levy multiplier, flux convolution with clip and unit-mean restore, advective
+weight x signed amplitude x bound taper for h and qt, second convolution,
+bounded amplitude-preserving add -- and the thermodynamic map to condensate.
+Synthetic seeded state (flux, h', qt') with those shapes stands in for the
+previous classes; there is no dataset.  Every field (4.3 GB) is larger than
+L2, so no flush is needed between steps.
+
+`value`: device-resident, CUDA events on the launching stream, max over
+ranks.  `e2e`: the same step through the public host-array API
+(steam_b200.simulate.field_step) with pinned host inputs/outputs, transfers
+inside the timed region.  `--impl reference` times the CPU oracle port of the
+same step on a bounded sub-box on the host cores.
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torchrun, each rank advances its own independent field (replicas).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+METRIC = "Mvoxels/s at 2048^2x256 FP32 (field step: noise, flux, 2 scalar convolutions, bounded add, condensate)"
+ALPHA, C1, H, HZ = 1.8, 0.1, 1.0 / 3.0, 5.0 / 9.0
+BOUNDS = (315 * 1004, 355 * 1004, 0.0, 0.03)
+# Algorithmic HBM bytes per voxel of one FP32 field step: flux read+write (8),
+# h' and qt' read+write (16), qc and qi written (8).
+STEP_BYTES_PER_VOXEL = 32
+
+
+def parse(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--ny", type=int, default=2048)
+    ap.add_argument("--nz", type=int, default=256)
+    ap.add_argument("--dtype", choices=("f32", "f64"), default="f32")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, nargs=3, default=(128, 128, 256),
+                    metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# Workload setup (host, shared by both arms)
+# ---------------------------------------------------------------------------
+
+def workload(nx, ny, nz):
+    from steam_b200 import simulate as sim
+    height = nz * 100.0
+    zp = np.arange(int(height / 50.0) + 1) * 50.0
+    hp = (340e3 - 20e3 * zp / zp[-1]).astype(np.float32)
+    qp = (0.018 - 0.016 * zp / zp[-1]).astype(np.float32)
+    sph = np.full(zp.size, 1000.0)
+    k = 200.0
+    outer = nx * 100.0
+    grids = sim._compute_all_grids(np.array([k]), nx * 100.0, ny * 100.0, height, (1, 1, 1),
+                                   sph, zp)
+    shape = (int(grids['nx'][0]), int(grids['ny'][0]), int(grids['nz'][0]))
+    assert shape == (nx, ny, nz), shape
+    kzl = sim._k_z('piecewise_isotropic_below_spheroscale', outer, sph)
+    C_h = sim._compute_normalization(hp, zp, kzl, np.array([k]), outer, grids,
+                                     hurst_horizontal=H)[0]
+    C_q = sim._compute_normalization(qp, zp, kzl, np.array([k]), outer, grids,
+                                     hurst_horizontal=H)[0]
+    b_h = sim._bound_buffers([C_h], 1, H)[0]
+    b_q = sim._bound_buffers([C_q], 1, H)[0]
+    aspect = (sim._k_z('piecewise_isotropic_below_spheroscale', k,
+                       np.interp(grids['z_arrays'][0], zp, sph)) / k).astype(np.float32)
+    # finest class key of a seed-0 root run over this domain
+    n_classes = int(round(np.log(outer / 200.0) / np.log(2.0))) + 1
+    key = sim.class_key(np.random.SeedSequence(0).spawn(n_classes)[-1])
+    return dict(sim=sim, grids=grids, zp=zp, hp=hp, qp=qp, C_h=C_h, C_q=C_q, b_h=b_h,
+                b_q=b_q, aspect=aspect, key=key, shape=shape)
+
+
+# ---------------------------------------------------------------------------
+# Clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '', 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace('.', '', 1).isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        loaded = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# Per-call device timing (one instrumented step, outside the timed region)
+# ---------------------------------------------------------------------------
+
+class CallTimer:
+    """Wraps the library's entry points with CUDA events on torch's current
+    stream (the stream every call is launched on)."""
+
+    def __init__(self, lib, torch):
+        self.lib, self.torch = lib, torch
+        self.records = []
+        self.saved = {}
+
+    def __enter__(self):
+        from steam_b200 import _lib
+        for name in _lib.exported_symbols():
+            fn = getattr(self.lib, name)
+            self.saved[name] = fn
+
+            def wrapped(*args, _fn=fn, _name=name):
+                s = self.torch.cuda.Event(enable_timing=True)
+                e = self.torch.cuda.Event(enable_timing=True)
+                s.record()
+                rc = _fn(*args)
+                e.record()
+                self.records.append((_name, s, e))
+                return rc
+            setattr(self.lib, name, wrapped)
+        return self
+
+    def __exit__(self, *exc):
+        for name, fn in self.saved.items():
+            setattr(self.lib, name, fn)
+
+    def totals(self):
+        self.torch.cuda.synchronize()
+        out = {}
+        for name, s, e in self.records:
+            if name.endswith("workspace_bytes") or name in ("steam_last_error",
+                                                           "steam_launch_count"):
+                continue
+            t, n = out.get(name, (0.0, 0))
+            out[name] = (t + s.elapsed_time(e), n + 1)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port of the same step on a bounded sub-box
+# ---------------------------------------------------------------------------
+
+def cpu_step(nx, ny, nz):
+    """Time one oracle field step on (nx, ny, nz); returns (seconds, threads)."""
+    from oracle import steam_oracle as O
+    w = workload(nx, ny, nz)
+    z = w['grids']['z_arrays'][0]
+    hm = np.interp(z, w['zp'], w['hp']).astype(np.float32)
+    qm = np.interp(z, w['zp'], w['qp']).astype(np.float32)
+    rng = np.random.default_rng(1)
+    shape = (nx, ny, nz)
+    h = (600.0 * rng.standard_normal(shape)).astype(np.float32)
+    q = (0.0006 * rng.standard_normal(shape)).astype(np.float32)
+    F = (1.0 + 0.1 * rng.random(shape)).astype(np.float32)
+    kern = O.turbulon_envelope(1, 0.5, 0.5, 0.5)
+    t0 = time.perf_counter()
+    O.class_step(h, q, F, tuple(int(k) for k in w['key']), kern, h_mean=hm, qt_mean=qm,
+                 z_coords=z, dx=100.0, dy=100.0, aspect=w['aspect'], C_h=w['C_h'],
+                 C_qt=w['C_q'], b_h=w['b_h'], b_qt=w['b_q'], h_min=BOUNDS[0],
+                 h_max=BOUNDS[1], qt_min=BOUNDS[2], qt_max=BOUNDS[3], flux_noise_scale=C1,
+                 n_per_dyad=1, sparsity_factors=(1, 1, 1), n_zero=2, alpha=ALPHA)
+    O.recover_diagnostics(np.clip(h + hm, BOUNDS[0], BOUNDS[1]),
+                          np.clip(q + qm, BOUNDS[2], BOUNDS[3]), z, 101325.0)
+    return time.perf_counter() - t0, O.N_THREADS
+
+
+def cpu_baseline(sample):
+    nx, ny, nz = sample
+    secs, threads = cpu_step(nx, ny, nz)
+    return {"value": nx * ny * nz / secs / 1e6, "unit": "Mvoxels/s", "cores": threads,
+            "kind": "port",
+            "sample": f"one oracle field step on a {nx}x{ny}x{nz} sub-box of the workload "
+                      f"({secs:.1f} s on {threads} host threads; numpy/scipy restatement "
+                      f"of the reference's CPU path)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    nx, ny, nz = args.cpu_sample
+    for _ in range(max(0, args.warmup) and 1):
+        cpu_step(min(nx, 32), min(ny, 32), nz)
+    times = []
+    threads = 1
+    for _ in range(max(1, args.steps)):
+        secs, threads = cpu_step(nx, ny, nz)
+        times.append(secs)
+    per = float(np.mean(times))
+    value = nx * ny * nz / per / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mvoxels/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype.replace("f", "f"), "data": "synthetic (seeded)",
+        "impl": "reference",
+        "config": {"workload": f"field step, {args.nx}x{args.ny}x{args.nz} domain; each "
+                               f"reference step a {nx}x{ny}x{nz} sub-box",
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "Mvoxels/s", "cores": threads,
+                         "kind": "port",
+                         "sample": f"{nx}x{ny}x{nz} sub-box per step, mean of {len(times)}"},
+        "e2e": {"value": value, "unit": "Mvoxels/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Device arm
+# ---------------------------------------------------------------------------
+
+def main(argv=None):
+    args = parse(argv)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from steam_b200 import _lib
+    lib = _lib.load()
+    np_t = np.float32 if args.dtype == "f32" else np.float64
+    tdt = torch.float32 if args.dtype == "f32" else torch.float64
+    w = workload(args.nx, args.ny, args.nz)
+    sim = w['sim']
+    shape = w['shape']
+    nvox = shape[0] * shape[1] * shape[2]
+    setup = sim.make_class_setup(
+        w['grids'], 0, h_profile=w['hp'], qt_profile=w['qp'], z_profile=w['zp'],
+        C_h=w['C_h'], C_qt=w['C_q'], b_h=w['b_h'], b_qt=w['b_q'], aspect=w['aspect'],
+        bounds=BOUNDS, key=w['key'], flux_noise_scale=C1, flux_alpha=ALPHA, dtype=np_t)
+    from steam_b200.thermodynamics import recover_diagnostics_device
+    from steam_b200.ledger import ClassLedger
+
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    h0 = 600.0 * torch.randn(shape, generator=gen, device="cuda", dtype=tdt)
+    q0 = 0.0006 * torch.randn(shape, generator=gen, device="cuda", dtype=tdt)
+    F0 = 1.0 + 0.1 * torch.rand(shape, generator=gen, device="cuda", dtype=tdt)
+    hp, qp, F = h0, q0, F0
+    diag = {k: torch.empty_like(hp) for k in ("T", "qv", "qc", "qi", "p")}
+    bounds = [float(np_t(b)) for b in BOUNDS]
+
+    def step():
+        # each step advances the resident state by one class: identical work
+        # per step, and the state stays a realistic cascade state
+        sim.run_class(hp, qp, F, None, None, None, setup, ClassLedger())
+        recover_diagnostics_device(hp, qp, setup.z, 101325.0, out=diag,
+                                   h_mean=setup.h_mean, qt_mean=setup.qt_mean, bounds=bounds)
+
+    for _ in range(max(0, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.steam_launch_count()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for _ in range(args.steps):
+        step()
+    t_end.record()
+    torch.cuda.synchronize()
+    launches = lib.steam_launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    ms = t_start.elapsed_time(t_end)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / max(args.steps, 1)
+    value = world * nvox * args.steps / (ms / 1e3) / 1e6
+
+    # one instrumented step: per-entry device time for the roofline
+    with CallTimer(lib, torch) as timer:
+        step()
+    calls = timer.totals()
+    dominant = max(calls.items(), key=lambda kv: kv[1][0])
+    elem = 4 if args.dtype == "f32" else 8
+    # algorithmic bytes of one launch of each entry point at this shape
+    alg = {
+        "steam_conv_separable": 2 * elem * nvox,        # read input, write output
+        "steam_flux_noise": 2 * elem * nvox,            # read flux, write product
+        "steam_scalar_pattern": 3 * elem * nvox,        # read pert + product, write W
+        "steam_bounded_add": 3 * elem * nvox,           # read pert + increment, write pert
+        "steam_thermo": 7 * elem * nvox,                # read h', qt'; write T, qv, qc, qi, p
+        "steam_scale": 2 * elem * nvox,
+    }
+    name, (tot_ms, n_calls) = dominant
+    per_launch_ms = tot_ms / n_calls
+    peaks = {}
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg.get(name, 2 * elem * nvox) / (per_launch_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "per_launch_ms": per_launch_ms,
+                "peak_source": "measured" if peaks else "fallback",
+                "breakdown_ms": {k: round(v[0], 3) for k, v in sorted(
+                    calls.items(), key=lambda kv: -kv[1][0])}}
+
+    # end to end through the public host-array API, pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        def pinned_copy(t):
+            host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            host.copy_(t)
+            return host.numpy()
+        h_host, q_host, F_host = pinned_copy(hp), pinned_copy(qp), pinned_copy(F)
+        del diag
+        sim.field_step(h_host, q_host, F_host, setup)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        total = 0.0
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out, _ = sim.field_step(h_host, q_host, F_host, setup)
+            e1.record()
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([total], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        e2e = {"value": world * nvox * args.e2e_steps / (total / 1e3) / 1e6,
+               "unit": "Mvoxels/s", "h2d_bytes_per_step": 3 * elem * nvox,
+               "d2h_bytes_per_step": 5 * elem * nvox,
+               "api": "steam_b200.simulate.field_step (numpy in, numpy out)"}
+        del h_host, q_host, F_host
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(tuple(args.cpu_sample))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mvoxels/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.dtype, "data": "synthetic (seeded state and noise)",
+            "config": {"workload": f"field step at {shape[0]}x{shape[1]}x{shape[2]} "
+                                   f"(finest class of the 2048^2x256 domain, k=200 m, "
+                                   f"dx=dz=100 m) + condensate",
+                       "alpha": ALPHA, "C1": C1, "H": H, "Hz": HZ, "seed": 0,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (4.3 GB fields); no flush"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

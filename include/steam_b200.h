@@ -1,0 +1,254 @@
+/*
+ * steam_b200.h -- C ABI of the B200 (sm_100a) STEAM field-generation path.
+ *
+ * Conventions shared by every entry point:
+ *   - Fields are C-order (nx, ny, nz) arrays, z fastest, in device memory the
+ *     caller owns (e.g. torch CUDA tensors).  `dtype` selects float32
+ *     (STEAM_F32) or float64 (STEAM_F64) element type for every field
+ *     argument of the call.
+ *   - Per-level vectors (length nz) and small parameter tables are HOST
+ *     pointers unless the name ends in `_dev`.
+ *   - `stream` is a cudaStream_t; all work is enqueued on it.  Entry points
+ *     that return host scalars synchronise that stream before returning.
+ *   - Entries that need scratch device memory take (workspace,
+ *     workspace_bytes); the matching *_workspace_bytes() query gives the size.
+ *   - Every entry returns 0 (STEAM_OK) or a STEAM_ERR_* code; the message is
+ *     available from steam_last_error() on the calling thread.
+ *   - A `window` (x0, x1, y0, y1) restricts every realized mean to a nest's
+ *     own extent; NULL means the whole array (a root run).
+ *
+ * Each declaration names the reference (thomasdewitt/STEAM) interface it
+ * replaces, by file:line.
+ */
+#ifndef STEAM_B200_H
+#define STEAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* steam_stream_t;
+
+enum { STEAM_F32 = 0, STEAM_F64 = 1 };
+
+enum {
+  STEAM_OK = 0,
+  STEAM_ERR_ARG = 1,          /* bad argument (maps to ValueError)         */
+  STEAM_ERR_CUDA = 2,         /* CUDA runtime error (maps to RuntimeError) */
+  STEAM_ERR_WORKSPACE = 3,    /* workspace too small (maps to MemoryError) */
+  STEAM_ERR_UNSUPPORTED = 4   /* shape/option outside the kernels' range   */
+};
+
+/* Where a working array sits in the world (steam/simulate.py:520-551,
+ * NoiseRegion): array shape, world index of cell (0,0,0) on this class's
+ * world grid, the world grid's shape (x and y wrap, z never does), the
+ * sparsity factors and the class's 96-bit Philox key (steam/noise.py:133). */
+typedef struct {
+  int64_t shape[3];
+  int64_t origin[3];
+  int64_t world[3];
+  int32_t sparsity[3];
+  uint32_t key[3];
+} steam_region_t;
+
+/* Domain window (steam/simulate.py:2049, _inner_view). */
+typedef struct {
+  int64_t x0, x1, y0, y1;
+} steam_window_t;
+
+const char* steam_last_error(void);
+int steam_version(void);
+/* Number of kernels this library has enqueued since it was loaded. */
+unsigned long long steam_launch_count(void);
+
+/* ---- a1-a3: world-keyed uniforms --------------------------------------
+ * Replaces keyed_uniforms (steam/noise.py:103-130).  world_i* are DEVICE
+ * int64 index vectors (already wrapped by the caller; iy must lie in
+ * [0, 2^32)); lane0/lane1 are DEVICE float32 outputs of length nx*ny*nz in
+ * C order over (ix, iy, iz). */
+int steam_keyed_uniforms(const int64_t* world_ix, int64_t nx,
+                         const int64_t* world_iy, int64_t ny,
+                         const int64_t* world_iz, int64_t nz,
+                         uint32_t key0, uint32_t key1, uint32_t key2,
+                         float* lane0, float* lane1, steam_stream_t stream);
+
+/* ---- a5-a6: sparse world-keyed extremal Levy field --------------------
+ * Replaces _keyed_sparse_levy (steam/simulate.py:554-598) with its CMS
+ * transform (_levy_from_uniforms, steam/simulate.py:441-479).  Writes the
+ * generator gamma (zero off the turbulon-centre sub-lattice) to `out`. */
+int steam_levy_field(int dtype, const steam_region_t* region, double alpha,
+                     void* out, steam_stream_t stream);
+
+/* ---- a7 + a11 measure: multiplier noise fused with the entering sums ----
+ * Replaces the first half of _advance_flux (steam/simulate.py:2128-2188):
+ * gamma -> zero bottom/top n_zero levels -> eps = expm1(scale*gamma - shift)
+ * (0 off-centre) -> product = eps * flux.  sums_out (HOST, 4 doubles) gets
+ * { sum(flux) over window, count of window cells, sum|eps| over window,
+ *   count of nonzero eps over window }. */
+size_t steam_flux_noise_workspace_bytes(void);
+int steam_flux_noise(int dtype, const steam_region_t* region, double alpha,
+                     double per_class_scale, double shift, int32_t n_zero,
+                     int32_t zero_bottom, int32_t zero_top, const void* flux,
+                     void* product, const steam_window_t* window,
+                     double* sums_out, void* workspace, size_t workspace_bytes,
+                     steam_stream_t stream);
+
+/* ---- a9/a10/a13: convolution, circular x/y and linear z ----------------
+ * Replaces convolve_fft_xy_oa_z (steam/utils.py:293-427) and the CONVOLVE
+ * hook (steam/simulate.py:41).  The kernel is given as a separable network
+ * (exactly what the turbulon kernels are, up to float32 rounding):
+ *   u_c   = f  (*)_z  Z_c                     c < n_z
+ *   v_p   = u_{pair_z[p]} (*)_y Y_{pair_y[p]} p < n_pairs
+ *   w_a   = sum_p mix[a * n_pairs + p] v_p    a < n_x
+ *   out   = epilogue( sum_a w_a (*)_x X_a )
+ * with x and y circular over the array period and z linear (zero padded);
+ * each axis' filter of length k has its centre at index c (out[i] =
+ * sum_j F[j] in[i - j + c]).  Taps are HOST doubles: z_taps[n_z*kz],
+ * y_taps[n_y*ky], x_taps[n_x*kx].
+ * `pre_div`/`pre_mul` (HOST per-level, may be NULL) scale the input on the
+ * fly: f' = (f / pre_div[z]) * pre_mul[z] (the pattern normalisation of
+ * steam/simulate.py:1989-1992).
+ * Epilogues: STEAM_EPI_STORE writes out; STEAM_EPI_FLUX treats `out` as the
+ * flux F and applies F = max(F + conv, 0) (steam/simulate.py:2192-2203),
+ * writing to sums_out (HOST, 3 doubles) { sum(F) over window, window cells,
+ * count of F+conv < 0 over the whole array }. */
+enum { STEAM_EPI_STORE = 0, STEAM_EPI_FLUX = 1 };
+typedef struct {
+  int32_t kz, ky, kx;
+  int32_t cz, cy, cx;
+  int32_t n_z, n_y, n_x, n_pairs;
+  int32_t pair_z[16];
+  int32_t pair_y[16];
+  double mix[64];
+} steam_sepconv_t;
+size_t steam_conv_workspace_bytes(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                  const steam_sepconv_t* spec);
+int steam_conv_separable(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                         const steam_sepconv_t* spec, const double* z_taps,
+                         const double* y_taps, const double* x_taps,
+                         const void* in, const double* pre_div,
+                         const double* pre_mul, void* out, int32_t epilogue,
+                         const steam_window_t* window, double* sums_out,
+                         void* workspace, size_t workspace_bytes,
+                         steam_stream_t stream);
+/* Dense-kernel form (any kernel; direct summation over the taps).  `kernel`
+ * is a DEVICE array (kx, ky, kz) of the call's dtype, already folded onto the
+ * field period; centres are (k-1)//2 per axis. */
+int steam_conv_dense(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                     const void* kernel, int32_t kx, int32_t ky, int32_t kz,
+                     const void* in, void* out, steam_stream_t stream);
+
+/* ---- a11 apply: scalar rescale ----------------------------------------
+ * field *= scale (the volume-mean restore of steam/simulate.py:2208-2215;
+ * scale is rounded to the dtype first) or, with fill != 0, field = scale. */
+int steam_scale(int dtype, int64_t n, void* field, double scale, int32_t fill,
+                steam_stream_t stream);
+
+/* ---- level-weighted accumulate ------------------------------------------
+ * acc += coef[z] * (a - b), or coef[z] * a when b is NULL: the compensation
+ * deficit update of cascade_loop (steam/simulate.py:1917, 2024).  coef is a
+ * HOST per-level vector. */
+int steam_accumulate_levels(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                            void* acc, const void* a, const void* b,
+                            const double* coef, steam_stream_t stream);
+
+/* ---- per-level reductions (steam/simulate.py:2933-2947) ---------------
+ * For each level z: sums_out[4*z + {0,1,2,3}] = { sum f, sum |f|, count of
+ * nonzero f, count of cells } over the window (HOST output, 4*nz doubles). */
+size_t steam_level_sums_workspace_bytes(int64_t nz);
+int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                     const void* field, const steam_window_t* window,
+                     double* sums_out, void* workspace, size_t workspace_bytes,
+                     steam_stream_t stream);
+
+/* ---- a12: scalar pattern ----------------------------------------------
+ * Replaces the per-scalar pattern of cascade_loop (steam/simulate.py:
+ * 1928-1983): running = pert + mean_1d; W = advective weight (periodic
+ * x/y, np.gradient z, steam/simulate.py:2787-2868); W *= product * s_scale
+ * (the signed amplitude S_k); W *= bound taper (steam/simulate.py:2905-2930).
+ * Writes W and level_sums_out (HOST, 2*nz doubles) { sum|W|, count W != 0 }
+ * per level over the window.  z_coords (HOST, nz doubles) are the level
+ * heights (np.gradient semantics), aspect and buffer_b are HOST per-level.
+ * product == NULL leaves out the amplitude and buffer_b == NULL the taper,
+ * which gives the advective weight alone (steam/simulate.py:2843-2868). */
+size_t steam_scalar_pattern_workspace_bytes(int64_t nz);
+int steam_scalar_pattern(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                         const void* pert, const double* mean_1d,
+                         const void* product, double s_scale, double dx,
+                         double dy, const double* z_coords,
+                         const double* aspect, const double* buffer_b,
+                         double phi_min, double phi_max, void* w_out,
+                         const steam_window_t* window, double* level_sums_out,
+                         void* workspace, size_t workspace_bytes,
+                         steam_stream_t stream);
+
+/* ---- a14: bounded amplitude-preserving add -----------------------------
+ * Replaces _bounded_amplitude_add (steam/simulate.py:3114-3283): per level,
+ * the demean / clip / rescale-to-A0 loop (at most n_rescale steps), a final
+ * demean and clip, then the zero-mean shift mu, solved exactly (bracketed
+ * Newton on the piecewise-linear level mean) instead of by 60 bisection
+ * sweeps.  pert += delta; with record_applied the increment buffer is left
+ * holding pert_after - pert_before.  ledger_out (HOST, may be NULL) receives
+ * per level { a0, n_loop, final_demean, mu (NaN if none), n_sweeps }. */
+size_t steam_bounded_add_workspace_bytes(int64_t nz, int32_t n_rescale);
+int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                      void* pert, const double* mean_1d, void* increment,
+                      double phi_min, double phi_max,
+                      const steam_window_t* window, int32_t n_rescale,
+                      int32_t record_applied, double* ledger_out,
+                      void* workspace, size_t workspace_bytes,
+                      steam_stream_t stream);
+
+/* ---- a16: mean-preserving projection onto bounds -----------------------
+ * Replaces _project_onto_bounds (steam/simulate.py:3417-3489) for levels
+ * with a violation; float64 level arithmetic.  mu_out (HOST, nz doubles,
+ * may be NULL) is NaN for untouched levels. */
+int steam_project_bounds(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                         void* pert, const double* mean_1d, double phi_min,
+                         double phi_max, const steam_window_t* window,
+                         double* mu_out, void* workspace,
+                         size_t workspace_bytes, steam_stream_t stream);
+
+/* ---- a15: periodic trilinear regrid -------------------------------------
+ * Replaces zoom_trilinear (steam/utils.py:507-534): align_corners=False,
+ * x/y wrap when periodic_x/periodic_y, z clamps.  Upsampling or identity on
+ * periodic axes. */
+int steam_regrid(int dtype, const void* in, int64_t nx, int64_t ny, int64_t nz,
+                 void* out, int64_t mx, int64_t my, int64_t mz,
+                 int32_t periodic_x, int32_t periodic_y, steam_stream_t stream);
+
+/* ---- a17: thermodynamic column solve ------------------------------------
+ * Replaces recover_diagnostics (steam/thermodynamics.py:25-123): dry
+ * temperature, Bolton saturation, 5 Newton steps, ice/liquid partition and a
+ * float64 hypsometric pressure march.  z_values (HOST, nz doubles); surface
+ * pressure is a scalar unless ps_field_dev (DEVICE float64 nx*ny) is given.
+ * With h_mean/qt_mean (HOST per-level, both or neither) the inputs are
+ * perturbations and the output composition of a deficit-free run is fused in
+ * front (steam/simulate.py:3586-3598): h = clamp(h' + h_mean, bounds[0..1]),
+ * qt = clamp(qt' + qt_mean, bounds[2..3]).
+ * Outputs T, qv, qc, qi, p are DEVICE arrays of the call's dtype. */
+int steam_thermo(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* h,
+                 const void* qt, const double* z_values, const double* h_mean,
+                 const double* qt_mean, const double* bounds,
+                 double surface_pressure, const double* ps_field_dev,
+                 void* T, void* qv, void* qc, void* qi, void* p,
+                 steam_stream_t stream);
+
+/* ---- a8: turbulon kernel build ------------------------------------------
+ * Replaces _turbulon_envelope (steam/simulate.py:2503-2556) with the shapes
+ * of steam/turbulons.py:23-48 (shape 0 mexican_hat, 1 morlet_omega0_6):
+ * box +-ceil(support*k/d) per axis, Gaussian-weighted zero-sum correction
+ * with its two sums taken in float64 on the device.  `out` is a DEVICE
+ * array of shape dims_out (HOST, 3 int64, filled by a NULL-out call). */
+int steam_kernel_build(int dtype, double k, double dx, double dy, double dz,
+                       double support_factor, int32_t shape, void* out,
+                       int64_t* dims_out, steam_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STEAM_B200_H */

@@ -1,0 +1,216 @@
+// Shared device helpers for the STEAM B200 kernels: error plumbing, the
+// Philox4x32-10 counter generator, the Chambers-Mallows-Stuck transform,
+// deterministic block reductions and launch geometry.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string>
+
+#include "../../include/steam_b200.h"
+
+namespace steam {
+
+// ---------------------------------------------------------------------------
+// Error plumbing: every C-ABI entry returns a status and records a message.
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define STEAM_CUDA(call)                                                       \
+  do {                                                                         \
+    cudaError_t err__ = (call);                                                \
+    if (err__ != cudaSuccess)                                                  \
+      return ::steam::fail(STEAM_ERR_CUDA,                                     \
+                           std::string(#call) + ": " +                         \
+                               cudaGetErrorString(err__));                     \
+  } while (0)
+
+// Counts every kernel this library enqueues (steam_launch_count()).
+void count_launch();
+
+#define STEAM_LAUNCH_CHECK(name)                                               \
+  do {                                                                         \
+    ::steam::count_launch();                                                   \
+    cudaError_t err__ = cudaGetLastError();                                    \
+    if (err__ != cudaSuccess)                                                  \
+      return ::steam::fail(STEAM_ERR_CUDA, std::string(name) + " launch: " +   \
+                                               cudaGetErrorString(err__));     \
+  } while (0)
+
+#define STEAM_REQUIRE(cond, msg)                                               \
+  do {                                                                         \
+    if (!(cond)) return ::steam::fail(STEAM_ERR_ARG, (msg));                   \
+  } while (0)
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+// Grid size for a grid-stride kernel over n items with `per_block` items per
+// block-iteration: a multiple of the SM count, never more than needed.
+int stride_grid(int64_t n, int per_block, int blocks_per_sm = 8);
+
+// Workspace carving: bump allocator over the caller's workspace buffer.
+struct Carver {
+  char* base;
+  size_t size;
+  size_t used = 0;
+  Carver(void* b, size_t s) : base(static_cast<char*>(b)), size(s) {}
+  template <typename T>
+  T* take(size_t count) {
+    size_t off = (used + 255) & ~size_t(255);
+    size_t bytes = count * sizeof(T);
+    if (base == nullptr || off + bytes > size) return nullptr;
+    used = off + bytes;
+    return reinterpret_cast<T*>(base + off);
+  }
+};
+inline size_t carve_bytes(size_t count, size_t elem) {
+  return ((count * elem) + 255) & ~size_t(255);
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al. 2011), in the counter/key layout of the
+// reference's world-keyed generator: counter (ix, iy, iz, key2), key
+// (key0, key1).  Round 0 sees the raw 64-bit world indices of x and z, so an
+// index outside [0, 2^32) (a negative z below a nest's ground) multiplies
+// modulo 2^64 exactly as the reference's uint64 arithmetic does; every word
+// is 32-bit from round 1 on.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void philox_site(int64_t ix, uint32_t iy, int64_t iz,
+                                            uint32_t key0, uint32_t key1,
+                                            uint32_t key2, uint32_t& r0,
+                                            uint32_t& r1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+  uint32_t c0, c1, c2, c3;
+  {
+    unsigned long long p0 = (unsigned long long)M0 * (unsigned long long)ix;
+    unsigned long long p1 = (unsigned long long)M1 * (unsigned long long)iz;
+    c0 = (uint32_t)(p1 >> 32) ^ iy ^ key0;
+    c1 = (uint32_t)p1;
+    c2 = (uint32_t)(p0 >> 32) ^ key2 ^ key1;
+    c3 = (uint32_t)p0;
+  }
+  uint32_t k0 = key0, k1 = key1;
+#pragma unroll
+  for (int r = 1; r < 10; ++r) {
+    k0 += W0;
+    k1 += W1;
+    uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
+    uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+    uint32_t n0 = hi1 ^ c1 ^ k0;
+    uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  r0 = c0;
+  r1 = c1;
+}
+
+// (r >> 8) * 2^-24: the float32 lattice of numpy's next_float.
+__device__ __forceinline__ float lattice_uniform(uint32_t r) {
+  return (float)(r >> 8) * (1.0f / 16777216.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Chambers-Mallows-Stuck extremal stable draw, in the operation order of the
+// reference transform: phi=(u0-1/2)pi, R=-log(max(u1,eps)),
+// fac=(max(cos phi,eps)|a-1|)^(-1/a), sh=a(phi-phi0),
+// tail=(max(cos(phi-sh),eps)/R)^((1-a)/a), gamma=sin(sh)*sign*fac*tail.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct LevyParams {
+  T alpha, phi0, sign, am1, fexp, texp, pi;
+};
+
+template <typename T>
+LevyParams<T> make_levy(double alpha) {
+  LevyParams<T> p;
+  const double PI = 3.14159265358979323846;
+  p.alpha = (T)alpha;
+  p.phi0 = (T)(-(PI / 2.0) * (1.0 - fabs(1.0 - alpha)) / alpha);
+  p.sign = (T)(alpha > 1.0 ? 1.0 : -1.0);
+  p.am1 = (T)fabs(alpha - 1.0);
+  p.fexp = (T)(-1.0 / alpha);
+  p.texp = (T)((1.0 - alpha) / alpha);
+  p.pi = (T)PI;
+  return p;
+}
+
+__device__ __forceinline__ float d_cos(float x) { return cosf(x); }
+__device__ __forceinline__ double d_cos(double x) { return cos(x); }
+__device__ __forceinline__ float d_sin(float x) { return sinf(x); }
+__device__ __forceinline__ double d_sin(double x) { return sin(x); }
+__device__ __forceinline__ float d_log(float x) { return logf(x); }
+__device__ __forceinline__ double d_log(double x) { return log(x); }
+__device__ __forceinline__ float d_pow(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ double d_pow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float d_exp(float x) { return expf(x); }
+__device__ __forceinline__ double d_exp(double x) { return exp(x); }
+__device__ __forceinline__ float d_expm1(float x) { return expm1f(x); }
+__device__ __forceinline__ double d_expm1(double x) { return expm1(x); }
+__device__ __forceinline__ float d_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double d_sqrt(double x) { return sqrt(x); }
+
+// Uncontracted arithmetic: the reference evaluates these products and sums as
+// separate rounded operations, so they are kept out of FMA contraction.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ T levy_draw(T u0, T u1, const LevyParams<T>& p) {
+  const T eps = (T)1e-6;
+  T phi = mul_rn(sub_rn(u0, (T)0.5), p.pi);
+  T R = -d_log(u1 > eps ? u1 : eps);
+  T c = d_cos(phi);
+  T fac = d_pow(mul_rn(c > eps ? c : eps, p.am1), p.fexp);
+  T sh = mul_rn(sub_rn(phi, p.phi0), p.alpha);
+  T c2 = d_cos(sub_rn(phi, sh));
+  T tail = d_pow((c2 > eps ? c2 : eps) / R, p.texp);
+  return mul_rn(mul_rn(mul_rn(d_sin(sh), p.sign), fac), tail);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions: per-thread float64 accumulators, a fixed-shape
+// block tree, per-block partials, and a final fixed-order pass.  The sum of
+// the same data on the same device is therefore bit-identical run to run.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sums `v` over the block (blockDim.x a multiple of 32, <= 1024). Result valid
+// in thread 0. `scratch` holds >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* scratch) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    r = lane < nw ? scratch[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;
+}
+
+// Sums partials[q * nblocks + b] over b for q < nq, in fixed order; writes
+// out[q].  Launch with one block of 256 threads per q.
+__global__ void reduce_partials_kernel(const double* __restrict__ partials,
+                                       int nblocks, double* __restrict__ out);
+
+int reduce_partials(const double* partials, int nblocks, int nq, double* out,
+                    cudaStream_t stream);
+
+}  // namespace steam

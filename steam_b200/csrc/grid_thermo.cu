@@ -1,0 +1,421 @@
+// Class-to-class periodic trilinear regrid, the turbulon kernel build and the
+// thermodynamic column solve.
+#include "common.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace steam {
+
+// ---- a15: regrid ------------------------------------------------------------
+// One axis of torch's align_corners=False linear resample over the wrapped-pad
+// geometry of the reference (pad p source cells, crop c target cells per
+// periodic side, p/c = n_in/n_out in lowest terms).  Source indices are mapped
+// back onto the unpadded source periodically.
+struct Axis {
+  int64_t n_in, n_out, pad, crop, big_in;
+  float scale;
+  int periodic;
+};
+
+static int64_t gcd64(int64_t a, int64_t b) {
+  while (b) {
+    int64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+static Axis make_axis(int64_t n_in, int64_t n_out, bool periodic) {
+  Axis a;
+  a.n_in = n_in;
+  a.n_out = n_out;
+  a.periodic = periodic ? 1 : 0;
+  if (periodic) {
+    int64_t g = gcd64(n_in, n_out);
+    a.pad = n_in / g;
+    a.crop = n_out / g;
+  } else {
+    a.pad = 0;
+    a.crop = 0;
+  }
+  a.big_in = n_in + 2 * a.pad;
+  const int64_t big_out = n_out + 2 * a.crop;
+  a.scale = (float)a.big_in / (float)big_out;
+  return a;
+}
+
+__device__ __forceinline__ void axis_weights(const Axis& a, int64_t t,
+                                             int64_t& i0, int64_t& i1,
+                                             float& l1) {
+  float src = __fsub_rn(__fmul_rn(a.scale, (float)(t + a.crop) + 0.5f), 0.5f);
+  if (src < 0.f) src = 0.f;
+  int64_t f = (int64_t)floorf(src);
+  if (f > a.big_in - 1) f = a.big_in - 1;
+  float lam = src - (float)f;
+  lam = lam < 0.f ? 0.f : (lam > 1.f ? 1.f : lam);
+  int64_t g = f + (f < a.big_in - 1 ? 1 : 0);
+  if (a.periodic) {
+    i0 = ((f - a.pad) % a.n_in + a.n_in) % a.n_in;
+    i1 = ((g - a.pad) % a.n_in + a.n_in) % a.n_in;
+  } else {
+    i0 = f;
+    i1 = g;
+  }
+  l1 = lam;
+}
+
+template <typename T>
+__global__ void regrid_kernel(const T* __restrict__ in, Axis ax, Axis ay,
+                              Axis az, T* __restrict__ out) {
+  const int64_t n = ax.n_out * ay.n_out * az.n_out;
+  const int64_t ny = ay.n_in, nz = az.n_in;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = i % az.n_out;
+    const int64_t col = i / az.n_out;
+    const int64_t j = col % ay.n_out;
+    const int64_t t = col / ay.n_out;
+    int64_t x0, x1, y0, y1, z0, z1;
+    float lx, ly, lz;
+    axis_weights(ax, t, x0, x1, lx);
+    axis_weights(ay, j, y0, y1, ly);
+    axis_weights(az, k, z0, z1, lz);
+    const T wx1 = (T)lx, wx0 = (T)1 - wx1;
+    const T wy1 = (T)ly, wy0 = (T)1 - wy1;
+    const T wz1 = (T)lz, wz0 = (T)1 - wz1;
+    const T* p00 = in + (x0 * ny + y0) * nz;
+    const T* p01 = in + (x0 * ny + y1) * nz;
+    const T* p10 = in + (x1 * ny + y0) * nz;
+    const T* p11 = in + (x1 * ny + y1) * nz;
+    T v0 = wy0 * (wz0 * p00[z0] + wz1 * p00[z1]) +
+           wy1 * (wz0 * p01[z0] + wz1 * p01[z1]);
+    T v1 = wy0 * (wz0 * p10[z0] + wz1 * p10[z1]) +
+           wy1 * (wz0 * p11[z0] + wz1 * p11[z1]);
+    out[i] = wx0 * v0 + wx1 * v1;
+  }
+}
+
+// ---- a8: kernel build ---------------------------------------------------------
+template <typename T>
+__global__ void kernel_build_kernel(int hx, int hy, int hz, T dx, T dy, T dz,
+                                    T sigma2, T two_sigma2, T omega, int shape,
+                                    T* __restrict__ out) {
+  __shared__ double scratch[32];
+  __shared__ double ratio_s;
+  const int kx = 2 * hx + 1, ky = 2 * hy + 1, kz = 2 * hz + 1;
+  const int64_t n = (int64_t)kx * ky * kz;
+  double s_env = 0.0, s_g = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const int c = (int)(i % kz);
+    const int b = (int)((i / kz) % ky);
+    const int a = (int)(i / ((int64_t)kz * ky));
+    const T x = mul_rn((T)(a - hx), dx), y = mul_rn((T)(b - hy), dy),
+            z = mul_rn((T)(c - hz), dz);
+    const T r2 = add_rn(add_rn(mul_rn(x, x), mul_rn(y, y)), mul_rn(z, z));
+    const T rho = r2 / sigma2;
+    T env;
+    if (shape == 0)
+      env = mul_rn(sub_rn((T)3, rho), d_exp(-rho / (T)2));
+    else
+      env = mul_rn(d_cos(mul_rn(omega, d_sqrt(r2))), d_exp(-rho / (T)2));
+    const T g = d_exp(-r2 / two_sigma2);
+    out[i] = env;
+    s_env += (double)env;
+    s_g += (double)g;
+  }
+  double te = block_sum(s_env, scratch);
+  double tg = block_sum(s_g, scratch);
+  if (threadIdx.x == 0) ratio_s = te / tg;
+  __syncthreads();
+  const T ratio = (T)ratio_s;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const int c = (int)(i % kz);
+    const int b = (int)((i / kz) % ky);
+    const int a = (int)(i / ((int64_t)kz * ky));
+    const T x = mul_rn((T)(a - hx), dx), y = mul_rn((T)(b - hy), dy),
+            z = mul_rn((T)(c - hz), dz);
+    const T r2 = add_rn(add_rn(mul_rn(x, x), mul_rn(y, y)), mul_rn(z, z));
+    const T g = d_exp(-r2 / two_sigma2);
+    out[i] = sub_rn(out[i], mul_rn(g, ratio));
+  }
+}
+
+// ---- a17: thermodynamics ------------------------------------------------------
+// A warp owns 32 consecutive columns (contiguous in memory).  Levels are staged
+// 32 at a time through shared memory so that loads and stores are coalesced;
+// each lane then marches its own column with a float64 pressure accumulator.
+constexpr int kThZ = 16;
+constexpr int kThWarps = 4;
+constexpr int kThPitch = kThZ + 1;
+
+template <typename T>
+struct ThermoConst {
+  T cp, lv, g, t0, t1, dt, c622, es0, ea, eb, ec, dq;
+};
+
+template <typename T>
+__device__ __forceinline__ T bolton(T Tk, const ThermoConst<T>& k) {
+  return mul_rn(k.es0, d_exp(mul_rn(k.ea, sub_rn(Tk, k.eb)) / sub_rn(Tk, k.ec)));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
+    const T* __restrict__ h, const T* __restrict__ qt,
+    const double* __restrict__ zv, const double* __restrict__ dzv,
+    const double* __restrict__ hm, const double* __restrict__ qm, int compose,
+    T hlo, T hhi, T qlo, T qhi, int64_t ncol,
+    int nz, double ps, const double* __restrict__ ps_field, ThermoConst<T> k,
+    T* __restrict__ To, T* __restrict__ qvo, T* __restrict__ qco,
+    T* __restrict__ qio, T* __restrict__ po) {
+  extern __shared__ unsigned char th_smem[];
+  T* base = reinterpret_cast<T*>(th_smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // sh(a, c, z): array a (h, qt, T, qv, qc, qi, p) of column c, level z
+  auto sh = [&](int a, int c, int z) -> T& {
+    return base[(((size_t)warp * 7 + a) * 32 + c) * kThPitch + z];
+  };
+  const int64_t col0 =
+      ((int64_t)blockIdx.x * kThWarps + warp) * 32;
+  if (col0 >= ncol) return;
+  const int ncols = (int)((ncol - col0) < 32 ? (ncol - col0) : 32);
+  const int64_t mycol = col0 + lane;
+  double p_cur = ps_field ? (lane < ncols ? ps_field[mycol] : 0.0) : ps;
+  const double g = 9.81, Rd = 287.04;
+  for (int z0 = 0; z0 < nz; z0 += kThZ) {
+    const int zc = (nz - z0) < kThZ ? (nz - z0) : kThZ;
+    for (int c = 0; c < ncols; ++c) {
+      if (lane < zc) {
+        const int64_t o = (col0 + c) * nz + z0 + lane;
+        sh(0, c, lane) = h[o];
+        sh(1, c, lane) = qt[o];
+      }
+    }
+    __syncwarp();
+    if (lane < ncols) {
+      for (int zz = 0; zz < zc; ++zz) {
+        const int z = z0 + zz;
+        T hl = sh(0, lane, zz), ql = sh(1, lane, zz);
+        if (compose) {
+          // _compose_output without a deficit: state + mean, clamped to bounds
+          hl = add_rn(hl, (T)hm[z]);
+          ql = add_rn(ql, (T)qm[z]);
+          hl = hl < hlo ? hlo : (hl > hhi ? hhi : hl);
+          ql = ql < qlo ? qlo : (ql > qhi ? qhi : ql);
+        }
+        const T pl = (T)p_cur;
+        const T zt = (T)zv[z];
+        const T Td = sub_rn(sub_rn(hl, mul_rn(k.lv, ql)), mul_rn(k.g, zt)) / k.cp;
+        T es = bolton(Td, k);
+        const T qvs = mul_rn(k.c622, es) / sub_rn(pl, es);
+        T Tl = Td, qvl = ql;
+        if (ql > qvs) {
+          T Tn = Td;
+#pragma unroll 1
+          for (int it = 0; it < 5; ++it) {
+            const T e = bolton(Tn, k);
+            const T pe = sub_rn(pl, e);
+            const T q = mul_rn(k.c622, e) / pe;
+            const T f = sub_rn(add_rn(add_rn(mul_rn(k.cp, Tn), mul_rn(k.lv, q)),
+                                      mul_rn(k.g, zt)),
+                               hl);
+            const T tm = sub_rn(Tn, k.ec);
+            const T de = mul_rn(k.dq, e) / mul_rn(tm, tm);
+            const T dq = mul_rn(mul_rn(k.c622, pl) / mul_rn(pe, pe), de);
+            Tn = sub_rn(Tn, f / add_rn(k.cp, mul_rn(k.lv, dq)));
+          }
+          Tl = Tn;
+          const T e = bolton(Tn, k);
+          qvl = mul_rn(k.c622, e) / sub_rn(pl, e);
+        }
+        T cond = sub_rn(ql, qvl);
+        cond = cond > (T)0 ? cond : (T)0;
+        T lam = sub_rn(Tl, k.t0) / k.dt;
+        lam = lam < (T)0 ? (T)0 : (lam > (T)1 ? (T)1 : lam);
+        sh(2, lane, zz) = Tl;
+        sh(3, lane, zz) = qvl;
+        sh(4, lane, zz) = mul_rn(lam, cond);
+        sh(5, lane, zz) = mul_rn(sub_rn((T)1, lam), cond);
+        sh(6, lane, zz) = pl;
+        if (z < nz - 1) {
+          const double Tv = (double)Tl * (1.0 + 0.608 * (double)qvl);
+          p_cur *= exp(-g * dzv[z] / (Rd * Tv));
+        }
+      }
+    }
+    __syncwarp();
+    for (int c = 0; c < ncols; ++c) {
+      if (lane < zc) {
+        const int64_t o = (col0 + c) * nz + z0 + lane;
+        To[o] = sh(2, c, lane);
+        qvo[o] = sh(3, c, lane);
+        qco[o] = sh(4, c, lane);
+        qio[o] = sh(5, c, lane);
+        po[o] = sh(6, c, lane);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T>
+static ThermoConst<T> thermo_const() {
+  ThermoConst<T> k;
+  k.cp = (T)1004.0;
+  k.lv = (T)2.5e6;
+  k.g = (T)9.81;
+  k.t0 = (T)235.15;
+  k.dt = (T)(273.15 - 235.15);
+  k.c622 = (T)0.622;
+  k.es0 = (T)611.2;
+  k.ea = (T)17.67;
+  k.eb = (T)273.15;
+  k.ec = (T)29.65;
+  k.dq = (T)4302.6;
+  return k;
+}
+
+}  // namespace steam
+
+using namespace steam;
+
+extern "C" int steam_regrid(int dtype, const void* in, int64_t nx, int64_t ny,
+                            int64_t nz, void* out, int64_t mx, int64_t my,
+                            int64_t mz, int32_t periodic_x, int32_t periodic_y,
+                            steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 1 && ny >= 1 && nz >= 1 && mx >= 1 && my >= 1 && mz >= 1,
+                "steam_regrid: extents must be >= 1");
+  STEAM_REQUIRE(!periodic_x || mx >= nx,
+                "steam_regrid: periodic resampling only goes finer (x)");
+  STEAM_REQUIRE(!periodic_y || my >= ny,
+                "steam_regrid: periodic resampling only goes finer (y)");
+  STEAM_REQUIRE(in && out, "steam_regrid: null pointer");
+  Axis ax = make_axis(nx, mx, periodic_x != 0);
+  Axis ay = make_axis(ny, my, periodic_y != 0);
+  Axis az = make_axis(nz, mz, false);
+  const int64_t n = mx * my * mz;
+  int grid = stride_grid(n, 256, 8);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    regrid_kernel<float><<<grid, 256, 0, s>>>((const float*)in, ax, ay, az,
+                                              (float*)out);
+  else if (dtype == STEAM_F64)
+    regrid_kernel<double><<<grid, 256, 0, s>>>((const double*)in, ax, ay, az,
+                                               (double*)out);
+  else
+    return fail(STEAM_ERR_ARG, "steam_regrid: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_regrid");
+  return STEAM_OK;
+}
+
+extern "C" int steam_kernel_build(int dtype, double k, double dx, double dy,
+                                  double dz, double support_factor,
+                                  int32_t shape, void* out, int64_t* dims_out,
+                                  steam_stream_t stream) {
+  STEAM_REQUIRE(k > 0 && dx > 0 && dy > 0 && dz > 0 && support_factor > 0,
+                "steam_kernel_build: scales must be positive");
+  STEAM_REQUIRE(shape == 0 || shape == 1, "steam_kernel_build: unknown shape");
+  STEAM_REQUIRE(dims_out != nullptr, "steam_kernel_build: null dims_out");
+  const double hxd = std::ceil(support_factor * k / dx);
+  const double hyd = std::ceil(support_factor * k / dy);
+  const double hzd = std::ceil(support_factor * k / dz);
+  STEAM_REQUIRE(hxd < 4096 && hyd < 4096 && hzd < 4096,
+                "steam_kernel_build: kernel support too large");
+  const int hx = (int)hxd, hy = (int)hyd, hz = (int)hzd;
+  dims_out[0] = 2 * hx + 1;
+  dims_out[1] = 2 * hy + 1;
+  dims_out[2] = 2 * hz + 1;
+  if (out == nullptr) return STEAM_OK;
+  const double PI = 3.14159265358979323846;
+  const double sigma2 = (k / PI) * (k / PI);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    kernel_build_kernel<float><<<1, 1024, 0, s>>>(
+        hx, hy, hz, (float)dx, (float)dy, (float)dz, (float)sigma2,
+        (float)(2.0 * sigma2), (float)(6.0 / k), shape, (float*)out);
+  else if (dtype == STEAM_F64)
+    kernel_build_kernel<double><<<1, 1024, 0, s>>>(
+        hx, hy, hz, dx, dy, dz, sigma2, 2.0 * sigma2, 6.0 / k, shape,
+        (double*)out);
+  else
+    return fail(STEAM_ERR_ARG, "steam_kernel_build: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_kernel_build");
+  return STEAM_OK;
+}
+
+extern "C" int steam_thermo(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                            const void* h, const void* qt,
+                            const double* z_values, const double* h_mean,
+                            const double* qt_mean, const double* bounds,
+                            double surface_pressure,
+                            const double* ps_field_dev, void* T, void* qv,
+                            void* qc, void* qi, void* p,
+                            steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_thermo: negative extent");
+  const int64_t ncol = nx * ny;
+  if (ncol * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(h && qt && z_values && T && qv && qc && qi && p,
+                "steam_thermo: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  // z and dz go to the device through a small staging buffer owned here.
+  STEAM_REQUIRE((h_mean == nullptr) == (qt_mean == nullptr),
+                "steam_thermo: give both mean profiles or neither");
+  const int compose = h_mean != nullptr;
+  STEAM_REQUIRE(!compose || bounds != nullptr,
+                "steam_thermo: composing with mean profiles needs bounds");
+  std::vector<double> hz(4 * nz, 0.0);
+  for (int64_t z = 0; z < nz; ++z) {
+    hz[z] = z_values[z];
+    hz[nz + z] = z + 1 < nz ? (z_values[z + 1] - z_values[z]) : 0.0;
+    hz[2 * nz + z] = compose ? h_mean[z] : 0.0;
+    hz[3 * nz + z] = compose ? qt_mean[z] : 0.0;
+  }
+  const double b0 = compose ? bounds[0] : 0.0, b1 = compose ? bounds[1] : 0.0;
+  const double b2 = compose ? bounds[2] : 0.0, b3 = compose ? bounds[3] : 0.0;
+  double* dz_dev = nullptr;
+  STEAM_CUDA(cudaMallocAsync((void**)&dz_dev, sizeof(double) * 4 * nz, s));
+  cudaError_t e = cudaMemcpyAsync(dz_dev, hz.data(), sizeof(double) * 4 * nz,
+                                  cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(dz_dev, s);
+    return fail(STEAM_ERR_CUDA, std::string("steam_thermo: ") + cudaGetErrorString(e));
+  }
+  const int64_t blocks = (ncol + 32 * kThWarps - 1) / (32 * kThWarps);
+  const size_t sm_f = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(float);
+  const size_t sm_d = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(double);
+  if (dtype == STEAM_F32) {
+    e = cudaFuncSetAttribute(thermo_kernel<float>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_f);
+  } else if (dtype == STEAM_F64) {
+    e = cudaFuncSetAttribute(thermo_kernel<double>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_d);
+  }
+  if (e != cudaSuccess) {
+    cudaFreeAsync(dz_dev, s);
+    return fail(STEAM_ERR_CUDA, std::string("steam_thermo: ") + cudaGetErrorString(e));
+  }
+  if (dtype == STEAM_F32)
+    thermo_kernel<float><<<(unsigned)blocks, 32 * kThWarps, sm_f, s>>>(
+        (const float*)h, (const float*)qt, dz_dev, dz_dev + nz, dz_dev + 2 * nz,
+        dz_dev + 3 * nz, compose, (float)b0, (float)b1, (float)b2, (float)b3,
+        ncol, (int)nz,
+        surface_pressure, ps_field_dev, thermo_const<float>(), (float*)T,
+        (float*)qv, (float*)qc, (float*)qi, (float*)p);
+  else if (dtype == STEAM_F64)
+    thermo_kernel<double><<<(unsigned)blocks, 32 * kThWarps, sm_d, s>>>(
+        (const double*)h, (const double*)qt, dz_dev, dz_dev + nz, dz_dev + 2 * nz,
+        dz_dev + 3 * nz, compose, b0, b1, b2, b3, ncol, (int)nz, surface_pressure, ps_field_dev, thermo_const<double>(),
+        (double*)T, (double*)qv, (double*)qc, (double*)qi, (double*)p);
+  else {
+    cudaFreeAsync(dz_dev, s);
+    return fail(STEAM_ERR_ARG, "steam_thermo: bad dtype");
+  }
+  count_launch();
+  e = cudaGetLastError();
+  cudaFreeAsync(dz_dev, s);
+  if (e != cudaSuccess)
+    return fail(STEAM_ERR_CUDA, std::string("steam_thermo launch: ") + cudaGetErrorString(e));
+  STEAM_CUDA(cudaStreamSynchronize(s));
+  return STEAM_OK;
+}

@@ -1,0 +1,1004 @@
+// Per-level work on the z-fastest layout: level sums, the scalar pattern
+// (advective weight x signed amplitude x bound taper), the bounded
+// amplitude-preserving add and the mean-preserving projection.
+//
+// Every kernel here uses a level-fixed thread mapping: a thread keeps one (or,
+// for nz > 256, up to four) z-levels for its whole life and walks columns, so
+// loads are coalesced along z and per-level sums stay in registers.  Block
+// partials are reduced in a fixed order, so sums are reproducible.
+#include "common.cuh"
+
+#include <cmath>
+#include <limits>
+#include <vector>
+
+namespace steam {
+
+constexpr int kLvThreads = 256;
+constexpr int kLvMaxJ = 4;  // nz <= 1024
+constexpr int kLvBlocksPerSm = 4;
+
+struct LevelMap {
+  int nz;
+  int G;  // columns per block-iteration (packed mode)
+  int J;  // levels per thread (unpacked mode)
+  bool packed;
+};
+
+static LevelMap make_map(int64_t nz) {
+  LevelMap m;
+  m.nz = (int)nz;
+  if (nz <= kLvThreads) {
+    m.packed = true;
+    m.G = kLvThreads / (int)nz;
+    m.J = 1;
+  } else {
+    m.packed = false;
+    m.G = 1;
+    m.J = (int)((nz + kLvThreads - 1) / kLvThreads);
+  }
+  return m;
+}
+
+static int level_grid(int64_t ncol, const LevelMap& m) {
+  int64_t per = m.packed ? m.G : 1;
+  return stride_grid((ncol + per - 1) / per, 1, kLvBlocksPerSm);
+}
+
+struct Win {
+  int64_t x0, x1, y0, y1;
+  __device__ __forceinline__ bool in(int64_t x, int64_t y) const {
+    return x >= x0 && x < x1 && y >= y0 && y < y1;
+  }
+};
+
+static Win make_win(const steam_window_t* w, int64_t nx, int64_t ny) {
+  Win r;
+  r.x0 = w ? w->x0 : 0;
+  r.x1 = w ? w->x1 : nx;
+  r.y0 = w ? w->y0 : 0;
+  r.y1 = w ? w->y1 : ny;
+  return r;
+}
+
+static int check_win(const steam_window_t* w, int64_t nx, int64_t ny,
+                     const char* who) {
+  if (!w) return STEAM_OK;
+  STEAM_REQUIRE(w->x0 >= 0 && w->x1 <= nx && w->x0 <= w->x1 && w->y0 >= 0 &&
+                    w->y1 <= ny && w->y0 <= w->y1,
+                std::string(who) + ": window outside the array");
+  return STEAM_OK;
+}
+
+// Reduce acc[Q][J] of every thread to per-level block partials:
+// partials[(q * nz + z) * nblocks + blockIdx.x].
+template <int Q>
+__device__ void store_level_partials(const LevelMap& m, double (&acc)[Q][kLvMaxJ],
+                                     double* red, double* partials) {
+  const int t = threadIdx.x;
+  const int nb = gridDim.x;
+  if (m.packed) {
+    const int active = m.G * m.nz;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      __syncthreads();
+      if (t < active) red[t] = acc[q][0];
+      __syncthreads();
+      if (t < m.nz) {
+        double s = 0.0;
+        for (int g = 0; g < m.G; ++g) s += red[g * m.nz + t];
+        partials[((size_t)q * m.nz + t) * nb + blockIdx.x] = s;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      for (int j = 0; j < m.J; ++j) {
+        int z = t + j * kLvThreads;
+        if (z < m.nz) partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][j];
+      }
+  }
+}
+
+// Iterate (column, level) pairs of this thread.  fn(col, z, j).
+template <typename F>
+__device__ __forceinline__ void for_levels(const LevelMap& m, int64_t ncol, F fn) {
+  const int t = threadIdx.x;
+  if (m.packed) {
+    if (t >= m.G * m.nz) return;
+    const int z = t % m.nz;
+    const int64_t cofs = t / m.nz;
+    const int64_t step = (int64_t)gridDim.x * m.G;
+    for (int64_t col = (int64_t)blockIdx.x * m.G + cofs; col < ncol; col += step)
+      fn(col, z, 0);
+  } else {
+    for (int64_t col = blockIdx.x; col < ncol; col += gridDim.x)
+      for (int j = 0; j < m.J; ++j) {
+        int z = t + j * kLvThreads;
+        if (z < m.nz) fn(col, z, j);
+      }
+  }
+}
+
+// ---- level sums ---------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kLvThreads) level_sums_kernel(
+    const T* __restrict__ f, int64_t nx, int64_t ny, LevelMap m, Win w,
+    double* __restrict__ partials) {
+  __shared__ double red[kLvThreads];
+  double acc[3][kLvMaxJ];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int j = 0; j < kLvMaxJ; ++j) acc[q][j] = 0.0;
+  const int64_t ncol = nx * ny;
+  for_levels(m, ncol, [&](int64_t col, int z, int j) {
+    const int64_t x = col / ny, y = col - x * ny;
+    if (!w.in(x, y)) return;
+    T v = f[col * m.nz + z];
+    acc[0][j] += (double)v;
+    acc[1][j] += (double)(v < (T)0 ? -v : v);
+    acc[2][j] += v != (T)0 ? 1.0 : 0.0;
+  });
+  store_level_partials<3>(m, acc, red, partials);
+}
+
+// ---- scalar pattern -------------------------------------------------------------
+template <typename T>
+struct PatternArgs {
+  T two_dx, two_dy, two_dz, dz_first, dz_last, lo, span, s_scale;
+  int uniform_z;
+  int has_prod;   // 0: no signed amplitude (W alone)
+  int has_taper;  // 0: no bound taper
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kLvThreads) pattern_kernel(
+    const T* __restrict__ pert, const T* __restrict__ mean,
+    const T* __restrict__ prod, const T* __restrict__ za,
+    const T* __restrict__ zb, const T* __restrict__ zc,
+    const T* __restrict__ aspect, const T* __restrict__ bbuf, int64_t nx,
+    int64_t ny, LevelMap m, Win w, PatternArgs<T> a, T* __restrict__ out,
+    double* __restrict__ partials) {
+  __shared__ double red[kLvThreads];
+  double acc[2][kLvMaxJ];
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int j = 0; j < kLvMaxJ; ++j) acc[q][j] = 0.0;
+  const int nz = m.nz;
+  const int64_t ncol = nx * ny;
+  for_levels(m, ncol, [&](int64_t col, int z, int j) {
+    const int64_t x = col / ny, y = col - x * ny;
+    const int64_t xp = x + 1 < nx ? x + 1 : 0, xm = x > 0 ? x - 1 : nx - 1;
+    const int64_t yp = y + 1 < ny ? y + 1 : 0, ym = y > 0 ? y - 1 : ny - 1;
+    const T mz = mean[z];
+    const int64_t i = col * nz + z;
+    const T r = add_rn(pert[i], mz);
+    const T rxp = add_rn(pert[(xp * ny + y) * nz + z], mz);
+    const T rxm = add_rn(pert[(xm * ny + y) * nz + z], mz);
+    const T ryp = add_rn(pert[(x * ny + yp) * nz + z], mz);
+    const T rym = add_rn(pert[(x * ny + ym) * nz + z], mz);
+    const T gx = sub_rn(rxp, rxm) / a.two_dx;
+    const T gy = sub_rn(ryp, rym) / a.two_dy;
+    const T gh = d_sqrt(add_rn(mul_rn(gx, gx), mul_rn(gy, gy)));
+    T gz;
+    if (z == 0) {
+      const T r1 = add_rn(pert[i + 1], mean[1]);
+      gz = sub_rn(r1, r) / a.dz_first;
+    } else if (z == nz - 1) {
+      const T r0 = add_rn(pert[i - 1], mean[z - 1]);
+      gz = sub_rn(r, r0) / a.dz_last;
+    } else {
+      const T rzm = add_rn(pert[i - 1], mean[z - 1]);
+      const T rzp = add_rn(pert[i + 1], mean[z + 1]);
+      if (a.uniform_z) {
+        gz = sub_rn(rzp, rzm) / a.two_dz;
+      } else {
+        gz = add_rn(add_rn(mul_rn(za[z - 1], rzm), mul_rn(zb[z - 1], r)),
+                    mul_rn(zc[z - 1], rzp));
+      }
+    }
+    gz = gz < (T)0 ? -gz : gz;
+    T W = add_rn(mul_rn(gz, aspect[z]), gh);
+    if (a.has_prod) {
+      const T S = mul_rn(prod[i], a.s_scale);
+      W = mul_rn(W, S);
+    }
+    if (a.has_taper) {
+      T g = sub_rn(r, a.lo);
+      const T g2 = sub_rn(a.span, g);
+      g = g2 < g ? g2 : g;
+      const T bz = bbuf[z];
+      g = g / (bz > (T)0 ? bz : (T)1e-30);
+      g = g < (T)0 ? (T)0 : (g > (T)1 ? (T)1 : g);
+      W = mul_rn(W, g);
+    }
+    out[i] = W;
+    if (w.in(x, y)) {
+      acc[0][j] += (double)(W < (T)0 ? -W : W);
+      acc[1][j] += W != (T)0 ? 1.0 : 0.0;
+    }
+  });
+  store_level_partials<2>(m, acc, red, partials);
+}
+
+// ---- bounded add sweeps --------------------------------------------------------
+// Per-level chain, replayed from the raw increment on every sweep:
+//   for s < nsteps[z]:  d = clip(d - demean[z,s], caps) * scale[z,s]
+//   if has_final[z]:    d = clip(d - final_dm[z], caps)
+//   if has_mu[z]:       d = clip(d - mu[z], caps)
+// with caps = (lo - phi, hi - phi), phi = pert + mean.
+constexpr int kMuCand = 4;
+enum { BA_STATS = 0, BA_MU = 1, BA_APPLY = 2 };
+
+template <typename T>
+struct BAChain {
+  const int* nsteps;
+  const T* demean;  // [nz][R]
+  const T* scale;   // [nz][R]
+  const int* has_final;
+  const T* final_dm;
+  const int* has_mu;
+  const T* mu;
+  const T* cand;  // [nz][kMuCand]
+  const T* mean;
+  int R;
+  T lo, hi;
+};
+
+template <typename T>
+__device__ __forceinline__ T clampv(T v, T a, T b) {
+  v = v > a ? v : a;
+  return v < b ? v : b;
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
+    const T* __restrict__ d0, T* __restrict__ pert, T* __restrict__ inc_out,
+    int record, int64_t nx, int64_t ny, LevelMap m, Win w, BAChain<T> c,
+    double* __restrict__ partials) {
+  __shared__ double red[kLvThreads];
+  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
+  double acc[Q][kLvMaxJ];
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int j = 0; j < kLvMaxJ; ++j) acc[q][j] = 0.0;
+  const int nz = m.nz;
+  const int64_t ncol = nx * ny;
+  for_levels(m, ncol, [&](int64_t col, int z, int j) {
+    const int64_t i = col * nz + z;
+    const T p0 = pert[i];
+    const T phi = add_rn(p0, c.mean[z]);
+    const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
+    T d = d0[i];
+    const int ns = c.nsteps[z];
+    for (int s = 0; s < ns; ++s) {
+      d = clampv(sub_rn(d, c.demean[z * c.R + s]), clo, chi);
+      d = mul_rn(d, c.scale[z * c.R + s]);
+    }
+    if (c.has_final[z]) d = clampv(sub_rn(d, c.final_dm[z]), clo, chi);
+    if (MODE == BA_APPLY) {
+      if (c.has_mu[z]) d = clampv(sub_rn(d, c.mu[z]), clo, chi);
+      const T pn = add_rn(p0, d);
+      pert[i] = pn;
+      if (record) inc_out[i] = sub_rn(pn, p0);
+      return;
+    }
+    const int64_t x = col / ny, y = col - x * ny;
+    if (!w.in(x, y)) return;
+    if (MODE == BA_STATS) {
+      acc[0][j] += (double)d;
+      acc[1 % Q][j] += (double)(d < (T)0 ? -d : d);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kMuCand; ++k) {
+        const T raw = sub_rn(d, c.cand[z * kMuCand + k]);
+        const T t = clampv(raw, clo, chi);
+        acc[2 * k][j] += (double)t;
+        acc[(2 * k + 1) % Q][j] += (raw > clo && raw < chi) ? 1.0 : 0.0;
+      }
+    }
+  });
+  if (MODE != BA_APPLY) store_level_partials<Q>(m, acc, red, partials);
+}
+
+// ---- projection sweeps (float64 level arithmetic) -----------------------------
+enum { PJ_STATS = 0, PJ_MU = 1, PJ_APPLY = 2 };
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
+    T* __restrict__ pert, const double* __restrict__ mean, double lo,
+    double hi, const int* __restrict__ active, const double* __restrict__ mu,
+    const double* __restrict__ cand, int64_t nx, int64_t ny, LevelMap m,
+    Win w, double* __restrict__ partials) {
+  __shared__ double red[kLvThreads];
+  constexpr int Q = MODE == PJ_MU ? 2 * kMuCand : 3;
+  double acc[Q][kLvMaxJ];
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int j = 0; j < kLvMaxJ; ++j)
+      acc[q][j] = (MODE == PJ_STATS && q == 1) ? INFINITY
+                  : (MODE == PJ_STATS && q == 2) ? -INFINITY
+                                                  : 0.0;
+  const int nz = m.nz;
+  const int64_t ncol = nx * ny;
+  for_levels(m, ncol, [&](int64_t col, int z, int j) {
+    const int64_t i = col * nz + z;
+    const double f = (double)pert[i] + mean[z];
+    if (MODE == PJ_STATS) {
+      acc[1][j] = fmin(acc[1][j], f);
+      acc[2 % Q][j] = fmax(acc[2 % Q][j], f);
+      const int64_t x = col / ny, y = col - x * ny;
+      if (w.in(x, y)) acc[0][j] += f;
+      return;
+    }
+    if (!active[z]) return;
+    if (MODE == PJ_APPLY) {
+      pert[i] = (T)(fmin(fmax(f - mu[z], lo), hi) - mean[z]);
+      return;
+    }
+    const int64_t x = col / ny, y = col - x * ny;
+    if (!w.in(x, y)) return;
+#pragma unroll
+    for (int k = 0; k < kMuCand; ++k) {
+      const double raw = f - cand[z * kMuCand + k];
+      acc[2 * k][j] += fmin(fmax(raw, lo), hi);
+      acc[(2 * k + 1) % Q][j] += (raw > lo && raw < hi) ? 1.0 : 0.0;
+    }
+  });
+  if (MODE == PJ_APPLY) return;
+  if (MODE == PJ_STATS) {
+    // min/max are reduced like sums but combine with fmin/fmax: store raw.
+    const int t = threadIdx.x;
+    const int nb = gridDim.x;
+    if (m.packed) {
+      for (int q = 0; q < 3; ++q) {
+        __syncthreads();
+        if (t < m.G * m.nz) red[t] = acc[q][0];
+        __syncthreads();
+        if (t < m.nz) {
+          double s = q == 0 ? 0.0 : (q == 1 ? INFINITY : -INFINITY);
+          for (int g = 0; g < m.G; ++g) {
+            double v = red[g * m.nz + t];
+            s = q == 0 ? s + v : (q == 1 ? fmin(s, v) : fmax(s, v));
+          }
+          partials[((size_t)q * m.nz + t) * nb + blockIdx.x] = s;
+        }
+      }
+    } else {
+      for (int q = 0; q < 3; ++q)
+        for (int jj = 0; jj < m.J; ++jj) {
+          int z = t + jj * kLvThreads;
+          if (z < m.nz)
+            partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][jj];
+        }
+    }
+  } else {
+    store_level_partials<Q>(m, acc, red, partials);
+  }
+}
+
+__global__ void reduce_minmax_kernel(const double* __restrict__ partials,
+                                     int nblocks, int nz,
+                                     double* __restrict__ out) {
+  // out[z] = sum (q=0); out[nz+z] = min (q=1); out[2nz+z] = max (q=2)
+  const int q = blockIdx.y;
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz;
+       z += gridDim.x * blockDim.x) {
+    const double* src = partials + ((size_t)q * nz + z) * nblocks;
+    double s = q == 0 ? 0.0 : (q == 1 ? INFINITY : -INFINITY);
+    for (int b = 0; b < nblocks; ++b)
+      s = q == 0 ? s + src[b] : (q == 1 ? fmin(s, src[b]) : fmax(s, src[b]));
+    out[(size_t)q * nz + z] = s;
+  }
+}
+
+// ---- host helpers ----------------------------------------------------------------
+template <typename T>
+static int upload(T* dst, const std::vector<T>& src, cudaStream_t s) {
+  if (src.empty()) return STEAM_OK;
+  STEAM_CUDA(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(),
+                             cudaMemcpyHostToDevice, s));
+  return STEAM_OK;
+}
+
+static int fetch(std::vector<double>& dst, const double* src, size_t n,
+                 cudaStream_t s) {
+  dst.resize(n);
+  STEAM_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * n,
+                             cudaMemcpyDeviceToHost, s));
+  STEAM_CUDA(cudaStreamSynchronize(s));
+  return STEAM_OK;
+}
+
+static size_t level_partial_bytes(int64_t nz, int q) {
+  return carve_bytes((size_t)sm_count() * kLvBlocksPerSm * q * nz, sizeof(double)) +
+         carve_bytes((size_t)q * nz, sizeof(double));
+}
+
+// Per-level bracketed Newton on a non-increasing piecewise-linear function
+// m(mu) (the level mean of a clipped, shifted field, minus a target).  The
+// bracket [a, b] always holds a sign change in the reference's bisection
+// sense: m(a) > 0 >= m(b).  Each sweep evaluates kMuCand candidates; the
+// result is the midpoint of the final bracket, as the bisection returns.
+struct MuSolver {
+  double a, b;
+  double best_mu, best_m, best_slope;
+  bool have_best = false;
+  bool done = false;
+  double rel_tol, abs_tol;
+
+  // The bisection this replaces stops at 2*width/2^60; so does this.
+  void init(double width, double tol) {
+    a = -width;
+    b = width;
+    rel_tol = tol;
+    abs_tol = ldexp(2.0 * width, -60);
+    have_best = false;
+    done = false;
+  }
+
+  void candidates(double* out) const {
+    const double mid = 0.5 * (a + b);
+    double c0 = mid;
+    if (have_best && best_slope < 0.0) {
+      double nt = best_mu - best_m / best_slope;  // Newton
+      if (nt > a && nt < b) c0 = nt;
+    }
+    const double span = b - a;
+    double eps = fabs(c0) * rel_tol * 4.0 + 1e-300;
+    if (eps > 0.25 * span) eps = 0.25 * span;
+    out[0] = c0;
+    out[1] = c0 - eps > a ? c0 - eps : 0.5 * (a + c0);
+    out[2] = c0 + eps < b ? c0 + eps : 0.5 * (c0 + b);
+    out[3] = mid;
+  }
+
+  void update(const double* cand, const double* mval, const double* slope) {
+    for (int k = 0; k < kMuCand; ++k) {
+      if (mval[k] > 0.0) {
+        if (cand[k] > a) a = cand[k];
+      } else {
+        if (cand[k] < b) b = cand[k];
+      }
+    }
+    int kb = -1;
+    for (int k = 0; k < kMuCand; ++k)
+      if (kb < 0 || fabs(mval[k]) < fabs(mval[kb])) kb = k;
+    if (kb >= 0) {
+      have_best = true;
+      best_mu = cand[kb];
+      best_m = mval[kb];
+      best_slope = slope[kb];
+    }
+    const double scale = fmax(fabs(a), fabs(b));
+    if (b - a <= scale * rel_tol || b - a <= abs_tol) done = true;
+  }
+  double result() const { return 0.5 * (a + b); }
+};
+
+template <typename T>
+static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
+                            const double* mean_1d, T* inc, double phi_min,
+                            double phi_max, const steam_window_t* window,
+                            int R, int record, double* ledger_out, void* ws,
+                            size_t ws_bytes, cudaStream_t s) {
+  const LevelMap m = make_map(nz);
+  const int64_t ncol = nx * ny;
+  const int grid = level_grid(ncol, m);
+  const Win w = make_win(window, nx, ny);
+  const double N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
+  const int Qmax = 2 * kMuCand;
+  Carver c(ws, ws_bytes);
+  double* partials = c.take<double>((size_t)grid * Qmax * nz);
+  double* totals = c.take<double>((size_t)Qmax * nz);
+  T* d_mean = c.take<T>(nz);
+  int* d_nsteps = c.take<int>(nz);
+  T* d_demean = c.take<T>((size_t)nz * R);
+  T* d_scale = c.take<T>((size_t)nz * R);
+  int* d_hasfinal = c.take<int>(nz);
+  T* d_final = c.take<T>(nz);
+  int* d_hasmu = c.take<int>(nz);
+  T* d_mu = c.take<T>(nz);
+  T* d_cand = c.take<T>((size_t)nz * kMuCand);
+  if (!partials || !totals || !d_mean || !d_nsteps || !d_demean || !d_scale ||
+      !d_hasfinal || !d_final || !d_hasmu || !d_mu || !d_cand)
+    return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
+
+  std::vector<T> h_mean(nz), h_demean((size_t)nz * R, (T)0),
+      h_scale((size_t)nz * R, (T)1), h_final(nz, (T)0), h_mu(nz, (T)0),
+      h_cand((size_t)nz * kMuCand, (T)0);
+  std::vector<int> h_nsteps(nz, 0), h_hasfinal(nz, 0), h_hasmu(nz, 0);
+  for (int64_t z = 0; z < nz; ++z) h_mean[z] = (T)mean_1d[z];
+  int rc;
+  if ((rc = upload(d_mean, h_mean, s))) return rc;
+
+  BAChain<T> ch;
+  ch.nsteps = d_nsteps;
+  ch.demean = d_demean;
+  ch.scale = d_scale;
+  ch.has_final = d_hasfinal;
+  ch.final_dm = d_final;
+  ch.has_mu = d_hasmu;
+  ch.mu = d_mu;
+  ch.cand = d_cand;
+  ch.mean = d_mean;
+  ch.R = R;
+  ch.lo = (T)phi_min;
+  ch.hi = (T)phi_max;
+
+  std::vector<double> tot;
+  int n_sweeps = 0;
+  auto push_chain = [&]() -> int {
+    int r2;
+    if ((r2 = upload(d_nsteps, h_nsteps, s))) return r2;
+    if ((r2 = upload(d_demean, h_demean, s))) return r2;
+    if ((r2 = upload(d_scale, h_scale, s))) return r2;
+    if ((r2 = upload(d_hasfinal, h_hasfinal, s))) return r2;
+    if ((r2 = upload(d_final, h_final, s))) return r2;
+    if ((r2 = upload(d_hasmu, h_hasmu, s))) return r2;
+    if ((r2 = upload(d_mu, h_mu, s))) return r2;
+    if ((r2 = upload(d_cand, h_cand, s))) return r2;
+    return STEAM_OK;
+  };
+  auto stats_sweep = [&]() -> int {
+    int r2 = push_chain();
+    if (r2) return r2;
+    ba_sweep_kernel<T, BA_STATS><<<grid, kLvThreads, 0, s>>>(
+        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
+    STEAM_LAUNCH_CHECK("bounded_add stats sweep");
+    if ((r2 = reduce_partials(partials, grid, 2 * (int)nz, totals, s))) return r2;
+    ++n_sweeps;
+    return fetch(tot, totals, 2 * nz, s);
+  };
+
+  // Sweep 0: a0 = mean|d|, mean d.
+  if ((rc = stats_sweep())) return rc;
+  std::vector<double> a0(nz), cur_mean(nz), final_dm(nz, 0.0),
+      mu(nz, std::numeric_limits<double>::quiet_NaN());
+  std::vector<int> active(nz, 0), n_loop(nz, 0);
+  for (int64_t z = 0; z < nz; ++z) {
+    a0[z] = tot[nz + z] / N;
+    cur_mean[z] = tot[z] / N;
+    if (a0[z] <= 0.0) {
+      h_hasfinal[z] = 1;  // clip only
+      h_final[z] = (T)0;
+    } else {
+      active[z] = 1;
+    }
+  }
+  // Demean / clip / rescale-to-A0 loop.
+  std::vector<int> still(active);
+  for (int k = 0; k < R; ++k) {
+    bool any = false;
+    for (int64_t z = 0; z < nz; ++z)
+      if (still[z]) {
+        any = true;
+        h_demean[z * R + k] = (T)cur_mean[z];
+        h_scale[z * R + k] = (T)1;
+        h_nsteps[z] = k + 1;
+        n_loop[z] = k + 1;
+      }
+    if (!any) break;
+    if ((rc = stats_sweep())) return rc;
+    for (int64_t z = 0; z < nz; ++z) {
+      if (!still[z]) continue;
+      const double sum_d = tot[z], m_abs = tot[nz + z] / N;
+      cur_mean[z] = sum_d / N;
+      if (m_abs <= 0.0) {
+        still[z] = 0;
+        continue;
+      }
+      double sc = a0[z] / m_abs;
+      if (sc > 2.0) sc = 2.0;
+      if (fabs(sc - 1.0) < 1e-4) {
+        still[z] = 0;
+        continue;
+      }
+      h_scale[z * R + k] = (T)sc;
+      cur_mean[z] = (double)(T)sc * sum_d / N;
+    }
+  }
+  // Final demean and clip.
+  for (int64_t z = 0; z < nz; ++z)
+    if (active[z]) {
+      final_dm[z] = cur_mean[z];
+      h_hasfinal[z] = 1;
+      h_final[z] = (T)cur_mean[z];
+    }
+  if ((rc = stats_sweep())) return rc;
+  // Zero-mean shift mu where the clip left a mean.
+  const double width = phi_max - phi_min;
+  const double tol = sizeof(T) == 4 ? 1.0 / (1 << 26) : 1.0e-16;
+  std::vector<MuSolver> solver(nz);
+  std::vector<int> need(nz, 0);
+  bool any_mu = false;
+  for (int64_t z = 0; z < nz; ++z) {
+    if (!active[z]) continue;
+    if (fabs(tot[z] / N) > 1e-9 * a0[z]) {
+      need[z] = 1;
+      any_mu = true;
+      solver[z].init(width, tol);
+    }
+  }
+  for (int it = 0; any_mu && it < 80; ++it) {
+    std::vector<double> cands((size_t)nz * kMuCand, 0.0);
+    bool pending = false;
+    for (int64_t z = 0; z < nz; ++z) {
+      if (!need[z] || solver[z].done) continue;
+      pending = true;
+      solver[z].candidates(&cands[z * kMuCand]);
+      for (int k = 0; k < kMuCand; ++k)
+        h_cand[z * kMuCand + k] = (T)cands[z * kMuCand + k];
+    }
+    if (!pending) break;
+    if ((rc = push_chain())) return rc;
+    ba_sweep_kernel<T, BA_MU><<<grid, kLvThreads, 0, s>>>(
+        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
+    STEAM_LAUNCH_CHECK("bounded_add mu sweep");
+    if ((rc = reduce_partials(partials, grid, Qmax * (int)nz, totals, s))) return rc;
+    ++n_sweeps;
+    if ((rc = fetch(tot, totals, (size_t)Qmax * nz, s))) return rc;
+    for (int64_t z = 0; z < nz; ++z) {
+      if (!need[z] || solver[z].done) continue;
+      double mv[kMuCand], sl[kMuCand], cv[kMuCand];
+      for (int k = 0; k < kMuCand; ++k) {
+        // The candidate actually evaluated is the dtype-rounded one.
+        cv[k] = (double)h_cand[z * kMuCand + k];
+        mv[k] = tot[(size_t)(2 * k) * nz + z] / N;
+        sl[k] = -tot[(size_t)(2 * k + 1) * nz + z] / N;
+      }
+      solver[z].update(cv, mv, sl);
+    }
+  }
+  for (int64_t z = 0; z < nz; ++z)
+    if (need[z]) {
+      mu[z] = solver[z].result();
+      h_hasmu[z] = 1;
+      h_mu[z] = (T)mu[z];
+    }
+  // Apply.
+  if ((rc = push_chain())) return rc;
+  ba_sweep_kernel<T, BA_APPLY><<<grid, kLvThreads, 0, s>>>(
+      inc, pert, inc, record, nx, ny, m, w, ch, partials);
+  STEAM_LAUNCH_CHECK("bounded_add apply sweep");
+  ++n_sweeps;
+  if (ledger_out) {
+    for (int64_t z = 0; z < nz; ++z) {
+      ledger_out[5 * z + 0] = a0[z];
+      ledger_out[5 * z + 1] = n_loop[z];
+      ledger_out[5 * z + 2] = final_dm[z];
+      ledger_out[5 * z + 3] = mu[z];
+      ledger_out[5 * z + 4] = n_sweeps;
+    }
+  }
+  STEAM_CUDA(cudaStreamSynchronize(s));
+  return STEAM_OK;
+}
+
+template <typename T>
+static int project_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
+                        const double* mean_1d, double lo, double hi,
+                        const steam_window_t* window, double* mu_out, void* ws,
+                        size_t ws_bytes, cudaStream_t s) {
+  const LevelMap m = make_map(nz);
+  const int64_t ncol = nx * ny;
+  const int grid = level_grid(ncol, m);
+  const Win w = make_win(window, nx, ny);
+  const double N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
+  const int Qmax = 2 * kMuCand;
+  Carver c(ws, ws_bytes);
+  double* partials = c.take<double>((size_t)grid * Qmax * nz);
+  double* totals = c.take<double>((size_t)Qmax * nz);
+  double* d_mean = c.take<double>(nz);
+  int* d_active = c.take<int>(nz);
+  double* d_mu = c.take<double>(nz);
+  double* d_cand = c.take<double>((size_t)nz * kMuCand);
+  if (!partials || !totals || !d_mean || !d_active || !d_mu || !d_cand)
+    return fail(STEAM_ERR_WORKSPACE, "steam_project_bounds: workspace too small");
+  std::vector<double> h_mean(mean_1d, mean_1d + nz);
+  int rc;
+  if ((rc = upload(d_mean, h_mean, s))) return rc;
+  proj_sweep_kernel<T, PJ_STATS><<<grid, kLvThreads, 0, s>>>(
+      pert, d_mean, lo, hi, nullptr, nullptr, nullptr, nx, ny, m, w, partials);
+  STEAM_LAUNCH_CHECK("project stats sweep");
+  {
+    dim3 g2((unsigned)((nz + 127) / 128), 3);
+    reduce_minmax_kernel<<<g2, 128, 0, s>>>(partials, grid, (int)nz, totals);
+    STEAM_LAUNCH_CHECK("project minmax reduce");
+  }
+  std::vector<double> tot;
+  if ((rc = fetch(tot, totals, 3 * nz, s))) return rc;
+  std::vector<int> active(nz, 0);
+  std::vector<double> target(nz, 0.0), mu(nz, std::numeric_limits<double>::quiet_NaN());
+  bool any = false;
+  for (int64_t z = 0; z < nz; ++z) {
+    if (tot[nz + z] < lo || tot[2 * nz + z] > hi) {
+      active[z] = 1;
+      any = true;
+      target[z] = tot[z] / N;
+    }
+  }
+  if (mu_out)
+    for (int64_t z = 0; z < nz; ++z) mu_out[z] = mu[z];
+  if (!any) return STEAM_OK;
+  if ((rc = upload(d_active, active, s))) return rc;
+  const double width = hi - lo;
+  std::vector<MuSolver> solver(nz);
+  for (int64_t z = 0; z < nz; ++z)
+    if (active[z]) solver[z].init(width, 1e-16);
+  std::vector<double> cands((size_t)nz * kMuCand, 0.0);
+  for (int it = 0; it < 80; ++it) {
+    bool pending = false;
+    for (int64_t z = 0; z < nz; ++z) {
+      if (!active[z] || solver[z].done) continue;
+      pending = true;
+      solver[z].candidates(&cands[z * kMuCand]);
+    }
+    if (!pending) break;
+    if ((rc = upload(d_cand, cands, s))) return rc;
+    proj_sweep_kernel<T, PJ_MU><<<grid, kLvThreads, 0, s>>>(
+        pert, d_mean, lo, hi, d_active, nullptr, d_cand, nx, ny, m, w, partials);
+    STEAM_LAUNCH_CHECK("project mu sweep");
+    if ((rc = reduce_partials(partials, grid, Qmax * (int)nz, totals, s))) return rc;
+    if ((rc = fetch(tot, totals, (size_t)Qmax * nz, s))) return rc;
+    for (int64_t z = 0; z < nz; ++z) {
+      if (!active[z] || solver[z].done) continue;
+      double mv[kMuCand], sl[kMuCand];
+      for (int k = 0; k < kMuCand; ++k) {
+        mv[k] = tot[(size_t)(2 * k) * nz + z] / N - target[z];
+        sl[k] = -tot[(size_t)(2 * k + 1) * nz + z] / N;
+      }
+      solver[z].update(&cands[z * kMuCand], mv, sl);
+    }
+  }
+  for (int64_t z = 0; z < nz; ++z)
+    if (active[z]) mu[z] = solver[z].result();
+  std::vector<double> h_mu(nz, 0.0);
+  for (int64_t z = 0; z < nz; ++z) h_mu[z] = active[z] ? mu[z] : 0.0;
+  if ((rc = upload(d_mu, h_mu, s))) return rc;
+  proj_sweep_kernel<T, PJ_APPLY><<<grid, kLvThreads, 0, s>>>(
+      pert, d_mean, lo, hi, d_active, d_mu, nullptr, nx, ny, m, w, partials);
+  STEAM_LAUNCH_CHECK("project apply sweep");
+  STEAM_CUDA(cudaStreamSynchronize(s));
+  if (mu_out)
+    for (int64_t z = 0; z < nz; ++z) mu_out[z] = mu[z];
+  return STEAM_OK;
+}
+
+}  // namespace steam
+
+using namespace steam;
+
+extern "C" size_t steam_level_sums_workspace_bytes(int64_t nz) {
+  return level_partial_bytes(nz, 3);
+}
+
+extern "C" int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                const void* field,
+                                const steam_window_t* window, double* sums_out,
+                                void* workspace, size_t workspace_bytes,
+                                steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_level_sums: negative extent");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_level_sums: nz above 1024");
+  STEAM_REQUIRE(sums_out != nullptr, "steam_level_sums: null sums_out");
+  int rc = check_win(window, nx, ny, "steam_level_sums");
+  if (rc) return rc;
+  if (nz == 0) return STEAM_OK;
+  const Win w = make_win(window, nx, ny);
+  const double cells = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
+  if (nx * ny == 0) {
+    for (int64_t z = 0; z < nz; ++z) {
+      sums_out[4 * z] = sums_out[4 * z + 1] = sums_out[4 * z + 2] = 0.0;
+      sums_out[4 * z + 3] = cells;
+    }
+    return STEAM_OK;
+  }
+  STEAM_REQUIRE(field != nullptr, "steam_level_sums: null field");
+  const LevelMap m = make_map(nz);
+  const int grid = level_grid(nx * ny, m);
+  Carver c(workspace, workspace_bytes);
+  double* partials = c.take<double>((size_t)grid * 3 * nz);
+  double* totals = c.take<double>((size_t)3 * nz);
+  if (!partials || !totals)
+    return fail(STEAM_ERR_WORKSPACE, "steam_level_sums: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    level_sums_kernel<float><<<grid, kLvThreads, 0, s>>>((const float*)field, nx,
+                                                         ny, m, w, partials);
+  else if (dtype == STEAM_F64)
+    level_sums_kernel<double><<<grid, kLvThreads, 0, s>>>(
+        (const double*)field, nx, ny, m, w, partials);
+  else
+    return fail(STEAM_ERR_ARG, "steam_level_sums: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_level_sums");
+  rc = reduce_partials(partials, grid, 3 * (int)nz, totals, s);
+  if (rc) return rc;
+  std::vector<double> h;
+  rc = fetch(h, totals, 3 * nz, s);
+  if (rc) return rc;
+  for (int64_t z = 0; z < nz; ++z) {
+    sums_out[4 * z + 0] = h[z];
+    sums_out[4 * z + 1] = h[nz + z];
+    sums_out[4 * z + 2] = h[2 * nz + z];
+    sums_out[4 * z + 3] = cells;
+  }
+  return STEAM_OK;
+}
+
+extern "C" size_t steam_scalar_pattern_workspace_bytes(int64_t nz) {
+  return level_partial_bytes(nz, 2) + 8 * carve_bytes(nz, sizeof(double));
+}
+
+template <typename T>
+static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
+                        const double* mean_1d, const T* prod, double s_scale,
+                        double dx, double dy, const double* z_coords,
+                        const double* aspect, const double* bbuf,
+                        double phi_min, double phi_max, T* out,
+                        const steam_window_t* window, double* sums_out,
+                        void* ws, size_t ws_bytes, cudaStream_t s) {
+  const LevelMap m = make_map(nz);
+  const int grid = level_grid(nx * ny, m);
+  const Win w = make_win(window, nx, ny);
+  Carver c(ws, ws_bytes);
+  double* partials = c.take<double>((size_t)grid * 2 * nz);
+  double* totals = c.take<double>((size_t)2 * nz);
+  T* d_vec = c.take<T>((size_t)6 * nz);
+  if (!partials || !totals || !d_vec)
+    return fail(STEAM_ERR_WORKSPACE, "steam_scalar_pattern: workspace too small");
+  // np.gradient's z coefficients from float32 (or float64) level heights.
+  std::vector<T> zc(nz), dz(nz > 1 ? nz - 1 : 0);
+  for (int64_t z = 0; z < nz; ++z) zc[z] = (T)z_coords[z];
+  for (int64_t z = 0; z + 1 < nz; ++z) dz[z] = zc[z + 1] - zc[z];
+  bool uniform = true;
+  for (int64_t z = 1; z + 1 < nz; ++z)
+    if (dz[z] != dz[0]) uniform = false;
+  std::vector<T> h((size_t)6 * nz, (T)0);
+  // [0] mean, [1] a, [2] b, [3] c, [4] aspect, [5] buffer
+  for (int64_t z = 0; z < nz; ++z) {
+    h[z] = (T)mean_1d[z];
+    h[4 * nz + z] = (T)aspect[z];
+    h[5 * nz + z] = bbuf ? (T)bbuf[z] : (T)1;
+  }
+  if (!uniform) {
+    for (int64_t z = 0; z + 2 < nz; ++z) {
+      T d1 = dz[z], d2 = dz[z + 1];
+      h[nz + z] = -(d2) / (d1 * (d1 + d2));
+      h[2 * nz + z] = (d2 - d1) / (d1 * d2);
+      h[3 * nz + z] = d1 / (d2 * (d1 + d2));
+    }
+  }
+  int rc = upload(d_vec, h, s);
+  if (rc) return rc;
+  PatternArgs<T> a;
+  a.two_dx = (T)(2 * dx);
+  a.two_dy = (T)(2 * dy);
+  a.two_dz = uniform ? (T)2 * dz[0] : (T)0;
+  a.dz_first = dz[0];
+  a.dz_last = dz[nz - 2];
+  a.lo = (T)phi_min;
+  a.span = (T)(phi_max - phi_min);
+  a.s_scale = (T)s_scale;
+  a.uniform_z = uniform ? 1 : 0;
+  a.has_prod = prod != nullptr;
+  a.has_taper = bbuf != nullptr;
+  pattern_kernel<T><<<grid, kLvThreads, 0, s>>>(
+      pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
+      d_vec + 4 * nz, d_vec + 5 * nz, nx, ny, m, w, a, out, partials);
+  STEAM_LAUNCH_CHECK("steam_scalar_pattern");
+  rc = reduce_partials(partials, grid, 2 * (int)nz, totals, s);
+  if (rc) return rc;
+  std::vector<double> t;
+  rc = fetch(t, totals, 2 * nz, s);
+  if (rc) return rc;
+  for (int64_t z = 0; z < nz; ++z) {
+    sums_out[2 * z] = t[z];
+    sums_out[2 * z + 1] = t[nz + z];
+  }
+  return STEAM_OK;
+}
+
+extern "C" int steam_scalar_pattern(
+    int dtype, int64_t nx, int64_t ny, int64_t nz, const void* pert,
+    const double* mean_1d, const void* product, double s_scale, double dx,
+    double dy, const double* z_coords, const double* aspect,
+    const double* buffer_b, double phi_min, double phi_max, void* w_out,
+    const steam_window_t* window, double* level_sums_out, void* workspace,
+    size_t workspace_bytes, steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 1 && ny >= 1, "steam_scalar_pattern: empty horizontal extent");
+  STEAM_REQUIRE(nz >= 2, "steam_scalar_pattern: the z gradient needs nz >= 2");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_scalar_pattern: nz above 1024");
+  STEAM_REQUIRE(pert && w_out && mean_1d && z_coords && aspect && level_sums_out,
+                "steam_scalar_pattern: null pointer");
+  int rc = check_win(window, nx, ny, "steam_scalar_pattern");
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    return pattern_impl<float>(nx, ny, nz, (const float*)pert, mean_1d,
+                               (const float*)product, s_scale, dx, dy, z_coords,
+                               aspect, buffer_b, phi_min, phi_max,
+                               (float*)w_out, window, level_sums_out, workspace,
+                               workspace_bytes, s);
+  if (dtype == STEAM_F64)
+    return pattern_impl<double>(nx, ny, nz, (const double*)pert, mean_1d,
+                                (const double*)product, s_scale, dx, dy,
+                                z_coords, aspect, buffer_b, phi_min, phi_max,
+                                (double*)w_out, window, level_sums_out,
+                                workspace, workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_scalar_pattern: bad dtype");
+}
+
+extern "C" size_t steam_bounded_add_workspace_bytes(int64_t nz, int32_t n_rescale) {
+  const size_t R = n_rescale > 0 ? (size_t)n_rescale : 1;
+  return level_partial_bytes(nz, 2 * kMuCand) +
+         carve_bytes(nz, 8) * 8 + carve_bytes((size_t)nz * R, 8) * 2 +
+         carve_bytes((size_t)nz * kMuCand, 8);
+}
+
+extern "C" int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                 void* pert, const double* mean_1d,
+                                 void* increment, double phi_min,
+                                 double phi_max, const steam_window_t* window,
+                                 int32_t n_rescale, int32_t record_applied,
+                                 double* ledger_out, void* workspace,
+                                 size_t workspace_bytes,
+                                 steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_bounded_add: negative extent");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_bounded_add: nz above 1024");
+  STEAM_REQUIRE(n_rescale >= 0 && n_rescale <= 64,
+                "steam_bounded_add: n_rescale out of range");
+  STEAM_REQUIRE(phi_max > phi_min, "steam_bounded_add: phi_max must exceed phi_min");
+  int rc = check_win(window, nx, ny, "steam_bounded_add");
+  if (rc) return rc;
+  if (window) {
+    STEAM_REQUIRE(window->x1 > window->x0 && window->y1 > window->y0,
+                  "steam_bounded_add: empty window");
+  }
+  if (nx * ny * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(pert && increment && mean_1d, "steam_bounded_add: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int R = n_rescale > 0 ? n_rescale : 1;
+  if (dtype == STEAM_F32)
+    return bounded_add_impl<float>(nx, ny, nz, (float*)pert, mean_1d,
+                                   (float*)increment, phi_min, phi_max, window,
+                                   n_rescale > 0 ? R : 0, record_applied,
+                                   ledger_out, workspace, workspace_bytes, s);
+  if (dtype == STEAM_F64)
+    return bounded_add_impl<double>(nx, ny, nz, (double*)pert, mean_1d,
+                                    (double*)increment, phi_min, phi_max,
+                                    window, n_rescale > 0 ? R : 0,
+                                    record_applied, ledger_out, workspace,
+                                    workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_bounded_add: bad dtype");
+}
+
+extern "C" int steam_project_bounds(int dtype, int64_t nx, int64_t ny,
+                                    int64_t nz, void* pert,
+                                    const double* mean_1d, double phi_min,
+                                    double phi_max,
+                                    const steam_window_t* window,
+                                    double* mu_out, void* workspace,
+                                    size_t workspace_bytes,
+                                    steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_project_bounds: negative extent");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_project_bounds: nz above 1024");
+  STEAM_REQUIRE(phi_max > phi_min, "steam_project_bounds: phi_max must exceed phi_min");
+  int rc = check_win(window, nx, ny, "steam_project_bounds");
+  if (rc) return rc;
+  if (nx * ny * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(pert && mean_1d, "steam_project_bounds: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    return project_impl<float>(nx, ny, nz, (float*)pert, mean_1d, phi_min,
+                               phi_max, window, mu_out, workspace,
+                               workspace_bytes, s);
+  if (dtype == STEAM_F64)
+    return project_impl<double>(nx, ny, nz, (double*)pert, mean_1d, phi_min,
+                                phi_max, window, mu_out, workspace,
+                                workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_project_bounds: bad dtype");
+}

@@ -1,0 +1,305 @@
+"""Convolution and regrid entry points (steam/utils.py:222-534).
+
+``convolve_fft_xy_oa_z`` keeps the reference's semantics -- x and y circular
+over the full array period, z linear with zero padding, the kernel centred at
+(k-1)//2 after being folded onto a narrower field -- but not its method.  A
+turbulon kernel is a sum of a few separable terms, so the convolution runs as
+three coalesced 1D stencil passes on the device (z, then y, then x) over a
+Tucker factorisation of the kernel taken on the host in float64.  A kernel
+that does not factor into a few terms runs as a dense direct sum.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+from dataclasses import dataclass
+from math import gcd
+
+import numpy as np
+
+from . import _lib
+from ._device import check_device, is_tensor, to_device, to_host
+
+MAX_Z_FILTERS = 8
+MAX_PAIRS = 16
+MAX_X_FILTERS = 4
+MAX_TAPS = 1536
+
+# Relative Frobenius error allowed when a kernel is factored: well under the
+# float32 rounding of the kernel itself for float32 fields, and at float64
+# roundoff for float64 fields.
+FACTOR_TOL = {np.float32: 1e-6, np.float64: 1e-12}
+
+
+def fold_kernel_to_field(kernel, field_shape):
+    """Periodise a kernel wider than the field on x and y (steam/utils.py:222-242)."""
+    result = kernel
+    for axis in (0, 1):
+        n_field = field_shape[axis]
+        n_kern = result.shape[axis]
+        if n_kern <= n_field:
+            continue
+        shape = list(result.shape)
+        shape[axis] = n_field
+        folded = np.zeros(shape, dtype=result.dtype)
+        center = n_kern // 2
+        for i in range(n_kern):
+            dst = [slice(None)] * 3
+            src = [slice(None)] * 3
+            dst[axis] = (i - center) % n_field
+            src[axis] = i
+            folded[tuple(dst)] += result[tuple(src)]
+        result = np.roll(folded, n_field // 2, axis=axis)
+    return result
+
+
+def effective_centre(k: int, n: int) -> int:
+    """Centre tap of a kernel axis convolved circularly over period n.
+
+    convolve_fft_xy_oa_z folds a kernel wider than the field (rolling the fold
+    by n//2) and then centres it at (n-1)//2; as a circular convolution with
+    the UNFOLDED taps that is a centre of k//2 - (1 if n is even else 0).  A
+    kernel that fits keeps (k-1)//2.
+    """
+    if k <= n:
+        return (k - 1) // 2
+    return k // 2 - (1 if n % 2 == 0 else 0)
+
+
+def _mode_basis(unfolded, tol_abs):
+    U, s, _ = np.linalg.svd(unfolded, full_matrices=False)
+    tail = np.sqrt(np.cumsum((s ** 2)[::-1]))[::-1]  # tail[r] = ||s[r:]||
+    r = int(np.count_nonzero(tail > tol_abs))
+    return U[:, :max(r, 1)]
+
+
+@dataclass
+class ConvPlan:
+    """A kernel prepared for one field period (nx, ny) and dtype."""
+    kind: str
+    shape: tuple
+    spec: object = None
+    z_taps: object = None
+    y_taps: object = None
+    x_taps: object = None
+    dense: object = None           # folded kernel (host ndarray)
+    dense_dev: object = None       # folded kernel on the device
+    error: float = 0.0             # relative Frobenius error of the factorisation
+
+
+def factor_kernel(kernel, tol):
+    """Tucker factorisation K ~ sum core[a,b,c] X_a(x) Y_b(y) Z_c(z).
+
+    Returns (Px, Py, Pz, core, rel_err) with orthonormal factor columns.
+    """
+    K = np.asarray(kernel, dtype=np.float64)
+    kx, ky, kz = K.shape
+    norm = float(np.linalg.norm(K))
+    if norm == 0.0:
+        return (np.zeros((kx, 1)), np.zeros((ky, 1)), np.zeros((kz, 1)),
+                np.zeros((1, 1, 1)), 0.0)
+    tol_abs = tol * norm / np.sqrt(3.0)
+    Px = _mode_basis(K.reshape(kx, -1), tol_abs)
+    Py = _mode_basis(K.transpose(1, 0, 2).reshape(ky, -1), tol_abs)
+    Pz = _mode_basis(K.transpose(2, 0, 1).reshape(kz, -1), tol_abs)
+    core = np.einsum('ijk,ia,jb,kc->abc', K, Px, Py, Pz, optimize=True)
+    approx = np.einsum('abc,ia,jb,kc->ijk', core, Px, Py, Pz, optimize=True)
+    err = float(np.linalg.norm(K - approx)) / norm
+    return Px, Py, Pz, core, err
+
+
+def plan_from_factors(Px, Py, Pz, core, kshape, field_shape, err=0.0):
+    """Separable plan from explicit factors (x: Px[:, a], ...), or None when
+    the factor counts exceed the kernels' limits."""
+    kx, ky, kz = kshape
+    nx, ny = int(field_shape[0]), int(field_shape[1])
+    rx, ry, rz = Px.shape[1], Py.shape[1], Pz.shape[1]
+    npairs = ry * rz
+    taps = rz * kz + ry * ky + rx * kx
+    if rz > MAX_Z_FILTERS or rx > MAX_X_FILTERS or npairs > MAX_PAIRS or taps > MAX_TAPS:
+        return None
+    spec = _lib.SepConv()
+    spec.kz, spec.ky, spec.kx = kz, ky, kx
+    spec.cz = (kz - 1) // 2
+    spec.cy = effective_centre(ky, ny)
+    spec.cx = effective_centre(kx, nx)
+    spec.n_z, spec.n_y, spec.n_x, spec.n_pairs = rz, ry, rx, npairs
+    for c in range(rz):
+        for b in range(ry):
+            q = c * ry + b
+            spec.pair_z[q] = c
+            spec.pair_y[q] = b
+            for a in range(rx):
+                spec.mix[a * npairs + q] = float(core[a, b, c])
+    return ConvPlan(
+        kind='separable', shape=(kx, ky, kz), spec=spec,
+        z_taps=_lib.dvec(Pz.T.ravel()), y_taps=_lib.dvec(Py.T.ravel()),
+        x_taps=_lib.dvec(Px.T.ravel()), error=err)
+
+
+_PLAN_CACHE: dict = {}
+
+
+def plan_convolution(kernel, field_shape, dtype=np.float32, tol=None):
+    """Prepare ``kernel`` for fields of ``field_shape`` (cached)."""
+    kernel = np.asarray(kernel)
+    if kernel.ndim != 3:
+        raise ValueError(f"kernel must be 3D, got shape {kernel.shape}")
+    dtype = np.dtype(dtype).type
+    tol = FACTOR_TOL[dtype] if tol is None else float(tol)
+    nx, ny = int(field_shape[0]), int(field_shape[1])
+    key = (hashlib.sha1(np.ascontiguousarray(kernel, dtype=np.float64).tobytes()).hexdigest(),
+           kernel.shape, nx, ny, dtype, tol)
+    plan = _PLAN_CACHE.get(key)
+    if plan is not None:
+        return plan
+    Px, Py, Pz, core, err = factor_kernel(kernel, tol)
+    plan = None
+    if err <= tol:
+        plan = plan_from_factors(Px, Py, Pz, core, kernel.shape, (nx, ny), err)
+    if plan is None:
+        folded = fold_kernel_to_field(np.asarray(kernel, dtype=np.float64), (nx, ny))
+        plan = ConvPlan(kind='dense', shape=folded.shape, dense=folded)
+    if len(_PLAN_CACHE) > 256:
+        _PLAN_CACHE.clear()
+    _PLAN_CACHE[key] = plan
+    return plan
+
+
+def run_plan(plan, field_t, out_t, pre_div=None, pre_mul=None,
+             epilogue=_lib.STEAM_EPI_STORE, window=None):
+    """Launch a planned convolution on device tensors; returns the epilogue
+    sums (flux epilogue) or None."""
+    import torch
+    lib = _lib.load()
+    nx, ny, nz = (int(n) for n in field_t.shape)
+    code = _lib.dtype_code(field_t)
+    if plan.kind == 'dense':
+        if epilogue != _lib.STEAM_EPI_STORE or pre_div is not None or pre_mul is not None:
+            tmp_in = field_t
+            if pre_div is not None or pre_mul is not None:
+                d = torch.as_tensor(np.asarray(pre_div if pre_div is not None else np.ones(nz)),
+                                    dtype=field_t.dtype, device=field_t.device)
+                m = torch.as_tensor(np.asarray(pre_mul if pre_mul is not None else np.ones(nz)),
+                                    dtype=field_t.dtype, device=field_t.device)
+                tmp_in = (field_t / d) * m
+            conv = torch.empty_like(field_t)
+            _dense(lib, plan, tmp_in, conv, code)
+            if epilogue == _lib.STEAM_EPI_STORE:
+                out_t.copy_(conv)
+                return None
+            return _flux_epilogue_dense(out_t, conv, window)
+        _dense(lib, plan, field_t, out_t, code)
+        return None
+    nbytes = lib.steam_conv_workspace_bytes(code, nx, ny, nz, ctypes.byref(plan.spec))
+    ws = _lib.WORKSPACE.get(nbytes)
+    sums = _lib.dout(3)
+    pd = _lib.dvec(pre_div) if pre_div is not None else None
+    pm = _lib.dvec(pre_mul) if pre_mul is not None else None
+    _lib.check(lib.steam_conv_separable(
+        code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps, plan.x_taps,
+        _lib.ptr(field_t), pd, pm, _lib.ptr(out_t), epilogue, _lib.window_arg(window),
+        sums, _lib.ptr(ws), ws.numel(), _lib.stream()))
+    if epilogue == _lib.STEAM_EPI_FLUX:
+        return (sums[0], sums[1], sums[2])
+    return None
+
+
+def _dense(lib, plan, field_t, out_t, code):
+    import torch
+    key = (field_t.dtype, field_t.device)
+    if plan.dense_dev is None or plan.dense_dev[0] != key:
+        plan.dense_dev = (key, torch.as_tensor(plan.dense, dtype=field_t.dtype,
+                                               device=field_t.device).contiguous())
+    kdev = plan.dense_dev[1]
+    nx, ny, nz = (int(n) for n in field_t.shape)
+    kx, ky, kz = plan.shape
+    _lib.check(lib.steam_conv_dense(code, nx, ny, nz, _lib.ptr(kdev), kx, ky, kz,
+                                    _lib.ptr(field_t), _lib.ptr(out_t), _lib.stream()))
+
+
+def _flux_epilogue_dense(flux_t, conv_t, window):
+    """F = max(F + conv, 0) with the flux epilogue's sums, for the dense path."""
+    flux_t.add_(conv_t)
+    n_clipped = int((flux_t < 0).sum().item())
+    flux_t.clamp_(min=0)
+    inner = flux_t if window is None else flux_t[window[0]:window[1], window[2]:window[3]]
+    return (float(inner.sum(dtype=flux_t.new_zeros(()).double().dtype).item()),
+            float(inner.numel() // flux_t.shape[2]), float(n_clipped))
+
+
+def convolve_device(field_t, kernel, out=None, tol=None):
+    """Convolve a CUDA tensor; returns a new (or the given) CUDA tensor."""
+    import torch
+    if field_t.ndim != 3:
+        raise ValueError(f"field must be 3D, got shape {tuple(field_t.shape)}")
+    np_dtype = np.float64 if field_t.dtype == torch.float64 else np.float32
+    plan = plan_convolution(kernel, field_t.shape, np_dtype, tol)
+    if out is None:
+        out = torch.empty_like(field_t)
+    if field_t.numel() == 0:
+        return out
+    run_plan(plan, field_t, out)
+    return out
+
+
+def convolve_fft_xy_oa_z(field, kernel, device='cuda'):
+    """Convolution with circular x/y and linear zero-padded z
+    (steam/utils.py:293-427).  Numpy in -> numpy out (transfers inside the
+    call, as the reference's device='cuda' path does); a CUDA tensor in -> a
+    CUDA tensor out."""
+    check_device(device, "convolve_fft_xy_oa_z")
+    t, host = to_device(field)
+    out = convolve_device(t, np.asarray(kernel))
+    if host is None:
+        return out
+    return to_host(out).astype(host.dtype, copy=False)
+
+
+# ---------------------------------------------------------------------------
+# Regrid (steam/utils.py:435-534)
+# ---------------------------------------------------------------------------
+
+def wrap_pad_factor(source_shape, target_shape, periodic=(True, True, False)):
+    """Working-array growth the reference's wrapped pad would need
+    (steam/utils.py:537-564).  The device regrid wraps natively, so this is
+    informational only."""
+    padded = 1
+    target = 1
+    for n_in, n_out, per in zip(source_shape, target_shape, periodic):
+        target *= n_out
+        if not per or n_out < n_in:
+            padded *= n_out
+            continue
+        padded *= n_out + 2 * (n_out // gcd(n_in, n_out))
+    return padded / target if target else 1.0
+
+
+def zoom_device(field_t, target_shape, periodic=(True, True, False)):
+    import torch
+    nx, ny, nz = (int(n) for n in field_t.shape)
+    mx, my, mz = (int(n) for n in target_shape)
+    if periodic[2]:
+        raise NotImplementedError("z never wraps in the cascade regrid")
+    for axis, (n_in, n_out, per) in enumerate(zip((nx, ny), (mx, my), periodic[:2])):
+        if per and n_out < n_in:
+            raise NotImplementedError(
+                f"Periodic resampling downsamples on axis {axis} ({n_in} -> {n_out}); "
+                f"the cascade's hops only go finer.")
+    out = torch.empty((mx, my, mz), dtype=field_t.dtype, device=field_t.device)
+    lib = _lib.load()
+    _lib.check(lib.steam_regrid(_lib.dtype_code(field_t), _lib.ptr(field_t), nx, ny, nz,
+                                _lib.ptr(out), mx, my, mz, int(bool(periodic[0])),
+                                int(bool(periodic[1])), _lib.stream()))
+    return out
+
+
+def zoom_trilinear(field, target_shape, periodic=(True, True, False)):
+    """Cell-consistent trilinear resample, x/y periodic (steam/utils.py:507-534)."""
+    _lib.require_cuda("zoom_trilinear")
+    t, host = to_device(field)
+    out = zoom_device(t, target_shape, periodic)
+    if host is None:
+        return out
+    return to_host(out).astype(np.float32, copy=False)

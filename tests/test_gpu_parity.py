@@ -1,0 +1,428 @@
+"""CUDA path against the oracle and the reference fixtures (needs a B200).
+
+Tolerances: integer work (Philox, the uniform lattice, the centre lattice) is
+bit-exact.  Float32 stages agree with the reference's float32 arithmetic to a
+few float32 ulps (rtol 1e-5 unless stated).  Float64 stages agree with the
+float64 oracle to 1e-10 relative.  The flux agrees with the float64 oracle to
+<= 1e-5 relative L2 in log-flux on the oracle's positive cells.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import steam_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    n = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (n if n > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def steam():
+    import steam_b200.noise
+    import steam_b200.simulate
+    import steam_b200.thermodynamics
+    import steam_b200.utils
+    return steam_b200
+
+
+# ---------------------------------------------------------------------------
+# Keyed noise
+# ---------------------------------------------------------------------------
+
+def test_keyed_uniforms_bit_exact(golden, steam):
+    key = golden["ku_key"]
+    n = golden["ku_lane0"].size
+    l0 = np.empty(n, np.float32)
+    l1 = np.empty(n, np.float32)
+    steam.noise.keyed_uniforms(golden["ku_ix"], golden["ku_iy"], golden["ku_iz"],
+                               key[0], key[1], key[2], l0, l1)
+    assert np.array_equal(l0.view(np.uint32), golden["ku_lane0"].view(np.uint32))
+    assert np.array_equal(l1.view(np.uint32), golden["ku_lane1"].view(np.uint32))
+
+
+def test_keyed_uniforms_large_box_matches_oracle(steam, torch):
+    key = O.class_key(np.random.SeedSequence(123))
+    ix = np.arange(0, 40) * 977 + 5
+    iy = np.arange(0, 33) * 131
+    iz = np.arange(-4, 60)
+    n = ix.size * iy.size * iz.size
+    l0 = torch.empty(n, dtype=torch.float32, device='cuda')
+    l1 = torch.empty(n, dtype=torch.float32, device='cuda')
+    steam.noise.keyed_uniforms(torch.as_tensor(ix, device='cuda'),
+                               torch.as_tensor(iy, device='cuda'),
+                               torch.as_tensor(iz, device='cuda'), *key, l0, l1)
+    r0, r1 = O.keyed_uniforms(ix, iy, iz, key)
+    assert np.array_equal(l0.cpu().numpy().view(np.uint32), r0.view(np.uint32))
+    assert np.array_equal(l1.cpu().numpy().view(np.uint32), r1.view(np.uint32))
+
+
+def test_sparse_levy_fixtures(golden, steam):
+    sim = steam.simulate
+    root = sim.NoiseRegion(tuple(int(v) for v in golden["sl_root_key"]), (0, 0, 0), (8, 6, 5))
+    got = sim._keyed_sparse_levy((8, 6, 5), (1, 1, 1), 1.8, root)
+    np.testing.assert_allclose(got, golden["sl_root"], rtol=1e-5, atol=1e-6)
+    halo = sim.NoiseRegion(tuple(int(v) for v in golden["sl_halo_key"]), (3, 5, 1), (10, 12, 20))
+    got = sim._keyed_sparse_levy((9, 7, 11), (2, 2, 3), 1.8, halo)
+    assert np.array_equal(got != 0, golden["sl_halo"] != 0)
+    np.testing.assert_allclose(got, golden["sl_halo"], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("alpha", [1.5, 1.8, 1.95, 2.0])
+def test_levy_float64_against_oracle(steam, alpha):
+    sim = steam.simulate
+    key = O.class_key(np.random.SeedSequence(77))
+    region = sim.NoiseRegion(key, (0, 0, 0), (24, 20, 16))
+    got = sim._keyed_sparse_levy((24, 20, 16), (1, 1, 1), alpha, region, dtype=np.float64)
+    want = O.keyed_sparse_levy((24, 20, 16), (1, 1, 1), alpha, key, dtype=np.float64)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+    got32 = sim._keyed_sparse_levy((24, 20, 16), (1, 1, 1), alpha, region)
+    want32 = O.keyed_sparse_levy((24, 20, 16), (1, 1, 1), alpha, key)
+    np.testing.assert_allclose(got32, want32, rtol=2e-5, atol=2e-5)
+
+
+def test_world_restriction_is_exact(steam):
+    """A tile's noise is the world's noise restricted to the tile, bit for bit,
+    including a halo that wraps around the periodic edge."""
+    sim = steam.simulate
+    key = O.class_key(np.random.SeedSequence(3))
+    world = (32, 24, 12)
+    full = sim._keyed_sparse_levy(world, (2, 2, 1), 1.8, sim.NoiseRegion(key, (0, 0, 0), world))
+    tile = sim._keyed_sparse_levy((12, 10, 12), (2, 2, 1), 1.8,
+                                  sim.NoiseRegion(key, (26, 19, 0), world))
+    xs = (26 + np.arange(12)) % 32
+    ys = (19 + np.arange(10)) % 24
+    assert np.array_equal(tile.view(np.uint32), full[np.ix_(xs, ys)].view(np.uint32))
+
+
+# ---------------------------------------------------------------------------
+# Kernel build
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("name,args,shape", [
+    ("kern_s1", (1, 0.5, 0.5, 0.5), "mexican_hat"),
+    ("kern_s2", (1, 0.25, 0.25, 0.25), "mexican_hat"),
+    ("kern_aniso", (1, 0.5, 0.5, 0.3), "mexican_hat"),
+    ("kern_morlet", (1, 0.5, 0.5, 0.5), "morlet_omega0_6"),
+])
+def test_kernel_build(golden, steam, name, args, shape):
+    got = steam.simulate._turbulon_envelope(*args, shape=shape)
+    assert got.shape == golden[name].shape
+    np.testing.assert_allclose(got, golden[name], rtol=1e-5, atol=2e-6)
+    g64 = steam.simulate._turbulon_envelope(*args, shape=shape, dtype=np.float64)
+    w64 = O.turbulon_envelope(*args, shape=shape, dtype=np.float64)
+    np.testing.assert_allclose(g64, w64, rtol=1e-12, atol=1e-13)
+
+
+# ---------------------------------------------------------------------------
+# Convolution
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("tag,kernel", [("conv1", "kern_s1"), ("conv2", "conv2_kernel"),
+                                        ("conv3", "kern_s1")])
+def test_convolution_fixtures(golden, steam, tag, kernel):
+    got = steam.utils.convolve_fft_xy_oa_z(golden[f"{tag}_field"], golden[kernel])
+    assert got.dtype == np.float32
+    assert rel_l2(got, golden[f"{tag}_out"]) < 2e-6
+
+
+@pytest.mark.parametrize("shape", [(40, 36, 30), (7, 9, 20), (64, 48, 5), (33, 17, 70)])
+def test_convolution_float64_against_oracle(steam, shape):
+    rng = np.random.default_rng(sum(shape))
+    f = rng.standard_normal(shape)
+    k = O.turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=np.float64)
+    got = steam.utils.convolve_fft_xy_oa_z(f, k)
+    assert got.dtype == np.float64
+    assert rel_l2(got, O.convolve(f, k)) < 1e-12
+
+
+def test_convolution_small_full_rank_kernel_float64(steam):
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal((20, 18, 15))
+    k = rng.standard_normal((3, 3, 3))
+    got = steam.utils.convolve_fft_xy_oa_z(f, k)
+    assert rel_l2(got, O.convolve(f, k)) < 1e-12
+
+
+def test_convolution_empty_field(steam):
+    out = steam.utils.convolve_fft_xy_oa_z(np.zeros((0, 4, 4), np.float32),
+                                          np.ones((3, 3, 3), np.float32))
+    assert out.shape == (0, 4, 4)
+
+
+# ---------------------------------------------------------------------------
+# Flux advance
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("tag,shape,sp,kern", [("fa1", (16, 12, 10), (1, 1, 1), "kern_s1"),
+                                               ("fa2", (16, 16, 12), (2, 2, 2), "kern_s2")])
+def test_advance_flux_fixtures(golden, steam, tag, shape, sp, kern):
+    sim = steam.simulate
+    flux = golden[f"{tag}_flux_in"].copy()
+    region = sim.NoiseRegion(tuple(int(v) for v in golden[f"{tag}_key"]), (0, 0, 0), shape)
+    S, led, diag = sim._advance_flux(flux, region, golden[kern], 0.1, 1, sp, n_zero=2,
+                                     zero_bottom=True, zero_top=True)
+    ref = golden[f"{tag}_ledger"]
+    assert led.entering.total == pytest.approx(ref[0], rel=1e-12)
+    assert led.noise_abs.count == ref[3]
+    assert led.noise_abs.total == pytest.approx(ref[2], rel=1e-5)
+    assert abs(led.n_clipped - ref[6]) <= 1
+    assert rel_l2(S, golden[f"{tag}_S"]) < 1e-5
+    assert rel_l2(flux, golden[f"{tag}_flux_out"]) < 1e-5
+
+
+def test_advance_flux_float64_against_oracle(steam):
+    sim = steam.simulate
+    shape = (24, 20, 18)
+    rng = np.random.default_rng(8)
+    flux0 = 1.0 + 0.3 * rng.random(shape)
+    key = O.class_key(np.random.SeedSequence(21))
+    kern = O.turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=np.float64)
+    f_gpu = flux0.copy()
+    S, led, _ = sim._advance_flux(f_gpu, sim.NoiseRegion(key, (0, 0, 0), shape), kern, 0.1,
+                                  1, (1, 1, 1), n_zero=2, zero_bottom=True, zero_top=True)
+    f_ora = flux0.copy()
+    S_o, rec = O.advance_flux(f_ora, key, kern, 0.1, 1, (1, 1, 1), n_zero=2,
+                              zero_bottom=True, zero_top=True)
+    assert led.n_clipped == rec['n_clipped']
+    assert rel_l2(f_gpu, f_ora) < 1e-10
+    assert rel_l2(S, S_o) < 1e-10
+
+
+def test_log_flux_error_float32_vs_float64_oracle(steam):
+    """FP32 device flux against the FP64 oracle: <= 1e-5 relative L2 in
+    log-flux over the oracle's positive cells, clip masks reported apart."""
+    sim = steam.simulate
+    shape = (48, 40, 32)
+    key = O.class_key(np.random.SeedSequence(99))
+    k32 = O.turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=np.float32)
+    k64 = O.turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=np.float64)
+    f32 = np.ones(shape, np.float32)
+    sim._advance_flux(f32, sim.NoiseRegion(key, (0, 0, 0), shape), k32, 0.1, 1, (1, 1, 1),
+                      n_zero=2, zero_bottom=True, zero_top=True)
+    f64 = np.ones(shape, np.float64)
+    O.advance_flux(f64, key, k64, 0.1, 1, (1, 1, 1), n_zero=2, zero_bottom=True,
+                   zero_top=True)
+    pos = (f64 > 0) & (f32 > 0)
+    assert np.count_nonzero((f64 > 0) != (f32 > 0)) <= max(1, pos.size // 10000)
+    err = rel_l2(np.log(f32[pos].astype(np.float64)), np.log(f64[pos]))
+    assert err <= 1e-5, err
+
+
+# ---------------------------------------------------------------------------
+# Scalar pattern, bounded add, projection
+# ---------------------------------------------------------------------------
+
+def test_advective_weight_fixtures(golden, steam):
+    for z in ("uni", "var"):
+        got = steam.simulate._advective_weight(golden["aw_field"], 100.0, 80.0,
+                                               golden[f"aw_z_{z}"], golden["aw_aspect"])
+        np.testing.assert_allclose(got, golden[f"aw_{z}"], rtol=2e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float32, 2e-5), (np.float64, 1e-11)])
+def test_scalar_pattern_against_oracle(steam, torch, dtype, tol):
+    sim = steam.simulate
+    rng = np.random.default_rng(4)
+    shape = (20, 16, 14)
+    z = np.concatenate([[0.0], np.cumsum(60.0 + 20.0 * rng.random(13))])
+    mean = np.linspace(340e3, 320e3, 14).astype(np.float32)
+    pert = (1500.0 * rng.standard_normal(shape)).astype(dtype)
+    prod = rng.standard_normal(shape).astype(dtype) * (rng.random(shape) < 0.5)
+    aspect = (0.3 + rng.random(14)).astype(np.float32)
+    b = (2e3 + 4e3 * rng.random(14)).astype(np.float32)
+    C = (100.0 + 50 * rng.random(14)).astype(np.float32)
+    s_scale = float(dtype(1.0 / 0.37))
+    S = (prod * dtype(s_scale)).astype(dtype)
+    Wo, tot, cnt = O.scalar_pattern(pert, mean, S, 100.0, 100.0, z, aspect, b, 315e3, 355e3, C)
+    pt = torch.as_tensor(pert, device='cuda')
+    W, gtot, gcnt = sim.pattern_device(pt, mean, torch.as_tensor(prod, device='cuda'),
+                                       s_scale, 100.0, 100.0, z, aspect, b, 315e3, 355e3)
+    assert np.array_equal(gcnt, cnt)
+    np.testing.assert_allclose(gtot, tot, rtol=tol)
+    lm = (gtot / np.maximum(gcnt, 1)).astype(np.float32)
+    Wn = (W.cpu().numpy() / np.where(lm > 0, lm, 1)[None, None, :]) * C[None, None, :]
+    assert rel_l2(Wn, Wo) < tol * 10
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_bounded_add_against_oracle(golden, steam, dtype):
+    sim = steam.simulate
+    pert = golden["ba_pert_in"].astype(dtype)
+    inc = golden["ba_inc_in"].astype(dtype)
+    p_o, i_o = pert.copy(), inc.copy()
+    rec = O.bounded_amplitude_add(p_o, golden["ba_mean"], i_o, 0.0, 0.03, record_applied=True)
+    p_g, i_g = pert.copy(), inc.copy()
+    led = sim._bounded_amplitude_add(p_g, golden["ba_mean"], i_g, 0.0, 0.03,
+                                     record_applied=True)
+    atol = 2e-9 if dtype == np.float32 else 1e-13
+    np.testing.assert_allclose(p_g, p_o, rtol=0, atol=atol)
+    np.testing.assert_allclose(i_g, i_o, rtol=0, atol=atol)
+    np.testing.assert_allclose(led.a0, rec['a0'], rtol=1e-10)
+    if dtype == np.float32:
+        np.testing.assert_allclose(p_g, golden["ba_pert_out"], rtol=0, atol=atol)
+    # the three deposit conditions: bounds, zero level mean
+    field = p_g + golden["ba_mean"][None, None, :].astype(dtype)
+    assert field.min() >= -1e-9 and field.max() <= 0.03 + 1e-9
+    assert np.all(np.abs(i_g.mean(axis=(0, 1))) < 1e-6 * np.maximum(led.a0, 1e-30) + 1e-12)
+
+
+def test_bounded_add_larger_levels(steam):
+    """Many levels, some against each bound, some interior, a clip-only level."""
+    sim = steam.simulate
+    rng = np.random.default_rng(12)
+    nz = 40
+    shape = (64, 48, nz)
+    mean = np.linspace(0.0005, 0.029, nz).astype(np.float32)
+    pert = np.clip(0.003 * rng.standard_normal(shape) + mean, 0, 0.03).astype(np.float32) - mean
+    inc = (0.005 * rng.standard_normal(shape)).astype(np.float32)
+    inc[:, :, 7] = 0.0
+    p_o, i_o = pert.copy(), inc.copy()
+    O.bounded_amplitude_add(p_o, mean, i_o, 0.0, 0.03, record_applied=True)
+    p_g, i_g = pert.copy(), inc.copy()
+    sim._bounded_amplitude_add(p_g, mean, i_g, 0.0, 0.03, record_applied=True)
+    np.testing.assert_allclose(p_g, p_o, rtol=0, atol=5e-9)
+
+
+def test_projection_against_oracle(steam):
+    sim = steam.simulate
+    rng = np.random.default_rng(6)
+    shape = (30, 20, 12)
+    mean = np.linspace(0.001, 0.02, 12).astype(np.float32)
+    pert = (0.004 * rng.standard_normal(shape)).astype(np.float32)
+    p_o = pert.copy()
+    mu_o = O.project_onto_bounds(p_o, mean, 0.0, 0.03)
+    p_g = pert.copy()
+    led = sim._project_onto_bounds(p_g, mean, 0.0, 0.03)
+    assert np.array_equal(np.isnan(led.mu), np.isnan(mu_o))
+    np.testing.assert_allclose(p_g, p_o, rtol=0, atol=2e-9)
+
+
+# ---------------------------------------------------------------------------
+# Regrid, thermodynamics
+# ---------------------------------------------------------------------------
+
+def test_zoom_fixtures(golden, steam):
+    np.testing.assert_allclose(steam.utils.zoom_trilinear(golden["zoom_src"], (10, 8, 9)),
+                               golden["zoom_dyadic"], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(steam.utils.zoom_trilinear(golden["zoom_src"], (15, 6, 7)),
+                               golden["zoom_odd"], rtol=1e-5, atol=1e-6)
+
+
+def test_thermodynamics_fixtures(golden, steam):
+    out = steam.thermodynamics.recover_diagnostics(golden["th_h"], golden["th_qt"],
+                                                    golden["th_z"], 101325.0)
+    np.testing.assert_allclose(out["T"], golden["th_T"], rtol=0, atol=2e-3)
+    np.testing.assert_allclose(out["p"], golden["th_p"], rtol=2e-6)
+    for k in ("qv", "qc", "qi"):
+        np.testing.assert_allclose(out[k], golden[f"th_{k}"], rtol=0, atol=2e-7)
+
+
+def test_thermodynamics_float64_against_oracle(golden, steam):
+    h = golden["th_h"].astype(np.float64)
+    q = golden["th_qt"].astype(np.float64)
+    out = steam.thermodynamics.recover_diagnostics(h, q, golden["th_z"], 101325.0)
+    want = O.recover_diagnostics(h, q, golden["th_z"], 101325.0)
+    for k in ("T", "qv", "qc", "qi", "p"):
+        np.testing.assert_allclose(out[k], want[k], rtol=1e-10, atol=1e-14)
+
+
+# ---------------------------------------------------------------------------
+# One class of the cascade, and a whole small run
+# ---------------------------------------------------------------------------
+
+def _one_class_setup(nx=32, ny=24, nz=20):
+    from steam_b200 import simulate as sim
+    zp = np.arange(64) * 50.0
+    hp = (340e3 - 20e3 * zp / zp.max()).astype(np.float32)
+    qp = (0.018 - 0.016 * zp / zp.max()).astype(np.float32)
+    k = 200.0
+    grids = sim._compute_all_grids(np.array([k]), nx * 100.0, ny * 100.0, nz * 100.0,
+                                   (1, 1, 1), np.full(64, 1000.0), zp)
+    assert (grids['nx'][0], grids['ny'][0], grids['nz'][0]) == (nx, ny, nz)
+    kzl = sim._k_z('piecewise_isotropic_below_spheroscale', 12800.0, np.full(64, 1000.0))
+    C_h = sim._compute_normalization(hp, zp, kzl, np.array([k]), 12800.0, grids)
+    C_q = sim._compute_normalization(qp, zp, kzl, np.array([k]), 12800.0, grids)
+    return sim, zp, hp, qp, grids, C_h, C_q
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_single_class_step_against_oracle(steam, dtype):
+    sim, zp, hp, qp, grids, C_h, C_q = _one_class_setup()
+    b_h = sim._bound_buffers(C_h, 1)
+    b_q = sim._bound_buffers(C_q, 1)
+    aspect = [np.ones(20, np.float32)]
+    seeds = np.random.SeedSequence(0).spawn(1)
+    rng = np.random.default_rng(0)
+    shape = (32, 24, 20)
+    h0 = (800.0 * rng.standard_normal(shape)).astype(dtype)
+    q0 = (0.0008 * rng.standard_normal(shape)).astype(dtype)
+    F0 = (1.0 + 0.2 * rng.random(shape)).astype(dtype)
+    out = sim.cascade_loop(hp, qp, zp, grids, C_h, C_q, b_h, b_q, aspect, 315 * 1004,
+                           355 * 1004, 0.0, 0.03, 1, (1, 1, 1), seeds,
+                           h_perturbation=h0, qt_perturbation=q0, flux=F0,
+                           comp_k=[np.ones(20, np.float32)], dtype=dtype)
+    h_g, q_g, F_g = out[0], out[1], out[2]
+    z = grids['z_arrays'][0]
+    key = O.class_key(seeds[0])
+    kern = O.turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=dtype)
+    h_o, q_o, F_o = h0.copy(), q0.copy(), F0.copy()
+    O.class_step(h_o, q_o, F_o, key, kern,
+                 h_mean=np.interp(z, zp, hp).astype(np.float32),
+                 qt_mean=np.interp(z, zp, qp).astype(np.float32), z_coords=z,
+                 dx=100.0, dy=100.0, aspect=aspect[0], C_h=C_h[0], C_qt=C_q[0], b_h=b_h[0],
+                 b_qt=b_q[0], h_min=315 * 1004, h_max=355 * 1004, qt_min=0.0, qt_max=0.03,
+                 flux_noise_scale=sim.FLUX_SCALE, n_per_dyad=1, sparsity_factors=(1, 1, 1),
+                 n_zero=2)
+    tol = 1e-9 if dtype == np.float64 else 1e-5
+    assert rel_l2(F_g, F_o) < tol
+    assert rel_l2(h_g - h0, h_o - h0) < tol * 10
+    assert rel_l2(q_g - q0, q_o - q0) < tol * 10
+
+
+def test_small_root_run_statistics(golden, steam):
+    """A whole 16 x 16 root run (4 classes) against the reference's own run of
+    the same configuration.  The cascade's clip and bounded add amplify
+    roundoff, so the comparison is statistical: level means and spreads."""
+    sim = steam.simulate
+    zp = np.arange(28) * 30.0
+    hp = 340e3 - 20e3 * zp / zp.max()
+    qp = 0.018 - 0.016 * zp / zp.max()
+    res = sim.simulate(h_profile=hp, qt_profile=qp, nx=16, ny=16, dx=125.0, dy=125.0,
+                       outer_scale=2000.0, spheroscale=100.0, domain_height=800.0,
+                       profile_dz=30.0, output_path=None, seed=42)
+    for name, span in (("h", 40 * 1004), ("qt", 0.03)):
+        got, ref = res[name], golden[f"sim_{name}"]
+        assert got.shape == ref.shape
+        lm_g = got.mean(axis=(0, 1))
+        lm_r = ref.mean(axis=(0, 1))
+        assert np.max(np.abs(lm_g - lm_r)) < 1e-3 * span
+        sd_g, sd_r = got.std(axis=(0, 1)), ref.std(axis=(0, 1))
+        assert np.max(np.abs(sd_g - sd_r) / np.maximum(sd_r, 1e-12 * span)) < 0.25
+    assert res["flux"].mean() == pytest.approx(golden["sim_flux"].mean(), rel=1e-3)
+
+
+def test_repeat_runs_are_bit_identical(steam):
+    sim = steam.simulate
+    key = O.class_key(np.random.SeedSequence(17))
+    kern = O.turbulon_envelope(1, 0.5, 0.5, 0.5)
+    outs = []
+    for _ in range(2):
+        f = np.ones((40, 32, 24), np.float32)
+        S, led, _ = sim._advance_flux(f, sim.NoiseRegion(key, (0, 0, 0), f.shape), kern, 0.1,
+                                      1, (1, 1, 1))
+        outs.append((f, S, led.realized.total))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]

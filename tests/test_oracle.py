@@ -1,0 +1,155 @@
+"""The oracle restatement pinned against fixtures produced by the reference.
+
+Integer work must match bit for bit; float32 stages that restate the
+reference's own numpy arithmetic must match to float32 roundoff; the FFT-based
+stages agree to the reference's own FFT accuracy.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import steam_oracle as O
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    d = np.linalg.norm(a - b)
+    n = np.linalg.norm(b)
+    return d / n if n > 0 else d
+
+
+def test_philox_known_answers(golden):
+    for c, k, o in zip(golden["kat_counter"], golden["kat_key"], golden["kat_out"]):
+        got = O.philox4x32_10(*[np.uint64(v) for v in c], int(k[0]), int(k[1]))
+        assert tuple(int(v) for v in got) == tuple(int(v) for v in o)
+
+
+def test_keyed_uniforms_bit_exact(golden):
+    key = tuple(int(v) for v in golden["ku_key"])
+    l0, l1 = O.keyed_uniforms(golden["ku_ix"], golden["ku_iy"], golden["ku_iz"], key)
+    assert np.array_equal(l0.view(np.uint32), golden["ku_lane0"].view(np.uint32))
+    assert np.array_equal(l1.view(np.uint32), golden["ku_lane1"].view(np.uint32))
+
+
+def test_uniform_lattice(golden):
+    for lane in (golden["ku_lane0"], golden["ku_lane1"]):
+        s = lane.astype(np.float64) * 2.0 ** 24
+        assert np.all(s == np.round(s))
+        assert lane.min() >= 0.0 and lane.max() < 1.0
+
+
+@pytest.mark.parametrize("alpha", [1.5, 1.8, 1.95, 2.0])
+def test_levy_float32_matches_reference(golden, alpha):
+    got = O.levy_from_uniforms(alpha, golden["ku_lane0"], golden["ku_lane1"], np.float32)
+    ref = golden[f"levy_{alpha}"]
+    assert got.dtype == np.float32
+    np.testing.assert_allclose(got, ref, rtol=2e-6, atol=1e-6)
+
+
+def test_levy_float64_close_to_float32(golden):
+    got = O.levy_from_uniforms(1.8, golden["ku_lane0"], golden["ku_lane1"], np.float64)
+    assert rel_l2(got, golden["levy_1.8"]) < 1e-5
+
+
+def test_sparse_levy_fields(golden):
+    root = O.keyed_sparse_levy((8, 6, 5), (1, 1, 1), 1.8, tuple(golden["sl_root_key"]))
+    np.testing.assert_allclose(root, golden["sl_root"], rtol=2e-6, atol=1e-6)
+    halo = O.keyed_sparse_levy((9, 7, 11), (2, 2, 3), 1.8, tuple(golden["sl_halo_key"]),
+                               origin=(3, 5, 1), world_shape=(10, 12, 20))
+    assert np.array_equal(halo != 0, golden["sl_halo"] != 0)
+    np.testing.assert_allclose(halo, golden["sl_halo"], rtol=2e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("name,args,shape", [
+    ("kern_s1", (1, 0.5, 0.5, 0.5), "mexican_hat"),
+    ("kern_s2", (1, 0.25, 0.25, 0.25), "mexican_hat"),
+    ("kern_aniso", (1, 0.5, 0.5, 0.3), "mexican_hat"),
+    ("kern_morlet", (1, 0.5, 0.5, 0.5), "morlet_omega0_6"),
+])
+def test_kernel_build(golden, name, args, shape):
+    got = O.turbulon_envelope(*args, shape=shape)
+    np.testing.assert_allclose(got, golden[name], rtol=1e-6, atol=1e-6)
+
+
+def test_kernel_known_peaks(golden):
+    # Gaussian-weighted admissibility: the centre tap is A_opt = 2.96781718 at
+    # s=1 and 3 at s=2 (the reference's kernel tests pin these values).
+    k1 = O.turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=np.float64)
+    assert k1[6, 6, 6] == pytest.approx(2.96781718, abs=1e-7)
+    k2 = O.turbulon_envelope(1, 0.25, 0.25, 0.25, dtype=np.float64)
+    assert k2[12, 12, 12] == pytest.approx(3.0, abs=1e-9)
+    assert abs(k1.sum()) < 1e-12 and abs(k2.sum()) < 1e-12
+
+
+@pytest.mark.parametrize("tag,kernel", [("conv1", "kern_s1"), ("conv2", "conv2_kernel"),
+                                        ("conv3", "kern_s1")])
+def test_convolution(golden, tag, kernel):
+    got = O.convolve(golden[f"{tag}_field"].astype(np.float64), golden[kernel])
+    assert rel_l2(got, golden[f"{tag}_out"]) < 1e-6
+
+
+def test_convolution_direct_matches_fft():
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal((6, 5, 7))
+    k = rng.standard_normal((3, 3, 5))
+    out = np.zeros_like(f)
+    for x in range(6):
+        for y in range(5):
+            for z in range(7):
+                acc = 0.0
+                for i in range(3):
+                    for j in range(3):
+                        for l in range(5):
+                            zs = z - l + 2
+                            if 0 <= zs < 7:
+                                acc += k[i, j, l] * f[(x - i + 1) % 6, (y - j + 1) % 5, zs]
+                out[x, y, z] = acc
+    np.testing.assert_allclose(O.convolve(f, k), out, rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("tag,shape,sp,kern", [("fa1", (16, 12, 10), (1, 1, 1), "kern_s1"),
+                                               ("fa2", (16, 16, 12), (2, 2, 2), "kern_s2")])
+def test_advance_flux(golden, tag, shape, sp, kern):
+    flux = golden[f"{tag}_flux_in"].copy()
+    S, rec = O.advance_flux(flux, tuple(golden[f"{tag}_key"]), golden[kern], 0.1, 1, sp,
+                            n_zero=2, zero_bottom=True, zero_top=True)
+    led = golden[f"{tag}_ledger"]
+    assert rec['entering'][0] == pytest.approx(led[0], rel=1e-12)
+    assert rec['noise_abs'][1] == led[3]
+    assert rec['noise_abs'][0] == pytest.approx(led[2], rel=1e-6)
+    assert rec['n_clipped'] == led[6]
+    assert rel_l2(S, golden[f"{tag}_S"]) < 1e-6
+    assert rel_l2(flux, golden[f"{tag}_flux_out"]) < 1e-6
+
+
+def test_advective_weight_and_taper(golden):
+    for z in ("uni", "var"):
+        got = O.advective_weight(golden["aw_field"], 100.0, 80.0, golden[f"aw_z_{z}"],
+                                 golden["aw_aspect"])
+        np.testing.assert_allclose(got, golden[f"aw_{z}"], rtol=1e-6, atol=1e-9)
+    g = O.bound_taper(golden["aw_field"], golden["taper_b"], 295e3, 305e3)
+    np.testing.assert_allclose(g, golden["taper"], rtol=1e-6, atol=1e-7)
+
+
+def test_bounded_add(golden):
+    pert = golden["ba_pert_in"].copy()
+    inc = golden["ba_inc_in"].copy()
+    rec = O.bounded_amplitude_add(pert, golden["ba_mean"], inc, 0.0, 0.03,
+                                  record_applied=True)
+    np.testing.assert_allclose(pert, golden["ba_pert_out"], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(inc, golden["ba_inc_out"], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(rec['a0'], golden["ba_a0"], rtol=1e-12)
+
+
+def test_zoom(golden):
+    np.testing.assert_allclose(O.zoom_trilinear(golden["zoom_src"], (10, 8, 9)),
+                               golden["zoom_dyadic"], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(O.zoom_trilinear(golden["zoom_src"], (15, 6, 7)),
+                               golden["zoom_odd"], rtol=1e-6, atol=1e-6)
+
+
+def test_thermodynamics(golden):
+    out = O.recover_diagnostics(golden["th_h"], golden["th_qt"], golden["th_z"], 101325.0)
+    for k in ("T", "qv", "qc", "qi", "p"):
+        np.testing.assert_allclose(out[k], golden[f"th_{k}"], rtol=1e-6, atol=1e-9)
