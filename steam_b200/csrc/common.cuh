@@ -164,6 +164,30 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
+__device__ __forceinline__ float d_sinpi(float x) { return sinpif(x); }
+__device__ __forceinline__ double d_sinpi(double x) { return sinpi(x); }
+
+// float32 form of the same draw with exact angle reduction.  With
+// v = 1 - u0 (exact: u0 lies on the 2^-24 lattice) and alpha in (1, 2]:
+//   cos(phi) = sin(pi v),  cos(phi - sh) = sin(pi (alpha-1) v),
+//   sin(sh) = sin(pi alpha v),
+// because phi = pi (1/2 - v) and sh = alpha (phi - phi0) = pi (1 - alpha v).
+// The literal float32 evaluation loses most digits where the cosines near
+// their zeros feed the negative powers (0.4-1.7 % relative L2 over the draws
+// against float64); this form keeps every factor to a few float32 ulps.
+__device__ __forceinline__ float levy_draw_f32(float u0, float u1,
+                                               const LevyParams<float>& p) {
+  const float eps = 1e-6f;
+  const float v = 1.0f - u0;
+  const float R = -logf(u1 > eps ? u1 : eps);
+  const float c = sinpif(v);
+  const float fac = powf(__fmul_rn(c > eps ? c : eps, p.am1), p.fexp);
+  const float c2 = sinpif(__fmul_rn(p.am1, v));
+  const float tail = powf((c2 > eps ? c2 : eps) / R, p.texp);
+  return __fmul_rn(__fmul_rn(__fmul_rn(sinpif(__fmul_rn(p.alpha, v)), p.sign), fac),
+                   tail);
+}
+
 template <typename T>
 __device__ __forceinline__ T levy_draw(T u0, T u1, const LevyParams<T>& p) {
   const T eps = (T)1e-6;

@@ -18,19 +18,24 @@ constexpr int kMaxZ = 8;
 constexpr int kMaxPairs = 16;
 constexpr int kMaxX = 4;
 
+// Taps, mixing weights and every accumulator are float64 for both storage
+// dtypes: the turbulon kernel's terms cancel (it has zero sum), and float32
+// taps with float32 sums put ~1e-5 relative error into the log of a flux
+// advanced next to its clip.  Fields and intermediates stay in the storage
+// dtype.
 template <typename T>
 struct SepParams {
   int kz, ky, kx, cz, cy, cx;
   int nzf, nyf, nxf, npairs;
   int pair_z[kMaxPairs];
   int pair_y[kMaxPairs];
-  T mix[kMaxX * kMaxPairs];
-  T taps[kMaxTaps];  // z taps, then y taps, then x taps
-  __host__ __device__ const T* ztap(int f) const { return taps + f * kz; }
-  __host__ __device__ const T* ytap(int f) const {
+  double mix[kMaxX * kMaxPairs];
+  double taps[kMaxTaps];  // z taps, then y taps, then x taps
+  __host__ __device__ const double* ztap(int f) const { return taps + f * kz; }
+  __host__ __device__ const double* ytap(int f) const {
     return taps + nzf * kz + f * ky;
   }
-  __host__ __device__ const T* xtap(int f) const {
+  __host__ __device__ const double* xtap(int f) const {
     return taps + nzf * kz + nyf * ky + f * kx;
   }
 };
@@ -50,7 +55,7 @@ __global__ void __launch_bounds__(256) zpass_kernel(
     SepParams<T> p, T* __restrict__ out, int64_t plane) {
   extern __shared__ unsigned char smem_raw[];
   T* buf = reinterpret_cast<T*>(smem_raw);
-  __shared__ T taps_s[kMaxZ * 256];
+  __shared__ double taps_s[kMaxZ * 256];
   const int kz = p.kz;
   const int len = nz + kz - 1;
   const int padlo = kz - 1 - p.cz;
@@ -74,11 +79,11 @@ __global__ void __launch_bounds__(256) zpass_kernel(
     for (int i = threadIdx.x; i < ncb * nz; i += blockDim.x) {
       int c = i / nz, z = i - c * nz;
       const T* b = buf + c * len + z + kz - 1;
-      T acc[kMaxZ];
+      double acc[kMaxZ];
 #pragma unroll
-      for (int f = 0; f < kMaxZ; ++f) acc[f] = (T)0;
+      for (int f = 0; f < kMaxZ; ++f) acc[f] = 0.0;
       for (int l = 0; l < kz; ++l) {
-        T x = b[-l];
+        const double x = (double)b[-l];
 #pragma unroll
         for (int f = 0; f < kMaxZ; ++f)
           if (f < p.nzf) acc[f] += taps_s[f * kz + l] * x;
@@ -86,7 +91,7 @@ __global__ void __launch_bounds__(256) zpass_kernel(
       const int64_t o = (col0 + c) * nz + z;
 #pragma unroll
       for (int f = 0; f < kMaxZ; ++f)
-        if (f < p.nzf) out[f * plane + o] = acc[f];
+        if (f < p.nzf) out[f * plane + o] = (T)acc[f];
     }
   }
 }
@@ -133,10 +138,10 @@ __global__ void __launch_bounds__(256) ypass_kernel(
       if (y >= ny || zz >= tz) continue;
       for (int q = 0; q < p.npairs; ++q) {
         const T* col = buf + (p.pair_z[q] * rows + r + ky - 1) * kTZ + zz;
-        const T* tp = p.ytap(p.pair_y[q]);
-        T acc = (T)0;
-        for (int j = 0; j < ky; ++j) acc += tp[j] * col[-j * kTZ];
-        v[(int64_t)q * plane + (x * ny + y) * nz + z0 + zz] = acc;
+        const double* tp = p.ytap(p.pair_y[q]);
+        double acc = 0.0;
+        for (int j = 0; j < ky; ++j) acc += tp[j] * (double)col[-j * kTZ];
+        v[(int64_t)q * plane + (x * ny + y) * nz + z0 + zz] = (T)acc;
       }
     }
   }
@@ -157,7 +162,7 @@ __global__ void __launch_bounds__(256) xpass_kernel(
     T* __restrict__ out, int64_t plane, XEpi epi,
     double* __restrict__ partials) {
   extern __shared__ unsigned char smem_raw[];
-  T* buf = reinterpret_cast<T*>(smem_raw);  // [nxf][TX+kx-1][TE]
+  double* buf = reinterpret_cast<double*>(smem_raw);  // [nxf][TX+kx-1][TE]
   __shared__ double scratch[32];
   const int kx = p.kx;
   const int rows = kTX + kx - 1;
@@ -176,14 +181,14 @@ __global__ void __launch_bounds__(256) xpass_kernel(
     __syncthreads();
     for (int i = threadIdx.x; i < rows * kTE; i += blockDim.x) {
       int r = i / kTE, ee = i - r * kTE;
-      T w[kMaxX];
+      double w[kMaxX];
 #pragma unroll
-      for (int a = 0; a < kMaxX; ++a) w[a] = (T)0;
+      for (int a = 0; a < kMaxX; ++a) w[a] = 0.0;
       if (ee < te) {
         int64_t xs = wrapi(x0 - padlo + r, nx);
         const int64_t off = xs * pe + e0 + ee;
         for (int q = 0; q < p.npairs; ++q) {
-          T vq = v[(int64_t)q * plane + off];
+          const double vq = (double)v[(int64_t)q * plane + off];
 #pragma unroll
           for (int a = 0; a < kMaxX; ++a)
             if (a < p.nxf) w[a] += p.mix[a * p.npairs + q] * vq;
@@ -198,15 +203,16 @@ __global__ void __launch_bounds__(256) xpass_kernel(
       int r = i / kTE, ee = i - r * kTE;
       int64_t x = x0 + r;
       if (x >= nx || ee >= te) continue;
-      T acc = (T)0;
+      double acc = 0.0;
       for (int a = 0; a < p.nxf; ++a) {
-        const T* col = buf + (a * rows + r + kx - 1) * kTE + ee;
-        const T* tp = p.xtap(a);
+        const double* col = buf + (a * rows + r + kx - 1) * kTE + ee;
+        const double* tp = p.xtap(a);
         for (int j = 0; j < kx; ++j) acc += tp[j] * col[-j * kTE];
       }
       const int64_t o = x * pe + e0 + ee;
       if (epi.mode == STEAM_EPI_FLUX) {
-        T f = add_rn(out[o], acc);
+        // F + conv rounded once to the storage dtype
+        T f = (T)((double)out[o] + acc);
         if (f < (T)0) {
           s_clip += 1.0;
           f = (T)0;
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(256) xpass_kernel(
         if (x >= epi.wx0 && x < epi.wx1 && y >= epi.wy0 && y < epi.wy1)
           s_f += (double)f;
       } else {
-        out[o] = acc;
+        out[o] = (T)acc;
       }
     }
   }
@@ -297,12 +303,12 @@ static int fill_params(const steam_sepconv_t* s, const double* zt,
     }
   }
   for (int i = 0; i < kMaxX * kMaxPairs; ++i)
-    p.mix[i] = i < s->n_x * s->n_pairs ? (T)s->mix[i] : (T)0;
+    p.mix[i] = i < s->n_x * s->n_pairs ? s->mix[i] : 0.0;
   int o = 0;
-  for (int i = 0; i < s->n_z * s->kz; ++i) p.taps[o++] = (T)zt[i];
-  for (int i = 0; i < s->n_y * s->ky; ++i) p.taps[o++] = (T)yt[i];
-  for (int i = 0; i < s->n_x * s->kx; ++i) p.taps[o++] = (T)xt[i];
-  for (; o < kMaxTaps; ++o) p.taps[o] = (T)0;
+  for (int i = 0; i < s->n_z * s->kz; ++i) p.taps[o++] = zt[i];
+  for (int i = 0; i < s->n_y * s->ky; ++i) p.taps[o++] = yt[i];
+  for (int i = 0; i < s->n_x * s->kx; ++i) p.taps[o++] = xt[i];
+  for (; o < kMaxTaps; ++o) p.taps[o] = 0.0;
   return STEAM_OK;
 }
 
@@ -393,7 +399,7 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   }
   // x-pass with epilogue
   {
-    size_t sm = (size_t)p.nxf * (kTX + p.kx - 1) * kTE * sizeof(T);
+    size_t sm = (size_t)p.nxf * (kTX + p.kx - 1) * kTE * sizeof(double);
     STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: x filter too long");
     STEAM_CUDA(cudaFuncSetAttribute(xpass_kernel<T>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -420,36 +420,49 @@ static size_t level_partial_bytes(int64_t nz, int q) {
 }
 
 // Per-level bracketed Newton on a non-increasing piecewise-linear function
-// m(mu) (the level mean of a clipped, shifted field, minus a target).  The
-// bracket [a, b] always holds a sign change in the reference's bisection
-// sense: m(a) > 0 >= m(b).  Each sweep evaluates kMuCand candidates; the
-// result is the midpoint of the final bracket, as the bisection returns.
+// m(mu) (the level mean of a clipped, shifted field, minus a target),
+// evaluated at mu rounded to the working dtype T -- which is how the
+// reference's bisection evaluates it too.  The bracket [a, b] always holds the
+// sign change in the bisection's sense, m(a) > 0 >= m(b), with a and b values
+// of T.  Each sweep evaluates kMuCand candidates (the Newton point, two
+// points straddling it, the bracket midpoint); the solve ends when no value
+// of T lies strictly inside the bracket, and returns its midpoint, as the
+// bisection does.
+template <typename T>
 struct MuSolver {
   double a, b;
   double best_mu, best_m, best_slope;
   bool have_best = false;
   bool done = false;
-  double rel_tol, abs_tol;
 
-  // The bisection this replaces stops at 2*width/2^60; so does this.
+  double abs_tol = 0.0;
+
+  // abs_tol: a bracket this narrow is accepted as converged.  In float32 the
+  // level mean is a staircase in mu at the scale of the field's own ulps, so
+  // below that scale any mu of the bracket gives the same field up to
+  // single-ulp flips in a vanishing fraction of cells.
   void init(double width, double tol) {
-    a = -width;
-    b = width;
-    rel_tol = tol;
-    abs_tol = ldexp(2.0 * width, -60);
+    a = (double)(T)(-width);
+    b = (double)(T)width;
+    abs_tol = tol;
     have_best = false;
     done = false;
+  }
+
+  static double next_up(double x) {
+    return (double)nextafter((T)x, (T)INFINITY);
   }
 
   void candidates(double* out) const {
     const double mid = 0.5 * (a + b);
     double c0 = mid;
     if (have_best && best_slope < 0.0) {
-      double nt = best_mu - best_m / best_slope;  // Newton
+      const double nt = best_mu - best_m / best_slope;  // Newton
       if (nt > a && nt < b) c0 = nt;
     }
     const double span = b - a;
-    double eps = fabs(c0) * rel_tol * 4.0 + 1e-300;
+    double eps = fabs(c0) * (sizeof(T) == 4 ? 2.4e-7 : 4.5e-16) * 4.0;
+    if (eps < 0.5 * abs_tol) eps = 0.5 * abs_tol;
     if (eps > 0.25 * span) eps = 0.25 * span;
     out[0] = c0;
     out[1] = c0 - eps > a ? c0 - eps : 0.5 * (a + c0);
@@ -457,13 +470,14 @@ struct MuSolver {
     out[3] = mid;
   }
 
+  // cand: the T-rounded candidates actually evaluated.
   void update(const double* cand, const double* mval, const double* slope) {
     for (int k = 0; k < kMuCand; ++k) {
-      if (mval[k] > 0.0) {
-        if (cand[k] > a) a = cand[k];
-      } else {
-        if (cand[k] < b) b = cand[k];
-      }
+      if (cand[k] <= a || cand[k] >= b) continue;
+      if (mval[k] > 0.0)
+        a = cand[k];
+      else
+        b = cand[k];
     }
     int kb = -1;
     for (int k = 0; k < kMuCand; ++k)
@@ -474,8 +488,7 @@ struct MuSolver {
       best_m = mval[kb];
       best_slope = slope[kb];
     }
-    const double scale = fmax(fabs(a), fabs(b));
-    if (b - a <= scale * rel_tol || b - a <= abs_tol) done = true;
+    if (next_up(a) >= b || b - a <= abs_tol) done = true;
   }
   double result() const { return 0.5 * (a + b); }
 };
@@ -612,8 +625,7 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   if ((rc = stats_sweep())) return rc;
   // Zero-mean shift mu where the clip left a mean.
   const double width = phi_max - phi_min;
-  const double tol = sizeof(T) == 4 ? 1.0 / (1 << 26) : 1.0e-16;
-  std::vector<MuSolver> solver(nz);
+  std::vector<MuSolver<T>> solver(nz);
   std::vector<int> need(nz, 0);
   bool any_mu = false;
   for (int64_t z = 0; z < nz; ++z) {
@@ -621,7 +633,7 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
     if (fabs(tot[z] / N) > 1e-9 * a0[z]) {
       need[z] = 1;
       any_mu = true;
-      solver[z].init(width, tol);
+      solver[z].init(width, a0[z] * (sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49)));
     }
   }
   for (int it = 0; any_mu && it < 80; ++it) {
@@ -727,9 +739,9 @@ static int project_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   if (!any) return STEAM_OK;
   if ((rc = upload(d_active, active, s))) return rc;
   const double width = hi - lo;
-  std::vector<MuSolver> solver(nz);
+  std::vector<MuSolver<double>> solver(nz);
   for (int64_t z = 0; z < nz; ++z)
-    if (active[z]) solver[z].init(width, 1e-16);
+    if (active[z]) solver[z].init(width, 1e-12 * width);
   std::vector<double> cands((size_t)nz * kMuCand, 0.0);
   for (int it = 0; it < 80; ++it) {
     bool pending = false;

@@ -70,6 +70,21 @@ __device__ __forceinline__ T region_gamma(const RegionDev& r, int64_t x,
   return levy_draw<T>((T)lattice_uniform(r0), (T)lattice_uniform(r1), lp);
 }
 
+// float32: the exactly reduced form (see levy_draw_f32).
+template <>
+__device__ __forceinline__ float region_gamma<float>(const RegionDev& r, int64_t x,
+                                                     int64_t y, int64_t z,
+                                                     const LevyParams<float>& lp) {
+  int64_t gx = wrap_mod(x + r.ox, r.wx);
+  int64_t gy = wrap_mod(y + r.oy, r.wy);
+  int64_t gz = z + r.oz;
+  if (!divisible(gx, r.sx) || !divisible(gy, r.sy) || !divisible(gz, r.sz))
+    return 0.0f;
+  uint32_t r0, r1;
+  philox_site(gx, (uint32_t)gy, gz, r.k0, r.k1, r.k2, r0, r1);
+  return levy_draw_f32(lattice_uniform(r0), lattice_uniform(r1), lp);
+}
+
 __global__ void keyed_uniforms_kernel(const int64_t* __restrict__ ix,
                                       const int64_t* __restrict__ iy,
                                       const int64_t* __restrict__ iz,

@@ -696,8 +696,12 @@ def run_class(hp, qp, F, dh, dq, dF, cs, cl, increment_dir=None, index=0):
                                      cs.z, cs.aspect, b, lo, hi, cs.window)
         if cl.pattern.get(name) is None:
             cl.pattern[name] = PatternLedger(tot, cnt)
-        level_mean = cl.pattern[name].level_mean
-        div = np.where(level_mean > 0, level_mean, np.float32(1.0))
+        led = cl.pattern[name]
+        # the reference divides by the level mean rounded to float32; the
+        # float64 form keeps it in float64
+        np_t = np.float64 if pert.dtype == torch.float64 else np.float32
+        level_mean = (led.level_total / np.maximum(led.level_count, 1)).astype(np_t)
+        div = np.where(level_mean > 0, level_mean, np_t(1.0))
         inc = torch.empty_like(W)
         _utils.run_plan(cs.plan, W, inc, pre_div=div, pre_mul=np.asarray(C, dtype=np.float32))
         del W
@@ -762,9 +766,11 @@ def cascade_loop(h_profile, qt_profile, z_profile, grids, C_h_k, C_qt_k,
         increment_dir = Path(increment_dir)
         increment_dir.mkdir(parents=True, exist_ok=True)
     keys = [class_key(c) for c in class_seeds]
+    # The kernel's normalisation and its separable factors are float64 for
+    # both storage dtypes; float32 fields are convolved with float64 taps.
     kernel = _turbulon_envelope(1, 1 / (2 * s_x), 1 / (2 * s_y), 1 / (2 * s_z),
                                 support_factor=SUPPORT_FACTOR, shape=turbulon_shape,
-                                dtype=np_t)
+                                dtype=np.float64)
     c_noise = FLUX_SCALE if flux_noise_scale is None else flux_noise_scale
 
     def dev(a):
@@ -870,7 +876,7 @@ def simulate_flux_only(grids, sparsity_factors=(1, 1, 1), seed=None, flux_noise_
     n_zero = int(round(2 * s_z * min_distance_to_ground))
     kernel = _turbulon_envelope(1, 1 / (2 * s_x), 1 / (2 * s_y), 1 / (2 * s_z),
                                 support_factor=SUPPORT_FACTOR, shape=turbulon_shape,
-                                dtype=np_t)
+                                dtype=np.float64)
     F = None
     steps = []
     total_clipped = total_points = 0
@@ -1072,7 +1078,7 @@ def make_class_setup(grids, i, *, h_profile, qt_profile, z_profile, C_h, C_qt, b
     np_t = np.dtype(dtype).type
     kernel = _turbulon_envelope(1, 1 / (2 * s_x), 1 / (2 * s_y), 1 / (2 * s_z),
                                 support_factor=SUPPORT_FACTOR, shape=turbulon_shape,
-                                dtype=np_t)
+                                dtype=np.float64)
     deficit = None
     if comp is not None:
         d = np.asarray(comp, dtype=np.float32) - np.float32(1.0)
