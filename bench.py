@@ -350,9 +350,13 @@ def main(argv=None):
     value = world * nvox * args.steps / (ms / 1e3) / 1e6
 
     # one instrumented step: per-entry device time for the roofline
+    cl = ClassLedger()
     with CallTimer(lib, torch) as timer:
-        step()
+        sim.run_class(hp, qp, F, None, None, None, setup, cl)
+        recover_diagnostics_device(hp, qp, setup.z, 101325.0, out=diag,
+                                   h_mean=setup.h_mean, qt_mean=setup.qt_mean, bounds=bounds)
     calls = timer.totals()
+    ba_sweeps = {k: int(v.n_sweeps) for k, v in cl.bounded_add.items()}
     dominant = max(calls.items(), key=lambda kv: kv[1][0])
     elem = 4 if args.dtype == "f32" else 8
     # algorithmic bytes of one launch of each entry point at this shape
@@ -377,6 +381,7 @@ def main(argv=None):
                 "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                 "per_launch_ms": per_launch_ms,
                 "peak_source": "measured" if peaks else "fallback",
+                "bounded_add_sweeps": ba_sweeps,
                 "breakdown_ms": {k: round(v[0], 3) for k, v in sorted(
                     calls.items(), key=lambda kv: -kv[1][0])}}
 

@@ -124,6 +124,7 @@ __device__ __forceinline__ float lattice_uniform(uint32_t r) {
 template <typename T>
 struct LevyParams {
   T alpha, phi0, sign, am1, fexp, texp, pi;
+  double alpha_d, am1_d;  // alpha and alpha - 1 unrounded (float32 form)
 };
 
 template <typename T>
@@ -137,6 +138,8 @@ LevyParams<T> make_levy(double alpha) {
   p.fexp = (T)(-1.0 / alpha);
   p.texp = (T)((1.0 - alpha) / alpha);
   p.pi = (T)PI;
+  p.alpha_d = alpha;
+  p.am1_d = fabs(alpha - 1.0);
   return p;
 }
 
@@ -175,6 +178,16 @@ __device__ __forceinline__ double d_sinpi(double x) { return sinpi(x); }
 // The literal float32 evaluation loses most digits where the cosines near
 // their zeros feed the negative powers (0.4-1.7 % relative L2 over the draws
 // against float64); this form keeps every factor to a few float32 ulps.
+// sin(pi * a * v) with the product formed in float64 and reduced by its
+// nearest integer n exactly, so the float32 sine sees an exact small argument:
+// sin(pi a v) = (-1)^n sin(pi (a v - n)).
+__device__ __forceinline__ float sinpi_scaled(double a, float v) {
+  const double av = a * (double)v;
+  const double n = rint(av);
+  const float s = sinpif((float)(av - n));
+  return ((long long)n & 1) ? -s : s;
+}
+
 __device__ __forceinline__ float levy_draw_f32(float u0, float u1,
                                                const LevyParams<float>& p) {
   const float eps = 1e-6f;
@@ -182,10 +195,9 @@ __device__ __forceinline__ float levy_draw_f32(float u0, float u1,
   const float R = -logf(u1 > eps ? u1 : eps);
   const float c = sinpif(v);
   const float fac = powf(__fmul_rn(c > eps ? c : eps, p.am1), p.fexp);
-  const float c2 = sinpif(__fmul_rn(p.am1, v));
+  const float c2 = sinpi_scaled(p.am1_d, v);
   const float tail = powf((c2 > eps ? c2 : eps) / R, p.texp);
-  return __fmul_rn(__fmul_rn(__fmul_rn(sinpif(__fmul_rn(p.alpha, v)), p.sign), fac),
-                   tail);
+  return __fmul_rn(__fmul_rn(__fmul_rn(sinpi_scaled(p.alpha_d, v), p.sign), fac), tail);
 }
 
 template <typename T>

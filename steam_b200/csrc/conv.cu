@@ -236,6 +236,267 @@ __global__ void __launch_bounds__(256) xpass_kernel(
   }
 }
 
+// ---- fused pencil convolution ----------------------------------------------
+// One CTA owns a (kFY x kFZ) cross-section of y and z and marches along a
+// chunk of x.  For every input x-plane it stages the plane's (y, z) slab with
+// its halo in shared memory (in float64), runs the z filters (4 outputs per
+// thread, sliding window) and the y filters (2 rows per thread) on chip, and
+// folds the mixed result into a ring of K per-output-plane accumulators held
+// in registers (indices static through a uniform switch on the ring phase).
+// The next plane's slab is loaded into registers while the current plane is
+// computed (two slab buffers).  An output plane is final K-1 planes after its
+// first contribution and goes straight through the epilogue.  HBM sees the
+// input once (halo re-reads hit L2) and the output once.
+constexpr int kFY = 32;
+constexpr int kFZ = 16;
+constexpr int kFThreads = 256;
+constexpr int kFChunk = 256;  // x planes per CTA
+constexpr int kFMaxZ = 2, kFMaxPairs = 4, kFMaxX = 2;
+
+template <typename T>
+struct FusedGeom {
+  int64_t nx, ny;
+  int nz;
+  int nzt, nyt;   // z and y tiles
+  int64_t chunk;  // x planes per CTA
+  int use_pre;
+};
+
+template <int K>
+struct FusedShape {
+  static constexpr int R = kFY + K - 1;          // staged rows
+  static constexpr int C = kFZ + K - 1;          // staged columns
+  static constexpr int NL = (R * C + kFThreads - 1) / kFThreads;  // loads/thread
+  static constexpr int ZT = R * (kFZ / 4);       // z-filter tasks (4 outputs each)
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kernel(
+    const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
+    SepParams<T> p, FusedGeom<T> g, XEpi epi, double* __restrict__ partials) {
+  using S = FusedShape<K>;
+  constexpr int R = S::R, C = S::C, NL = S::NL;
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double scratch[32];
+  __shared__ double s_zt[kFMaxZ][K], s_yt[2][K], s_xt[kFMaxX][K];
+  __shared__ double s_mix[kFMaxX * kFMaxPairs];
+  __shared__ T s_pre[2][C];
+  double* s_in0 = reinterpret_cast<double*>(smem_raw);  // [2][R*C]
+  double* s_u = s_in0 + 2 * R * C;                       // [2][R][kFZ]
+  const int t = threadIdx.x;
+  const int nzf = p.nzf, nxf = p.nxf, npairs = p.npairs;
+  for (int i = t; i < K; i += kFThreads) {
+    s_zt[0][i] = p.taps[i];
+    s_zt[1][i] = nzf > 1 ? p.taps[K + i] : 0.0;
+    s_yt[0][i] = p.ytap(0)[i];
+    s_yt[1][i] = p.nyf > 1 ? p.ytap(1)[i] : 0.0;
+    s_xt[0][i] = p.xtap(0)[i];
+    s_xt[1][i] = nxf > 1 ? p.xtap(1)[i] : 0.0;
+  }
+  if (t < kFMaxX * kFMaxPairs) {
+    // mix re-indexed by (a, c, b): pairs are enumerated c-major, b-minor
+    const int a = t / kFMaxPairs, cb = t % kFMaxPairs;
+    const int c = cb / 2, b = cb % 2;
+    double v = 0.0;
+    for (int q = 0; q < npairs; ++q)
+      if (a < nxf && p.pair_z[q] == c && p.pair_y[q] == b) v += p.mix[a * npairs + q];
+    s_mix[t] = v;
+  }
+  const int zt_i = blockIdx.x % g.nzt;
+  const int yt_i = (blockIdx.x / g.nzt) % g.nyt;
+  const int64_t xc = blockIdx.x / ((int64_t)g.nzt * g.nyt);
+  const int64_t y0 = (int64_t)yt_i * kFY;
+  const int z0 = zt_i * kFZ;
+  const int64_t xb = xc * g.chunk;
+  const int64_t xe = (xb + g.chunk) < g.nx ? (xb + g.chunk) : g.nx;
+  const int64_t count = (xe - xb) + K - 1;  // planes to process
+  const int64_t xin0 = xb - (K - 1 - p.cx);
+  const int padz = K - 1 - p.cz, pady = K - 1 - p.cy;
+  for (int c = t; c < C; c += kFThreads) {
+    const int z = z0 - padz + c;
+    const bool in_z = z >= 0 && z < g.nz;
+    s_pre[0][c] = (in_z && g.use_pre) ? pre[z] : (T)1;
+    s_pre[1][c] = (in_z && g.use_pre) ? pre[g.nz + z] : (T)1;
+  }
+  // this thread's staged elements e = t + i*kFThreads: their offset within
+  // an input plane (-1 for zero padding) and their staged column
+  int goff[NL];
+  unsigned char gcol[NL];
+#pragma unroll
+  for (int i = 0; i < NL; ++i) {
+    const int e = t + i * kFThreads;
+    const int r = e / C, c = e - r * C;
+    const int z = z0 - padz + c;
+    const bool v = e < R * C && z >= 0 && z < g.nz;
+    goff[i] = v ? (int)(wrapi(y0 - pady + r, g.ny) * g.nz + z) : -1;
+    gcol[i] = (unsigned char)(e < R * C ? c : 0);
+  }
+  const int64_t plane_elems = g.ny * (int64_t)g.nz;
+  T ld[NL];
+  auto issue_loads = [&](int64_t k) {
+    const T* base = in + wrapi(xin0 + k, g.nx) * plane_elems;
+#pragma unroll
+    for (int i = 0; i < NL; ++i) ld[i] = goff[i] >= 0 ? base[goff[i]] : (T)0;
+  };
+  auto commit_loads = [&](double* dst) {
+#pragma unroll
+    for (int i = 0; i < NL; ++i) {
+      const int e = t + i * kFThreads;
+      if (e < R * C) {
+        const int c = gcol[i];
+        T v = ld[i];
+        if (g.use_pre) v = mul_rn(v / s_pre[0][c], s_pre[1][c]);
+        dst[e] = (double)v;
+      }
+    }
+  };
+  // output points of this thread: rows 2*yp, 2*yp+1 at column zq
+  const int zq = t % kFZ, yp = t / kFZ;
+  int64_t oy[2];
+  bool ok[2];
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    oy[m] = y0 + 2 * yp + m;
+    ok[m] = oy[m] < g.ny && z0 + zq < g.nz;
+  }
+  double acc[K][2];
+#pragma unroll
+  for (int sl = 0; sl < K; ++sl) acc[sl][0] = acc[sl][1] = 0.0;
+  double s_f = 0.0, s_clip = 0.0;
+  __syncthreads();
+  issue_loads(0);
+  commit_loads(s_in0);
+  __syncthreads();
+  for (int64_t k = 0; k < count; ++k) {
+    double* s_in = s_in0 + (k & 1) * R * C;
+    if (k + 1 < count) issue_loads(k + 1);
+    // ---- z filters, 4 outputs per task: u_c[r][z4 .. z4+3]
+    for (int task = t; task < S::ZT; task += kFThreads) {
+      const int r = task / (kFZ / 4), z4 = (task % (kFZ / 4)) * 4;
+      const double* b = s_in + r * C + z4;
+      double win[K + 3];
+#pragma unroll
+      for (int i = 0; i < K + 3; ++i) win[i] = b[i];
+      double a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int l = 0; l < K; ++l) {
+        const double t0 = s_zt[0][l], t1 = s_zt[1][l];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+          // out[z] uses staged column z + K - 1 - l
+          a0[o] += t0 * win[o + K - 1 - l];
+          a1[o] += t1 * win[o + K - 1 - l];
+        }
+      }
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        s_u[(r)*kFZ + z4 + o] = a0[o];
+        s_u[R * kFZ + r * kFZ + z4 + o] = a1[o];
+      }
+    }
+    __syncthreads();
+    // ---- y filters for rows 2yp, 2yp+1 at column zq, then the mixing
+    double w0[2] = {0, 0}, w1[2] = {0, 0};
+#pragma unroll
+    for (int c = 0; c < kFMaxZ; ++c) {
+      double col[K + 1];
+      const double* src = s_u + c * R * kFZ + (2 * yp) * kFZ + zq;
+#pragma unroll
+      for (int i = 0; i < K + 1; ++i) col[i] = src[i * kFZ];
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+          const double tj = s_yt[b][j];
+          v0 += tj * col[K - 1 - j];
+          v1 += tj * col[K - j];
+        }
+        const double m0 = s_mix[0 * kFMaxPairs + c * 2 + b];
+        const double m1 = s_mix[1 * kFMaxPairs + c * 2 + b];
+        w0[0] += m0 * v0;
+        w0[1] += m0 * v1;
+        w1[0] += m1 * v0;
+        w1[1] += m1 * v1;
+      }
+    }
+    // ---- fold into the ring: plane k feeds output j = k + i - (K-1) in slot
+    //      j mod K; output k - (K-1) is then complete and leaves the ring
+    const int rph = (int)(k % K);
+    const int64_t j = k - (K - 1);
+#pragma unroll
+    for (int rr = 0; rr < K; ++rr) {
+      if (rr == rph) {
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const int slot = (rr + i + 1) % K;
+          const double c0 = s_xt[0][i], c1 = s_xt[1][i];
+          acc[slot][0] += c0 * w0[0] + c1 * w1[0];
+          acc[slot][1] += c0 * w0[1] + c1 * w1[1];
+        }
+        const int es = (rr + 1) % K;
+        if (j >= 0) {
+          const int64_t x = xb + j;
+#pragma unroll
+          for (int m = 0; m < 2; ++m) {
+            if (ok[m]) {
+              const int64_t o = (x * g.ny + oy[m]) * g.nz + z0 + zq;
+              if (epi.mode == STEAM_EPI_FLUX) {
+                T f = (T)((double)out[o] + acc[es][m]);
+                if (f < (T)0) {
+                  s_clip += 1.0;
+                  f = (T)0;
+                }
+                out[o] = f;
+                if (x >= epi.wx0 && x < epi.wx1 && oy[m] >= epi.wy0 && oy[m] < epi.wy1)
+                  s_f += (double)f;
+              } else {
+                out[o] = (T)acc[es][m];
+              }
+            }
+          }
+        }
+        // a slot leaving the ring is cleared whether or not its output lies
+        // in this chunk (planes before the chunk only feed the halo)
+        acc[es][0] = 0.0;
+        acc[es][1] = 0.0;
+      }
+    }
+    if (k + 1 < count) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
+    __syncthreads();
+  }
+  if (epi.mode == STEAM_EPI_FLUX) {
+    double t0 = block_sum(s_f, scratch);
+    double t1 = block_sum(s_clip, scratch);
+    if (threadIdx.x == 0) {
+      partials[blockIdx.x] = t0;
+      partials[gridDim.x + blockIdx.x] = t1;
+    }
+  }
+}
+
+template <typename T>
+static bool fused_supported(const SepParams<T>& p) {
+  const bool cube = p.kx == p.ky && p.ky == p.kz && (p.kx == 13 || p.kx == 25);
+  if (!cube || p.nzf > kFMaxZ || p.nyf > 2 || p.nxf > kFMaxX || p.npairs > kFMaxPairs)
+    return false;
+  for (int q = 0; q < p.npairs; ++q)
+    if (p.pair_z[q] >= 2 || p.pair_y[q] >= 2) return false;
+  return true;
+}
+
+static size_t fused_smem(int k, size_t elem) {
+  (void)elem;
+  const int R = kFY + k - 1, C = kFZ + k - 1;
+  return sizeof(double) * ((size_t)2 * R * C + (size_t)kFMaxZ * R * kFZ);
+}
+
+static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz) {
+  const int64_t nzt = (nz + kFZ - 1) / kFZ, nyt = (ny + kFY - 1) / kFY;
+  const int64_t nxc = (nx + kFChunk - 1) / kFChunk;
+  return nzt * nyt * nxc;
+}
+
 // ---- dense direct convolution ----------------------------------------------
 template <typename T>
 __global__ void dense_conv_kernel(const T* __restrict__ in, int64_t nx,
@@ -326,6 +587,70 @@ static int64_t epi_cells(const steam_window_t* w, int64_t nx, int64_t ny) {
 }
 
 template <typename T>
+static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
+                     const void* in_v, const double* pre_div,
+                     const double* pre_mul, void* out_v, int epilogue,
+                     const steam_window_t* win, double* sums_out, void* ws,
+                     size_t ws_bytes, cudaStream_t s) {
+  const int64_t grid = fused_grid(nx, ny, nz);
+  Carver c(ws, ws_bytes);
+  const bool use_pre = pre_div != nullptr || pre_mul != nullptr;
+  T* pre = c.take<T>((size_t)2 * nz);
+  double* partials = c.take<double>((size_t)grid * 2);
+  double* totals = c.take<double>(2);
+  if (!pre || !partials || !totals)
+    return fail(STEAM_ERR_WORKSPACE, "steam_conv_separable: workspace too small");
+  if (use_pre) {
+    std::vector<T> h(2 * nz);
+    for (int64_t z = 0; z < nz; ++z) {
+      h[z] = pre_div ? (T)pre_div[z] : (T)1;
+      h[nz + z] = pre_mul ? (T)pre_mul[z] : (T)1;
+    }
+    STEAM_CUDA(cudaMemcpyAsync(pre, h.data(), sizeof(T) * 2 * nz,
+                               cudaMemcpyHostToDevice, s));
+  }
+  FusedGeom<T> g;
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = (int)nz;
+  g.nzt = (int)((nz + kFZ - 1) / kFZ);
+  g.nyt = (int)((ny + kFY - 1) / kFY);
+  g.chunk = kFChunk;
+  g.use_pre = use_pre ? 1 : 0;
+  XEpi epi;
+  epi.mode = epilogue;
+  epi.wx0 = win ? win->x0 : 0;
+  epi.wx1 = win ? win->x1 : nx;
+  epi.wy0 = win ? win->y0 : 0;
+  epi.wy1 = win ? win->y1 : ny;
+  const size_t sm = fused_smem(p.kx, sizeof(T));
+  STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: filters too long for the fused path");
+  if (p.kx == 13) {
+    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, 13>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    fused_conv_kernel<T, 13><<<(unsigned)grid, kFThreads, sm, s>>>(
+        (const T*)in_v, (T*)out_v, pre, p, g, epi, partials);
+  } else {
+    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, 25>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    fused_conv_kernel<T, 25><<<(unsigned)grid, kFThreads, sm, s>>>(
+        (const T*)in_v, (T*)out_v, pre, p, g, epi, partials);
+  }
+  STEAM_LAUNCH_CHECK("conv fused");
+  if (epilogue == STEAM_EPI_FLUX) {
+    int rc = reduce_partials(partials, (int)grid, 2, totals, s);
+    if (rc) return rc;
+    double h[2];
+    STEAM_CUDA(cudaMemcpyAsync(h, totals, sizeof(h), cudaMemcpyDeviceToHost, s));
+    STEAM_CUDA(cudaStreamSynchronize(s));
+    sums_out[0] = h[0];
+    sums_out[1] = (double)(epi_cells(win, nx, ny) * nz);
+    sums_out[2] = h[1];
+  }
+  return STEAM_OK;
+}
+
+template <typename T>
 static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                          const steam_sepconv_t* spec, const double* zt,
                          const double* yt, const double* xt, const void* in_v,
@@ -339,6 +664,10 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   if (rc) return rc;
   SepParams<T>& p = *pp;
   const int64_t plane = nx * ny * nz;
+  if (fused_supported(p) && fused_grid(nx, ny, nz) < ((int64_t)1 << 31) &&
+      ny * nz < ((int64_t)1 << 31))
+    return run_fused<T>(nx, ny, nz, p, in_v, pre_div, pre_mul, out_v, epilogue,
+                        win, sums_out, ws, ws_bytes, s);
   Carver c(ws, ws_bytes);
   T* u = c.take<T>((size_t)p.nzf * plane);
   T* v = c.take<T>((size_t)p.npairs * plane);
@@ -438,11 +767,22 @@ extern "C" size_t steam_conv_workspace_bytes(int dtype, int64_t nx, int64_t ny,
   size_t elem = dtype == STEAM_F64 ? 8 : 4;
   size_t plane = (size_t)(nx * ny * nz);
   int xgrid = stride_grid(((nx + kTX - 1) / kTX) * ((ny * nz + kTE - 1) / kTE), 1, 4);
-  return carve_bytes((size_t)spec->n_z * plane, elem) +
-         carve_bytes((size_t)spec->n_pairs * plane, elem) +
-         carve_bytes((size_t)2 * nz, elem) +
-         carve_bytes((size_t)xgrid * 2, sizeof(double)) +
-         carve_bytes(2, sizeof(double));
+  const size_t multi = carve_bytes((size_t)spec->n_z * plane, elem) +
+                      carve_bytes((size_t)spec->n_pairs * plane, elem) +
+                      carve_bytes((size_t)2 * nz, elem) +
+                      carve_bytes((size_t)xgrid * 2, sizeof(double)) +
+                      carve_bytes(2, sizeof(double));
+  bool fused = spec->kx == spec->ky && spec->ky == spec->kz &&
+               (spec->kx == 13 || spec->kx == 25) && spec->n_z <= kFMaxZ &&
+               spec->n_y <= 2 && spec->n_x <= kFMaxX && spec->n_pairs <= kFMaxPairs &&
+               fused_grid(nx, ny, nz) < ((int64_t)1 << 31) && ny * nz < ((int64_t)1 << 31);
+  for (int q = 0; fused && q < spec->n_pairs; ++q)
+    if (spec->pair_z[q] >= 2 || spec->pair_y[q] >= 2) fused = false;
+  if (fused)
+    return carve_bytes((size_t)2 * nz, elem) +
+           carve_bytes((size_t)fused_grid(nx, ny, nz) * 2, sizeof(double)) +
+           carve_bytes(2, sizeof(double));
+  return multi;
 }
 
 extern "C" int steam_conv_separable(

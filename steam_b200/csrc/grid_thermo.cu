@@ -146,7 +146,7 @@ __global__ void kernel_build_kernel(int hx, int hy, int hz, T dx, T dy, T dz,
 // A warp owns 32 consecutive columns (contiguous in memory).  Levels are staged
 // 32 at a time through shared memory so that loads and stores are coalesced;
 // each lane then marches its own column with a float64 pressure accumulator.
-constexpr int kThZ = 16;
+constexpr int kThZ = 8;
 constexpr int kThWarps = 4;
 constexpr int kThPitch = kThZ + 1;
 
@@ -214,15 +214,18 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
           T Tn = Td;
 #pragma unroll 1
           for (int it = 0; it < 5; ++it) {
-            const T e = bolton(Tn, k);
-            const T pe = sub_rn(pl, e);
-            const T q = mul_rn(k.c622, e) / pe;
+            // f(T) = cp T + Lv qvs(T, p) + g z - h and its derivative, with the
+            // two reciprocals 1/(T - 29.65) and 1/(p - es) shared between the
+            // Bolton exponent, qvs, des/dT and dqvs/dT
+            const T i1 = (T)1 / sub_rn(Tn, k.ec);
+            const T e = mul_rn(k.es0, d_exp(mul_rn(mul_rn(k.ea, sub_rn(Tn, k.eb)), i1)));
+            const T i2 = (T)1 / sub_rn(pl, e);
+            const T q = mul_rn(mul_rn(k.c622, e), i2);
             const T f = sub_rn(add_rn(add_rn(mul_rn(k.cp, Tn), mul_rn(k.lv, q)),
                                       mul_rn(k.g, zt)),
                                hl);
-            const T tm = sub_rn(Tn, k.ec);
-            const T de = mul_rn(k.dq, e) / mul_rn(tm, tm);
-            const T dq = mul_rn(mul_rn(k.c622, pl) / mul_rn(pe, pe), de);
+            const T de = mul_rn(mul_rn(k.dq, e), mul_rn(i1, i1));
+            const T dq = mul_rn(mul_rn(mul_rn(k.c622, pl), mul_rn(i2, i2)), de);
             Tn = sub_rn(Tn, f / add_rn(k.cp, mul_rn(k.lv, dq)));
           }
           Tl = Tn;

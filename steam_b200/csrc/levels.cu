@@ -16,7 +16,8 @@ namespace steam {
 
 constexpr int kLvThreads = 256;
 constexpr int kLvMaxJ = 4;  // nz <= 1024
-constexpr int kLvBlocksPerSm = 4;
+constexpr int kLvBlocksPerSm = 8;
+constexpr int kLvUnroll = 4;  // columns per thread per iteration (loads in flight)
 
 struct LevelMap {
   int nz;
@@ -93,9 +94,11 @@ __device__ void store_level_partials(const LevelMap& m, double (&acc)[Q][kLvMaxJ
   } else {
 #pragma unroll
     for (int q = 0; q < Q; ++q)
-      for (int j = 0; j < m.J; ++j) {
-        int z = t + j * kLvThreads;
-        if (z < m.nz) partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][j];
+#pragma unroll
+      for (int j = 0; j < kLvMaxJ; ++j) {
+        const int z = t + j * kLvThreads;
+        if (j < m.J && z < m.nz)
+          partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][j];
       }
   }
 }
@@ -109,14 +112,23 @@ __device__ __forceinline__ void for_levels(const LevelMap& m, int64_t ncol, F fn
     const int z = t % m.nz;
     const int64_t cofs = t / m.nz;
     const int64_t step = (int64_t)gridDim.x * m.G;
-    for (int64_t col = (int64_t)blockIdx.x * m.G + cofs; col < ncol; col += step)
-      fn(col, z, 0);
+    int64_t col = (int64_t)blockIdx.x * m.G + cofs;
+    // kLvUnroll independent columns per iteration so their loads overlap
+    for (; col + (kLvUnroll - 1) * step < ncol; col += kLvUnroll * step) {
+#pragma unroll
+      for (int u = 0; u < kLvUnroll; ++u) fn(col + u * step, z, 0);
+    }
+    for (; col < ncol; col += step) fn(col, z, 0);
   } else {
-    for (int64_t col = blockIdx.x; col < ncol; col += gridDim.x)
-      for (int j = 0; j < m.J; ++j) {
-        int z = t + j * kLvThreads;
-        if (z < m.nz) fn(col, z, j);
+    // j is a compile-time index after unrolling, so per-level accumulators
+    // indexed by it stay in registers
+    for (int64_t col = blockIdx.x; col < ncol; col += gridDim.x) {
+#pragma unroll
+      for (int j = 0; j < kLvMaxJ; ++j) {
+        const int z = t + j * kLvThreads;
+        if (j < m.J && z < m.nz) fn(col, z, j);
       }
+    }
   }
 }
 
@@ -355,6 +367,7 @@ __global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
     const int t = threadIdx.x;
     const int nb = gridDim.x;
     if (m.packed) {
+#pragma unroll
       for (int q = 0; q < 3; ++q) {
         __syncthreads();
         if (t < m.G * m.nz) red[t] = acc[q][0];
@@ -369,10 +382,12 @@ __global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
         }
       }
     } else {
+#pragma unroll
       for (int q = 0; q < 3; ++q)
-        for (int jj = 0; jj < m.J; ++jj) {
-          int z = t + jj * kLvThreads;
-          if (z < m.nz)
+#pragma unroll
+        for (int jj = 0; jj < kLvMaxJ; ++jj) {
+          const int z = t + jj * kLvThreads;
+          if (jj < m.J && z < m.nz)
             partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][jj];
         }
     }
@@ -508,26 +523,53 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   Carver c(ws, ws_bytes);
   double* partials = c.take<double>((size_t)grid * Qmax * nz);
   double* totals = c.take<double>((size_t)Qmax * nz);
-  T* d_mean = c.take<T>(nz);
-  int* d_nsteps = c.take<int>(nz);
-  T* d_demean = c.take<T>((size_t)nz * R);
-  T* d_scale = c.take<T>((size_t)nz * R);
-  int* d_hasfinal = c.take<int>(nz);
-  T* d_final = c.take<T>(nz);
-  int* d_hasmu = c.take<int>(nz);
-  T* d_mu = c.take<T>(nz);
-  T* d_cand = c.take<T>((size_t)nz * kMuCand);
-  if (!partials || !totals || !d_mean || !d_nsteps || !d_demean || !d_scale ||
-      !d_hasfinal || !d_final || !d_hasmu || !d_mu || !d_cand)
+  // All per-level chain parameters live in one block, mirrored on the host
+  // and pushed with a single copy per sweep.
+  const size_t n_int = (size_t)3 * nz;
+  const size_t n_t = (size_t)nz * (2 * (size_t)R + 3 + kMuCand);
+  const size_t blk_bytes = ((n_int * sizeof(int) + sizeof(T) - 1) / sizeof(T)) * sizeof(T) +
+                           n_t * sizeof(T);
+  unsigned char* d_blk = c.take<unsigned char>(blk_bytes);
+  if (!partials || !totals || !d_blk)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
-
-  std::vector<T> h_mean(nz), h_demean((size_t)nz * R, (T)0),
-      h_scale((size_t)nz * R, (T)1), h_final(nz, (T)0), h_mu(nz, (T)0),
-      h_cand((size_t)nz * kMuCand, (T)0);
-  std::vector<int> h_nsteps(nz, 0), h_hasfinal(nz, 0), h_hasmu(nz, 0);
-  for (int64_t z = 0; z < nz; ++z) h_mean[z] = (T)mean_1d[z];
+  std::vector<unsigned char> h_blk(blk_bytes, 0);
+  int* h_nsteps_p = reinterpret_cast<int*>(h_blk.data());
+  int* h_hasfinal_p = h_nsteps_p + nz;
+  int* h_hasmu_p = h_hasfinal_p + nz;
+  T* h_t = reinterpret_cast<T*>(h_blk.data() + (blk_bytes - n_t * sizeof(T)));
+  T* h_demean_p = h_t;
+  T* h_scale_p = h_demean_p + (size_t)nz * R;
+  T* h_final_p = h_scale_p + (size_t)nz * R;
+  T* h_mu_p = h_final_p + nz;
+  T* h_mean_p = h_mu_p + nz;
+  T* h_cand_p = h_mean_p + nz;
+  auto dev = [&](const void* hp) {
+    return d_blk + (reinterpret_cast<const unsigned char*>(hp) - h_blk.data());
+  };
+  int* d_nsteps = reinterpret_cast<int*>(dev(h_nsteps_p));
+  int* d_hasfinal = reinterpret_cast<int*>(dev(h_hasfinal_p));
+  int* d_hasmu = reinterpret_cast<int*>(dev(h_hasmu_p));
+  T* d_demean = reinterpret_cast<T*>(dev(h_demean_p));
+  T* d_scale = reinterpret_cast<T*>(dev(h_scale_p));
+  T* d_final = reinterpret_cast<T*>(dev(h_final_p));
+  T* d_mu = reinterpret_cast<T*>(dev(h_mu_p));
+  T* d_mean = reinterpret_cast<T*>(dev(h_mean_p));
+  T* d_cand = reinterpret_cast<T*>(dev(h_cand_p));
+  for (int64_t z = 0; z < nz; ++z) h_mean_p[z] = (T)mean_1d[z];
+  for (size_t i = 0; i < (size_t)nz * R; ++i) h_scale_p[i] = (T)1;
+  // host views with the indexing the solve below uses
+  struct View {
+    T* p;
+    T& operator[](size_t i) { return p[i]; }
+  };
+  struct IView {
+    int* p;
+    int& operator[](size_t i) { return p[i]; }
+  };
+  View h_demean{h_demean_p}, h_scale{h_scale_p}, h_final{h_final_p}, h_mu{h_mu_p},
+      h_cand{h_cand_p};
+  IView h_nsteps{h_nsteps_p}, h_hasfinal{h_hasfinal_p}, h_hasmu{h_hasmu_p};
   int rc;
-  if ((rc = upload(d_mean, h_mean, s))) return rc;
 
   BAChain<T> ch;
   ch.nsteps = d_nsteps;
@@ -546,15 +588,7 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   std::vector<double> tot;
   int n_sweeps = 0;
   auto push_chain = [&]() -> int {
-    int r2;
-    if ((r2 = upload(d_nsteps, h_nsteps, s))) return r2;
-    if ((r2 = upload(d_demean, h_demean, s))) return r2;
-    if ((r2 = upload(d_scale, h_scale, s))) return r2;
-    if ((r2 = upload(d_hasfinal, h_hasfinal, s))) return r2;
-    if ((r2 = upload(d_final, h_final, s))) return r2;
-    if ((r2 = upload(d_hasmu, h_hasmu, s))) return r2;
-    if ((r2 = upload(d_mu, h_mu, s))) return r2;
-    if ((r2 = upload(d_cand, h_cand, s))) return r2;
+    STEAM_CUDA(cudaMemcpyAsync(d_blk, h_blk.data(), blk_bytes, cudaMemcpyHostToDevice, s));
     return STEAM_OK;
   };
   auto stats_sweep = [&]() -> int {
