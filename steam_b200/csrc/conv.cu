@@ -321,7 +321,6 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
   // this thread's staged elements e = t + i*kFThreads: their offset within
   // an input plane (-1 for zero padding) and their staged column
   int goff[NL];
-  unsigned char gcol[NL];
 #pragma unroll
   for (int i = 0; i < NL; ++i) {
     const int e = t + i * kFThreads;
@@ -329,7 +328,6 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
     const int z = z0 - padz + c;
     const bool v = e < R * C && z >= 0 && z < g.nz;
     goff[i] = v ? (int)(wrapi(y0 - pady + r, g.ny) * g.nz + z) : -1;
-    gcol[i] = (unsigned char)(e < R * C ? c : 0);
   }
   const int64_t plane_elems = g.ny * (int64_t)g.nz;
   T ld[NL];
@@ -343,7 +341,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
     for (int i = 0; i < NL; ++i) {
       const int e = t + i * kFThreads;
       if (e < R * C) {
-        const int c = gcol[i];
+        const int c = e % C;  // C is a compile-time constant
         T v = ld[i];
         if (g.use_pre) v = mul_rn(v / s_pre[0][c], s_pre[1][c]);
         dst[e] = (double)v;
@@ -352,13 +350,11 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
   };
   // output points of this thread: rows 2*yp, 2*yp+1 at column zq
   const int zq = t % kFZ, yp = t / kFZ;
-  int64_t oy[2];
-  bool ok[2];
-#pragma unroll
-  for (int m = 0; m < 2; ++m) {
-    oy[m] = y0 + 2 * yp + m;
-    ok[m] = oy[m] < g.ny && z0 + zq < g.nz;
-  }
+  const int64_t oy0 = y0 + 2 * yp;
+  const bool okz = z0 + zq < g.nz;
+  // output rows oy0, oy0 + 1 (each valid when inside the array)
+#define OY(m) (oy0 + (m))
+#define OK(m) (okz && OY(m) < g.ny)
   double acc[K][2];
 #pragma unroll
   for (int sl = 0; sl < K; ++sl) acc[sl][0] = acc[sl][1] = 0.0;
@@ -367,9 +363,19 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
   issue_loads(0);
   commit_loads(s_in0);
   __syncthreads();
+  const bool flux_epi = epi.mode == STEAM_EPI_FLUX;
   for (int64_t k = 0; k < count; ++k) {
     double* s_in = s_in0 + (k & 1) * R * C;
     if (k + 1 < count) issue_loads(k + 1);
+    // the flux under the output plane this iteration completes, loaded now so
+    // that the load overlaps the plane's filters
+    T fprev[2] = {(T)0, (T)0};
+    if (flux_epi && k >= K - 1) {
+      const int64_t x = xb + (k - (K - 1));
+#pragma unroll
+      for (int m = 0; m < 2; ++m)
+        if (OK(m)) fprev[m] = out[(x * g.ny + OY(m)) * g.nz + z0 + zq];
+    }
     // ---- z filters, 4 outputs per task: u_c[r][z4 .. z4+3]
     for (int task = t; task < S::ZT; task += kFThreads) {
       const int r = task / (kFZ / 4), z4 = (task % (kFZ / 4)) * 4;
@@ -439,16 +445,16 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
           const int64_t x = xb + j;
 #pragma unroll
           for (int m = 0; m < 2; ++m) {
-            if (ok[m]) {
-              const int64_t o = (x * g.ny + oy[m]) * g.nz + z0 + zq;
-              if (epi.mode == STEAM_EPI_FLUX) {
-                T f = (T)((double)out[o] + acc[es][m]);
+            if (OK(m)) {
+              const int64_t o = (x * g.ny + OY(m)) * g.nz + z0 + zq;
+              if (flux_epi) {
+                T f = (T)((double)fprev[m] + acc[es][m]);
                 if (f < (T)0) {
                   s_clip += 1.0;
                   f = (T)0;
                 }
                 out[o] = f;
-                if (x >= epi.wx0 && x < epi.wx1 && oy[m] >= epi.wy0 && oy[m] < epi.wy1)
+                if (x >= epi.wx0 && x < epi.wx1 && OY(m) >= epi.wy0 && OY(m) < epi.wy1)
                   s_f += (double)f;
               } else {
                 out[o] = (T)acc[es][m];
@@ -465,6 +471,8 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
     if (k + 1 < count) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
     __syncthreads();
   }
+#undef OY
+#undef OK
   if (epi.mode == STEAM_EPI_FLUX) {
     double t0 = block_sum(s_f, scratch);
     double t1 = block_sum(s_clip, scratch);

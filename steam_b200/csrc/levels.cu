@@ -48,8 +48,9 @@ static int level_grid(int64_t ncol, const LevelMap& m) {
 
 struct Win {
   int64_t x0, x1, y0, y1;
+  int full;  // the window is the whole array: no test needed
   __device__ __forceinline__ bool in(int64_t x, int64_t y) const {
-    return x >= x0 && x < x1 && y >= y0 && y < y1;
+    return full || (x >= x0 && x < x1 && y >= y0 && y < y1);
   }
 };
 
@@ -59,6 +60,7 @@ static Win make_win(const steam_window_t* w, int64_t nx, int64_t ny) {
   r.x1 = w ? w->x1 : nx;
   r.y0 = w ? w->y0 : 0;
   r.y1 = w ? w->y1 : ny;
+  r.full = r.x0 == 0 && r.x1 == nx && r.y0 == 0 && r.y1 == ny;
   return r;
 }
 
@@ -73,8 +75,8 @@ static int check_win(const steam_window_t* w, int64_t nx, int64_t ny,
 
 // Reduce acc[Q][J] of every thread to per-level block partials:
 // partials[(q * nz + z) * nblocks + blockIdx.x].
-template <int Q>
-__device__ void store_level_partials(const LevelMap& m, double (&acc)[Q][kLvMaxJ],
+template <int Q, int JM>
+__device__ void store_level_partials(const LevelMap& m, double (&acc)[Q][JM],
                                      double* red, double* partials) {
   const int t = threadIdx.x;
   const int nb = gridDim.x;
@@ -95,7 +97,7 @@ __device__ void store_level_partials(const LevelMap& m, double (&acc)[Q][kLvMaxJ
 #pragma unroll
     for (int q = 0; q < Q; ++q)
 #pragma unroll
-      for (int j = 0; j < kLvMaxJ; ++j) {
+      for (int j = 0; j < JM; ++j) {
         const int z = t + j * kLvThreads;
         if (j < m.J && z < m.nz)
           partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][j];
@@ -103,56 +105,86 @@ __device__ void store_level_partials(const LevelMap& m, double (&acc)[Q][kLvMaxJ
   }
 }
 
-// Iterate (column, level) pairs of this thread.  fn(col, z, j).
-template <typename F>
-__device__ __forceinline__ void for_levels(const LevelMap& m, int64_t ncol, F fn) {
+// Iterate (column, level) pairs of this thread: fn(col, x, y, z, j).  The
+// column's x and y advance incrementally (no division per element).
+struct ColWalk {
+  int64_t col, x, y;
+  int64_t sx, sy, ny;
+  __device__ __forceinline__ void init(int64_t c, int64_t step, int64_t ny_) {
+    ny = ny_;
+    col = c;
+    x = c / ny;
+    y = c - x * ny;
+    sx = step / ny;
+    sy = step - sx * ny;
+  }
+  __device__ __forceinline__ void advance(int64_t step) {
+    col += step;
+    x += sx;
+    y += sy;
+    if (y >= ny) {
+      y -= ny;
+      x += 1;
+    }
+  }
+};
+
+template <int JM, typename F>
+__device__ __forceinline__ void for_levels(const LevelMap& m, int64_t ncol, int64_t ny, F fn) {
   const int t = threadIdx.x;
   if (m.packed) {
     if (t >= m.G * m.nz) return;
     const int z = t % m.nz;
     const int64_t cofs = t / m.nz;
     const int64_t step = (int64_t)gridDim.x * m.G;
-    int64_t col = (int64_t)blockIdx.x * m.G + cofs;
+    ColWalk w;
+    w.init((int64_t)blockIdx.x * m.G + cofs, step, ny);
     // kLvUnroll independent columns per iteration so their loads overlap
-    for (; col + (kLvUnroll - 1) * step < ncol; col += kLvUnroll * step) {
+    while (w.col + (kLvUnroll - 1) * step < ncol) {
+      ColWalk u = w;
 #pragma unroll
-      for (int u = 0; u < kLvUnroll; ++u) fn(col + u * step, z, 0);
+      for (int k = 0; k < kLvUnroll; ++k) {
+        fn(u.col, u.x, u.y, z, 0);
+        u.advance(step);
+      }
+      w = u;
     }
-    for (; col < ncol; col += step) fn(col, z, 0);
+    for (; w.col < ncol; w.advance(step)) fn(w.col, w.x, w.y, z, 0);
   } else {
     // j is a compile-time index after unrolling, so per-level accumulators
     // indexed by it stay in registers
-    for (int64_t col = blockIdx.x; col < ncol; col += gridDim.x) {
+    ColWalk w;
+    w.init(blockIdx.x, gridDim.x, ny);
+    for (; w.col < ncol; w.advance(gridDim.x)) {
 #pragma unroll
-      for (int j = 0; j < kLvMaxJ; ++j) {
+      for (int j = 0; j < JM; ++j) {
         const int z = t + j * kLvThreads;
-        if (j < m.J && z < m.nz) fn(col, z, j);
+        if (j < m.J && z < m.nz) fn(w.col, w.x, w.y, z, j);
       }
     }
   }
 }
 
 // ---- level sums ---------------------------------------------------------------
-template <typename T>
+template <typename T, int JM>
 __global__ void __launch_bounds__(kLvThreads) level_sums_kernel(
     const T* __restrict__ f, int64_t nx, int64_t ny, LevelMap m, Win w,
     double* __restrict__ partials) {
   __shared__ double red[kLvThreads];
-  double acc[3][kLvMaxJ];
+  double acc[3][JM];
 #pragma unroll
   for (int q = 0; q < 3; ++q)
 #pragma unroll
-    for (int j = 0; j < kLvMaxJ; ++j) acc[q][j] = 0.0;
+    for (int j = 0; j < JM; ++j) acc[q][j] = 0.0;
   const int64_t ncol = nx * ny;
-  for_levels(m, ncol, [&](int64_t col, int z, int j) {
-    const int64_t x = col / ny, y = col - x * ny;
+  for_levels<JM>(m, ncol, ny, [&](int64_t col, int64_t x, int64_t y, int z, int j) {
     if (!w.in(x, y)) return;
     T v = f[col * m.nz + z];
     acc[0][j] += (double)v;
     acc[1][j] += (double)(v < (T)0 ? -v : v);
     acc[2][j] += v != (T)0 ? 1.0 : 0.0;
   });
-  store_level_partials<3>(m, acc, red, partials);
+  store_level_partials<3, JM>(m, acc, red, partials);
 }
 
 // ---- scalar pattern -------------------------------------------------------------
@@ -164,7 +196,7 @@ struct PatternArgs {
   int has_taper;  // 0: no bound taper
 };
 
-template <typename T>
+template <typename T, int JM>
 __global__ void __launch_bounds__(kLvThreads) pattern_kernel(
     const T* __restrict__ pert, const T* __restrict__ mean,
     const T* __restrict__ prod, const T* __restrict__ za,
@@ -173,15 +205,14 @@ __global__ void __launch_bounds__(kLvThreads) pattern_kernel(
     int64_t ny, LevelMap m, Win w, PatternArgs<T> a, T* __restrict__ out,
     double* __restrict__ partials) {
   __shared__ double red[kLvThreads];
-  double acc[2][kLvMaxJ];
+  double acc[2][JM];
 #pragma unroll
   for (int q = 0; q < 2; ++q)
 #pragma unroll
-    for (int j = 0; j < kLvMaxJ; ++j) acc[q][j] = 0.0;
+    for (int j = 0; j < JM; ++j) acc[q][j] = 0.0;
   const int nz = m.nz;
   const int64_t ncol = nx * ny;
-  for_levels(m, ncol, [&](int64_t col, int z, int j) {
-    const int64_t x = col / ny, y = col - x * ny;
+  for_levels<JM>(m, ncol, ny, [&](int64_t col, int64_t x, int64_t y, int z, int j) {
     const int64_t xp = x + 1 < nx ? x + 1 : 0, xm = x > 0 ? x - 1 : nx - 1;
     const int64_t yp = y + 1 < ny ? y + 1 : 0, ym = y > 0 ? y - 1 : ny - 1;
     const T mz = mean[z];
@@ -232,7 +263,7 @@ __global__ void __launch_bounds__(kLvThreads) pattern_kernel(
       acc[1][j] += W != (T)0 ? 1.0 : 0.0;
     }
   });
-  store_level_partials<2>(m, acc, red, partials);
+  store_level_partials<2, JM>(m, acc, red, partials);
 }
 
 // ---- bounded add sweeps --------------------------------------------------------
@@ -265,40 +296,71 @@ __device__ __forceinline__ T clampv(T v, T a, T b) {
   return v < b ? v : b;
 }
 
-template <typename T, int MODE>
+template <typename T>
+static size_t ba_smem_bytes(int64_t nz, int R) {
+  return sizeof(T) * (size_t)nz * (2 * (size_t)R + 4 + kMuCand) + sizeof(int) * 3 * (size_t)nz;
+}
+
+template <typename T, int MODE, int JM>
 __global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
     const T* __restrict__ d0, T* __restrict__ pert, T* __restrict__ inc_out,
     int record, int64_t nx, int64_t ny, LevelMap m, Win w, BAChain<T> c,
     double* __restrict__ partials) {
   __shared__ double red[kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  const int nz = m.nz, R = c.R;
+  // the chain, level-fastest: s_dm[s * nz + z]
+  T* s_dm = reinterpret_cast<T*>(ba_smem);
+  T* s_sc = s_dm + (size_t)R * nz;
+  T* s_fin = s_sc + (size_t)R * nz;
+  T* s_mu = s_fin + nz;
+  T* s_mean = s_mu + nz;
+  T* s_cand = s_mean + nz;  // [kMuCand][nz]
+  int* s_ns = reinterpret_cast<int*>(s_cand + (size_t)kMuCand * nz);
+  int* s_hf = s_ns + nz;
+  int* s_hm = s_hf + nz;
+  for (int i = threadIdx.x; i < R * nz; i += blockDim.x) {
+    const int z = i % nz, st = i / nz;
+    s_dm[i] = c.demean[z * R + st];
+    s_sc[i] = c.scale[z * R + st];
+  }
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    s_fin[z] = c.final_dm[z];
+    s_mu[z] = c.mu[z];
+    s_mean[z] = c.mean[z];
+    s_ns[z] = c.nsteps[z];
+    s_hf[z] = c.has_final[z];
+    s_hm[z] = c.has_mu[z];
+#pragma unroll
+    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = c.cand[z * kMuCand + k];
+  }
+  __syncthreads();
   constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
-  double acc[Q][kLvMaxJ];
+  double acc[Q][JM];
 #pragma unroll
   for (int q = 0; q < Q; ++q)
 #pragma unroll
-    for (int j = 0; j < kLvMaxJ; ++j) acc[q][j] = 0.0;
-  const int nz = m.nz;
+    for (int j = 0; j < JM; ++j) acc[q][j] = 0.0;
   const int64_t ncol = nx * ny;
-  for_levels(m, ncol, [&](int64_t col, int z, int j) {
+  for_levels<JM>(m, ncol, ny, [&](int64_t col, int64_t x, int64_t y, int z, int j) {
     const int64_t i = col * nz + z;
     const T p0 = pert[i];
-    const T phi = add_rn(p0, c.mean[z]);
-    const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
     T d = d0[i];
-    const int ns = c.nsteps[z];
-    for (int s = 0; s < ns; ++s) {
-      d = clampv(sub_rn(d, c.demean[z * c.R + s]), clo, chi);
-      d = mul_rn(d, c.scale[z * c.R + s]);
+    const T phi = add_rn(p0, s_mean[z]);
+    const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
+    const int ns = s_ns[z];
+    for (int st = 0; st < ns; ++st) {
+      d = clampv(sub_rn(d, s_dm[st * nz + z]), clo, chi);
+      d = mul_rn(d, s_sc[st * nz + z]);
     }
-    if (c.has_final[z]) d = clampv(sub_rn(d, c.final_dm[z]), clo, chi);
+    if (s_hf[z]) d = clampv(sub_rn(d, s_fin[z]), clo, chi);
     if (MODE == BA_APPLY) {
-      if (c.has_mu[z]) d = clampv(sub_rn(d, c.mu[z]), clo, chi);
+      if (s_hm[z]) d = clampv(sub_rn(d, s_mu[z]), clo, chi);
       const T pn = add_rn(p0, d);
       pert[i] = pn;
       if (record) inc_out[i] = sub_rn(pn, p0);
       return;
     }
-    const int64_t x = col / ny, y = col - x * ny;
     if (!w.in(x, y)) return;
     if (MODE == BA_STATS) {
       acc[0][j] += (double)d;
@@ -306,20 +368,20 @@ __global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
     } else {
 #pragma unroll
       for (int k = 0; k < kMuCand; ++k) {
-        const T raw = sub_rn(d, c.cand[z * kMuCand + k]);
-        const T t = clampv(raw, clo, chi);
-        acc[2 * k][j] += (double)t;
+        const T raw = sub_rn(d, s_cand[k * nz + z]);
+        const T tv = clampv(raw, clo, chi);
+        acc[2 * k][j] += (double)tv;
         acc[(2 * k + 1) % Q][j] += (raw > clo && raw < chi) ? 1.0 : 0.0;
       }
     }
   });
-  if (MODE != BA_APPLY) store_level_partials<Q>(m, acc, red, partials);
+  if (MODE != BA_APPLY) store_level_partials<Q, JM>(m, acc, red, partials);
 }
 
 // ---- projection sweeps (float64 level arithmetic) -----------------------------
 enum { PJ_STATS = 0, PJ_MU = 1, PJ_APPLY = 2 };
 
-template <typename T, int MODE>
+template <typename T, int MODE, int JM>
 __global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
     T* __restrict__ pert, const double* __restrict__ mean, double lo,
     double hi, const int* __restrict__ active, const double* __restrict__ mu,
@@ -327,23 +389,22 @@ __global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
     Win w, double* __restrict__ partials) {
   __shared__ double red[kLvThreads];
   constexpr int Q = MODE == PJ_MU ? 2 * kMuCand : 3;
-  double acc[Q][kLvMaxJ];
+  double acc[Q][JM];
 #pragma unroll
   for (int q = 0; q < Q; ++q)
 #pragma unroll
-    for (int j = 0; j < kLvMaxJ; ++j)
+    for (int j = 0; j < JM; ++j)
       acc[q][j] = (MODE == PJ_STATS && q == 1) ? INFINITY
                   : (MODE == PJ_STATS && q == 2) ? -INFINITY
                                                   : 0.0;
   const int nz = m.nz;
   const int64_t ncol = nx * ny;
-  for_levels(m, ncol, [&](int64_t col, int z, int j) {
+  for_levels<JM>(m, ncol, ny, [&](int64_t col, int64_t x, int64_t y, int z, int j) {
     const int64_t i = col * nz + z;
     const double f = (double)pert[i] + mean[z];
     if (MODE == PJ_STATS) {
       acc[1][j] = fmin(acc[1][j], f);
       acc[2 % Q][j] = fmax(acc[2 % Q][j], f);
-      const int64_t x = col / ny, y = col - x * ny;
       if (w.in(x, y)) acc[0][j] += f;
       return;
     }
@@ -352,7 +413,6 @@ __global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
       pert[i] = (T)(fmin(fmax(f - mu[z], lo), hi) - mean[z]);
       return;
     }
-    const int64_t x = col / ny, y = col - x * ny;
     if (!w.in(x, y)) return;
 #pragma unroll
     for (int k = 0; k < kMuCand; ++k) {
@@ -385,14 +445,14 @@ __global__ void __launch_bounds__(kLvThreads) proj_sweep_kernel(
 #pragma unroll
       for (int q = 0; q < 3; ++q)
 #pragma unroll
-        for (int jj = 0; jj < kLvMaxJ; ++jj) {
+        for (int jj = 0; jj < JM; ++jj) {
           const int z = t + jj * kLvThreads;
           if (jj < m.J && z < m.nz)
             partials[((size_t)q * m.nz + z) * nb + blockIdx.x] = acc[q][jj];
         }
     }
   } else {
-    store_level_partials<Q>(m, acc, red, partials);
+    store_level_partials<Q, JM>(m, acc, red, partials);
   }
 }
 
@@ -571,6 +631,20 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   IView h_nsteps{h_nsteps_p}, h_hasfinal{h_hasfinal_p}, h_hasmu{h_hasmu_p};
   int rc;
 
+  const size_t ba_sm = ba_smem_bytes<T>(nz, R);
+  STEAM_REQUIRE(ba_sm <= 200 * 1024, "steam_bounded_add: n_rescale * nz too large");
+  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_MU, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, kLvMaxJ>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_MU, kLvMaxJ>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, kLvMaxJ>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
   BAChain<T> ch;
   ch.nsteps = d_nsteps;
   ch.demean = d_demean;
@@ -594,7 +668,11 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   auto stats_sweep = [&]() -> int {
     int r2 = push_chain();
     if (r2) return r2;
-    ba_sweep_kernel<T, BA_STATS><<<grid, kLvThreads, 0, s>>>(
+        if (m.packed)
+      ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
+        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
+    else
+      ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
         inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
     STEAM_LAUNCH_CHECK("bounded_add stats sweep");
     if ((r2 = reduce_partials(partials, grid, 2 * (int)nz, totals, s))) return r2;
@@ -682,7 +760,11 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
     }
     if (!pending) break;
     if ((rc = push_chain())) return rc;
-    ba_sweep_kernel<T, BA_MU><<<grid, kLvThreads, 0, s>>>(
+        if (m.packed)
+      ba_sweep_kernel<T, BA_MU, 1><<<grid, kLvThreads, ba_sm, s>>>(
+        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
+    else
+      ba_sweep_kernel<T, BA_MU, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
         inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
     STEAM_LAUNCH_CHECK("bounded_add mu sweep");
     if ((rc = reduce_partials(partials, grid, Qmax * (int)nz, totals, s))) return rc;
@@ -708,7 +790,11 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
     }
   // Apply.
   if ((rc = push_chain())) return rc;
-  ba_sweep_kernel<T, BA_APPLY><<<grid, kLvThreads, 0, s>>>(
+    if (m.packed)
+    ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
+      inc, pert, inc, record, nx, ny, m, w, ch, partials);
+  else
+    ba_sweep_kernel<T, BA_APPLY, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
       inc, pert, inc, record, nx, ny, m, w, ch, partials);
   STEAM_LAUNCH_CHECK("bounded_add apply sweep");
   ++n_sweeps;
@@ -748,7 +834,11 @@ static int project_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   std::vector<double> h_mean(mean_1d, mean_1d + nz);
   int rc;
   if ((rc = upload(d_mean, h_mean, s))) return rc;
-  proj_sweep_kernel<T, PJ_STATS><<<grid, kLvThreads, 0, s>>>(
+    if (m.packed)
+    proj_sweep_kernel<T, PJ_STATS, 1><<<grid, kLvThreads, 0, s>>>(
+      pert, d_mean, lo, hi, nullptr, nullptr, nullptr, nx, ny, m, w, partials);
+  else
+    proj_sweep_kernel<T, PJ_STATS, kLvMaxJ><<<grid, kLvThreads, 0, s>>>(
       pert, d_mean, lo, hi, nullptr, nullptr, nullptr, nx, ny, m, w, partials);
   STEAM_LAUNCH_CHECK("project stats sweep");
   {
@@ -786,7 +876,11 @@ static int project_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
     }
     if (!pending) break;
     if ((rc = upload(d_cand, cands, s))) return rc;
-    proj_sweep_kernel<T, PJ_MU><<<grid, kLvThreads, 0, s>>>(
+        if (m.packed)
+      proj_sweep_kernel<T, PJ_MU, 1><<<grid, kLvThreads, 0, s>>>(
+        pert, d_mean, lo, hi, d_active, nullptr, d_cand, nx, ny, m, w, partials);
+    else
+      proj_sweep_kernel<T, PJ_MU, kLvMaxJ><<<grid, kLvThreads, 0, s>>>(
         pert, d_mean, lo, hi, d_active, nullptr, d_cand, nx, ny, m, w, partials);
     STEAM_LAUNCH_CHECK("project mu sweep");
     if ((rc = reduce_partials(partials, grid, Qmax * (int)nz, totals, s))) return rc;
@@ -806,7 +900,11 @@ static int project_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   std::vector<double> h_mu(nz, 0.0);
   for (int64_t z = 0; z < nz; ++z) h_mu[z] = active[z] ? mu[z] : 0.0;
   if ((rc = upload(d_mu, h_mu, s))) return rc;
-  proj_sweep_kernel<T, PJ_APPLY><<<grid, kLvThreads, 0, s>>>(
+    if (m.packed)
+    proj_sweep_kernel<T, PJ_APPLY, 1><<<grid, kLvThreads, 0, s>>>(
+      pert, d_mean, lo, hi, d_active, d_mu, nullptr, nx, ny, m, w, partials);
+  else
+    proj_sweep_kernel<T, PJ_APPLY, kLvMaxJ><<<grid, kLvThreads, 0, s>>>(
       pert, d_mean, lo, hi, d_active, d_mu, nullptr, nx, ny, m, w, partials);
   STEAM_LAUNCH_CHECK("project apply sweep");
   STEAM_CUDA(cudaStreamSynchronize(s));
@@ -853,10 +951,18 @@ extern "C" int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
     return fail(STEAM_ERR_WORKSPACE, "steam_level_sums: workspace too small");
   cudaStream_t s = (cudaStream_t)stream;
   if (dtype == STEAM_F32)
-    level_sums_kernel<float><<<grid, kLvThreads, 0, s>>>((const float*)field, nx,
+        if (m.packed)
+      level_sums_kernel<float, 1><<<grid, kLvThreads, 0, s>>>((const float*)field, nx,
+                                                         ny, m, w, partials);
+    else
+      level_sums_kernel<float, kLvMaxJ><<<grid, kLvThreads, 0, s>>>((const float*)field, nx,
                                                          ny, m, w, partials);
   else if (dtype == STEAM_F64)
-    level_sums_kernel<double><<<grid, kLvThreads, 0, s>>>(
+        if (m.packed)
+      level_sums_kernel<double, 1><<<grid, kLvThreads, 0, s>>>(
+        (const double*)field, nx, ny, m, w, partials);
+    else
+      level_sums_kernel<double, kLvMaxJ><<<grid, kLvThreads, 0, s>>>(
         (const double*)field, nx, ny, m, w, partials);
   else
     return fail(STEAM_ERR_ARG, "steam_level_sums: bad dtype");
@@ -932,7 +1038,12 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
   a.uniform_z = uniform ? 1 : 0;
   a.has_prod = prod != nullptr;
   a.has_taper = bbuf != nullptr;
-  pattern_kernel<T><<<grid, kLvThreads, 0, s>>>(
+    if (m.packed)
+    pattern_kernel<T, 1><<<grid, kLvThreads, 0, s>>>(
+      pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
+      d_vec + 4 * nz, d_vec + 5 * nz, nx, ny, m, w, a, out, partials);
+  else
+    pattern_kernel<T, kLvMaxJ><<<grid, kLvThreads, 0, s>>>(
       pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
       d_vec + 4 * nz, d_vec + 5 * nz, nx, ny, m, w, a, out, partials);
   STEAM_LAUNCH_CHECK("steam_scalar_pattern");

@@ -5,6 +5,7 @@
 namespace steam {
 
 __device__ __forceinline__ int64_t wrap_mod(int64_t v, int64_t n) {
+  if (v >= 0 && v < n) return v;  // the common case: no division
   int64_t r = v % n;
   return r < 0 ? r + n : r;
 }
@@ -127,33 +128,44 @@ struct NoiseArgs {
 
 // eps = expm1(gamma*scale - shift) at centres (0 elsewhere), product =
 // eps * flux; block partials of {sum flux, sum |eps|, nnz eps} over window.
+// Threads walk the z levels of a column (coalesced), blocks walk columns, so
+// the column's x and y come from one 32-bit division per column.
 template <typename T>
 __global__ void __launch_bounds__(256) flux_noise_kernel(
     RegionDev r, LevyParams<T> lp, NoiseArgs a, const T* __restrict__ flux,
     T* __restrict__ product, double* __restrict__ partials) {
   __shared__ double scratch[32];
   const T scale = (T)a.scale, shift = (T)a.shift;
-  const int64_t n = r.nx * r.ny * r.nz;
+  const uint32_t ncol = (uint32_t)(r.nx * r.ny);
+  const uint32_t ny = (uint32_t)r.ny;
+  const int nz = (int)r.nz;
+  const int zlanes = nz < (int)blockDim.x ? nz : (int)blockDim.x;
+  const int cols_per_iter = (int)blockDim.x / zlanes;
+  const int cofs = threadIdx.x / zlanes;
+  const int zt = threadIdx.x - cofs * zlanes;
   double s_flux = 0.0, s_abs = 0.0, s_nnz = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t z = i % r.nz;
-    int64_t col = i / r.nz;
-    int64_t y = col % r.ny;
-    int64_t x = col / r.ny;
-    T gamma = region_gamma<T>(r, x, y, z, lp);
-    if (a.n_zero > 0) {
-      if (a.zero_bottom && z < a.n_zero) gamma = (T)0;
-      if (a.zero_top && z >= r.nz - a.n_zero) gamma = (T)0;
-    }
-    T g = mul_rn(gamma, scale);
-    T e = (g == (T)0) ? (T)0 : d_expm1(sub_rn(g, shift));
-    T f = flux[i];
-    product[i] = mul_rn(e, f);
-    if (x >= a.wx0 && x < a.wx1 && y >= a.wy0 && y < a.wy1) {
-      s_flux += (double)f;
-      s_abs += (double)(e < (T)0 ? -e : e);
-      s_nnz += (e != (T)0) ? 1.0 : 0.0;
+  if (cofs < cols_per_iter) {
+    for (uint32_t col = blockIdx.x * cols_per_iter + cofs; col < ncol;
+         col += gridDim.x * cols_per_iter) {
+      const uint32_t x = col / ny, y = col - x * ny;
+      const bool in_win = x >= a.wx0 && x < a.wx1 && y >= a.wy0 && y < a.wy1;
+      const int64_t base = (int64_t)col * nz;
+      for (int z = zt; z < nz; z += zlanes) {
+        T gamma = region_gamma<T>(r, x, y, z, lp);
+        if (a.n_zero > 0) {
+          if (a.zero_bottom && z < a.n_zero) gamma = (T)0;
+          if (a.zero_top && z >= nz - a.n_zero) gamma = (T)0;
+        }
+        T g = mul_rn(gamma, scale);
+        T e = (g == (T)0) ? (T)0 : d_expm1(sub_rn(g, shift));
+        T f = flux[base + z];
+        product[base + z] = mul_rn(e, f);
+        if (in_win) {
+          s_flux += (double)f;
+          s_abs += (double)(e < (T)0 ? -e : e);
+          s_nnz += (e != (T)0) ? 1.0 : 0.0;
+        }
+      }
     }
   }
   double t0 = block_sum(s_flux, scratch);
@@ -267,7 +279,11 @@ extern "C" int steam_flux_noise(int dtype, const steam_region_t* region,
     return STEAM_OK;
   }
   STEAM_REQUIRE(flux && product, "steam_flux_noise: null field pointer");
-  int grid = stride_grid(n, 256, kNoiseBlocksPerSm);
+  STEAM_REQUIRE(r.nx * r.ny < ((int64_t)1 << 32),
+                "steam_flux_noise: more than 2^32 columns");
+  const int64_t cols_per_block = r.nz < 256 ? 256 / r.nz : 1;
+  int grid = stride_grid((r.nx * r.ny + cols_per_block - 1) / cols_per_block, 1,
+                         kNoiseBlocksPerSm);
   Carver c(workspace, workspace_bytes);
   double* partials = c.take<double>((size_t)grid * 3);
   double* totals = c.take<double>(4);

@@ -705,8 +705,10 @@ def run_class(hp, qp, F, dh, dq, dF, cs, cl, increment_dir=None, index=0):
         inc = torch.empty_like(W)
         _utils.run_plan(cs.plan, W, inc, pre_div=div, pre_mul=np.asarray(C, dtype=np.float32))
         del W
+        # the applied increment is only needed for a deficit or a record
+        record = (dfield is not None and cs.deficit is not None) or increment_dir is not None
         cl.bounded_add[name] = bounded_add_device(pert, mean_1d, inc, lo, hi, cs.window,
-                                                  record_applied=True)
+                                                  record_applied=record)
         if dfield is not None and cs.deficit is not None:
             _accumulate(dfield, inc, None, cs.deficit)
         if increment_dir is not None:
