@@ -174,7 +174,7 @@ int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
  * heights (np.gradient semantics), aspect and buffer_b are HOST per-level.
  * product == NULL leaves out the amplitude and buffer_b == NULL the taper,
  * which gives the advective weight alone (steam/simulate.py:2843-2868). */
-size_t steam_scalar_pattern_workspace_bytes(int64_t nz);
+size_t steam_scalar_pattern_workspace_bytes(int64_t nx, int64_t ny, int64_t nz);
 int steam_scalar_pattern(int dtype, int64_t nx, int64_t ny, int64_t nz,
                          const void* pert, const double* mean_1d,
                          const void* product, double s_scale, double dx,

@@ -266,6 +266,171 @@ __global__ void __launch_bounds__(kLvThreads) pattern_kernel(
   store_level_partials<2, JM>(m, acc, red, partials);
 }
 
+template <typename T>
+struct V4 {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ V4<T> ld4(const T* p) {
+  V4<T> r;
+  if (sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    r.v[0] = (T)q.x; r.v[1] = (T)q.y; r.v[2] = (T)q.z; r.v[3] = (T)q.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    r.v[0] = (T)a.x; r.v[1] = (T)a.y; r.v[2] = (T)b.x; r.v[3] = (T)b.y;
+  }
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void st4(T* p, const V4<T>& r) {
+  if (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)r.v[0], (float)r.v[1],
+                                                (float)r.v[2], (float)r.v[3]);
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2((double)r.v[0], (double)r.v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2((double)r.v[2], (double)r.v[3]);
+  }
+}
+
+// ---- scalar pattern, marching in x ----------------------------------------------
+// A block owns TY = 1024 / nz rows of y and every z (nz % 4 == 0, nz <= 1024),
+// and marches x over a chunk.  The running field r = pert + mean of planes
+// x-1, x, x+1 -- each with one halo row on either side in y -- sits in a
+// three-plane ring in shared memory, so every input plane is read from HBM
+// once (16-byte loads); a thread computes 4 consecutive levels of one row.
+constexpr int kPatChunk = 256;
+
+template <typename T>
+__device__ __forceinline__ T pattern_cell(T r, T rxm, T rxp, T rym, T ryp, T rzm, T rzp,
+                                          int z, int nz, T prod, T az, T bz, T cz,
+                                          T asp, T bb, const PatternArgs<T>& a) {
+  const T gx = sub_rn(rxp, rxm) / a.two_dx;
+  const T gy = sub_rn(ryp, rym) / a.two_dy;
+  const T gh = d_sqrt(add_rn(mul_rn(gx, gx), mul_rn(gy, gy)));
+  T gz;
+  if (z == 0) {
+    gz = sub_rn(rzp, r) / a.dz_first;
+  } else if (z == nz - 1) {
+    gz = sub_rn(r, rzm) / a.dz_last;
+  } else if (a.uniform_z) {
+    gz = sub_rn(rzp, rzm) / a.two_dz;
+  } else {
+    gz = add_rn(add_rn(mul_rn(az, rzm), mul_rn(bz, r)), mul_rn(cz, rzp));
+  }
+  gz = gz < (T)0 ? -gz : gz;
+  T W = add_rn(mul_rn(gz, asp), gh);
+  if (a.has_prod) W = mul_rn(W, mul_rn(prod, a.s_scale));
+  if (a.has_taper) {
+    T g = sub_rn(r, a.lo);
+    const T g2 = sub_rn(a.span, g);
+    g = g2 < g ? g2 : g;
+    g = g / (bb > (T)0 ? bb : (T)1e-30);
+    g = g < (T)0 ? (T)0 : (g > (T)1 ? (T)1 : g);
+    W = mul_rn(W, g);
+  }
+  return W;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kLvThreads) pattern_march_kernel(
+    const T* __restrict__ pert, const T* __restrict__ vecs, const T* __restrict__ prod,
+    int64_t nx, int64_t ny, int nz, Win w, PatternArgs<T> a, T* __restrict__ out,
+    double* __restrict__ partials) {
+  extern __shared__ unsigned char pm_smem[];
+  const int nz4 = nz / 4;
+  const int TY = kLvThreads / nz4;
+  const int RW = TY + 2;  // staged rows per plane
+  T* ring = reinterpret_cast<T*>(pm_smem);  // [3][RW][nz]
+  T* s_vec = ring + (size_t)3 * RW * nz;      // [6][nz]: mean, a, b, c, aspect, buffer
+  __shared__ double red[4 * kLvThreads];
+  for (int i = threadIdx.x; i < 6 * nz; i += blockDim.x) s_vec[i] = vecs[i];
+  const int64_t nyt = (ny + TY - 1) / TY;
+  const int64_t yt = blockIdx.x % nyt;
+  const int64_t xc = blockIdx.x / nyt;
+  const int64_t y0 = yt * TY;
+  const int64_t xb = xc * kPatChunk;
+  const int64_t xe = (xb + kPatChunk) < nx ? (xb + kPatChunk) : nx;
+  const int t = threadIdx.x;
+  const int row = t / nz4, z4 = (t % nz4) * 4;
+  const bool rok = row < TY;  // threads past TY rows of nz4 groups idle
+  const int64_t y = y0 + row;
+  const bool yok = rok && y < ny;
+  __syncthreads();
+  // stage plane xs (wrapped) into ring slot `slot`: rows y0-1 .. y0+TY
+  auto stage = [&](int64_t xs, int slot) {
+    int64_t xw = xs % nx;
+    if (xw < 0) xw += nx;
+    T* dst = ring + (size_t)slot * RW * nz;
+    for (int i = threadIdx.x; i < RW * nz4; i += blockDim.x) {
+      const int rr = i / nz4, zz = (i % nz4) * 4;
+      int64_t yy = y0 - 1 + rr;
+      yy = yy < 0 ? yy + ny : (yy >= ny ? yy - ny : yy);
+      if (yy < 0) yy = ((yy % ny) + ny) % ny;
+      const V4<T> v = ld4(pert + (xw * ny + yy) * nz + zz);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) dst[rr * nz + zz + l] = add_rn(v.v[l], s_vec[zz + l]);
+    }
+  };
+  double acc0[4] = {0, 0, 0, 0}, acc1[4] = {0, 0, 0, 0};
+  stage(xb - 1, 0);
+  stage(xb, 1);
+  for (int64_t x = xb; x < xe; ++x) {
+    const int sm = (int)((x - xb) % 3), sc = (int)((x - xb + 1) % 3), sp = (int)((x - xb + 2) % 3);
+    stage(x + 1, sp);
+    __syncthreads();
+    if (yok) {
+      const T* pc = ring + (size_t)sc * RW * nz + (row + 1) * nz;
+      const T* pxm = ring + (size_t)sm * RW * nz + (row + 1) * nz;
+      const T* pxp = ring + (size_t)sp * RW * nz + (row + 1) * nz;
+      const T* pym = pc - nz;
+      const T* pyp = pc + nz;
+      const int64_t gi = (x * ny + y) * nz + z4;
+      V4<T> pr;
+      if (a.has_prod) pr = ld4(prod + gi);
+      else pr.v[0] = pr.v[1] = pr.v[2] = pr.v[3] = (T)0;
+      V4<T> o;
+      const bool in_w = w.in(x, y);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const int z = z4 + l;
+        const T r = pc[z];
+        const T rzm = z > 0 ? pc[z - 1] : r;
+        const T rzp = z < nz - 1 ? pc[z + 1] : r;
+        const T Wv = pattern_cell<T>(
+            r, pxm[z], pxp[z], pym[z], pyp[z], rzm, rzp, z, nz, pr.v[l],
+            z > 0 ? s_vec[nz + z - 1] : (T)0, z > 0 ? s_vec[2 * nz + z - 1] : (T)0,
+            z > 0 ? s_vec[3 * nz + z - 1] : (T)0, s_vec[4 * nz + z], s_vec[5 * nz + z], a);
+        o.v[l] = Wv;
+        if (in_w) {
+          acc0[l] += (double)(Wv < (T)0 ? -Wv : Wv);
+          acc1[l] += Wv != (T)0 ? 1.0 : 0.0;
+        }
+      }
+      st4(out + gi, o);
+    }
+    __syncthreads();  // the slot staged next iteration is read this iteration
+  }
+  // per-level partials: rows of the block in order
+  const int nb = gridDim.x;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    __syncthreads();
+    if (rok)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) red[row * nz + z4 + l] = q == 0 ? acc0[l] : acc1[l];
+    __syncthreads();
+    for (int z = t; z < nz; z += blockDim.x) {
+      double sacc = 0.0;
+      for (int rr = 0; rr < TY; ++rr) sacc += red[rr * nz + z];
+      partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
+    }
+  }
+}
+
 // ---- bounded add sweeps --------------------------------------------------------
 // Per-level chain, replayed from the raw increment on every sweep:
 //   for s < nsteps[z]:  d = clip(d - demean[z,s], caps) * scale[z,s]
@@ -376,6 +541,148 @@ __global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
     }
   });
   if (MODE != BA_APPLY) store_level_partials<Q, JM>(m, acc, red, partials);
+}
+
+// Vectorised form of the sweep for nz % 4 == 0: a thread owns 4 consecutive
+// levels, loads 16 bytes per field per column, and issues two columns' loads
+// before any arithmetic.  Same chain, same results as ba_sweep_kernel.
+constexpr int kBaU = 1;  // columns loaded ahead per thread
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 4)) ba_sweep4_kernel(
+    const T* __restrict__ d0, T* __restrict__ pert, T* __restrict__ inc_out,
+    int record, int64_t nx, int64_t ny, int nz, Win w, BAChain<T> c,
+    double* __restrict__ partials) {
+  extern __shared__ unsigned char ba_smem[];
+  __shared__ double red[4 * kLvThreads];  // [cpi][nz] with cpi * nz == 4 * 256 / 4 ... <= 1024
+  const int R = c.R;
+  T* s_dm = reinterpret_cast<T*>(ba_smem);
+  T* s_sc = s_dm + (size_t)R * nz;
+  T* s_fin = s_sc + (size_t)R * nz;
+  T* s_mu = s_fin + nz;
+  T* s_mean = s_mu + nz;
+  T* s_cand = s_mean + nz;
+  int* s_ns = reinterpret_cast<int*>(s_cand + (size_t)kMuCand * nz);
+  int* s_hf = s_ns + nz;
+  int* s_hm = s_hf + nz;
+  for (int i = threadIdx.x; i < R * nz; i += blockDim.x) {
+    const int z = i % nz, st = i / nz;
+    s_dm[i] = c.demean[z * R + st];
+    s_sc[i] = c.scale[z * R + st];
+  }
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    s_fin[z] = c.final_dm[z];
+    s_mu[z] = c.mu[z];
+    s_mean[z] = c.mean[z];
+    s_ns[z] = c.nsteps[z];
+    s_hf[z] = c.has_final[z];
+    s_hm[z] = c.has_mu[z];
+#pragma unroll
+    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = c.cand[z * kMuCand + k];
+  }
+  __syncthreads();
+  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
+  const int nz4 = nz / 4;
+  const int cpi = kLvThreads / nz4;  // columns per block-iteration
+  const int t = threadIdx.x;
+  const bool active = t < cpi * nz4;
+  const int z4 = (t % nz4) * 4;
+  const int cofs = t / nz4;
+  double acc[Q][4];
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int l = 0; l < 4; ++l) acc[q][l] = 0.0;
+  const int64_t ncol = nx * ny;
+  int nsmax = 0;
+#pragma unroll
+  for (int l = 0; l < 4; ++l) nsmax = s_ns[z4 + l] > nsmax ? s_ns[z4 + l] : nsmax;
+  auto process = [&](int64_t col, int64_t x, int64_t y, const V4<T>& dv, const V4<T>& pv) {
+    const int64_t i = col * nz + z4;
+    V4<T> pn, dn;
+    const bool in_w = w.in(x, y);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int zl = z4 + l;
+      const T p0 = pv.v[l];
+      T d = dv.v[l];
+      const T phi = add_rn(p0, s_mean[zl]);
+      const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
+      const int nsl = s_ns[zl];
+      for (int st = 0; st < nsmax; ++st) {
+        if (st < nsl) {
+          d = clampv(sub_rn(d, s_dm[st * nz + zl]), clo, chi);
+          d = mul_rn(d, s_sc[st * nz + zl]);
+        }
+      }
+      if (s_hf[zl]) d = clampv(sub_rn(d, s_fin[zl]), clo, chi);
+      if (MODE == BA_APPLY) {
+        if (s_hm[zl]) d = clampv(sub_rn(d, s_mu[zl]), clo, chi);
+        pn.v[l] = add_rn(p0, d);
+        dn.v[l] = sub_rn(pn.v[l], p0);
+      } else if (in_w) {
+        if (MODE == BA_STATS) {
+          acc[0][l] += (double)d;
+          acc[1 % Q][l] += (double)(d < (T)0 ? -d : d);
+        } else {
+#pragma unroll
+          for (int k = 0; k < kMuCand; ++k) {
+            const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
+            const T tv = clampv(raw, clo, chi);
+            acc[2 * k][l] += (double)tv;
+            acc[(2 * k + 1) % Q][l] += (raw > clo && raw < chi) ? 1.0 : 0.0;
+          }
+        }
+      }
+    }
+    if (MODE == BA_APPLY) {
+      st4(pert + i, pn);
+      if (record) st4(inc_out + i, dn);
+    }
+  };
+  if (active) {
+    const int64_t step = (int64_t)gridDim.x * cpi;
+    ColWalk cw;
+    cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
+    constexpr int U = MODE == BA_MU ? 1 : kBaU;
+    while (cw.col + (U - 1) * step < ncol) {
+      ColWalk u[U];
+      V4<T> dv[U], pv[U];
+      u[0] = cw;
+#pragma unroll
+      for (int k = 1; k < U; ++k) {
+        u[k] = u[k - 1];
+        u[k].advance(step);
+      }
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        dv[k] = ld4(d0 + u[k].col * nz + z4);
+        pv[k] = ld4(pert + u[k].col * nz + z4);
+      }
+#pragma unroll
+      for (int k = 0; k < U; ++k) process(u[k].col, u[k].x, u[k].y, dv[k], pv[k]);
+      cw = u[U - 1];
+      cw.advance(step);
+    }
+    for (; cw.col < ncol; cw.advance(step))
+      process(cw.col, cw.x, cw.y, ld4(d0 + cw.col * nz + z4), ld4(pert + cw.col * nz + z4));
+  }
+  if (MODE == BA_APPLY) return;
+  // deterministic reduction: per level, the cpi column slots in order
+  const int nb = gridDim.x;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    __syncthreads();
+    if (active)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) red[cofs * nz + z4 + l] = acc[q][l];
+    __syncthreads();
+    for (int z = t; z < nz; z += kLvThreads) {
+      double sacc = 0.0;
+      for (int cc = 0; cc < cpi; ++cc) sacc += red[cc * nz + z];
+      partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
+    }
+  }
 }
 
 // ---- projection sweeps (float64 level arithmetic) -----------------------------
@@ -645,6 +952,20 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
   STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, kLvMaxJ>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  const bool vec4 = nz % 4 == 0 && nz <= 4 * kLvThreads &&
+                    ((uintptr_t)pert % 16 == 0) && ((uintptr_t)inc % 16 == 0);
+  const int grid4 = vec4 ? stride_grid((ncol + (kLvThreads / (nz / 4)) - 1) /
+                                           (kLvThreads / (nz / 4)), 1, kLvBlocksPerSm)
+                         : 0;
+  if (vec4) {
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_STATS>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_MU>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_APPLY>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  }
+  const int sweep_grid = vec4 ? grid4 : grid;
   BAChain<T> ch;
   ch.nsteps = d_nsteps;
   ch.demean = d_demean;
@@ -668,14 +989,17 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
   auto stats_sweep = [&]() -> int {
     int r2 = push_chain();
     if (r2) return r2;
-        if (m.packed)
+        if (vec4)
+      ba_sweep4_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
+        inc, pert, nullptr, 0, nx, ny, (int)nz, w, ch, partials);
+    else if (m.packed)
       ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
         inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
     else
       ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
         inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
     STEAM_LAUNCH_CHECK("bounded_add stats sweep");
-    if ((r2 = reduce_partials(partials, grid, 2 * (int)nz, totals, s))) return r2;
+    if ((r2 = reduce_partials(partials, sweep_grid, 2 * (int)nz, totals, s))) return r2;
     ++n_sweeps;
     return fetch(tot, totals, 2 * nz, s);
   };
@@ -760,14 +1084,17 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
     }
     if (!pending) break;
     if ((rc = push_chain())) return rc;
-        if (m.packed)
+        if (vec4)
+      ba_sweep4_kernel<T, BA_MU><<<grid4, kLvThreads, ba_sm, s>>>(
+        inc, pert, nullptr, 0, nx, ny, (int)nz, w, ch, partials);
+    else if (m.packed)
       ba_sweep_kernel<T, BA_MU, 1><<<grid, kLvThreads, ba_sm, s>>>(
         inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
     else
       ba_sweep_kernel<T, BA_MU, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
         inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
     STEAM_LAUNCH_CHECK("bounded_add mu sweep");
-    if ((rc = reduce_partials(partials, grid, Qmax * (int)nz, totals, s))) return rc;
+    if ((rc = reduce_partials(partials, sweep_grid, Qmax * (int)nz, totals, s))) return rc;
     ++n_sweeps;
     if ((rc = fetch(tot, totals, (size_t)Qmax * nz, s))) return rc;
     for (int64_t z = 0; z < nz; ++z) {
@@ -790,7 +1117,10 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
     }
   // Apply.
   if ((rc = push_chain())) return rc;
-    if (m.packed)
+    if (vec4)
+    ba_sweep4_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_sm, s>>>(
+      inc, pert, inc, record, nx, ny, (int)nz, w, ch, partials);
+  else if (m.packed)
     ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
       inc, pert, inc, record, nx, ny, m, w, ch, partials);
   else
@@ -981,8 +1311,21 @@ extern "C" int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
   return STEAM_OK;
 }
 
-extern "C" size_t steam_scalar_pattern_workspace_bytes(int64_t nz) {
-  return level_partial_bytes(nz, 2) + 8 * carve_bytes(nz, sizeof(double));
+static bool pattern_march_ok(int64_t nz) { return nz % 4 == 0 && nz >= 4 && nz <= 4 * kLvThreads; }
+
+static int64_t pattern_march_grid(int64_t nx, int64_t ny, int64_t nz) {
+  const int64_t ty = kLvThreads / (nz / 4);
+  return ((ny + ty - 1) / ty) * ((nx + kPatChunk - 1) / kPatChunk);
+}
+
+extern "C" size_t steam_scalar_pattern_workspace_bytes(int64_t nx, int64_t ny, int64_t nz) {
+  size_t b = level_partial_bytes(nz, 2) + 8 * carve_bytes(nz, sizeof(double));
+  if (pattern_march_ok(nz)) {
+    const size_t m = carve_bytes((size_t)pattern_march_grid(nx, ny, nz) * 2 * nz, sizeof(double)) +
+                     carve_bytes((size_t)2 * nz, sizeof(double)) + 8 * carve_bytes(nz, sizeof(double));
+    b = m > b ? m : b;
+  }
+  return b;
 }
 
 template <typename T>
@@ -994,7 +1337,11 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
                         const steam_window_t* window, double* sums_out,
                         void* ws, size_t ws_bytes, cudaStream_t s) {
   const LevelMap m = make_map(nz);
-  const int grid = level_grid(nx * ny, m);
+  const bool march = pattern_march_ok(nz) && ((uintptr_t)pert % 16 == 0) &&
+                     ((uintptr_t)out % 16 == 0) && (!prod || (uintptr_t)prod % 16 == 0);
+  const int64_t grid64 = march ? pattern_march_grid(nx, ny, nz) : level_grid(nx * ny, m);
+  STEAM_REQUIRE(grid64 < ((int64_t)1 << 31), "steam_scalar_pattern: grid too large");
+  const int grid = (int)grid64;
   const Win w = make_win(window, nx, ny);
   Carver c(ws, ws_bytes);
   double* partials = c.take<double>((size_t)grid * 2 * nz);
@@ -1038,7 +1385,15 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
   a.uniform_z = uniform ? 1 : 0;
   a.has_prod = prod != nullptr;
   a.has_taper = bbuf != nullptr;
-    if (m.packed)
+    if (march) {
+    const int nz4 = (int)nz / 4, ty = kLvThreads / nz4;
+    const size_t sm = sizeof(T) * ((size_t)3 * (ty + 2) * nz + (size_t)6 * nz);
+    STEAM_REQUIRE(sm <= 200 * 1024, "steam_scalar_pattern: nz too large for the staged path");
+    STEAM_CUDA(cudaFuncSetAttribute(pattern_march_kernel<T>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    pattern_march_kernel<T><<<grid, kLvThreads, sm, s>>>(pert, d_vec, prod, nx, ny, (int)nz, w,
+                                                         a, out, partials);
+  } else if (m.packed)
     pattern_kernel<T, 1><<<grid, kLvThreads, 0, s>>>(
       pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
       d_vec + 4 * nz, d_vec + 5 * nz, nx, ny, m, w, a, out, partials);

@@ -433,7 +433,7 @@ def pattern_device(pert_t, mean_1d, product_t, s_scale, dx, dy, z_coords, aspect
     lib = _lib.load()
     nx, ny, nz = (int(n) for n in pert_t.shape)
     W = torch.empty_like(pert_t) if out is None else out
-    ws = _lib.WORKSPACE.get(lib.steam_scalar_pattern_workspace_bytes(nz))
+    ws = _lib.WORKSPACE.get(lib.steam_scalar_pattern_workspace_bytes(nx, ny, nz))
     sums = _lib.dout(2 * nz)
     _lib.check(lib.steam_scalar_pattern(
         _lib.dtype_code(pert_t), nx, ny, nz, _lib.ptr(pert_t), _lib.dvec(mean_1d),
