@@ -27,9 +27,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import threading
 import time
 from pathlib import Path
@@ -103,53 +101,71 @@ def workload(nx, ny, nz):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clocks and clock-event reasons sampled every 200 ms during the timed
+    region, from NVML in a thread of this process.  (A polling nvidia-smi
+    process stalls this process's CUDA calls while it queries: the field step
+    ran at half speed under it.)"""
 
-    def __init__(self, gpu_index):
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
+
+    def __init__(self, gpu_index, period=0.2):
         self.gpu = gpu_index
-        self.proc = None
-        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+        self.period = period
+        self.rows = []
+        self.thread = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.fh, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
         except Exception:
-            self.proc = None
+            self.thread = None
+            return
+        self.stop_ev = threading.Event()
+
+        def run():
+            while not self.stop_ev.is_set():
+                try:
+                    sm = self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+                    rs = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    self.rows.append((sm, rs))
+                except Exception:
+                    pass
+                self.stop_ev.wait(self.period)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        self.proc.terminate()
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        self.stop_ev.set()
+        self.thread.join()
         try:
-            self.proc.wait(timeout=5)
+            self.nv.nvmlShutdown()
         except Exception:
-            self.proc.kill()
-        self.fh.close()
-        rows = []
-        for line in self.path.read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace('.', '', 1).isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace('.', '', 1).isdigit()]
-        reasons = set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for r in rows:
-            for name, val in zip(names, r[5:9]):
-                if val.strip().lower() == "active":
-                    reasons.add(name)
-        loaded = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
-        return {"sm_mhz": statistics.median(loaded) if loaded else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(rows)}
+            pass
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"],
+                    "samples": 0}
+        sm = [float(r[0]) for r in self.rows]
+        reasons = sorted({name for _, bits in self.rows for name, bit in self.REASONS
+                          if bits & bit})
+        loaded = [v for v in sm if v > 0.5 * self.max_mhz] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": float(self.max_mhz),
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml"}
 
 
 # ---------------------------------------------------------------------------
