@@ -164,6 +164,23 @@ int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
                      double* sums_out, void* workspace, size_t workspace_bytes,
                      steam_stream_t stream);
 
+/* Allocation-free form of steam_level_sums, for callers that cannot allocate
+ * device memory (an application whose own allocator owns the device budget,
+ * a C FFI with no device allocator, a loop that must not allocate).  It has no
+ * counterpart in the reference.  Same arguments and results as
+ * steam_level_sums without (workspace, workspace_bytes): the scratch is one
+ * static device array of steam_level_sums_noalloc_scratch_bytes() (4 MiB) that
+ * every GPU loading this library holds until exit.  Limit: nz <= 1024
+ * (STEAM_ERR_UNSUPPORTED above that); any nx, ny.  The first call on a device
+ * resolves the array's address on that device, so make it before any stream
+ * capture.  All calls share the one array: calls whose work overlaps on the
+ * GPU (other streams, other host threads) race on it; serialise them.
+ * sums_out is written before return (the call synchronises its stream). */
+size_t steam_level_sums_noalloc_scratch_bytes(void);
+int steam_level_sums_noalloc(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                             const void* field, const steam_window_t* window,
+                             double* sums_out, steam_stream_t stream);
+
 /* ---- a12: scalar pattern ----------------------------------------------
  * Replaces the per-scalar pattern of cascade_loop (steam/simulate.py:
  * 1928-1983): running = pert + mean_1d; W = advective weight (periodic

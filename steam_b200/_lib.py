@@ -76,6 +76,9 @@ _SIGNATURES = {
     "steam_level_sums_workspace_bytes": (c_size, [c_i64]),
     "steam_level_sums": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                         ctypes.POINTER(Window), c_dp, c_vp, c_size, c_vp]),
+    "steam_level_sums_noalloc_scratch_bytes": (c_size, []),
+    "steam_level_sums_noalloc": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
+                                                ctypes.POINTER(Window), c_dp, c_vp]),
     "steam_scalar_pattern_workspace_bytes": (c_size, [c_i64, c_i64, c_i64]),
     "steam_scalar_pattern": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_dp,
                                             c_vp, c_dbl, c_dbl, c_dbl, c_dp, c_dp, c_dp,

@@ -10,6 +10,7 @@
 
 #include <cmath>
 #include <limits>
+#include <mutex>
 #include <vector>
 
 namespace steam {
@@ -1513,4 +1514,132 @@ extern "C" int steam_project_bounds(int dtype, int64_t nx, int64_t ny,
                                 phi_max, window, mu_out, workspace,
                                 workspace_bytes, s);
   return fail(STEAM_ERR_ARG, "steam_project_bounds: bad dtype");
+}
+
+// ---- per-level sums without a caller workspace ---------------------------------
+// steam_level_sums takes its scratch (block partials and totals) from a
+// workspace the caller allocates.  Some callers cannot allocate device memory
+// at all: a host application whose own allocator owns the whole device budget
+// and forbids other libraries from calling cudaMalloc, a binding through a
+// plain C FFI that has no device allocator to hand, or a latency-critical loop
+// that must not risk an allocation's synchronisation.  This variant keeps its
+// scratch in one file-scope device array instead.  The array is part of the
+// loaded library image, so every GPU that loads the library holds it
+// (kNoAllocScratchBytes) until the process exits.
+namespace steam {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB per device
+constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
+constexpr int kNoAllocMaxDevices = 64;
+
+// In host code this name is only a handle for the runtime; the device address
+// comes from cudaGetSymbolAddress below, once per device.
+__device__ __align__(256) double g_level_sums_scratch[kNoAllocScratchDoubles];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The first call
+// on a device resolves it (with that device current) and caches it.
+int noalloc_scratch(double** out) {
+  int dev = -1;
+  STEAM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(STEAM_ERR_UNSUPPORTED, "steam_level_sums_noalloc: device ordinal above 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_level_sums_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(STEAM_ERR_CUDA, std::string("steam_level_sums_noalloc: cudaGetSymbolAddress: ") +
+                                      cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return STEAM_OK;
+}
+
+// totals [3][nz] -> out [nz][4] = {sum, sum|f|, nonzero count, cells}
+__global__ void pack_level_sums_kernel(const double* __restrict__ totals, int nz,
+                                       double cells, double* __restrict__ out) {
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    out[4 * z + 0] = totals[z];
+    out[4 * z + 1] = totals[nz + z];
+    out[4 * z + 2] = totals[2 * nz + z];
+    out[4 * z + 3] = cells;
+  }
+}
+
+}  // namespace
+}  // namespace steam
+
+extern "C" size_t steam_level_sums_noalloc_scratch_bytes(void) {
+  return steam::kNoAllocScratchBytes;
+}
+
+extern "C" int steam_level_sums_noalloc(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                        const void* field, const steam_window_t* window,
+                                        double* sums_out, steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_level_sums_noalloc: negative extent");
+  if (nz > kLvThreads * kLvMaxJ)
+    return fail(STEAM_ERR_UNSUPPORTED,
+                "steam_level_sums_noalloc: nz = " + std::to_string(nz) +
+                    " is above the maximum of 1024 levels this entry point supports");
+  STEAM_REQUIRE(sums_out != nullptr, "steam_level_sums_noalloc: null sums_out");
+  STEAM_REQUIRE(dtype == STEAM_F32 || dtype == STEAM_F64, "steam_level_sums_noalloc: bad dtype");
+  int rc = check_win(window, nx, ny, "steam_level_sums_noalloc");
+  if (rc) return rc;
+  if (nz == 0) return STEAM_OK;
+  const Win w = make_win(window, nx, ny);
+  const double cells = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
+  if (nx * ny == 0) {
+    for (int64_t z = 0; z < nz; ++z) {
+      sums_out[4 * z] = sums_out[4 * z + 1] = sums_out[4 * z + 2] = 0.0;
+      sums_out[4 * z + 3] = cells;
+    }
+    return STEAM_OK;
+  }
+  STEAM_REQUIRE(field != nullptr, "steam_level_sums_noalloc: null field");
+  // Scratch layout (doubles): partials [3][nz][B] | totals [3][nz] | packed [nz][4].
+  // B, the block count, is the regular entry's grid capped so that the three
+  // regions fit the static array; every kernel below is grid-stride, so a
+  // smaller B changes only the order of the per-level double sums.
+  const LevelMap m = make_map(nz);
+  const size_t fixed = (size_t)7 * nz;
+  const size_t cap_blocks = (kNoAllocScratchDoubles - fixed) / ((size_t)3 * nz);
+  int grid = level_grid(nx * ny, m);
+  if ((size_t)grid > cap_blocks) grid = (int)cap_blocks;
+  double* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  double* partials = scratch;
+  double* totals = partials + (size_t)grid * 3 * nz;
+  double* packed = totals + (size_t)3 * nz;
+  cudaStream_t s = (cudaStream_t)stream;
+  // Every partial slot is written by its block before the reduction reads
+  // it, and every total before the pack reads it, so nothing carries over
+  // from the previous call's contents.
+  if (dtype == STEAM_F32) {
+    if (m.packed)
+      level_sums_kernel<float, 1><<<grid, kLvThreads, 0, s>>>((const float*)field, nx, ny, m, w,
+                                                              partials);
+    else
+      level_sums_kernel<float, kLvMaxJ><<<grid, kLvThreads, 0, s>>>((const float*)field, nx, ny,
+                                                                    m, w, partials);
+  } else {
+    if (m.packed)
+      level_sums_kernel<double, 1><<<grid, kLvThreads, 0, s>>>((const double*)field, nx, ny, m,
+                                                               w, partials);
+    else
+      level_sums_kernel<double, kLvMaxJ><<<grid, kLvThreads, 0, s>>>((const double*)field, nx,
+                                                                     ny, m, w, partials);
+  }
+  STEAM_LAUNCH_CHECK("steam_level_sums_noalloc");
+  if ((rc = reduce_partials(partials, grid, 3 * (int)nz, totals, s))) return rc;
+  pack_level_sums_kernel<<<(int)((nz + 255) / 256), 256, 0, s>>>(totals, (int)nz, cells, packed);
+  STEAM_LAUNCH_CHECK("steam_level_sums_noalloc pack");
+  STEAM_CUDA(cudaMemcpyAsync(sums_out, packed, (size_t)4 * nz * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+  STEAM_CUDA(cudaStreamSynchronize(s));
+  return STEAM_OK;
 }
