@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(256) xpass_kernel(
 // ---- fused pencil convolution ----------------------------------------------
 // One CTA owns a (kFY x kFZ) cross-section of y and z and marches along a
 // chunk of x.  For every input x-plane it stages the plane's (y, z) slab with
-// its halo in shared memory (in float64), runs the z filters (4 outputs per
+// its halo in shared memory (in the arithmetic type A), runs the z filters (4 outputs per
 // thread, sliding window) and the y filters (2 rows per thread) on chip, and
 // folds the mixed result into a ring of K per-output-plane accumulators held
 // in registers (indices static through a uniform switch on the ring phase).
@@ -247,6 +247,13 @@ __global__ void __launch_bounds__(256) xpass_kernel(
 // computed (two slab buffers).  An output plane is final K-1 planes after its
 // first contribution and goes straight through the epilogue.  HBM sees the
 // input once (halo re-reads hit L2) and the output once.
+//
+// A, the type of the taps, the staged slabs and every accumulator: the
+// field's own type for a plain convolution (float32 fields are filtered in
+// float32, the precision of the reference's float32 FFT, and land closer to
+// the float64 result than it does), float64 for the flux epilogue whatever
+// the field type: there F + conv cancels to near zero next to the clip, and
+// float32 accumulation alone moved the log-flux past 1e-5 relative L2.
 constexpr int kFY = 32;
 constexpr int kFZ = 16;
 constexpr int kFThreads = 256;
@@ -270,28 +277,28 @@ struct FusedShape {
   static constexpr int ZT = R * (kFZ / 4);       // z-filter tasks (4 outputs each)
 };
 
-template <typename T, int K>
-__global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kernel(
+template <typename T, typename A, int K>
+__global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
     const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
     SepParams<T> p, FusedGeom<T> g, XEpi epi, double* __restrict__ partials) {
   using S = FusedShape<K>;
   constexpr int R = S::R, C = S::C, NL = S::NL;
   extern __shared__ unsigned char smem_raw[];
   __shared__ double scratch[32];
-  __shared__ double s_zt[kFMaxZ][K], s_yt[2][K], s_xt[kFMaxX][K];
-  __shared__ double s_mix[kFMaxX * kFMaxPairs];
+  __shared__ A s_zt[kFMaxZ][K], s_yt[2][K], s_xt[kFMaxX][K];
+  __shared__ A s_mix[kFMaxX * kFMaxPairs];
   __shared__ T s_pre[2][C];
-  double* s_in0 = reinterpret_cast<double*>(smem_raw);  // [2][R*C]
-  double* s_u = s_in0 + 2 * R * C;                       // [2][R][kFZ]
+  A* s_in0 = reinterpret_cast<A*>(smem_raw);  // [2][R*C]
+  A* s_u = s_in0 + 2 * R * C;                            // [2][R][kFZ]
   const int t = threadIdx.x;
   const int nzf = p.nzf, nxf = p.nxf, npairs = p.npairs;
   for (int i = t; i < K; i += kFThreads) {
-    s_zt[0][i] = p.taps[i];
-    s_zt[1][i] = nzf > 1 ? p.taps[K + i] : 0.0;
-    s_yt[0][i] = p.ytap(0)[i];
-    s_yt[1][i] = p.nyf > 1 ? p.ytap(1)[i] : 0.0;
-    s_xt[0][i] = p.xtap(0)[i];
-    s_xt[1][i] = nxf > 1 ? p.xtap(1)[i] : 0.0;
+    s_zt[0][i] = (A)p.taps[i];
+    s_zt[1][i] = nzf > 1 ? (A)p.taps[K + i] : (A)0;
+    s_yt[0][i] = (A)p.ytap(0)[i];
+    s_yt[1][i] = p.nyf > 1 ? (A)p.ytap(1)[i] : (A)0;
+    s_xt[0][i] = (A)p.xtap(0)[i];
+    s_xt[1][i] = nxf > 1 ? (A)p.xtap(1)[i] : (A)0;
   }
   if (t < kFMaxX * kFMaxPairs) {
     // mix re-indexed by (a, c, b): pairs are enumerated c-major, b-minor
@@ -300,7 +307,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
     double v = 0.0;
     for (int q = 0; q < npairs; ++q)
       if (a < nxf && p.pair_z[q] == c && p.pair_y[q] == b) v += p.mix[a * npairs + q];
-    s_mix[t] = v;
+    s_mix[t] = (A)v;
   }
   const int zt_i = blockIdx.x % g.nzt;
   const int yt_i = (blockIdx.x / g.nzt) % g.nyt;
@@ -336,7 +343,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
 #pragma unroll
     for (int i = 0; i < NL; ++i) ld[i] = goff[i] >= 0 ? base[goff[i]] : (T)0;
   };
-  auto commit_loads = [&](double* dst) {
+  auto commit_loads = [&](A* dst) {
 #pragma unroll
     for (int i = 0; i < NL; ++i) {
       const int e = t + i * kFThreads;
@@ -344,7 +351,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
         const int c = e % C;  // C is a compile-time constant
         T v = ld[i];
         if (g.use_pre) v = mul_rn(v / s_pre[0][c], s_pre[1][c]);
-        dst[e] = (double)v;
+        dst[e] = (A)v;
       }
     }
   };
@@ -355,9 +362,9 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
   // output rows oy0, oy0 + 1 (each valid when inside the array)
 #define OY(m) (oy0 + (m))
 #define OK(m) (okz && OY(m) < g.ny)
-  double acc[K][2];
+  A acc[K][2];
 #pragma unroll
-  for (int sl = 0; sl < K; ++sl) acc[sl][0] = acc[sl][1] = 0.0;
+  for (int sl = 0; sl < K; ++sl) acc[sl][0] = acc[sl][1] = (A)0;
   double s_f = 0.0, s_clip = 0.0;
   __syncthreads();
   issue_loads(0);
@@ -365,7 +372,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
   __syncthreads();
   const bool flux_epi = epi.mode == STEAM_EPI_FLUX;
   for (int64_t k = 0; k < count; ++k) {
-    double* s_in = s_in0 + (k & 1) * R * C;
+    A* s_in = s_in0 + (k & 1) * R * C;
     if (k + 1 < count) issue_loads(k + 1);
     // the flux under the output plane this iteration completes, loaded now so
     // that the load overlaps the plane's filters
@@ -379,14 +386,14 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
     // ---- z filters, 4 outputs per task: u_c[r][z4 .. z4+3]
     for (int task = t; task < S::ZT; task += kFThreads) {
       const int r = task / (kFZ / 4), z4 = (task % (kFZ / 4)) * 4;
-      const double* b = s_in + r * C + z4;
-      double win[K + 3];
+      const A* b = s_in + r * C + z4;
+      A win[K + 3];
 #pragma unroll
       for (int i = 0; i < K + 3; ++i) win[i] = b[i];
-      double a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
+      A a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
 #pragma unroll
       for (int l = 0; l < K; ++l) {
-        const double t0 = s_zt[0][l], t1 = s_zt[1][l];
+        const A t0 = s_zt[0][l], t1 = s_zt[1][l];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
           // out[z] uses staged column z + K - 1 - l
@@ -402,24 +409,24 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
     }
     __syncthreads();
     // ---- y filters for rows 2yp, 2yp+1 at column zq, then the mixing
-    double w0[2] = {0, 0}, w1[2] = {0, 0};
+    A w0[2] = {0, 0}, w1[2] = {0, 0};
 #pragma unroll
     for (int c = 0; c < kFMaxZ; ++c) {
-      double col[K + 1];
-      const double* src = s_u + c * R * kFZ + (2 * yp) * kFZ + zq;
+      A col[K + 1];
+      const A* src = s_u + c * R * kFZ + (2 * yp) * kFZ + zq;
 #pragma unroll
       for (int i = 0; i < K + 1; ++i) col[i] = src[i * kFZ];
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        double v0 = 0.0, v1 = 0.0;
+        A v0 = 0, v1 = 0;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-          const double tj = s_yt[b][j];
+          const A tj = s_yt[b][j];
           v0 += tj * col[K - 1 - j];
           v1 += tj * col[K - j];
         }
-        const double m0 = s_mix[0 * kFMaxPairs + c * 2 + b];
-        const double m1 = s_mix[1 * kFMaxPairs + c * 2 + b];
+        const A m0 = s_mix[0 * kFMaxPairs + c * 2 + b];
+        const A m1 = s_mix[1 * kFMaxPairs + c * 2 + b];
         w0[0] += m0 * v0;
         w0[1] += m0 * v1;
         w1[0] += m1 * v0;
@@ -436,7 +443,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
 #pragma unroll
         for (int i = 0; i < K; ++i) {
           const int slot = (rr + i + 1) % K;
-          const double c0 = s_xt[0][i], c1 = s_xt[1][i];
+          const A c0 = s_xt[0][i], c1 = s_xt[1][i];
           acc[slot][0] += c0 * w0[0] + c1 * w1[0];
           acc[slot][1] += c0 * w0[1] + c1 * w1[1];
         }
@@ -448,7 +455,7 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
             if (OK(m)) {
               const int64_t o = (x * g.ny + OY(m)) * g.nz + z0 + zq;
               if (flux_epi) {
-                T f = (T)((double)fprev[m] + acc[es][m]);
+                T f = add_rn(fprev[m], (T)acc[es][m]);
                 if (f < (T)0) {
                   s_clip += 1.0;
                   f = (T)0;
@@ -464,8 +471,8 @@ __global__ void __launch_bounds__(kFThreads, (K <= 13 ? 2 : 1)) fused_conv_kerne
         }
         // a slot leaving the ring is cleared whether or not its output lies
         // in this chunk (planes before the chunk only feed the halo)
-        acc[es][0] = 0.0;
-        acc[es][1] = 0.0;
+        acc[es][0] = (A)0;
+        acc[es][1] = (A)0;
       }
     }
     if (k + 1 < count) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
@@ -494,9 +501,8 @@ static bool fused_supported(const SepParams<T>& p) {
 }
 
 static size_t fused_smem(int k, size_t elem) {
-  (void)elem;
   const int R = kFY + k - 1, C = kFZ + k - 1;
-  return sizeof(double) * ((size_t)2 * R * C + (size_t)kFMaxZ * R * kFZ);
+  return elem * ((size_t)2 * R * C + (size_t)kFMaxZ * R * kFZ);
 }
 
 static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz) {
@@ -594,6 +600,27 @@ static int64_t epi_cells(const steam_window_t* w, int64_t nx, int64_t ny) {
   return (w->x1 - w->x0) * (w->y1 - w->y0);
 }
 
+template <typename T, typename A>
+static int launch_fused(const SepParams<T>& p, int64_t grid, const T* in, T* out, const T* pre,
+                        const FusedGeom<T>& g, const XEpi& epi, double* partials,
+                        cudaStream_t s) {
+  const size_t sm = fused_smem(p.kx, sizeof(A));
+  STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: filters too long for the fused path");
+  if (p.kx == 13) {
+    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, A, 13>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    fused_conv_kernel<T, A, 13><<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, p, g, epi,
+                                                                      partials);
+  } else {
+    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, A, 25>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    fused_conv_kernel<T, A, 25><<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, p, g, epi,
+                                                                      partials);
+  }
+  STEAM_LAUNCH_CHECK("conv fused");
+  return STEAM_OK;
+}
+
 template <typename T>
 static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
                      const void* in_v, const double* pre_div,
@@ -631,20 +658,11 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
   epi.wx1 = win ? win->x1 : nx;
   epi.wy0 = win ? win->y0 : 0;
   epi.wy1 = win ? win->y1 : ny;
-  const size_t sm = fused_smem(p.kx, sizeof(T));
-  STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: filters too long for the fused path");
-  if (p.kx == 13) {
-    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, 13>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fused_conv_kernel<T, 13><<<(unsigned)grid, kFThreads, sm, s>>>(
-        (const T*)in_v, (T*)out_v, pre, p, g, epi, partials);
-  } else {
-    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, 25>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fused_conv_kernel<T, 25><<<(unsigned)grid, kFThreads, sm, s>>>(
-        (const T*)in_v, (T*)out_v, pre, p, g, epi, partials);
-  }
-  STEAM_LAUNCH_CHECK("conv fused");
+  int rc = epilogue == STEAM_EPI_FLUX
+               ? launch_fused<T, double>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi,
+                                         partials, s)
+               : launch_fused<T, T>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi, partials, s);
+  if (rc) return rc;
   if (epilogue == STEAM_EPI_FLUX) {
     int rc = reduce_partials(partials, (int)grid, 2, totals, s);
     if (rc) return rc;

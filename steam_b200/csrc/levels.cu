@@ -297,14 +297,13 @@ __device__ __forceinline__ void st4(T* p, const V4<T>& r) {
   }
 }
 
-// ---- scalar pattern, marching in x ----------------------------------------------
-// A block owns TY = 1024 / nz rows of y and every z (nz % 4 == 0, nz <= 1024),
-// and marches x over a chunk.  The running field r = pert + mean of planes
-// x-1, x, x+1 -- each with one halo row on either side in y -- sits in a
-// three-plane ring in shared memory, so every input plane is read from HBM
-// once (16-byte loads); a thread computes 4 consecutive levels of one row.
-constexpr int kPatChunk = 256;
-
+// ---- scalar pattern, one 4-level group per thread --------------------------------
+// For nz % 4 == 0 (nz <= 1024): a column's nz/4 threads each own 4 consecutive
+// levels for the whole grid-stride walk, so the per-level constants sit in
+// registers; a block covers 256 / (nz/4) consecutive columns per step.  The
+// x and y neighbours are 16-byte loads of adjacent columns.  The grid walks
+// columns in memory order, so planes x-1, x and x+1 are all resident in L2
+// while plane x is processed and DRAM sees every input once.
 template <typename T>
 __device__ __forceinline__ T pattern_cell(T r, T rxm, T rxp, T rym, T ryp, T rzm, T rzp,
                                           int z, int nz, T prod, T az, T bz, T cz,
@@ -337,96 +336,90 @@ __device__ __forceinline__ T pattern_cell(T r, T rxm, T rxp, T rym, T ryp, T rzm
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kLvThreads) pattern_march_kernel(
+__global__ void __launch_bounds__(kLvThreads) pattern_vec_kernel(
     const T* __restrict__ pert, const T* __restrict__ vecs, const T* __restrict__ prod,
     int64_t nx, int64_t ny, int nz, Win w, PatternArgs<T> a, T* __restrict__ out,
     double* __restrict__ partials) {
-  extern __shared__ unsigned char pm_smem[];
-  const int nz4 = nz / 4;
-  const int TY = kLvThreads / nz4;
-  const int RW = TY + 2;  // staged rows per plane
-  T* ring = reinterpret_cast<T*>(pm_smem);  // [3][RW][nz]
-  T* s_vec = ring + (size_t)3 * RW * nz;      // [6][nz]: mean, a, b, c, aspect, buffer
   __shared__ double red[4 * kLvThreads];
-  for (int i = threadIdx.x; i < 6 * nz; i += blockDim.x) s_vec[i] = vecs[i];
-  const int64_t nyt = (ny + TY - 1) / TY;
-  const int64_t yt = blockIdx.x % nyt;
-  const int64_t xc = blockIdx.x / nyt;
-  const int64_t y0 = yt * TY;
-  const int64_t xb = xc * kPatChunk;
-  const int64_t xe = (xb + kPatChunk) < nx ? (xb + kPatChunk) : nx;
+  const int nz4 = nz >> 2;
+  const int cpb = kLvThreads / nz4;
   const int t = threadIdx.x;
-  const int row = t / nz4, z4 = (t % nz4) * 4;
-  const bool rok = row < TY;  // threads past TY rows of nz4 groups idle
-  const int64_t y = y0 + row;
-  const bool yok = rok && y < ny;
-  __syncthreads();
-  // stage plane xs (wrapped) into ring slot `slot`: rows y0-1 .. y0+TY
-  auto stage = [&](int64_t xs, int slot) {
-    int64_t xw = xs % nx;
-    if (xw < 0) xw += nx;
-    T* dst = ring + (size_t)slot * RW * nz;
-    for (int i = threadIdx.x; i < RW * nz4; i += blockDim.x) {
-      const int rr = i / nz4, zz = (i % nz4) * 4;
-      int64_t yy = y0 - 1 + rr;
-      yy = yy < 0 ? yy + ny : (yy >= ny ? yy - ny : yy);
-      if (yy < 0) yy = ((yy % ny) + ny) % ny;
-      const V4<T> v = ld4(pert + (xw * ny + yy) * nz + zz);
+  const int cs = t / nz4;
+  const int z4 = (t - cs * nz4) * 4;
+  const bool act = cs < cpb;
+  // vecs: [0] mean, [1] a, [2] b, [3] c (np.gradient, indexed z-1), [4] aspect, [5] buffer
+  T mz[4], asp[4], bb[4], ca[4], cb[4], cc[4];
+  T m_lo = (T)0, m_hi = (T)0;
+  if (act) {
 #pragma unroll
-      for (int l = 0; l < 4; ++l) dst[rr * nz + zz + l] = add_rn(v.v[l], s_vec[zz + l]);
+    for (int l = 0; l < 4; ++l) {
+      const int z = z4 + l;
+      mz[l] = vecs[z];
+      asp[l] = vecs[4 * nz + z];
+      bb[l] = vecs[5 * nz + z];
+      ca[l] = z > 0 ? vecs[nz + z - 1] : (T)0;
+      cb[l] = z > 0 ? vecs[2 * nz + z - 1] : (T)0;
+      cc[l] = z > 0 ? vecs[3 * nz + z - 1] : (T)0;
     }
-  };
+    m_lo = z4 > 0 ? vecs[z4 - 1] : (T)0;
+    m_hi = z4 + 4 < nz ? vecs[z4 + 4] : (T)0;
+  }
   double acc0[4] = {0, 0, 0, 0}, acc1[4] = {0, 0, 0, 0};
-  stage(xb - 1, 0);
-  stage(xb, 1);
-  for (int64_t x = xb; x < xe; ++x) {
-    const int sm = (int)((x - xb) % 3), sc = (int)((x - xb + 1) % 3), sp = (int)((x - xb + 2) % 3);
-    stage(x + 1, sp);
-    __syncthreads();
-    if (yok) {
-      const T* pc = ring + (size_t)sc * RW * nz + (row + 1) * nz;
-      const T* pxm = ring + (size_t)sm * RW * nz + (row + 1) * nz;
-      const T* pxp = ring + (size_t)sp * RW * nz + (row + 1) * nz;
-      const T* pym = pc - nz;
-      const T* pyp = pc + nz;
-      const int64_t gi = (x * ny + y) * nz + z4;
+  const int64_t ncol = nx * ny;
+  const int64_t step = (int64_t)gridDim.x * cpb;
+  ColWalk cw;
+  cw.init((int64_t)blockIdx.x * cpb + cs, step, ny);
+  if (act) {
+    for (; cw.col < ncol; cw.advance(step)) {
+      const int64_t x = cw.x, y = cw.y;
+      const int64_t xp = x + 1 < nx ? x + 1 : 0, xm = x > 0 ? x - 1 : nx - 1;
+      const int64_t yp = y + 1 < ny ? y + 1 : 0, ym = y > 0 ? y - 1 : ny - 1;
+      const int64_t base = cw.col * nz + z4;
+      const V4<T> c = ld4(pert + base);
+      const V4<T> vxp = ld4(pert + (xp * ny + y) * nz + z4);
+      const V4<T> vxm = ld4(pert + (xm * ny + y) * nz + z4);
+      const V4<T> vyp = ld4(pert + (x * ny + yp) * nz + z4);
+      const V4<T> vym = ld4(pert + (x * ny + ym) * nz + z4);
+      const T below = z4 > 0 ? pert[base - 1] : (T)0;
+      const T above = z4 + 4 < nz ? pert[base + 4] : (T)0;
       V4<T> pr;
-      if (a.has_prod) pr = ld4(prod + gi);
+      if (a.has_prod) pr = ld4(prod + base);
       else pr.v[0] = pr.v[1] = pr.v[2] = pr.v[3] = (T)0;
+      T r[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) r[l] = add_rn(c.v[l], mz[l]);
+      const T r_lo = add_rn(below, m_lo), r_hi = add_rn(above, m_hi);
       V4<T> o;
       const bool in_w = w.in(x, y);
 #pragma unroll
       for (int l = 0; l < 4; ++l) {
         const int z = z4 + l;
-        const T r = pc[z];
-        const T rzm = z > 0 ? pc[z - 1] : r;
-        const T rzp = z < nz - 1 ? pc[z + 1] : r;
-        const T Wv = pattern_cell<T>(
-            r, pxm[z], pxp[z], pym[z], pyp[z], rzm, rzp, z, nz, pr.v[l],
-            z > 0 ? s_vec[nz + z - 1] : (T)0, z > 0 ? s_vec[2 * nz + z - 1] : (T)0,
-            z > 0 ? s_vec[3 * nz + z - 1] : (T)0, s_vec[4 * nz + z], s_vec[5 * nz + z], a);
+        const T rzm = l == 0 ? r_lo : r[l - 1];
+        const T rzp = l == 3 ? r_hi : r[l + 1];
+        const T Wv = pattern_cell<T>(r[l], add_rn(vxm.v[l], mz[l]), add_rn(vxp.v[l], mz[l]),
+                                     add_rn(vym.v[l], mz[l]), add_rn(vyp.v[l], mz[l]), rzm, rzp,
+                                     z, nz, pr.v[l], ca[l], cb[l], cc[l], asp[l], bb[l], a);
         o.v[l] = Wv;
         if (in_w) {
           acc0[l] += (double)(Wv < (T)0 ? -Wv : Wv);
           acc1[l] += Wv != (T)0 ? 1.0 : 0.0;
         }
       }
-      st4(out + gi, o);
+      st4(out + base, o);
     }
-    __syncthreads();  // the slot staged next iteration is read this iteration
   }
-  // per-level partials: rows of the block in order
+  // per-level partials: the block's column slots in order
   const int nb = gridDim.x;
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     __syncthreads();
-    if (rok)
+    if (act)
 #pragma unroll
-      for (int l = 0; l < 4; ++l) red[row * nz + z4 + l] = q == 0 ? acc0[l] : acc1[l];
+      for (int l = 0; l < 4; ++l) red[cs * nz + z4 + l] = q == 0 ? acc0[l] : acc1[l];
     __syncthreads();
     for (int z = t; z < nz; z += blockDim.x) {
       double sacc = 0.0;
-      for (int rr = 0; rr < TY; ++rr) sacc += red[rr * nz + z];
+      for (int k = 0; k < cpb; ++k) sacc += red[k * nz + z];
       partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
     }
   }
@@ -1059,19 +1052,19 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
       h_hasfinal[z] = 1;
       h_final[z] = (T)cur_mean[z];
     }
-  if ((rc = stats_sweep())) return rc;
-  // Zero-mean shift mu where the clip left a mean.
+  // Zero-mean shift mu where the final clip left a mean.  The bracket starts
+  // symmetric about 0, so the first mu sweep's first candidate is mu = 0: its
+  // mean is the mean after the final demean and clip, which decides whether
+  // the level needs a shift at all (no separate sweep for it).
   const double width = phi_max - phi_min;
   std::vector<MuSolver<T>> solver(nz);
   std::vector<int> need(nz, 0);
   bool any_mu = false;
   for (int64_t z = 0; z < nz; ++z) {
     if (!active[z]) continue;
-    if (fabs(tot[z] / N) > 1e-9 * a0[z]) {
-      need[z] = 1;
-      any_mu = true;
-      solver[z].init(width, a0[z] * (sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49)));
-    }
+    need[z] = 1;
+    any_mu = true;
+    solver[z].init(width, a0[z] * (sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49)));
   }
   for (int it = 0; any_mu && it < 80; ++it) {
     std::vector<double> cands((size_t)nz * kMuCand, 0.0);
@@ -1106,6 +1099,10 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
         cv[k] = (double)h_cand[z * kMuCand + k];
         mv[k] = tot[(size_t)(2 * k) * nz + z] / N;
         sl[k] = -tot[(size_t)(2 * k + 1) * nz + z] / N;
+      }
+      if (it == 0 && fabs(mv[0]) <= 1e-9 * a0[z]) {
+        need[z] = 0;  // the final clip left the level mean-free
+        continue;
       }
       solver[z].update(cv, mv, sl);
     }
@@ -1312,17 +1309,17 @@ extern "C" int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
   return STEAM_OK;
 }
 
-static bool pattern_march_ok(int64_t nz) { return nz % 4 == 0 && nz >= 4 && nz <= 4 * kLvThreads; }
+static bool pattern_vec_ok(int64_t nz) { return nz % 4 == 0 && nz >= 4 && nz <= 4 * kLvThreads; }
 
-static int64_t pattern_march_grid(int64_t nx, int64_t ny, int64_t nz) {
-  const int64_t ty = kLvThreads / (nz / 4);
-  return ((ny + ty - 1) / ty) * ((nx + kPatChunk - 1) / kPatChunk);
+static int pattern_vec_grid(int64_t nx, int64_t ny, int64_t nz) {
+  const int64_t cpb = kLvThreads / (nz / 4);
+  return stride_grid((nx * ny + cpb - 1) / cpb, 1, kLvBlocksPerSm);
 }
 
 extern "C" size_t steam_scalar_pattern_workspace_bytes(int64_t nx, int64_t ny, int64_t nz) {
   size_t b = level_partial_bytes(nz, 2) + 8 * carve_bytes(nz, sizeof(double));
-  if (pattern_march_ok(nz)) {
-    const size_t m = carve_bytes((size_t)pattern_march_grid(nx, ny, nz) * 2 * nz, sizeof(double)) +
+  if (pattern_vec_ok(nz)) {
+    const size_t m = carve_bytes((size_t)pattern_vec_grid(nx, ny, nz) * 2 * nz, sizeof(double)) +
                      carve_bytes((size_t)2 * nz, sizeof(double)) + 8 * carve_bytes(nz, sizeof(double));
     b = m > b ? m : b;
   }
@@ -1338,11 +1335,9 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
                         const steam_window_t* window, double* sums_out,
                         void* ws, size_t ws_bytes, cudaStream_t s) {
   const LevelMap m = make_map(nz);
-  const bool march = pattern_march_ok(nz) && ((uintptr_t)pert % 16 == 0) &&
-                     ((uintptr_t)out % 16 == 0) && (!prod || (uintptr_t)prod % 16 == 0);
-  const int64_t grid64 = march ? pattern_march_grid(nx, ny, nz) : level_grid(nx * ny, m);
-  STEAM_REQUIRE(grid64 < ((int64_t)1 << 31), "steam_scalar_pattern: grid too large");
-  const int grid = (int)grid64;
+  const bool vec = pattern_vec_ok(nz) && ((uintptr_t)pert % 16 == 0) &&
+                   ((uintptr_t)out % 16 == 0) && (!prod || (uintptr_t)prod % 16 == 0);
+  const int grid = vec ? pattern_vec_grid(nx, ny, nz) : level_grid(nx * ny, m);
   const Win w = make_win(window, nx, ny);
   Carver c(ws, ws_bytes);
   double* partials = c.take<double>((size_t)grid * 2 * nz);
@@ -1386,14 +1381,9 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
   a.uniform_z = uniform ? 1 : 0;
   a.has_prod = prod != nullptr;
   a.has_taper = bbuf != nullptr;
-    if (march) {
-    const int nz4 = (int)nz / 4, ty = kLvThreads / nz4;
-    const size_t sm = sizeof(T) * ((size_t)3 * (ty + 2) * nz + (size_t)6 * nz);
-    STEAM_REQUIRE(sm <= 200 * 1024, "steam_scalar_pattern: nz too large for the staged path");
-    STEAM_CUDA(cudaFuncSetAttribute(pattern_march_kernel<T>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    pattern_march_kernel<T><<<grid, kLvThreads, sm, s>>>(pert, d_vec, prod, nx, ny, (int)nz, w,
-                                                         a, out, partials);
+  if (vec) {
+    pattern_vec_kernel<T><<<grid, kLvThreads, 0, s>>>(pert, d_vec, prod, nx, ny, (int)nz, w, a,
+                                                       out, partials);
   } else if (m.packed)
     pattern_kernel<T, 1><<<grid, kLvThreads, 0, s>>>(
       pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
