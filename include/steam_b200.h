@@ -264,6 +264,97 @@ int steam_kernel_build(int dtype, double k, double dx, double dy, double dz,
                        double support_factor, int32_t shape, void* out,
                        int64_t* dims_out, steam_stream_t stream);
 
+/* ---- Resident (asynchronous) forms of the class step ---------------------
+ * The entries above return their scalars to the host and synchronise their
+ * stream, as the reference's stage functions do.  The *_async entries below
+ * keep every scalar in DEVICE memory and never synchronise or allocate: a
+ * class step built from them enqueues all of its work at once, with each
+ * data-dependent decision (the flux restore factor, the product norm, the
+ * pattern's level means, the bounded add's demean/rescale/shift solve) taken
+ * by small device kernels between the field sweeps.  Per-level vectors whose
+ * names end in _dev are device arrays; z_coords stays a host array (only
+ * scalars are derived from it).  Workspaces are the same as the synchronous
+ * forms'. */
+
+/* Multiplier noise fused with the entering sums (steam/simulate.py:
+ * 2128-2188).  sums_dev (DEVICE, 3 doubles) = { sum F over the window,
+ * sum |eps| over the window, count of nonzero eps over the window }. */
+int steam_flux_noise_async(int dtype, const steam_region_t* region, double alpha,
+                           double per_class_scale, double shift, int32_t n_zero,
+                           int32_t zero_bottom, int32_t zero_top, const void* flux,
+                           void* product, const steam_window_t* window,
+                           double* sums_dev, void* workspace, size_t workspace_bytes,
+                           steam_stream_t stream);
+
+/* Separable convolution (steam/utils.py:293-427).  pre_dev (DEVICE, [2][nz]
+ * of the call's dtype, may be NULL) scales the input: f' = (f / pre[0][z]) *
+ * pre[1][z].  With STEAM_EPI_FLUX, sums_dev (DEVICE, 2 doubles) = { sum F
+ * over the window after the clip, count of F + conv < 0 }. */
+int steam_conv_separable_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                               const steam_sepconv_t* spec, const double* z_taps,
+                               const double* y_taps, const double* x_taps, const void* in,
+                               const void* pre_dev, void* out, int32_t epilogue,
+                               const steam_window_t* window, double* sums_dev,
+                               void* workspace, size_t workspace_bytes,
+                               steam_stream_t stream);
+
+/* The flux advance's volume-mean restore (steam/simulate.py:2204-2218) from
+ * the device sums of the two calls above: F *= T(entering / realized), or
+ * F = T(entering) when the realized mean is not positive.  cells = window
+ * cells x nz.  ledger_dev (DEVICE, 10 doubles, may be NULL) = { entering sum,
+ * cells, sum |eps|, nonzero eps, realized sum, cells, clipped count,
+ * S scale 1/mean|eps| rounded to the dtype, restore factor, fill flag }. */
+int steam_flux_finish_async(int dtype, int64_t n, void* flux, const double* noise_sums_dev,
+                            const double* conv_sums_dev, double cells, double* ledger_dev,
+                            steam_stream_t stream);
+
+/* The scalar pattern's per-level vectors (steam/simulate.py:2787-2930),
+ * built once per class: vecs_dev (DEVICE, [6][nz] of the dtype) = mean,
+ * np.gradient's three z coefficients, aspect, taper buffer (1 when buffer_b
+ * is NULL).  Synchronises (set-up, not the step). */
+int steam_scalar_pattern_vectors(int dtype, int64_t nz, const double* mean_1d,
+                                 const double* z_coords, const double* aspect,
+                                 const double* buffer_b, void* vecs_dev,
+                                 steam_stream_t stream);
+
+/* steam_scalar_pattern with its per-level vectors and the S scale on the
+ * device (s_scale_dev: one double, e.g. the flux ledger's entry 7).
+ * level_sums_dev (DEVICE, [2][nz]) = { sum |W|, count W != 0 } per level
+ * over the window. */
+int steam_scalar_pattern_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                               const void* pert, const void* vecs_dev, const void* product,
+                               const double* s_scale_dev, double dx, double dy,
+                               const double* z_coords, int32_t has_taper, double phi_min,
+                               double phi_max, void* w_out, const steam_window_t* window,
+                               double* level_sums_dev, void* workspace,
+                               size_t workspace_bytes, steam_stream_t stream);
+
+/* The second convolution's input scaling from the pattern's level sums
+ * (steam/simulate.py:1989-1992): pre_dev[0][z] = level mean |W| rounded to
+ * the dtype (1 where not positive), pre_dev[1][z] = mul_dev[z] (C_k). */
+int steam_pattern_norm_async(int dtype, int64_t nz, const double* level_sums_dev,
+                             const double* mul_dev, void* pre_dev, steam_stream_t stream);
+
+/* steam_bounded_add with the level means on the device (mean_dev, nz
+ * doubles) and its ledger written to ledger_dev (DEVICE, [nz][5], may be
+ * NULL).  The launch sequence is fixed (one stats sweep, n_rescale rescale
+ * sweeps, 48 shift sweeps, one apply sweep); sweeps whose phase has ended
+ * exit at once. */
+int steam_bounded_add_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
+                            const double* mean_dev, void* increment, double phi_min,
+                            double phi_max, const steam_window_t* window, int32_t n_rescale,
+                            int32_t record_applied, double* ledger_dev, void* workspace,
+                            size_t workspace_bytes, steam_stream_t stream);
+
+/* steam_thermo with its level profiles on the device: prof_dev (DEVICE,
+ * [4][nz] doubles) = z, dz (z[k+1] - z[k], last 0), h mean, qt mean; compose
+ * != 0 adds and clamps the means as steam_thermo does with h_mean/qt_mean. */
+int steam_thermo_async(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* h,
+                       const void* qt, const double* prof_dev, int32_t compose,
+                       const double* bounds, double surface_pressure,
+                       const double* ps_field_dev, void* T, void* qv, void* qc, void* qi,
+                       void* p, steam_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

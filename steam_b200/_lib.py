@@ -98,6 +98,30 @@ _SIGNATURES = {
                                     c_vp, c_vp]),
     "steam_kernel_build": (ctypes.c_int, [ctypes.c_int, c_dbl, c_dbl, c_dbl, c_dbl, c_dbl,
                                           c_i32, c_vp, c_i64p, c_vp]),
+    "steam_flux_noise_async": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Region), c_dbl,
+                                              c_dbl, c_dbl, c_i32, c_i32, c_i32, c_vp, c_vp,
+                                              ctypes.POINTER(Window), c_vp, c_vp, c_size,
+                                              c_vp]),
+    "steam_conv_separable_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64,
+                                                  ctypes.POINTER(SepConv), c_dp, c_dp, c_dp,
+                                                  c_vp, c_vp, c_vp, c_i32,
+                                                  ctypes.POINTER(Window), c_vp, c_vp, c_size,
+                                                  c_vp]),
+    "steam_flux_finish_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_vp, c_vp, c_vp, c_dbl,
+                                               c_vp, c_vp]),
+    "steam_scalar_pattern_vectors": (ctypes.c_int, [ctypes.c_int, c_i64, c_dp, c_dp, c_dp,
+                                                    c_dp, c_vp, c_vp]),
+    "steam_scalar_pattern_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
+                                                  c_vp, c_vp, c_vp, c_dbl, c_dbl, c_dp, c_i32,
+                                                  c_dbl, c_dbl, c_vp, ctypes.POINTER(Window),
+                                                  c_vp, c_vp, c_size, c_vp]),
+    "steam_pattern_norm_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_vp, c_vp, c_vp, c_vp]),
+    "steam_bounded_add_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_vp,
+                                               c_vp, c_dbl, c_dbl, ctypes.POINTER(Window),
+                                               c_i32, c_i32, c_vp, c_vp, c_size, c_vp]),
+    "steam_thermo_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_vp, c_vp,
+                                          c_i32, c_dp, c_dbl, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                          c_vp, c_vp]),
 }
 
 _lock = threading.Lock()

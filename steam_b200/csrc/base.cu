@@ -126,6 +126,87 @@ extern "C" int steam_accumulate_levels(int dtype, int64_t nx, int64_t ny,
   return fail(STEAM_ERR_ARG, "steam_accumulate_levels: bad dtype");
 }
 
+// ---- flux advance, device-side finish ---------------------------------------------
+// The volume-mean restore of the flux advance (steam/simulate.py:2204-2218)
+// with its scalars read from device memory: every thread derives the same
+// factor from the entering and realized sums, so no host round trip is
+// needed between the convolution and the restore.
+template <typename T>
+__device__ __forceinline__ void flux_factor(const double* ns, const double* cs, double cells,
+                                            T& factor, int& fill) {
+  const double c = cells > 1.0 ? cells : 1.0;
+  const double entering = ns[0] / c, realized = cs[0] / c;
+  fill = !(realized > 0.0);
+  factor = fill ? (T)entering : (T)(entering / realized);
+}
+
+template <typename T>
+__global__ void flux_finish_kernel(int64_t n, T* __restrict__ f, const double* __restrict__ ns,
+                                   const double* __restrict__ cs, double cells,
+                                   double* __restrict__ ledger) {
+  T factor;
+  int fill;
+  flux_factor<T>(ns, cs, cells, factor, fill);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sizeof(T) == 4 && ((uintptr_t)f % 16) == 0) {
+    float4* f4 = reinterpret_cast<float4*>(f);
+    const int64_t n4 = n / 4;
+    for (int64_t i = i0; i < n4; i += stride) {
+      float4 v = f4[i];
+      if (fill) {
+        v.x = v.y = v.z = v.w = (float)factor;
+      } else {
+        v.x = __fmul_rn(v.x, (float)factor);
+        v.y = __fmul_rn(v.y, (float)factor);
+        v.z = __fmul_rn(v.z, (float)factor);
+        v.w = __fmul_rn(v.w, (float)factor);
+      }
+      f4[i] = v;
+    }
+    for (int64_t i = 4 * n4 + i0; i < n; i += stride) f[i] = fill ? factor : mul_rn(f[i], factor);
+  } else {
+    for (int64_t i = i0; i < n; i += stride) f[i] = fill ? factor : mul_rn(f[i], factor);
+  }
+  if (ledger && blockIdx.x == 0 && threadIdx.x == 0) {
+    // entering (sum, cells), |noise| (sum, count), realized (sum, cells),
+    // clipped count, S scale (rounded to T), restore factor (rounded to T)
+    const double nnz = ns[2];
+    const double mean_abs = ns[1] / (nnz > 1.0 ? nnz : 1.0);
+    ledger[0] = ns[0];
+    ledger[1] = cells;
+    ledger[2] = ns[1];
+    ledger[3] = nnz;
+    ledger[4] = cs[0];
+    ledger[5] = cells;
+    ledger[6] = cs[1];
+    ledger[7] = mean_abs > 0.0 ? (double)(T)(1.0 / mean_abs) : 1.0;
+    ledger[8] = (double)factor;
+    ledger[9] = fill;
+  }
+}
+
+extern "C" int steam_flux_finish_async(int dtype, int64_t n, void* flux,
+                                       const double* noise_sums_dev,
+                                       const double* conv_sums_dev, double cells,
+                                       double* ledger_dev, steam_stream_t stream) {
+  STEAM_REQUIRE(n >= 0, "steam_flux_finish_async: negative size");
+  STEAM_REQUIRE(noise_sums_dev && conv_sums_dev, "steam_flux_finish_async: null sums");
+  STEAM_REQUIRE(n == 0 || flux, "steam_flux_finish_async: null flux");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid = stride_grid(n > 0 ? (n + 3) / 4 : 1, 256);
+  if (dtype == STEAM_F32)
+    flux_finish_kernel<float><<<grid, 256, 0, s>>>(n, (float*)flux, noise_sums_dev,
+                                                   conv_sums_dev, cells, ledger_dev);
+  else if (dtype == STEAM_F64)
+    flux_finish_kernel<double><<<grid, 256, 0, s>>>(n, (double*)flux, noise_sums_dev,
+                                                    conv_sums_dev, cells, ledger_dev);
+  else
+    return fail(STEAM_ERR_ARG, "steam_flux_finish_async: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_flux_finish_async");
+  return STEAM_OK;
+}
+
 extern "C" const char* steam_last_error(void) { return g_last_error.c_str(); }
 
 extern "C" int steam_version(void) { return 1; }

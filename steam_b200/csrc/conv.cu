@@ -624,18 +624,21 @@ static int launch_fused(const SepParams<T>& p, int64_t grid, const T* in, T* out
 template <typename T>
 static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
                      const void* in_v, const double* pre_div,
-                     const double* pre_mul, void* out_v, int epilogue,
-                     const steam_window_t* win, double* sums_out, void* ws,
-                     size_t ws_bytes, cudaStream_t s) {
+                     const double* pre_mul, const T* pre_dev, void* out_v, int epilogue,
+                     const steam_window_t* win, double* sums_out, double* totals_dev,
+                     void* ws, size_t ws_bytes, cudaStream_t s) {
   const int64_t grid = fused_grid(nx, ny, nz);
   Carver c(ws, ws_bytes);
-  const bool use_pre = pre_div != nullptr || pre_mul != nullptr;
+  const bool use_pre = pre_div != nullptr || pre_mul != nullptr || pre_dev != nullptr;
   T* pre = c.take<T>((size_t)2 * nz);
   double* partials = c.take<double>((size_t)grid * 2);
   double* totals = c.take<double>(2);
   if (!pre || !partials || !totals)
     return fail(STEAM_ERR_WORKSPACE, "steam_conv_separable: workspace too small");
-  if (use_pre) {
+  if (totals_dev) totals = totals_dev;
+  if (pre_dev) {
+    pre = const_cast<T*>(pre_dev);
+  } else if (use_pre) {
     std::vector<T> h(2 * nz);
     for (int64_t z = 0; z < nz; ++z) {
       h[z] = pre_div ? (T)pre_div[z] : (T)1;
@@ -666,6 +669,7 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
   if (epilogue == STEAM_EPI_FLUX) {
     int rc = reduce_partials(partials, (int)grid, 2, totals, s);
     if (rc) return rc;
+    if (totals_dev) return STEAM_OK;
     double h[2];
     STEAM_CUDA(cudaMemcpyAsync(h, totals, sizeof(h), cudaMemcpyDeviceToHost, s));
     STEAM_CUDA(cudaStreamSynchronize(s));
@@ -680,9 +684,9 @@ template <typename T>
 static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                          const steam_sepconv_t* spec, const double* zt,
                          const double* yt, const double* xt, const void* in_v,
-                         const double* pre_div, const double* pre_mul,
+                         const double* pre_div, const double* pre_mul, const T* pre_dev,
                          void* out_v, int epilogue, const steam_window_t* win,
-                         double* sums_out, void* ws, size_t ws_bytes,
+                         double* sums_out, double* totals_dev, void* ws, size_t ws_bytes,
                          cudaStream_t s) {
   SepParams<T>* pp = new SepParams<T>();
   std::unique_ptr<SepParams<T>> guard(pp);
@@ -692,13 +696,13 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   const int64_t plane = nx * ny * nz;
   if (fused_supported(p) && fused_grid(nx, ny, nz) < ((int64_t)1 << 31) &&
       ny * nz < ((int64_t)1 << 31))
-    return run_fused<T>(nx, ny, nz, p, in_v, pre_div, pre_mul, out_v, epilogue,
-                        win, sums_out, ws, ws_bytes, s);
+    return run_fused<T>(nx, ny, nz, p, in_v, pre_div, pre_mul, pre_dev, out_v, epilogue,
+                        win, sums_out, totals_dev, ws, ws_bytes, s);
   Carver c(ws, ws_bytes);
   T* u = c.take<T>((size_t)p.nzf * plane);
   T* v = c.take<T>((size_t)p.npairs * plane);
   T* pre = nullptr;
-  const bool use_pre = pre_div != nullptr || pre_mul != nullptr;
+  const bool use_pre = pre_div != nullptr || pre_mul != nullptr || pre_dev != nullptr;
   if (use_pre) pre = c.take<T>((size_t)2 * nz);
   int xgrid = stride_grid(((nx + kTX - 1) / kTX) * ((ny * nz + kTE - 1) / kTE), 1, 4);
   double* partials = c.take<double>((size_t)xgrid * 2);
@@ -708,7 +712,10 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                 "steam_conv_separable: workspace too small");
   const T* in = (const T*)in_v;
   T* out = (T*)out_v;
-  if (use_pre) {
+  if (totals_dev) totals = totals_dev;
+  if (pre_dev) {
+    pre = const_cast<T*>(pre_dev);
+  } else if (use_pre) {
     std::vector<T> h(2 * nz);
     for (int64_t z = 0; z < nz; ++z) {
       h[z] = pre_div ? (T)pre_div[z] : (T)1;
@@ -772,6 +779,7 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   if (epilogue == STEAM_EPI_FLUX) {
     rc = reduce_partials(partials, xgrid, 2, totals, s);
     if (rc) return rc;
+    if (totals_dev) return STEAM_OK;
     double h[2];
     STEAM_CUDA(cudaMemcpyAsync(h, totals, sizeof(h), cudaMemcpyDeviceToHost, s));
     STEAM_CUDA(cudaStreamSynchronize(s));
@@ -843,13 +851,50 @@ extern "C" int steam_conv_separable(
   cudaStream_t s = (cudaStream_t)stream;
   if (dtype == STEAM_F32)
     return run_separable<float>(nx, ny, nz, spec, z_taps, y_taps, x_taps, in,
-                                pre_div, pre_mul, out, epilogue, window,
-                                sums_out, workspace, workspace_bytes, s);
+                                pre_div, pre_mul, nullptr, out, epilogue, window,
+                                sums_out, nullptr, workspace, workspace_bytes, s);
   if (dtype == STEAM_F64)
     return run_separable<double>(nx, ny, nz, spec, z_taps, y_taps, x_taps, in,
-                                 pre_div, pre_mul, out, epilogue, window,
-                                 sums_out, workspace, workspace_bytes, s);
+                                 pre_div, pre_mul, nullptr, out, epilogue, window,
+                                 sums_out, nullptr, workspace, workspace_bytes, s);
   return fail(STEAM_ERR_ARG, "steam_conv_separable: bad dtype");
+}
+
+extern "C" int steam_conv_separable_async(
+    int dtype, int64_t nx, int64_t ny, int64_t nz, const steam_sepconv_t* spec,
+    const double* z_taps, const double* y_taps, const double* x_taps,
+    const void* in, const void* pre_dev, void* out, int32_t epilogue,
+    const steam_window_t* window, double* sums_dev, void* workspace,
+    size_t workspace_bytes, steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0,
+                "steam_conv_separable_async: negative extent");
+  STEAM_REQUIRE(spec && z_taps && y_taps && x_taps,
+                "steam_conv_separable_async: null spec or taps");
+  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || epilogue == STEAM_EPI_FLUX,
+                "steam_conv_separable_async: unknown epilogue");
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_dev,
+                "steam_conv_separable_async: flux epilogue needs sums_dev");
+  if (window) {
+    STEAM_REQUIRE(window->x0 >= 0 && window->x1 <= nx &&
+                      window->x0 <= window->x1 && window->y0 >= 0 &&
+                      window->y1 <= ny && window->y0 <= window->y1,
+                  "steam_conv_separable_async: window outside the array");
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nx * ny * nz == 0) {
+    if (epilogue == STEAM_EPI_FLUX) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
+    return STEAM_OK;
+  }
+  STEAM_REQUIRE(in && out, "steam_conv_separable_async: null field pointer");
+  if (dtype == STEAM_F32)
+    return run_separable<float>(nx, ny, nz, spec, z_taps, y_taps, x_taps, in, nullptr,
+                                nullptr, (const float*)pre_dev, out, epilogue, window, nullptr,
+                                sums_dev, workspace, workspace_bytes, s);
+  if (dtype == STEAM_F64)
+    return run_separable<double>(nx, ny, nz, spec, z_taps, y_taps, x_taps, in, nullptr,
+                                 nullptr, (const double*)pre_dev, out, epilogue, window,
+                                 nullptr, sums_dev, workspace, workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_conv_separable_async: bad dtype");
 }
 
 extern "C" int steam_conv_dense(int dtype, int64_t nx, int64_t ny, int64_t nz,

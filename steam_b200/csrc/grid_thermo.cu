@@ -356,6 +356,48 @@ extern "C" int steam_kernel_build(int dtype, double k, double dx, double dy,
   return STEAM_OK;
 }
 
+extern "C" int steam_thermo_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                  const void* h, const void* qt, const double* prof_dev,
+                                  int32_t compose, const double* bounds,
+                                  double surface_pressure, const double* ps_field_dev,
+                                  void* T, void* qv, void* qc, void* qi, void* p,
+                                  steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_thermo_async: negative extent");
+  const int64_t ncol = nx * ny;
+  if (ncol * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(h && qt && prof_dev && T && qv && qc && qi && p,
+                "steam_thermo_async: null pointer");
+  STEAM_REQUIRE(!compose || bounds != nullptr,
+                "steam_thermo_async: composing with mean profiles needs bounds");
+  cudaStream_t s = (cudaStream_t)stream;
+  const double b0 = compose ? bounds[0] : 0.0, b1 = compose ? bounds[1] : 0.0;
+  const double b2 = compose ? bounds[2] : 0.0, b3 = compose ? bounds[3] : 0.0;
+  const int64_t blocks = (ncol + 32 * kThWarps - 1) / (32 * kThWarps);
+  const size_t sm_f = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(float);
+  const size_t sm_d = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(double);
+  const double* zv = prof_dev;
+  if (dtype == STEAM_F32) {
+    STEAM_CUDA(cudaFuncSetAttribute(thermo_kernel<float>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_f));
+    thermo_kernel<float><<<(unsigned)blocks, 32 * kThWarps, sm_f, s>>>(
+        (const float*)h, (const float*)qt, zv, zv + nz, zv + 2 * nz, zv + 3 * nz, compose,
+        (float)b0, (float)b1, (float)b2, (float)b3, ncol, (int)nz, surface_pressure,
+        ps_field_dev, thermo_const<float>(), (float*)T, (float*)qv, (float*)qc, (float*)qi,
+        (float*)p);
+  } else if (dtype == STEAM_F64) {
+    STEAM_CUDA(cudaFuncSetAttribute(thermo_kernel<double>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_d));
+    thermo_kernel<double><<<(unsigned)blocks, 32 * kThWarps, sm_d, s>>>(
+        (const double*)h, (const double*)qt, zv, zv + nz, zv + 2 * nz, zv + 3 * nz, compose, b0,
+        b1, b2, b3, ncol, (int)nz, surface_pressure, ps_field_dev, thermo_const<double>(),
+        (double*)T, (double*)qv, (double*)qc, (double*)qi, (double*)p);
+  } else {
+    return fail(STEAM_ERR_ARG, "steam_thermo_async: bad dtype");
+  }
+  STEAM_LAUNCH_CHECK("steam_thermo_async");
+  return STEAM_OK;
+}
+
 extern "C" int steam_thermo(int dtype, int64_t nx, int64_t ny, int64_t nz,
                             const void* h, const void* qt,
                             const double* z_values, const double* h_mean,

@@ -195,6 +195,7 @@ struct PatternArgs {
   int uniform_z;
   int has_prod;   // 0: no signed amplitude (W alone)
   int has_taper;  // 0: no bound taper
+  const double* s_scale_dev;  // non-NULL: s_scale is read here (device), rounded to T
 };
 
 template <typename T, int JM>
@@ -206,6 +207,7 @@ __global__ void __launch_bounds__(kLvThreads) pattern_kernel(
     int64_t ny, LevelMap m, Win w, PatternArgs<T> a, T* __restrict__ out,
     double* __restrict__ partials) {
   __shared__ double red[kLvThreads];
+  if (a.s_scale_dev) a.s_scale = (T)a.s_scale_dev[0];
   double acc[2][JM];
 #pragma unroll
   for (int q = 0; q < 2; ++q)
@@ -341,6 +343,7 @@ __global__ void __launch_bounds__(kLvThreads) pattern_vec_kernel(
     int64_t nx, int64_t ny, int nz, Win w, PatternArgs<T> a, T* __restrict__ out,
     double* __restrict__ partials) {
   __shared__ double red[4 * kLvThreads];
+  if (a.s_scale_dev) a.s_scale = (T)a.s_scale_dev[0];
   const int nz4 = nz >> 2;
   const int cpb = kLvThreads / nz4;
   const int t = threadIdx.x;
@@ -445,6 +448,7 @@ struct BAChain {
   const T* mu;
   const T* cand;  // [nz][kMuCand]
   const T* mean;
+  const int* run;  // device flag: the sweep returns at once when it is 0 (NULL: always run)
   int R;
   T lo, hi;
 };
@@ -465,6 +469,7 @@ __global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
     const T* __restrict__ d0, T* __restrict__ pert, T* __restrict__ inc_out,
     int record, int64_t nx, int64_t ny, LevelMap m, Win w, BAChain<T> c,
     double* __restrict__ partials) {
+  if (c.run && *c.run == 0) return;
   __shared__ double red[kLvThreads];
   extern __shared__ unsigned char ba_smem[];
   const int nz = m.nz, R = c.R;
@@ -547,6 +552,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 4)) ba_sweep4
     const T* __restrict__ d0, T* __restrict__ pert, T* __restrict__ inc_out,
     int record, int64_t nx, int64_t ny, int nz, Win w, BAChain<T> c,
     double* __restrict__ partials) {
+  if (c.run && *c.run == 0) return;
   extern __shared__ unsigned char ba_smem[];
   __shared__ double red[4 * kLvThreads];  // [cpi][nz] with cpi * nz == 4 * 256 / 4 ... <= 1024
   const int R = c.R;
@@ -803,33 +809,35 @@ static size_t level_partial_bytes(int64_t nz, int q) {
 // of T.  Each sweep evaluates kMuCand candidates (the Newton point, two
 // points straddling it, the bracket midpoint); the solve ends when no value
 // of T lies strictly inside the bracket, and returns its midpoint, as the
-// bisection does.
+// bisection does.  The solver state lives in device memory, one per level,
+// and is advanced by the update kernels between sweeps.
+template <typename T>
+__host__ __device__ inline double next_up_t(double x) {
+  if (sizeof(T) == 4) return (double)nextafterf((float)x, INFINITY);
+  return nextafter(x, (double)INFINITY);
+}
+
 template <typename T>
 struct MuSolver {
   double a, b;
   double best_mu, best_m, best_slope;
-  bool have_best = false;
-  bool done = false;
-
-  double abs_tol = 0.0;
+  double abs_tol;
+  int have_best;
+  int done;
 
   // abs_tol: a bracket this narrow is accepted as converged.  In float32 the
   // level mean is a staircase in mu at the scale of the field's own ulps, so
   // below that scale any mu of the bracket gives the same field up to
   // single-ulp flips in a vanishing fraction of cells.
-  void init(double width, double tol) {
+  __host__ __device__ void init(double width, double tol) {
     a = (double)(T)(-width);
     b = (double)(T)width;
     abs_tol = tol;
-    have_best = false;
-    done = false;
+    have_best = 0;
+    done = 0;
   }
 
-  static double next_up(double x) {
-    return (double)nextafter((T)x, (T)INFINITY);
-  }
-
-  void candidates(double* out) const {
+  __host__ __device__ void candidates(double* out) const {
     const double mid = 0.5 * (a + b);
     double c0 = mid;
     if (have_best && best_slope < 0.0) {
@@ -847,7 +855,7 @@ struct MuSolver {
   }
 
   // cand: the T-rounded candidates actually evaluated.
-  void update(const double* cand, const double* mval, const double* slope) {
+  __host__ __device__ void update(const double* cand, const double* mval, const double* slope) {
     for (int k = 0; k < kMuCand; ++k) {
       if (cand[k] <= a || cand[k] >= b) continue;
       if (mval[k] > 0.0)
@@ -859,98 +867,314 @@ struct MuSolver {
     for (int k = 0; k < kMuCand; ++k)
       if (kb < 0 || fabs(mval[k]) < fabs(mval[kb])) kb = k;
     if (kb >= 0) {
-      have_best = true;
+      have_best = 1;
       best_mu = cand[kb];
       best_m = mval[kb];
       best_slope = slope[kb];
     }
-    if (next_up(a) >= b || b - a <= abs_tol) done = true;
+    if (next_up_t<T>(a) >= b || b - a <= abs_tol) done = 1;
   }
-  double result() const { return 0.5 * (a + b); }
+  __host__ __device__ double result() const { return 0.5 * (a + b); }
+};
+
+// Most mu sweeps a solve may take (the bracket at least halves per sweep).
+constexpr int kMuMaxSweeps = 48;
+
+// Writable view of the chain the sweeps replay, plus the solver's state.
+template <typename T>
+struct BAState {
+  int* nsteps;
+  T* demean;  // [nz][R]
+  T* scale;   // [nz][R]
+  int* has_final;
+  T* final_dm;
+  int* has_mu;
+  T* mu;
+  T* cand;  // [nz][kMuCand]
+  T* mean;
+  double* a0;
+  double* cur_mean;
+  double* final_d;
+  int* active;
+  int* still;
+  int* n_loop;
+  int* need;
+  MuSolver<T>* solver;
+  // run flags: [0] the first sweep, [1 + k] rescale sweep k (k < R),
+  // [1 + R + it] mu sweep it (it < kMuMaxSweeps); [kFlagSweeps] sweeps run
+  int* flags;
+  int R, nz;
+  double N, width, tol_rel;
+  double* ledger;  // [nz][5]: a0, n_loop, final demean, mu (NaN if none), sweeps
 };
 
 template <typename T>
-static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
-                            const double* mean_1d, T* inc, double phi_min,
-                            double phi_max, const steam_window_t* window,
-                            int R, int record, double* ledger_out, void* ws,
-                            size_t ws_bytes, cudaStream_t s) {
+__host__ __device__ inline int ba_flag_count(int R) {
+  return 2 + R + kMuMaxSweeps;
+}
+
+// chain reset and the mean profile, in the working dtype
+template <typename T>
+__global__ void ba_init_kernel(BAState<T> st, const double* __restrict__ mean_1d) {
+  const int nz = st.nz, R = st.R;
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    st.nsteps[z] = 0;
+    st.has_final[z] = 0;
+    st.has_mu[z] = 0;
+    st.final_dm[z] = (T)0;
+    st.mu[z] = (T)0;
+    st.mean[z] = (T)mean_1d[z];
+    for (int k = 0; k < R; ++k) {
+      st.demean[z * R + k] = (T)0;
+      st.scale[z * R + k] = (T)1;
+    }
+    for (int k = 0; k < kMuCand; ++k) st.cand[z * kMuCand + k] = (T)0;
+    st.active[z] = 0;
+    st.still[z] = 0;
+    st.n_loop[z] = 0;
+    st.need[z] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int nf = ba_flag_count<T>(R);
+    for (int i = 0; i < nf; ++i) st.flags[i] = 0;
+    st.flags[0] = 1;  // the first stats sweep always runs
+  }
+}
+
+// reduce_partials_kernel that does nothing when its sweep did not run
+__global__ void reduce_partials_if_kernel(const double* __restrict__ partials, int nblocks,
+                                          double* __restrict__ out, const int* __restrict__ run) {
+  if (run && *run == 0) return;
+  __shared__ double scratch[32];
+  const double* src = partials + (size_t)blockIdx.x * nblocks;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) acc += src[i];
+  double s = block_sum(acc, scratch);
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+// Leaves the demean/clip/rescale loop: the final demean is the level's
+// current mean, and its shift solve starts from a bracket symmetric about 0.
+template <typename T>
+__device__ void ba_leave_loop(BAState<T>& st, int z) {
+  st.still[z] = 0;
+  st.final_d[z] = st.cur_mean[z];
+  st.has_final[z] = 1;
+  st.final_dm[z] = (T)st.cur_mean[z];
+}
+
+// Prepares rescale step k for a level still in the loop.
+template <typename T>
+__device__ void ba_prepare_step(BAState<T>& st, int z, int k, int* next_flag) {
+  st.demean[z * st.R + k] = (T)st.cur_mean[z];
+  st.scale[z * st.R + k] = (T)1;
+  st.nsteps[z] = k + 1;
+  st.n_loop[z] = k + 1;
+  atomicOr(next_flag, 1);
+}
+
+template <typename T>
+__device__ void ba_count_sweep(BAState<T>& st) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
+}
+
+// After the first stats sweep: a0 = mean|d| and the entering mean.
+template <typename T>
+__global__ void ba_a0_kernel(BAState<T> st, const double* __restrict__ tot) {
+  const int nz = st.nz;
+  ba_count_sweep(st);
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    const double a0 = tot[nz + z] / st.N;
+    st.a0[z] = a0;
+    st.cur_mean[z] = tot[z] / st.N;
+    if (a0 <= 0.0) {
+      st.has_final[z] = 1;  // clip only
+      st.final_dm[z] = (T)0;
+      st.final_d[z] = 0.0;
+      continue;
+    }
+    st.active[z] = 1;
+    st.still[z] = 1;
+    if (st.R > 0)
+      ba_prepare_step(st, z, 0, &st.flags[1]);
+    else
+      ba_leave_loop(st, z);
+  }
+}
+
+// After rescale sweep k.
+template <typename T>
+__global__ void ba_loop_kernel(BAState<T> st, const double* __restrict__ tot, int k) {
+  if (st.flags[1 + k] == 0) return;
+  const int nz = st.nz;
+  ba_count_sweep(st);
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    if (!st.still[z]) continue;
+    const double sum_d = tot[z], m_abs = tot[nz + z] / st.N;
+    st.cur_mean[z] = sum_d / st.N;
+    bool go = true;
+    if (m_abs <= 0.0) {
+      go = false;
+    } else {
+      double sc = st.a0[z] / m_abs;
+      if (sc > 2.0) sc = 2.0;
+      if (fabs(sc - 1.0) < 1e-4) {
+        go = false;
+      } else {
+        st.scale[z * st.R + k] = (T)sc;
+        st.cur_mean[z] = (double)(T)sc * sum_d / st.N;
+      }
+    }
+    if (go && k + 1 < st.R)
+      ba_prepare_step(st, z, k + 1, &st.flags[2 + k]);
+    else
+      ba_leave_loop(st, z);
+  }
+}
+
+// After the loop: every active level starts its shift solve.  Its first
+// candidate is mu = 0, whose mean is the post-clip level mean.
+template <typename T>
+__global__ void ba_mu_init_kernel(BAState<T> st) {
+  const int nz = st.nz;
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    if (!st.active[z]) continue;
+    st.need[z] = 1;
+    MuSolver<T> sv;
+    sv.init(st.width, st.a0[z] * st.tol_rel);
+    double c[kMuCand];
+    sv.candidates(c);
+    for (int q = 0; q < kMuCand; ++q) st.cand[z * kMuCand + q] = (T)c[q];
+    st.solver[z] = sv;
+    atomicOr(&st.flags[1 + st.R], 1);
+  }
+}
+
+// After mu sweep it.
+template <typename T>
+__global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int it) {
+  if (st.flags[1 + st.R + it] == 0) return;
+  const int nz = st.nz;
+  ba_count_sweep(st);
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    if (!st.need[z]) continue;
+    MuSolver<T> sv = st.solver[z];
+    if (sv.done) continue;
+    double mv[kMuCand], sl[kMuCand], cv[kMuCand];
+    for (int q = 0; q < kMuCand; ++q) {
+      // the candidate actually evaluated is the dtype-rounded one
+      cv[q] = (double)st.cand[z * kMuCand + q];
+      mv[q] = tot[(size_t)(2 * q) * nz + z] / st.N;
+      sl[q] = -tot[(size_t)(2 * q + 1) * nz + z] / st.N;
+    }
+    if (it == 0 && fabs(mv[0]) <= 1e-9 * st.a0[z]) {
+      st.need[z] = 0;  // the final clip left the level mean-free
+      continue;
+    }
+    sv.update(cv, mv, sl);
+    if (!sv.done && it + 1 < kMuMaxSweeps) {
+      double c[kMuCand];
+      sv.candidates(c);
+      for (int q = 0; q < kMuCand; ++q) st.cand[z * kMuCand + q] = (T)c[q];
+      atomicOr(&st.flags[2 + st.R + it], 1);
+    }
+    st.solver[z] = sv;
+  }
+}
+
+// Fixes mu for the levels that needed a shift and writes the ledger.
+template <typename T>
+__global__ void ba_finish_kernel(BAState<T> st) {
+  const int nz = st.nz;
+  const int sweeps = st.flags[ba_flag_count<T>(st.R) - 1] + 1;  // + the apply sweep
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    double mu = __longlong_as_double(0x7ff8000000000000LL);  // NaN: no shift
+    if (st.need[z]) {
+      mu = st.solver[z].result();
+      st.has_mu[z] = 1;
+      st.mu[z] = (T)mu;
+    }
+    if (st.ledger) {
+      double* l = st.ledger + 5 * (size_t)z;
+      l[0] = st.a0[z];
+      l[1] = st.n_loop[z];
+      l[2] = st.active[z] ? st.final_d[z] : 0.0;
+      l[3] = mu;
+      l[4] = sweeps;
+    }
+  }
+}
+
+static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
+  return carve_bytes((size_t)3 * nz, sizeof(int)) +                       // nsteps, has_final, has_mu
+         carve_bytes((size_t)nz * (2 * (size_t)R + 4 + kMuCand), elem) +   // chain values
+         carve_bytes((size_t)3 * nz, sizeof(double)) +                      // a0, cur_mean, final_d
+         carve_bytes((size_t)4 * nz, sizeof(int)) +                         // active, still, n_loop, need
+         carve_bytes((size_t)nz * sizeof(MuSolver<double>), 1) +
+         carve_bytes((size_t)(2 + R + kMuMaxSweeps), sizeof(int)) +
+         carve_bytes((size_t)5 * nz, sizeof(double)) +                      // ledger
+         carve_bytes((size_t)nz, sizeof(double));                           // mean upload
+}
+
+// Enqueues the whole bounded add on stream s: no host synchronisation and no
+// host decision between sweeps.  Sweeps whose phase has ended return at once
+// (their run flag is 0), so the launch sequence is fixed: one stats sweep,
+// R rescale sweeps, kMuMaxSweeps shift sweeps, one apply sweep.  mean_dev
+// (device, nz doubles) is the level mean profile; the ledger ends in
+// st.ledger (device, [nz][5]).
+template <typename T>
+static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
+                               const double* mean_dev, T* inc, double phi_min,
+                               double phi_max, const steam_window_t* window, int R,
+                               int record, Carver& c, double** ledger_dev,
+                               cudaStream_t s) {
   const LevelMap m = make_map(nz);
   const int64_t ncol = nx * ny;
   const int grid = level_grid(ncol, m);
   const Win w = make_win(window, nx, ny);
-  const double N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
   const int Qmax = 2 * kMuCand;
-  Carver c(ws, ws_bytes);
   double* partials = c.take<double>((size_t)grid * Qmax * nz);
   double* totals = c.take<double>((size_t)Qmax * nz);
-  // All per-level chain parameters live in one block, mirrored on the host
-  // and pushed with a single copy per sweep.
-  const size_t n_int = (size_t)3 * nz;
-  const size_t n_t = (size_t)nz * (2 * (size_t)R + 3 + kMuCand);
-  const size_t blk_bytes = ((n_int * sizeof(int) + sizeof(T) - 1) / sizeof(T)) * sizeof(T) +
-                           n_t * sizeof(T);
-  unsigned char* d_blk = c.take<unsigned char>(blk_bytes);
-  if (!partials || !totals || !d_blk)
+  BAState<T> st;
+  st.nsteps = c.take<int>(nz);
+  st.has_final = c.take<int>(nz);
+  st.has_mu = c.take<int>(nz);
+  st.demean = c.take<T>((size_t)nz * (R > 0 ? R : 1));
+  st.scale = c.take<T>((size_t)nz * (R > 0 ? R : 1));
+  st.final_dm = c.take<T>(nz);
+  st.mu = c.take<T>(nz);
+  st.mean = c.take<T>(nz);
+  st.cand = c.take<T>((size_t)nz * kMuCand);
+  st.a0 = c.take<double>(nz);
+  st.cur_mean = c.take<double>(nz);
+  st.final_d = c.take<double>(nz);
+  st.active = c.take<int>(nz);
+  st.still = c.take<int>(nz);
+  st.n_loop = c.take<int>(nz);
+  st.need = c.take<int>(nz);
+  st.solver = c.take<MuSolver<T>>(nz);
+  st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
+  st.ledger = c.take<double>((size_t)5 * nz);
+  if (!partials || !totals || !st.nsteps || !st.has_final || !st.has_mu || !st.demean ||
+      !st.scale || !st.final_dm || !st.mu || !st.mean || !st.cand || !st.a0 || !st.cur_mean ||
+      !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.solver ||
+      !st.flags || !st.ledger)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
-  std::vector<unsigned char> h_blk(blk_bytes, 0);
-  int* h_nsteps_p = reinterpret_cast<int*>(h_blk.data());
-  int* h_hasfinal_p = h_nsteps_p + nz;
-  int* h_hasmu_p = h_hasfinal_p + nz;
-  T* h_t = reinterpret_cast<T*>(h_blk.data() + (blk_bytes - n_t * sizeof(T)));
-  T* h_demean_p = h_t;
-  T* h_scale_p = h_demean_p + (size_t)nz * R;
-  T* h_final_p = h_scale_p + (size_t)nz * R;
-  T* h_mu_p = h_final_p + nz;
-  T* h_mean_p = h_mu_p + nz;
-  T* h_cand_p = h_mean_p + nz;
-  auto dev = [&](const void* hp) {
-    return d_blk + (reinterpret_cast<const unsigned char*>(hp) - h_blk.data());
-  };
-  int* d_nsteps = reinterpret_cast<int*>(dev(h_nsteps_p));
-  int* d_hasfinal = reinterpret_cast<int*>(dev(h_hasfinal_p));
-  int* d_hasmu = reinterpret_cast<int*>(dev(h_hasmu_p));
-  T* d_demean = reinterpret_cast<T*>(dev(h_demean_p));
-  T* d_scale = reinterpret_cast<T*>(dev(h_scale_p));
-  T* d_final = reinterpret_cast<T*>(dev(h_final_p));
-  T* d_mu = reinterpret_cast<T*>(dev(h_mu_p));
-  T* d_mean = reinterpret_cast<T*>(dev(h_mean_p));
-  T* d_cand = reinterpret_cast<T*>(dev(h_cand_p));
-  for (int64_t z = 0; z < nz; ++z) h_mean_p[z] = (T)mean_1d[z];
-  for (size_t i = 0; i < (size_t)nz * R; ++i) h_scale_p[i] = (T)1;
-  // host views with the indexing the solve below uses
-  struct View {
-    T* p;
-    T& operator[](size_t i) { return p[i]; }
-  };
-  struct IView {
-    int* p;
-    int& operator[](size_t i) { return p[i]; }
-  };
-  View h_demean{h_demean_p}, h_scale{h_scale_p}, h_final{h_final_p}, h_mu{h_mu_p},
-      h_cand{h_cand_p};
-  IView h_nsteps{h_nsteps_p}, h_hasfinal{h_hasfinal_p}, h_hasmu{h_hasmu_p};
-  int rc;
+  st.R = R;
+  st.nz = (int)nz;
+  st.N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
+  st.width = phi_max - phi_min;
+  st.tol_rel = sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49);
+  *ledger_dev = st.ledger;
 
   const size_t ba_sm = ba_smem_bytes<T>(nz, R);
   STEAM_REQUIRE(ba_sm <= 200 * 1024, "steam_bounded_add: n_rescale * nz too large");
-  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, 1>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_MU, 1>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, 1>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, kLvMaxJ>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_MU, kLvMaxJ>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-  STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, kLvMaxJ>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
   const bool vec4 = nz % 4 == 0 && nz <= 4 * kLvThreads &&
                     ((uintptr_t)pert % 16 == 0) && ((uintptr_t)inc % 16 == 0);
   const int grid4 = vec4 ? stride_grid((ncol + (kLvThreads / (nz / 4)) - 1) /
                                            (kLvThreads / (nz / 4)), 1, kLvBlocksPerSm)
                          : 0;
+  const int sweep_grid = vec4 ? grid4 : grid;
   if (vec4) {
     STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_STATS>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
@@ -958,184 +1182,106 @@ static int bounded_add_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
     STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_APPLY>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  } else if (m.packed) {
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, 1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_MU, 1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, 1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+  } else {
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, kLvMaxJ>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_MU, kLvMaxJ>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, kLvMaxJ>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
   }
-  const int sweep_grid = vec4 ? grid4 : grid;
   BAChain<T> ch;
-  ch.nsteps = d_nsteps;
-  ch.demean = d_demean;
-  ch.scale = d_scale;
-  ch.has_final = d_hasfinal;
-  ch.final_dm = d_final;
-  ch.has_mu = d_hasmu;
-  ch.mu = d_mu;
-  ch.cand = d_cand;
-  ch.mean = d_mean;
+  ch.nsteps = st.nsteps;
+  ch.demean = st.demean;
+  ch.scale = st.scale;
+  ch.has_final = st.has_final;
+  ch.final_dm = st.final_dm;
+  ch.has_mu = st.has_mu;
+  ch.mu = st.mu;
+  ch.cand = st.cand;
+  ch.mean = st.mean;
   ch.R = R;
   ch.lo = (T)phi_min;
   ch.hi = (T)phi_max;
+  const int lv_blocks = (int)((nz + 255) / 256);
 
-  std::vector<double> tot;
-  int n_sweeps = 0;
-  auto push_chain = [&]() -> int {
-    STEAM_CUDA(cudaMemcpyAsync(d_blk, h_blk.data(), blk_bytes, cudaMemcpyHostToDevice, s));
+  auto sweep = [&](int mode, const int* run, T* out, int rec) -> int {
+    ch.run = run;
+    if (mode == BA_STATS) {
+      if (vec4)
+        ba_sweep4_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, (int)nz, w, ch, partials);
+      else if (m.packed)
+        ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+      else
+        ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+    } else if (mode == BA_MU) {
+      if (vec4)
+        ba_sweep4_kernel<T, BA_MU><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, (int)nz, w, ch, partials);
+      else if (m.packed)
+        ba_sweep_kernel<T, BA_MU, 1><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+      else
+        ba_sweep_kernel<T, BA_MU, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+    } else {
+      if (vec4)
+        ba_sweep4_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, (int)nz, w, ch, partials);
+      else if (m.packed)
+        ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+      else
+        ba_sweep_kernel<T, BA_APPLY, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+    }
+    STEAM_LAUNCH_CHECK("bounded_add sweep");
     return STEAM_OK;
   };
-  auto stats_sweep = [&]() -> int {
-    int r2 = push_chain();
-    if (r2) return r2;
-        if (vec4)
-      ba_sweep4_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
-        inc, pert, nullptr, 0, nx, ny, (int)nz, w, ch, partials);
-    else if (m.packed)
-      ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
-        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
-    else
-      ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
-        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
-    STEAM_LAUNCH_CHECK("bounded_add stats sweep");
-    if ((r2 = reduce_partials(partials, sweep_grid, 2 * (int)nz, totals, s))) return r2;
-    ++n_sweeps;
-    return fetch(tot, totals, 2 * nz, s);
+  auto reduce = [&](int nq, const int* run) -> int {
+    reduce_partials_if_kernel<<<nq, 256, 0, s>>>(partials, sweep_grid, totals, run);
+    STEAM_LAUNCH_CHECK("bounded_add reduce");
+    return STEAM_OK;
   };
-
-  // Sweep 0: a0 = mean|d|, mean d.
-  if ((rc = stats_sweep())) return rc;
-  std::vector<double> a0(nz), cur_mean(nz), final_dm(nz, 0.0),
-      mu(nz, std::numeric_limits<double>::quiet_NaN());
-  std::vector<int> active(nz, 0), n_loop(nz, 0);
-  for (int64_t z = 0; z < nz; ++z) {
-    a0[z] = tot[nz + z] / N;
-    cur_mean[z] = tot[z] / N;
-    if (a0[z] <= 0.0) {
-      h_hasfinal[z] = 1;  // clip only
-      h_final[z] = (T)0;
-    } else {
-      active[z] = 1;
-    }
-  }
-  // Demean / clip / rescale-to-A0 loop.
-  std::vector<int> still(active);
+  int rc;
+  ba_init_kernel<T><<<lv_blocks, 256, 0, s>>>(st, mean_dev);
+  STEAM_LAUNCH_CHECK("bounded_add init");
+  // sweep 0: a0 = mean|d|, mean d
+  if ((rc = sweep(BA_STATS, &st.flags[0], nullptr, 0))) return rc;
+  if ((rc = reduce(2 * (int)nz, &st.flags[0]))) return rc;
+  ba_a0_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals);
+  STEAM_LAUNCH_CHECK("bounded_add a0");
+  // demean / clip / rescale-to-A0 loop
   for (int k = 0; k < R; ++k) {
-    bool any = false;
-    for (int64_t z = 0; z < nz; ++z)
-      if (still[z]) {
-        any = true;
-        h_demean[z * R + k] = (T)cur_mean[z];
-        h_scale[z * R + k] = (T)1;
-        h_nsteps[z] = k + 1;
-        n_loop[z] = k + 1;
-      }
-    if (!any) break;
-    if ((rc = stats_sweep())) return rc;
-    for (int64_t z = 0; z < nz; ++z) {
-      if (!still[z]) continue;
-      const double sum_d = tot[z], m_abs = tot[nz + z] / N;
-      cur_mean[z] = sum_d / N;
-      if (m_abs <= 0.0) {
-        still[z] = 0;
-        continue;
-      }
-      double sc = a0[z] / m_abs;
-      if (sc > 2.0) sc = 2.0;
-      if (fabs(sc - 1.0) < 1e-4) {
-        still[z] = 0;
-        continue;
-      }
-      h_scale[z * R + k] = (T)sc;
-      cur_mean[z] = (double)(T)sc * sum_d / N;
-    }
+    if ((rc = sweep(BA_STATS, &st.flags[1 + k], nullptr, 0))) return rc;
+    if ((rc = reduce(2 * (int)nz, &st.flags[1 + k]))) return rc;
+    ba_loop_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals, k);
+    STEAM_LAUNCH_CHECK("bounded_add loop");
   }
-  // Final demean and clip.
-  for (int64_t z = 0; z < nz; ++z)
-    if (active[z]) {
-      final_dm[z] = cur_mean[z];
-      h_hasfinal[z] = 1;
-      h_final[z] = (T)cur_mean[z];
-    }
-  // Zero-mean shift mu where the final clip left a mean.  The bracket starts
-  // symmetric about 0, so the first mu sweep's first candidate is mu = 0: its
-  // mean is the mean after the final demean and clip, which decides whether
-  // the level needs a shift at all (no separate sweep for it).
-  const double width = phi_max - phi_min;
-  std::vector<MuSolver<T>> solver(nz);
-  std::vector<int> need(nz, 0);
-  bool any_mu = false;
-  for (int64_t z = 0; z < nz; ++z) {
-    if (!active[z]) continue;
-    need[z] = 1;
-    any_mu = true;
-    solver[z].init(width, a0[z] * (sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49)));
+  // zero-mean shift
+  ba_mu_init_kernel<T><<<lv_blocks, 256, 0, s>>>(st);
+  STEAM_LAUNCH_CHECK("bounded_add mu init");
+  for (int it = 0; it < kMuMaxSweeps; ++it) {
+    const int* run = &st.flags[1 + R + it];
+    if ((rc = sweep(BA_MU, run, nullptr, 0))) return rc;
+    if ((rc = reduce(Qmax * (int)nz, run))) return rc;
+    ba_mu_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals, it);
+    STEAM_LAUNCH_CHECK("bounded_add mu");
   }
-  for (int it = 0; any_mu && it < 80; ++it) {
-    std::vector<double> cands((size_t)nz * kMuCand, 0.0);
-    bool pending = false;
-    for (int64_t z = 0; z < nz; ++z) {
-      if (!need[z] || solver[z].done) continue;
-      pending = true;
-      solver[z].candidates(&cands[z * kMuCand]);
-      for (int k = 0; k < kMuCand; ++k)
-        h_cand[z * kMuCand + k] = (T)cands[z * kMuCand + k];
-    }
-    if (!pending) break;
-    if ((rc = push_chain())) return rc;
-        if (vec4)
-      ba_sweep4_kernel<T, BA_MU><<<grid4, kLvThreads, ba_sm, s>>>(
-        inc, pert, nullptr, 0, nx, ny, (int)nz, w, ch, partials);
-    else if (m.packed)
-      ba_sweep_kernel<T, BA_MU, 1><<<grid, kLvThreads, ba_sm, s>>>(
-        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
-    else
-      ba_sweep_kernel<T, BA_MU, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
-        inc, pert, nullptr, 0, nx, ny, m, w, ch, partials);
-    STEAM_LAUNCH_CHECK("bounded_add mu sweep");
-    if ((rc = reduce_partials(partials, sweep_grid, Qmax * (int)nz, totals, s))) return rc;
-    ++n_sweeps;
-    if ((rc = fetch(tot, totals, (size_t)Qmax * nz, s))) return rc;
-    for (int64_t z = 0; z < nz; ++z) {
-      if (!need[z] || solver[z].done) continue;
-      double mv[kMuCand], sl[kMuCand], cv[kMuCand];
-      for (int k = 0; k < kMuCand; ++k) {
-        // The candidate actually evaluated is the dtype-rounded one.
-        cv[k] = (double)h_cand[z * kMuCand + k];
-        mv[k] = tot[(size_t)(2 * k) * nz + z] / N;
-        sl[k] = -tot[(size_t)(2 * k + 1) * nz + z] / N;
-      }
-      if (it == 0 && fabs(mv[0]) <= 1e-9 * a0[z]) {
-        need[z] = 0;  // the final clip left the level mean-free
-        continue;
-      }
-      solver[z].update(cv, mv, sl);
-    }
-  }
-  for (int64_t z = 0; z < nz; ++z)
-    if (need[z]) {
-      mu[z] = solver[z].result();
-      h_hasmu[z] = 1;
-      h_mu[z] = (T)mu[z];
-    }
-  // Apply.
-  if ((rc = push_chain())) return rc;
-    if (vec4)
-    ba_sweep4_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_sm, s>>>(
-      inc, pert, inc, record, nx, ny, (int)nz, w, ch, partials);
-  else if (m.packed)
-    ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
-      inc, pert, inc, record, nx, ny, m, w, ch, partials);
-  else
-    ba_sweep_kernel<T, BA_APPLY, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
-      inc, pert, inc, record, nx, ny, m, w, ch, partials);
-  STEAM_LAUNCH_CHECK("bounded_add apply sweep");
-  ++n_sweeps;
-  if (ledger_out) {
-    for (int64_t z = 0; z < nz; ++z) {
-      ledger_out[5 * z + 0] = a0[z];
-      ledger_out[5 * z + 1] = n_loop[z];
-      ledger_out[5 * z + 2] = final_dm[z];
-      ledger_out[5 * z + 3] = mu[z];
-      ledger_out[5 * z + 4] = n_sweeps;
-    }
-  }
-  STEAM_CUDA(cudaStreamSynchronize(s));
+  ba_finish_kernel<T><<<lv_blocks, 256, 0, s>>>(st);
+  STEAM_LAUNCH_CHECK("bounded_add finish");
+  // apply (always runs)
+  if ((rc = sweep(BA_APPLY, nullptr, inc, record))) return rc;
   return STEAM_OK;
 }
 
@@ -1326,37 +1472,23 @@ extern "C" size_t steam_scalar_pattern_workspace_bytes(int64_t nx, int64_t ny, i
   return b;
 }
 
+// Per-level vectors of the pattern kernels, [6][nz] in T: mean, the three
+// np.gradient coefficients (indexed z - 1), aspect, taper buffer; and the
+// z scalars of PatternArgs.
 template <typename T>
-static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
-                        const double* mean_1d, const T* prod, double s_scale,
-                        double dx, double dy, const double* z_coords,
-                        const double* aspect, const double* bbuf,
-                        double phi_min, double phi_max, T* out,
-                        const steam_window_t* window, double* sums_out,
-                        void* ws, size_t ws_bytes, cudaStream_t s) {
-  const LevelMap m = make_map(nz);
-  const bool vec = pattern_vec_ok(nz) && ((uintptr_t)pert % 16 == 0) &&
-                   ((uintptr_t)out % 16 == 0) && (!prod || (uintptr_t)prod % 16 == 0);
-  const int grid = vec ? pattern_vec_grid(nx, ny, nz) : level_grid(nx * ny, m);
-  const Win w = make_win(window, nx, ny);
-  Carver c(ws, ws_bytes);
-  double* partials = c.take<double>((size_t)grid * 2 * nz);
-  double* totals = c.take<double>((size_t)2 * nz);
-  T* d_vec = c.take<T>((size_t)6 * nz);
-  if (!partials || !totals || !d_vec)
-    return fail(STEAM_ERR_WORKSPACE, "steam_scalar_pattern: workspace too small");
-  // np.gradient's z coefficients from float32 (or float64) level heights.
+static void pattern_vectors(int64_t nz, const double* mean_1d, const double* z_coords,
+                            const double* aspect, const double* bbuf, std::vector<T>& h,
+                            PatternArgs<T>& a) {
   std::vector<T> zc(nz), dz(nz > 1 ? nz - 1 : 0);
   for (int64_t z = 0; z < nz; ++z) zc[z] = (T)z_coords[z];
   for (int64_t z = 0; z + 1 < nz; ++z) dz[z] = zc[z + 1] - zc[z];
   bool uniform = true;
   for (int64_t z = 1; z + 1 < nz; ++z)
     if (dz[z] != dz[0]) uniform = false;
-  std::vector<T> h((size_t)6 * nz, (T)0);
-  // [0] mean, [1] a, [2] b, [3] c, [4] aspect, [5] buffer
+  h.assign((size_t)6 * nz, (T)0);
   for (int64_t z = 0; z < nz; ++z) {
-    h[z] = (T)mean_1d[z];
-    h[4 * nz + z] = (T)aspect[z];
+    h[z] = mean_1d ? (T)mean_1d[z] : (T)0;
+    h[4 * nz + z] = aspect ? (T)aspect[z] : (T)0;
     h[5 * nz + z] = bbuf ? (T)bbuf[z] : (T)1;
   }
   if (!uniform) {
@@ -1367,20 +1499,21 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
       h[3 * nz + z] = d1 / (d2 * (d1 + d2));
     }
   }
-  int rc = upload(d_vec, h, s);
-  if (rc) return rc;
-  PatternArgs<T> a;
-  a.two_dx = (T)(2 * dx);
-  a.two_dy = (T)(2 * dy);
   a.two_dz = uniform ? (T)2 * dz[0] : (T)0;
   a.dz_first = dz[0];
   a.dz_last = dz[nz - 2];
-  a.lo = (T)phi_min;
-  a.span = (T)(phi_max - phi_min);
-  a.s_scale = (T)s_scale;
   a.uniform_z = uniform ? 1 : 0;
-  a.has_prod = prod != nullptr;
-  a.has_taper = bbuf != nullptr;
+}
+
+// Launches the pattern kernel and the per-level reduction into totals
+// (device, [2][nz]: sum |W|, count W != 0).
+template <typename T>
+static int pattern_launch(int64_t nx, int64_t ny, int64_t nz, const T* pert, const T* d_vec,
+                          const T* prod, const PatternArgs<T>& a, T* out,
+                          const steam_window_t* window, double* partials, double* totals,
+                          int grid, bool vec, cudaStream_t s) {
+  const LevelMap m = make_map(nz);
+  const Win w = make_win(window, nx, ny);
   if (vec) {
     pattern_vec_kernel<T><<<grid, kLvThreads, 0, s>>>(pert, d_vec, prod, nx, ny, (int)nz, w, a,
                                                        out, partials);
@@ -1393,8 +1526,54 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
       pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
       d_vec + 4 * nz, d_vec + 5 * nz, nx, ny, m, w, a, out, partials);
   STEAM_LAUNCH_CHECK("steam_scalar_pattern");
-  rc = reduce_partials(partials, grid, 2 * (int)nz, totals, s);
-  if (rc) return rc;
+  return reduce_partials(partials, grid, 2 * (int)nz, totals, s);
+}
+
+template <typename T>
+static bool pattern_use_vec(int64_t nz, const T* pert, const T* out, const T* prod) {
+  return pattern_vec_ok(nz) && ((uintptr_t)pert % 16 == 0) && ((uintptr_t)out % 16 == 0) &&
+         (!prod || (uintptr_t)prod % 16 == 0);
+}
+
+template <typename T>
+static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
+                        const double* mean_1d, const T* prod, double s_scale,
+                        double dx, double dy, const double* z_coords,
+                        const double* aspect, const double* bbuf,
+                        double phi_min, double phi_max, T* out,
+                        const steam_window_t* window, double* sums_out,
+                        const double* s_scale_dev, const T* vecs_dev, double* sums_dev,
+                        void* ws, size_t ws_bytes, cudaStream_t s) {
+  const LevelMap m = make_map(nz);
+  const bool vec = pattern_use_vec<T>(nz, pert, out, prod);
+  const int grid = vec ? pattern_vec_grid(nx, ny, nz) : level_grid(nx * ny, m);
+  Carver c(ws, ws_bytes);
+  double* partials = c.take<double>((size_t)grid * 2 * nz);
+  double* totals = c.take<double>((size_t)2 * nz);
+  T* d_vec = c.take<T>((size_t)6 * nz);
+  if (!partials || !totals || !d_vec)
+    return fail(STEAM_ERR_WORKSPACE, "steam_scalar_pattern: workspace too small");
+  std::vector<T> h;
+  PatternArgs<T> a;
+  pattern_vectors<T>(nz, mean_1d, z_coords, aspect, bbuf, h, a);
+  a.two_dx = (T)(2 * dx);
+  a.two_dy = (T)(2 * dy);
+  a.lo = (T)phi_min;
+  a.span = (T)(phi_max - phi_min);
+  a.s_scale = (T)s_scale;
+  a.s_scale_dev = s_scale_dev;
+  a.has_prod = prod != nullptr;
+  a.has_taper = bbuf != nullptr;
+  int rc;
+  if (vecs_dev) {
+    d_vec = const_cast<T*>(vecs_dev);
+  } else if ((rc = upload(d_vec, h, s))) {
+    return rc;
+  }
+  if (sums_dev) totals = sums_dev;
+  rc = pattern_launch<T>(nx, ny, nz, pert, d_vec, prod, a, out, window, partials, totals, grid,
+                         vec, s);
+  if (rc || sums_dev) return rc;
   std::vector<double> t;
   rc = fetch(t, totals, 2 * nz, s);
   if (rc) return rc;
@@ -1424,22 +1603,160 @@ extern "C" int steam_scalar_pattern(
     return pattern_impl<float>(nx, ny, nz, (const float*)pert, mean_1d,
                                (const float*)product, s_scale, dx, dy, z_coords,
                                aspect, buffer_b, phi_min, phi_max,
-                               (float*)w_out, window, level_sums_out, workspace,
-                               workspace_bytes, s);
+                               (float*)w_out, window, level_sums_out, nullptr, nullptr,
+                               nullptr, workspace, workspace_bytes, s);
   if (dtype == STEAM_F64)
     return pattern_impl<double>(nx, ny, nz, (const double*)pert, mean_1d,
                                 (const double*)product, s_scale, dx, dy,
                                 z_coords, aspect, buffer_b, phi_min, phi_max,
-                                (double*)w_out, window, level_sums_out,
-                                workspace, workspace_bytes, s);
+                                (double*)w_out, window, level_sums_out, nullptr, nullptr,
+                                nullptr, workspace, workspace_bytes, s);
   return fail(STEAM_ERR_ARG, "steam_scalar_pattern: bad dtype");
 }
 
+extern "C" int steam_scalar_pattern_vectors(int dtype, int64_t nz, const double* mean_1d,
+                                            const double* z_coords, const double* aspect,
+                                            const double* buffer_b, void* vecs_dev,
+                                            steam_stream_t stream) {
+  STEAM_REQUIRE(nz >= 2 && nz <= kLvThreads * kLvMaxJ,
+                "steam_scalar_pattern_vectors: nz outside [2, 1024]");
+  STEAM_REQUIRE(mean_1d && z_coords && aspect && vecs_dev,
+                "steam_scalar_pattern_vectors: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32) {
+    std::vector<float> h;
+    PatternArgs<float> a;
+    pattern_vectors<float>(nz, mean_1d, z_coords, aspect, buffer_b, h, a);
+    STEAM_CUDA(cudaMemcpyAsync(vecs_dev, h.data(), sizeof(float) * h.size(),
+                               cudaMemcpyHostToDevice, s));
+  } else if (dtype == STEAM_F64) {
+    std::vector<double> h;
+    PatternArgs<double> a;
+    pattern_vectors<double>(nz, mean_1d, z_coords, aspect, buffer_b, h, a);
+    STEAM_CUDA(cudaMemcpyAsync(vecs_dev, h.data(), sizeof(double) * h.size(),
+                               cudaMemcpyHostToDevice, s));
+  } else {
+    return fail(STEAM_ERR_ARG, "steam_scalar_pattern_vectors: bad dtype");
+  }
+  STEAM_CUDA(cudaStreamSynchronize(s));
+  return STEAM_OK;
+}
+
+extern "C" int steam_scalar_pattern_async(
+    int dtype, int64_t nx, int64_t ny, int64_t nz, const void* pert, const void* vecs_dev,
+    const void* product, const double* s_scale_dev, double dx, double dy,
+    const double* z_coords, int32_t has_taper, double phi_min, double phi_max, void* w_out,
+    const steam_window_t* window, double* level_sums_dev, void* workspace,
+    size_t workspace_bytes, steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 1 && ny >= 1, "steam_scalar_pattern_async: empty horizontal extent");
+  STEAM_REQUIRE(nz >= 2, "steam_scalar_pattern_async: the z gradient needs nz >= 2");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_scalar_pattern_async: nz above 1024");
+  STEAM_REQUIRE(pert && vecs_dev && w_out && z_coords && level_sums_dev,
+                "steam_scalar_pattern_async: null pointer");
+  STEAM_REQUIRE(!product || s_scale_dev,
+                "steam_scalar_pattern_async: a product needs s_scale_dev");
+  int rc = check_win(window, nx, ny, "steam_scalar_pattern_async");
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the vectors are given; only the z scalars are taken from z_coords
+  std::vector<double> zeros(nz, 0.0), ones(nz, 1.0);
+  const double* bb = has_taper ? ones.data() : nullptr;
+  if (dtype == STEAM_F32)
+    return pattern_impl<float>(nx, ny, nz, (const float*)pert, zeros.data(),
+                               (const float*)product, 1.0, dx, dy, z_coords, zeros.data(), bb,
+                               phi_min, phi_max, (float*)w_out, window, nullptr, s_scale_dev,
+                               (const float*)vecs_dev, level_sums_dev, workspace,
+                               workspace_bytes, s);
+  if (dtype == STEAM_F64)
+    return pattern_impl<double>(nx, ny, nz, (const double*)pert, zeros.data(),
+                                (const double*)product, 1.0, dx, dy, z_coords, zeros.data(),
+                                bb, phi_min, phi_max, (double*)w_out, window, nullptr,
+                                s_scale_dev, (const double*)vecs_dev, level_sums_dev,
+                                workspace, workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_scalar_pattern_async: bad dtype");
+}
+
+// pre (device, [2][nz] in T) for the second convolution's input scaling:
+// pre[0][z] = the level mean |W| rounded to T (1 where it is not positive),
+// pre[1][z] = mul_dev[z] rounded to T (steam/simulate.py:1989-1992).
+template <typename T>
+__global__ void pattern_norm_kernel(int nz, const double* __restrict__ sums,
+                                    const double* __restrict__ mul, T* __restrict__ pre) {
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    const double cnt = sums[nz + z];
+    const T mean = (T)(sums[z] / (cnt > 1.0 ? cnt : 1.0));
+    pre[z] = mean > (T)0 ? mean : (T)1;
+    pre[nz + z] = (T)mul[z];
+  }
+}
+
+extern "C" int steam_pattern_norm_async(int dtype, int64_t nz, const double* level_sums_dev,
+                                        const double* mul_dev, void* pre_dev,
+                                        steam_stream_t stream) {
+  STEAM_REQUIRE(nz >= 1 && level_sums_dev && mul_dev && pre_dev,
+                "steam_pattern_norm_async: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid = (int)((nz + 255) / 256);
+  if (dtype == STEAM_F32)
+    pattern_norm_kernel<float><<<grid, 256, 0, s>>>((int)nz, level_sums_dev, mul_dev,
+                                                    (float*)pre_dev);
+  else if (dtype == STEAM_F64)
+    pattern_norm_kernel<double><<<grid, 256, 0, s>>>((int)nz, level_sums_dev, mul_dev,
+                                                     (double*)pre_dev);
+  else
+    return fail(STEAM_ERR_ARG, "steam_pattern_norm_async: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_pattern_norm_async");
+  return STEAM_OK;
+}
+
 extern "C" size_t steam_bounded_add_workspace_bytes(int64_t nz, int32_t n_rescale) {
-  const size_t R = n_rescale > 0 ? (size_t)n_rescale : 1;
-  return level_partial_bytes(nz, 2 * kMuCand) +
-         carve_bytes(nz, 8) * 8 + carve_bytes((size_t)nz * R, 8) * 2 +
-         carve_bytes((size_t)nz * kMuCand, 8);
+  const int R = n_rescale > 0 ? n_rescale : 1;
+  return level_partial_bytes(nz, 2 * kMuCand) + ba_state_bytes(nz, R, sizeof(double));
+}
+
+static int bounded_add_check(int64_t nx, int64_t ny, int64_t nz, int32_t n_rescale,
+                             double phi_min, double phi_max, const steam_window_t* window,
+                             const char* who) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, std::string(who) + ": negative extent");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, std::string(who) + ": nz above 1024");
+  STEAM_REQUIRE(n_rescale >= 0 && n_rescale <= 64, std::string(who) + ": n_rescale out of range");
+  STEAM_REQUIRE(phi_max > phi_min, std::string(who) + ": phi_max must exceed phi_min");
+  int rc = check_win(window, nx, ny, who);
+  if (rc) return rc;
+  if (window) {
+    STEAM_REQUIRE(window->x1 > window->x0 && window->y1 > window->y0,
+                  std::string(who) + ": empty window");
+  }
+  return STEAM_OK;
+}
+
+template <typename T>
+static int bounded_add_entry(int64_t nx, int64_t ny, int64_t nz, T* pert,
+                             const double* mean_1d, int mean_on_device, T* inc,
+                             double phi_min, double phi_max, const steam_window_t* window,
+                             int R, int record, double* ledger_host, double* ledger_dev,
+                             void* ws, size_t ws_bytes, cudaStream_t s) {
+  Carver c(ws, ws_bytes);
+  const double* mean_dev = mean_1d;
+  if (!mean_on_device) {
+    double* up = c.take<double>(nz);
+    if (!up) return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
+    STEAM_CUDA(cudaMemcpyAsync(up, mean_1d, sizeof(double) * nz, cudaMemcpyHostToDevice, s));
+    mean_dev = up;
+  }
+  double* led = nullptr;
+  int rc = bounded_add_enqueue<T>(nx, ny, nz, pert, mean_dev, inc, phi_min, phi_max, window, R,
+                                  record, c, &led, s);
+  if (rc) return rc;
+  if (ledger_dev)
+    STEAM_CUDA(cudaMemcpyAsync(ledger_dev, led, sizeof(double) * 5 * nz,
+                               cudaMemcpyDeviceToDevice, s));
+  if (ledger_host) {
+    STEAM_CUDA(cudaMemcpyAsync(ledger_host, led, sizeof(double) * 5 * nz,
+                               cudaMemcpyDeviceToHost, s));
+    STEAM_CUDA(cudaStreamSynchronize(s));
+  }
+  return STEAM_OK;
 }
 
 extern "C" int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
@@ -1450,33 +1767,50 @@ extern "C" int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
                                  double* ledger_out, void* workspace,
                                  size_t workspace_bytes,
                                  steam_stream_t stream) {
-  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_bounded_add: negative extent");
-  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_bounded_add: nz above 1024");
-  STEAM_REQUIRE(n_rescale >= 0 && n_rescale <= 64,
-                "steam_bounded_add: n_rescale out of range");
-  STEAM_REQUIRE(phi_max > phi_min, "steam_bounded_add: phi_max must exceed phi_min");
-  int rc = check_win(window, nx, ny, "steam_bounded_add");
+  int rc = bounded_add_check(nx, ny, nz, n_rescale, phi_min, phi_max, window,
+                             "steam_bounded_add");
   if (rc) return rc;
-  if (window) {
-    STEAM_REQUIRE(window->x1 > window->x0 && window->y1 > window->y0,
-                  "steam_bounded_add: empty window");
-  }
   if (nx * ny * nz == 0) return STEAM_OK;
   STEAM_REQUIRE(pert && increment && mean_1d, "steam_bounded_add: null pointer");
   cudaStream_t s = (cudaStream_t)stream;
-  const int R = n_rescale > 0 ? n_rescale : 1;
   if (dtype == STEAM_F32)
-    return bounded_add_impl<float>(nx, ny, nz, (float*)pert, mean_1d,
-                                   (float*)increment, phi_min, phi_max, window,
-                                   n_rescale > 0 ? R : 0, record_applied,
-                                   ledger_out, workspace, workspace_bytes, s);
+    rc = bounded_add_entry<float>(nx, ny, nz, (float*)pert, mean_1d, 0, (float*)increment,
+                                  phi_min, phi_max, window, n_rescale, record_applied,
+                                  ledger_out, nullptr, workspace, workspace_bytes, s);
+  else if (dtype == STEAM_F64)
+    rc = bounded_add_entry<double>(nx, ny, nz, (double*)pert, mean_1d, 0, (double*)increment,
+                                   phi_min, phi_max, window, n_rescale, record_applied,
+                                   ledger_out, nullptr, workspace, workspace_bytes, s);
+  else
+    return fail(STEAM_ERR_ARG, "steam_bounded_add: bad dtype");
+  if (rc) return rc;
+  if (!ledger_out) STEAM_CUDA(cudaStreamSynchronize(s));
+  return STEAM_OK;
+}
+
+extern "C" int steam_bounded_add_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                       void* pert, const double* mean_dev, void* increment,
+                                       double phi_min, double phi_max,
+                                       const steam_window_t* window, int32_t n_rescale,
+                                       int32_t record_applied, double* ledger_dev,
+                                       void* workspace, size_t workspace_bytes,
+                                       steam_stream_t stream) {
+  int rc = bounded_add_check(nx, ny, nz, n_rescale, phi_min, phi_max, window,
+                             "steam_bounded_add_async");
+  if (rc) return rc;
+  if (nx * ny * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(pert && increment && mean_dev, "steam_bounded_add_async: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    return bounded_add_entry<float>(nx, ny, nz, (float*)pert, mean_dev, 1, (float*)increment,
+                                    phi_min, phi_max, window, n_rescale, record_applied,
+                                    nullptr, ledger_dev, workspace, workspace_bytes, s);
   if (dtype == STEAM_F64)
-    return bounded_add_impl<double>(nx, ny, nz, (double*)pert, mean_1d,
-                                    (double*)increment, phi_min, phi_max,
-                                    window, n_rescale > 0 ? R : 0,
-                                    record_applied, ledger_out, workspace,
-                                    workspace_bytes, s);
-  return fail(STEAM_ERR_ARG, "steam_bounded_add: bad dtype");
+    return bounded_add_entry<double>(nx, ny, nz, (double*)pert, mean_dev, 1,
+                                     (double*)increment, phi_min, phi_max, window, n_rescale,
+                                     record_applied, nullptr, ledger_dev, workspace,
+                                     workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_bounded_add_async: bad dtype");
 }
 
 extern "C" int steam_project_bounds(int dtype, int64_t nx, int64_t ny,

@@ -234,19 +234,17 @@ extern "C" size_t steam_flux_noise_workspace_bytes(void) {
          carve_bytes(4, sizeof(double));
 }
 
-extern "C" int steam_flux_noise(int dtype, const steam_region_t* region,
-                                double alpha, double per_class_scale,
-                                double shift, int32_t n_zero,
-                                int32_t zero_bottom, int32_t zero_top,
-                                const void* flux, void* product,
-                                const steam_window_t* window, double* sums_out,
-                                void* workspace, size_t workspace_bytes,
-                                steam_stream_t stream) {
-  int rc = check_region(region, "steam_flux_noise");
+// Launches the noise kernel and its reduction: totals (device) receives
+// { sum F over the window, sum |eps| over the window, nonzero eps count }.
+static int flux_noise_launch(int dtype, const steam_region_t* region, double alpha,
+                             double per_class_scale, double shift, int32_t n_zero,
+                             int32_t zero_bottom, int32_t zero_top, const void* flux,
+                             void* product, const steam_window_t* window, double* totals,
+                             double* cells_out, void* workspace, size_t workspace_bytes,
+                             cudaStream_t s, const char* who) {
+  int rc = check_region(region, who);
   if (rc) return rc;
-  STEAM_REQUIRE(alpha > 1.0 && alpha <= 2.0,
-                "steam_flux_noise: alpha must lie in (1, 2]");
-  STEAM_REQUIRE(sums_out != nullptr, "steam_flux_noise: null sums_out");
+  STEAM_REQUIRE(alpha > 1.0 && alpha <= 2.0, std::string(who) + ": alpha must lie in (1, 2]");
   RegionDev r = to_dev(*region);
   const int64_t n = r.nx * r.ny * r.nz;
   NoiseArgs a;
@@ -259,7 +257,7 @@ extern "C" int steam_flux_noise(int dtype, const steam_region_t* region,
     STEAM_REQUIRE(window->x0 >= 0 && window->x1 <= r.nx &&
                       window->x0 <= window->x1 && window->y0 >= 0 &&
                       window->y1 <= r.ny && window->y0 <= window->y1,
-                  "steam_flux_noise: window outside the array");
+                  std::string(who) + ": window outside the array");
     a.wx0 = window->x0;
     a.wx1 = window->x1;
     a.wy0 = window->y0;
@@ -270,26 +268,16 @@ extern "C" int steam_flux_noise(int dtype, const steam_region_t* region,
     a.wy0 = 0;
     a.wy1 = r.ny;
   }
-  const double cells = (double)((a.wx1 - a.wx0) * (a.wy1 - a.wy0) * r.nz);
-  if (n == 0) {
-    sums_out[0] = 0.0;
-    sums_out[1] = cells;
-    sums_out[2] = 0.0;
-    sums_out[3] = 0.0;
-    return STEAM_OK;
-  }
-  STEAM_REQUIRE(flux && product, "steam_flux_noise: null field pointer");
-  STEAM_REQUIRE(r.nx * r.ny < ((int64_t)1 << 32),
-                "steam_flux_noise: more than 2^32 columns");
+  *cells_out = (double)((a.wx1 - a.wx0) * (a.wy1 - a.wy0) * r.nz);
+  if (n == 0) return STEAM_OK;
+  STEAM_REQUIRE(flux && product, std::string(who) + ": null field pointer");
+  STEAM_REQUIRE(r.nx * r.ny < ((int64_t)1 << 32), std::string(who) + ": more than 2^32 columns");
   const int64_t cols_per_block = r.nz < 256 ? 256 / r.nz : 1;
   int grid = stride_grid((r.nx * r.ny + cols_per_block - 1) / cols_per_block, 1,
                          kNoiseBlocksPerSm);
   Carver c(workspace, workspace_bytes);
   double* partials = c.take<double>((size_t)grid * 3);
-  double* totals = c.take<double>(4);
-  if (!partials || !totals)
-    return fail(STEAM_ERR_WORKSPACE, "steam_flux_noise: workspace too small");
-  cudaStream_t s = (cudaStream_t)stream;
+  if (!partials) return fail(STEAM_ERR_WORKSPACE, std::string(who) + ": workspace too small");
   if (dtype == STEAM_F32)
     flux_noise_kernel<float><<<grid, 256, 0, s>>>(
         r, make_levy<float>(alpha), a, (const float*)flux, (float*)product,
@@ -299,16 +287,58 @@ extern "C" int steam_flux_noise(int dtype, const steam_region_t* region,
         r, make_levy<double>(alpha), a, (const double*)flux,
         (double*)product, partials);
   else
-    return fail(STEAM_ERR_ARG, "steam_flux_noise: bad dtype");
-  STEAM_LAUNCH_CHECK("steam_flux_noise");
-  rc = reduce_partials(partials, grid, 3, totals, s);
+    return fail(STEAM_ERR_ARG, std::string(who) + ": bad dtype");
+  STEAM_LAUNCH_CHECK(who);
+  return reduce_partials(partials, grid, 3, totals, s);
+}
+
+extern "C" int steam_flux_noise(int dtype, const steam_region_t* region,
+                                double alpha, double per_class_scale,
+                                double shift, int32_t n_zero,
+                                int32_t zero_bottom, int32_t zero_top,
+                                const void* flux, void* product,
+                                const steam_window_t* window, double* sums_out,
+                                void* workspace, size_t workspace_bytes,
+                                steam_stream_t stream) {
+  STEAM_REQUIRE(sums_out != nullptr, "steam_flux_noise: null sums_out");
+  STEAM_REQUIRE(region != nullptr, "steam_flux_noise: null region");
+  cudaStream_t s = (cudaStream_t)stream;
+  // totals go after the partials in the workspace
+  const size_t part = carve_bytes((size_t)sm_count() * kNoiseBlocksPerSm * 3, sizeof(double));
+  STEAM_REQUIRE(workspace_bytes >= part + carve_bytes(4, sizeof(double)) || workspace == nullptr,
+                "steam_flux_noise: workspace too small");
+  double* totals = workspace ? reinterpret_cast<double*>(static_cast<char*>(workspace) + part)
+                             : nullptr;
+  double cells = 0.0;
+  int rc = flux_noise_launch(dtype, region, alpha, per_class_scale, shift, n_zero, zero_bottom,
+                             zero_top, flux, product, window, totals, &cells, workspace, part,
+                             s, "steam_flux_noise");
   if (rc) return rc;
-  double h[3];
-  STEAM_CUDA(cudaMemcpyAsync(h, totals, sizeof(h), cudaMemcpyDeviceToHost, s));
-  STEAM_CUDA(cudaStreamSynchronize(s));
+  double h[3] = {0.0, 0.0, 0.0};
+  if (region->shape[0] * region->shape[1] * region->shape[2] > 0) {
+    STEAM_CUDA(cudaMemcpyAsync(h, totals, sizeof(h), cudaMemcpyDeviceToHost, s));
+    STEAM_CUDA(cudaStreamSynchronize(s));
+  }
   sums_out[0] = h[0];
   sums_out[1] = cells;
   sums_out[2] = h[1];
   sums_out[3] = h[2];
   return STEAM_OK;
+}
+
+extern "C" int steam_flux_noise_async(int dtype, const steam_region_t* region, double alpha,
+                                      double per_class_scale, double shift, int32_t n_zero,
+                                      int32_t zero_bottom, int32_t zero_top, const void* flux,
+                                      void* product, const steam_window_t* window,
+                                      double* sums_dev, void* workspace,
+                                      size_t workspace_bytes, steam_stream_t stream) {
+  STEAM_REQUIRE(sums_dev != nullptr, "steam_flux_noise_async: null sums_dev");
+  STEAM_REQUIRE(region != nullptr, "steam_flux_noise_async: null region");
+  cudaStream_t s = (cudaStream_t)stream;
+  double cells = 0.0;
+  if (region->shape[0] * region->shape[1] * region->shape[2] == 0)
+    STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 3 * sizeof(double), s));
+  return flux_noise_launch(dtype, region, alpha, per_class_scale, shift, n_zero, zero_bottom,
+                           zero_top, flux, product, window, sums_dev, &cells, workspace,
+                           workspace_bytes, s, "steam_flux_noise_async");
 }

@@ -1,0 +1,199 @@
+"""Resident, asynchronous form of one size class.
+
+``run_class`` in ``simulate`` reads every realized scalar back to the host
+between stages, as the reference's stage functions do.  This module runs the
+same class step (steam/simulate.py:1903-2029, plus the thermodynamic map of
+steam/thermodynamics.py:25-123) with every scalar kept in device memory: the
+flux restore factor, the product norm, the pattern's level means and the
+bounded add's whole demean/rescale/shift solve are decided by small device
+kernels between the field sweeps.  A step therefore enqueues all of its work
+without waiting on the GPU; its ledger is copied back asynchronously and read
+only when asked for.
+
+``ResidentClass`` holds what a class needs on the device across steps: the
+per-level vectors, the work fields (product, pattern, increment) and the
+ledger block.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .ledger import (BoundedAddLedger, ClassLedger, FluxAdvanceLedger, MeanReduction,
+                     PatternLedger)
+
+N_RESCALE = 10
+
+
+def _off(t, n_doubles):
+    """Device pointer ``n_doubles`` float64 elements into tensor ``t``."""
+    return ctypes.c_void_p(t.data_ptr() + 8 * int(n_doubles))
+
+
+class ResidentClass:
+    """Device-resident constants, work fields and ledger block of one class.
+
+    ``setup`` is a ``simulate.ClassSetup`` whose convolution plan is
+    separable (every turbulon kernel is)."""
+
+    def __init__(self, setup, dtype=None):
+        torch = _lib.require_cuda("resident class step")
+        from . import simulate as sim
+        self.lib = _lib.load()
+        self.setup = setup
+        if setup.plan.kind == 'dense':
+            raise NotImplementedError("resident class step: the kernel does not factor")
+        self.dtype = dtype if dtype is not None else torch.float32
+        self.np_t = np.float64 if self.dtype == torch.float64 else np.float32
+        self.code = _lib.STEAM_F64 if self.dtype == torch.float64 else _lib.STEAM_F32
+        nx, ny, nz = setup.shape
+        self.shape = (nx, ny, nz)
+        dev = torch.device('cuda', torch.cuda.current_device())
+        f64 = dict(dtype=torch.float64, device=dev)
+        z = np.asarray(setup.z, dtype=np.float64)
+        self.z = z
+        self.vecs, self.mean, self.mul, self.pre = {}, {}, {}, {}
+        for name, mean, C, b in (('h', setup.h_mean, setup.C_h, setup.b_h),
+                                 ('qt', setup.qt_mean, setup.C_qt, setup.b_qt)):
+            vec = torch.empty(6 * nz, dtype=self.dtype, device=dev)
+            _lib.check(self.lib.steam_scalar_pattern_vectors(
+                self.code, nz, _lib.dvec(mean), _lib.dvec(z), _lib.dvec(setup.aspect),
+                _lib.dvec(b), _lib.ptr(vec), _lib.stream()))
+            self.vecs[name] = vec
+            self.mean[name] = torch.as_tensor(np.asarray(mean, np.float64), **f64).contiguous()
+            self.mul[name] = torch.as_tensor(np.asarray(C, np.float32).astype(np.float64),
+                                             **f64).contiguous()
+            self.pre[name] = torch.empty(2 * nz, dtype=self.dtype, device=dev)
+        dz = np.zeros(nz)
+        dz[:-1] = np.diff(z)
+        prof = np.concatenate([z, dz, np.asarray(setup.h_mean, np.float64),
+                               np.asarray(setup.qt_mean, np.float64)])
+        self.prof = torch.as_tensor(prof, **f64).contiguous()
+        h_min, h_max, qt_min, qt_max = setup.bounds
+        self.bounds = [float(self.np_t(v)) for v in (h_min, h_max, qt_min, qt_max)]
+        # ledger block: noise sums [3] | conv sums [2] | flux ledger [10] |
+        # pattern sums h, qt [2][nz] each | bounded-add ledger h, qt [nz][5] each
+        self.o_ns, self.o_cs, self.o_fl = 0, 3, 5
+        self.o_ps = {'h': 15, 'qt': 15 + 2 * nz}
+        self.o_ba = {'h': 15 + 4 * nz, 'qt': 15 + 9 * nz}
+        n_led = 15 + 14 * nz
+        self.ledger = torch.zeros(n_led, **f64)
+        self.ledger_host = torch.empty(n_led, dtype=torch.float64, pin_memory=True)
+        self.ledger_ready = torch.cuda.Event()
+        self.work = None
+        # flux-noise constants (steam/simulate.py:2135-2143)
+        alpha = setup.alpha
+        pcs = setup.flux_noise_scale / setup.n_per_dyad ** (1.0 / alpha)
+        shift = sim.levy_log_mean(alpha) * pcs ** alpha
+        self.alpha = alpha
+        self.pcs = float(self.np_t(pcs))
+        self.shift = float(self.np_t(shift))
+        self.region = sim._region_struct(setup.region, self.shape, setup.sparsity)
+        w = setup.window
+        cols = nx * ny if w is None else (w[1] - w[0]) * (w[3] - w[2])
+        self.cells = float(cols * nz)
+
+    def _work(self, like):
+        import torch
+        if self.work is None or self.work[0].dtype != like.dtype:
+            self.work = tuple(torch.empty_like(like) for _ in range(3))
+        return self.work
+
+    def step(self, hp, qp, F, diagnostics=None, surface_pressure=101325.0):
+        """Enqueue one class step on the resident fields (mutated in place)
+        and, with ``diagnostics`` (a dict of tensors T, qv, qc, qi, p), the
+        composition + thermodynamics.  Returns without waiting on the GPU."""
+        lib, cs, code = self.lib, self.setup, self.code
+        nx, ny, nz = self.shape
+        for t in (hp, qp, F):
+            if tuple(t.shape) != self.shape or t.dtype != self.dtype or not t.is_contiguous():
+                raise ValueError("resident class step: fields must be contiguous "
+                                 f"{self.shape} {self.dtype} CUDA tensors")
+        product, W, inc = self._work(F)
+        stream = _lib.stream()
+        win = _lib.window_arg(cs.window)
+        L = self.ledger
+        plan = cs.plan
+        ws = _lib.WORKSPACE.get(max(
+            lib.steam_flux_noise_workspace_bytes(),
+            lib.steam_conv_workspace_bytes(code, nx, ny, nz, ctypes.byref(plan.spec)),
+            lib.steam_scalar_pattern_workspace_bytes(nx, ny, nz),
+            lib.steam_bounded_add_workspace_bytes(nz, N_RESCALE)))
+        wsp, wsn = _lib.ptr(ws), ws.numel()
+        # flux advance
+        _lib.check(lib.steam_flux_noise_async(
+            code, ctypes.byref(self.region), self.alpha, self.pcs, self.shift, int(cs.n_zero),
+            int(bool(cs.zero_bottom)), int(bool(cs.zero_top)), _lib.ptr(F), _lib.ptr(product),
+            win, _off(L, self.o_ns), wsp, wsn, stream))
+        _lib.check(lib.steam_conv_separable_async(
+            code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps, plan.x_taps,
+            _lib.ptr(product), None, _lib.ptr(F), _lib.STEAM_EPI_FLUX, win, _off(L, self.o_cs),
+            wsp, wsn, stream))
+        _lib.check(lib.steam_flux_finish_async(
+            code, F.numel(), _lib.ptr(F), _off(L, self.o_ns), _off(L, self.o_cs), self.cells,
+            _off(L, self.o_fl), stream))
+        # the two scalars
+        h_min, h_max, qt_min, qt_max = cs.bounds
+        for name, pert, lo, hi in (('h', hp, h_min, h_max), ('qt', qp, qt_min, qt_max)):
+            ps = _off(L, self.o_ps[name])
+            _lib.check(lib.steam_scalar_pattern_async(
+                code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.vecs[name]), _lib.ptr(product),
+                _off(L, self.o_fl + 7), float(cs.dx), float(cs.dy), _lib.dvec(self.z), 1,
+                float(lo), float(hi), _lib.ptr(W), win, ps, wsp, wsn, stream))
+            _lib.check(lib.steam_pattern_norm_async(
+                code, nz, ps, _lib.ptr(self.mul[name]), _lib.ptr(self.pre[name]), stream))
+            _lib.check(lib.steam_conv_separable_async(
+                code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps,
+                plan.x_taps, _lib.ptr(W), _lib.ptr(self.pre[name]), _lib.ptr(inc),
+                _lib.STEAM_EPI_STORE, win, None, wsp, wsn, stream))
+            _lib.check(lib.steam_bounded_add_async(
+                code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
+                float(lo), float(hi), win, N_RESCALE, 0, _off(L, self.o_ba[name]), wsp, wsn,
+                stream))
+        if diagnostics is not None:
+            d = diagnostics
+            _lib.check(lib.steam_thermo_async(
+                code, nx, ny, nz, _lib.ptr(hp), _lib.ptr(qp), _lib.ptr(self.prof), 1,
+                _lib.dvec(self.bounds), float(surface_pressure), None, _lib.ptr(d["T"]),
+                _lib.ptr(d["qv"]), _lib.ptr(d["qc"]), _lib.ptr(d["qi"]), _lib.ptr(d["p"]),
+                stream))
+        self.ledger_host.copy_(L, non_blocking=True)
+        self.ledger_ready.record()
+        return self
+
+    def class_ledger(self, cl=None):
+        """The step's ledger as a ``ClassLedger`` (waits for the step)."""
+        self.ledger_ready.synchronize()
+        v = self.ledger_host.numpy().copy()
+        nz = self.shape[2]
+        fl = v[self.o_fl:self.o_fl + 10]
+        cl = ClassLedger() if cl is None else cl
+        cl.flux = FluxAdvanceLedger(MeanReduction(fl[0], int(fl[1])),
+                                    MeanReduction(fl[2], int(fl[3])),
+                                    MeanReduction(fl[4], int(fl[5])), int(fl[6]))
+        for name in ('h', 'qt'):
+            ps = v[self.o_ps[name]:self.o_ps[name] + 2 * nz]
+            cl.pattern[name] = PatternLedger(ps[:nz].copy(), ps[nz:].astype(np.int64))
+            cl.bounded_add[name] = BoundedAddLedger.from_device(
+                v[self.o_ba[name]:self.o_ba[name] + 5 * nz])
+        return cl
+
+
+_CACHE = {}
+
+
+def resident_for(setup, dtype):
+    """The cached ResidentClass of ``setup`` on the current device."""
+    import torch
+    key = (id(setup), dtype, torch.cuda.current_device())
+    hit = _CACHE.get(key)
+    if hit is not None and hit.setup is setup:
+        return hit
+    if len(_CACHE) > 64:
+        _CACHE.clear()
+    rc = ResidentClass(setup, dtype)
+    _CACHE[key] = rc
+    return rc

@@ -670,13 +670,19 @@ class ClassSetup(NamedTuple):
     alpha: float
 
 
-def run_class(hp, qp, F, dh, dq, dF, cs, cl, increment_dir=None, index=0):
+def run_class(hp, qp, F, dh, dq, dF, cs, cl, increment_dir=None, index=0, resident=True):
     """One size class on resident fields (steam/simulate.py:1903-2029):
     flux advance, then for h and qt the pattern, the second convolution with
     the per-level normalisation fused into its input, and the bounded add.
     Mutates the state tensors and fills the class ledger ``cl``."""
     torch = _lib.require_cuda("cascade_loop")
     need_inc = cs.deficit is not None or increment_dir is not None
+    if (resident and not need_inc and cl.flux is None and not cl.pattern
+            and not cl.bounded_add and cs.plan.kind != 'dense'):
+        # measure mode: the resident step keeps every scalar on the device
+        from .resident import resident_for
+        resident_for(cs, F.dtype).step(hp, qp, F).class_ledger(cl)
+        return
     F_before = F.clone() if need_inc else None
     step = advance_flux_device(F, cs.region, cs.plan, cs.flux_noise_scale, cs.n_per_dyad,
                                cs.sparsity, cs.n_zero, cs.zero_bottom, cs.zero_top,
@@ -1121,9 +1127,21 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
     qp, q_host = to_device(qt_perturbation, dtype=hp.dtype)
     F, f_host = to_device(flux, dtype=hp.dtype)
     cl = ClassLedger() if ledger is None else ledger
-    run_class(hp, qp, F, None, None, None, setup, cl)
     diag = {}
-    if diagnostics:
+    resident = (ledger is None and setup.deficit is None and setup.plan.kind != 'dense'
+                and np.ndim(surface_pressure) == 0)
+    if resident:
+        from .resident import resident_for
+        rc = resident_for(setup, hp.dtype)
+        out = {k: torch.empty_like(hp) for k in ("T", "qv", "qc", "qi", "p")} \
+            if diagnostics else None
+        rc.step(hp, qp, F, diagnostics=out, surface_pressure=surface_pressure)
+        if diagnostics:
+            diag = {k: out[k] for k in diagnostics}
+        del out
+    else:
+        run_class(hp, qp, F, None, None, None, setup, cl)
+    if diagnostics and not resident:
         h_min, h_max, qt_min, qt_max = setup.bounds
         np_t = np.float64 if hp.dtype == torch.float64 else np.float32
         bounds = [float(np_t(h_min)), float(np_t(h_max)), float(np_t(qt_min)),
@@ -1138,4 +1156,6 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
         to_host(qp, out=qt_perturbation)
         to_host(F, out=flux)
         diag = {k: to_host(v) for k, v in diag.items()}
+    if resident:
+        rc.class_ledger(cl)
     return diag, cl

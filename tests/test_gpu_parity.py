@@ -480,3 +480,66 @@ def test_repeat_runs_are_bit_identical(steam):
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
     assert outs[0][2] == outs[1][2]
+
+
+# ---------------------------------------------------------------------------
+# Resident (asynchronous) class step against the stage-by-stage step
+# ---------------------------------------------------------------------------
+
+def _resident_case(dtype, shape, window):
+    import torch
+    from steam_b200 import simulate as sim
+    from steam_b200.ledger import ClassLedger
+    from steam_b200.resident import ResidentClass
+    nx, ny, nz = shape
+    sim_, zp, hp, qp, grids, C_h, C_q = _one_class_setup(nx, ny, nz)
+    b_h = sim._bound_buffers(C_h, 1)[0]
+    b_q = sim._bound_buffers(C_q, 1)[0]
+    key = O.class_key(np.random.SeedSequence(5))
+    setup = sim.make_class_setup(
+        grids, 0, h_profile=hp, qt_profile=qp, z_profile=zp, C_h=C_h[0], C_qt=C_q[0],
+        b_h=b_h, b_qt=b_q, aspect=np.ones(nz, np.float32),
+        bounds=(315 * 1004.0, 355 * 1004.0, 0.0, 0.03), key=key, flux_noise_scale=0.1,
+        window=window, dtype=dtype)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    rng = np.random.default_rng(3)
+    h0 = torch.as_tensor(800.0 * rng.standard_normal(shape), dtype=tdt, device='cuda')
+    q0 = torch.as_tensor(0.0008 * rng.standard_normal(shape), dtype=tdt, device='cuda')
+    F0 = torch.as_tensor(1.0 + 0.2 * rng.random(shape), dtype=tdt, device='cuda')
+    # stage by stage, every scalar through the host
+    hs, qs, Fs = h0.clone(), q0.clone(), F0.clone()
+    cl_s = ClassLedger()
+    sim.run_class(hs, qs, Fs, None, None, None, setup, cl_s, resident=False)
+    # resident: two steps in a row from the same state (the second reuses
+    # every resident buffer)
+    rc = ResidentClass(setup, tdt)
+    for _ in range(2):
+        hr, qr, Fr = h0.clone(), q0.clone(), F0.clone()
+        rc.step(hr, qr, Fr)
+        cl_r = rc.class_ledger()
+    return (hs, qs, Fs, cl_s), (hr, qr, Fr, cl_r)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("shape,window", [((32, 24, 20), None), ((40, 32, 16), (4, 36, 2, 30))])
+def test_resident_step_matches_stage_by_stage(steam, dtype, shape, window):
+    (hs, qs, Fs, cl_s), (hr, qr, Fr, cl_r) = _resident_case(dtype, shape, window)
+    # identical arithmetic, so identical bits
+    for a, b in ((hs, hr), (qs, qr), (Fs, Fr)):
+        assert bool((a == b).all()), float((a - b).abs().max())
+    fs, fr = cl_s.flux, cl_r.flux
+    for name in ('entering', 'noise_abs', 'realized'):
+        assert getattr(fs, name).total == getattr(fr, name).total
+        assert getattr(fs, name).count == getattr(fr, name).count
+    assert fs.n_clipped == fr.n_clipped
+    for name in ('h', 'qt'):
+        np.testing.assert_array_equal(cl_s.pattern[name].level_total,
+                                      cl_r.pattern[name].level_total)
+        np.testing.assert_array_equal(cl_s.pattern[name].level_count,
+                                      cl_r.pattern[name].level_count)
+        bs, br = cl_s.bounded_add[name], cl_r.bounded_add[name]
+        np.testing.assert_array_equal(bs.a0, br.a0)
+        np.testing.assert_array_equal(bs.n_loop, br.n_loop)
+        np.testing.assert_array_equal(bs.final_demean, br.final_demean)
+        np.testing.assert_array_equal(bs.mu, br.mu)
+        assert bs.n_sweeps == br.n_sweeps
