@@ -84,6 +84,7 @@ class ResidentClass:
         self.ledger_host = torch.empty(n_led, dtype=torch.float64, pin_memory=True)
         self.ledger_ready = torch.cuda.Event()
         self.work = None
+        self.io = None
         # flux-noise constants (steam/simulate.py:2135-2143)
         alpha = setup.alpha
         pcs = setup.flux_noise_scale / setup.n_per_dyad ** (1.0 / alpha)
@@ -102,10 +103,17 @@ class ResidentClass:
             self.work = tuple(torch.empty_like(like) for _ in range(3))
         return self.work
 
-    def step(self, hp, qp, F, diagnostics=None, surface_pressure=101325.0):
+    def step(self, hp, qp, F, diagnostics=None, surface_pressure=101325.0, ready=None,
+             done=None):
         """Enqueue one class step on the resident fields (mutated in place)
         and, with ``diagnostics`` (a dict of tensors T, qv, qc, qi, p), the
-        composition + thermodynamics.  Returns without waiting on the GPU."""
+        composition + thermodynamics.  Returns without waiting on the GPU.
+
+        ``ready`` maps 'h' / 'qt' to CUDA events the step waits for before it
+        first reads that field (an upload still in flight on another
+        stream); ``done``, a dict, receives events recorded when F, h, qt and
+        the diagnostics are final."""
+        import torch
         lib, cs, code = self.lib, self.setup, self.code
         nx, ny, nz = self.shape
         for t in (hp, qp, F):
@@ -135,9 +143,14 @@ class ResidentClass:
         _lib.check(lib.steam_flux_finish_async(
             code, F.numel(), _lib.ptr(F), _off(L, self.o_ns), _off(L, self.o_cs), self.cells,
             _off(L, self.o_fl), stream))
+        if done is not None:
+            done['F'] = torch.cuda.Event()
+            done['F'].record()
         # the two scalars
         h_min, h_max, qt_min, qt_max = cs.bounds
         for name, pert, lo, hi in (('h', hp, h_min, h_max), ('qt', qp, qt_min, qt_max)):
+            if ready is not None and name in ready:
+                torch.cuda.current_stream().wait_event(ready[name])
             ps = _off(L, self.o_ps[name])
             _lib.check(lib.steam_scalar_pattern_async(
                 code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.vecs[name]), _lib.ptr(product),
@@ -153,6 +166,9 @@ class ResidentClass:
                 code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
                 float(lo), float(hi), win, N_RESCALE, 0, _off(L, self.o_ba[name]), wsp, wsn,
                 stream))
+            if done is not None:
+                done[name] = torch.cuda.Event()
+                done[name].record()
         if diagnostics is not None:
             d = diagnostics
             _lib.check(lib.steam_thermo_async(
@@ -160,9 +176,83 @@ class ResidentClass:
                 _lib.dvec(self.bounds), float(surface_pressure), None, _lib.ptr(d["T"]),
                 _lib.ptr(d["qv"]), _lib.ptr(d["qc"]), _lib.ptr(d["qi"]), _lib.ptr(d["p"]),
                 stream))
+            if done is not None:
+                done['diag'] = torch.cuda.Event()
+                done['diag'].record()
         self.ledger_host.copy_(L, non_blocking=True)
         self.ledger_ready.record()
         return self
+
+    def host_step(self, h, qt, flux, diagnostics=('qc', 'qi'), out=None,
+                  surface_pressure=101325.0):
+        """One class step on host arrays, with the transfers pipelined.
+
+        h, qt, flux (numpy, updated in place) are uploaded on a copy stream
+        in the order the step needs them (F first; h and qt while the flux
+        advance runs), and each result is downloaded as soon as it is final
+        (F while the scalars run, h while qt runs, qt and the diagnostics
+        last), so copies overlap compute in both directions.  ``out`` maps
+        diagnostic names to host arrays to fill; page-locked arrays (e.g.
+        ``torch.empty(..., pin_memory=True).numpy()``) let every copy run
+        asynchronously at full PCIe bandwidth.  Returns the diagnostics."""
+        import torch
+        shape = self.shape
+        for name, a in (('h', h), ('qt', qt), ('flux', flux)):
+            if tuple(np.shape(a)) != shape:
+                raise ValueError(f"field_step: {name} has shape {np.shape(a)}, expected {shape}")
+        if self.io is None:
+            self.io = {k: torch.empty(shape, dtype=self.dtype, device='cuda')
+                       for k in ('h', 'qt', 'F', 'T', 'qv', 'qc', 'qi', 'p')}
+            self.copy_stream = torch.cuda.Stream()
+        io, cp = self.io, self.copy_stream
+        main = torch.cuda.current_stream()
+        src = {k: torch.from_numpy(np.ascontiguousarray(a, dtype=self.np_t))
+               for k, a in (('F', flux), ('h', h), ('qt', qt))}
+        cp.wait_stream(main)  # the device buffers are free once earlier work is done
+        ready = {}
+        with torch.cuda.stream(cp):
+            for k in ('F', 'h', 'qt'):
+                io[k].copy_(src[k], non_blocking=True)
+                ready[k] = torch.cuda.Event()
+                ready[k].record(cp)
+        main.wait_event(ready['F'])
+        done = {}
+        diag_dev = {k: io[k] for k in ('T', 'qv', 'qc', 'qi', 'p')} if diagnostics else None
+        self.step(io['h'], io['qt'], io['F'], diagnostics=diag_dev,
+                  surface_pressure=surface_pressure, ready=ready, done=done)
+        result = {}
+        if out is None:
+            out = {}
+        host_out = {}
+        for k in (diagnostics or ()):
+            if k in out:
+                host_out[k] = torch.from_numpy(out[k])
+            else:
+                host_out[k] = torch.empty(shape, dtype=self.dtype, pin_memory=True)
+        with torch.cuda.stream(cp):
+            for ev, pairs in (('F', (('F', flux),)), ('h', (('h', h),)), ('qt', (('qt', qt),))):
+                cp.wait_event(done[ev])
+                for k, host in pairs:
+                    dst = host if isinstance(host, np.ndarray) else None
+                    t = torch.from_numpy(dst) if dst is not None and dst.dtype == self.np_t \
+                        and dst.flags.c_contiguous else None
+                    if t is not None:
+                        t.copy_(io[k], non_blocking=True)
+                    else:
+                        host_out['_' + k] = torch.empty(shape, dtype=self.dtype,
+                                                        pin_memory=True)
+                        host_out['_' + k].copy_(io[k], non_blocking=True)
+            if diagnostics:
+                cp.wait_event(done['diag'])
+                for k in diagnostics:
+                    host_out[k].copy_(io[k], non_blocking=True)
+        cp.synchronize()
+        for k, host in (('F', flux), ('h', h), ('qt', qt)):
+            if '_' + k in host_out:
+                host[...] = host_out['_' + k].numpy()
+        for k in (diagnostics or ()):
+            result[k] = host_out[k].numpy()
+        return result
 
     def class_ledger(self, cl=None):
         """The step's ledger as a ``ClassLedger`` (waits for the step)."""

@@ -1110,7 +1110,7 @@ def make_class_setup(grids, i, *, h_profile, qt_profile, z_profile, C_h, C_qt, b
 
 
 def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=101325.0,
-               diagnostics=('qc', 'qi'), ledger=None):
+               diagnostics=('qc', 'qi'), ledger=None, out=None):
     """One size class plus the thermodynamic map to condensate.
 
     Advances the flux, adds the h and qt increments (pattern, second
@@ -1118,11 +1118,22 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
     to the bounds, and recovers the requested diagnostics
     (steam/thermodynamics.py:25-123).  numpy arrays are updated in place and
     host diagnostics returned; CUDA tensors stay on the device.  Returns
-    (diagnostics dict, ClassLedger).
+    (diagnostics dict, ClassLedger).  With numpy arrays, ``out`` (a dict of
+    host arrays) receives the diagnostics; page-locked arrays let the
+    pipelined transfers run at full PCIe bandwidth.
     """
     from .ledger import ClassLedger
     from .thermodynamics import recover_diagnostics_device
     torch = _lib.require_cuda("field_step")
+    if (not is_tensor(h_perturbation) and ledger is None and setup.deficit is None
+            and setup.plan.kind != 'dense' and np.ndim(surface_pressure) == 0):
+        # host arrays: the resident step with pipelined transfers
+        from .resident import resident_for
+        np_t = np.asarray(h_perturbation).dtype
+        rc = resident_for(setup, torch.float64 if np_t == np.float64 else torch.float32)
+        diag = rc.host_step(h_perturbation, qt_perturbation, flux, diagnostics=diagnostics,
+                            out=out, surface_pressure=surface_pressure)
+        return diag, rc.class_ledger()
     hp, h_host = to_device(h_perturbation)
     qp, q_host = to_device(qt_perturbation, dtype=hp.dtype)
     F, f_host = to_device(flux, dtype=hp.dtype)

@@ -543,3 +543,38 @@ def test_resident_step_matches_stage_by_stage(steam, dtype, shape, window):
         np.testing.assert_array_equal(bs.final_demean, br.final_demean)
         np.testing.assert_array_equal(bs.mu, br.mu)
         assert bs.n_sweeps == br.n_sweeps
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_field_step_host_arrays_match_resident_tensors(steam, dtype):
+    """field_step on numpy arrays (pipelined copies on a second stream) gives
+    the same bits as the resident step on device tensors, twice in a row."""
+    import torch
+    from steam_b200 import simulate as sim
+    from steam_b200.resident import ResidentClass
+    nx, ny, nz = 32, 24, 20
+    sim_, zp, hp, qp, grids, C_h, C_q = _one_class_setup(nx, ny, nz)
+    setup = sim.make_class_setup(
+        grids, 0, h_profile=hp, qt_profile=qp, z_profile=zp, C_h=C_h[0], C_qt=C_q[0],
+        b_h=sim._bound_buffers(C_h, 1)[0], b_qt=sim._bound_buffers(C_q, 1)[0],
+        aspect=np.ones(nz, np.float32), bounds=(315 * 1004.0, 355 * 1004.0, 0.0, 0.03),
+        key=O.class_key(np.random.SeedSequence(9)), flux_noise_scale=0.1, dtype=dtype)
+    rng = np.random.default_rng(4)
+    h = (800.0 * rng.standard_normal((nx, ny, nz))).astype(dtype)
+    q = (0.0008 * rng.standard_normal((nx, ny, nz))).astype(dtype)
+    F = (1.0 + 0.2 * rng.random((nx, ny, nz))).astype(dtype)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    ht, qt_, Ft = (torch.as_tensor(a, device='cuda') for a in (h, q, F))
+    rc = ResidentClass(setup, tdt)
+    for _ in range(2):
+        diag = {k: torch.empty_like(ht) for k in ("T", "qv", "qc", "qi", "p")}
+        rc.step(ht, qt_, Ft, diagnostics=diag)
+        out = {k: torch.empty((nx, ny, nz), dtype=tdt, pin_memory=True).numpy()
+               for k in ("qc",)}
+        got, _ = sim.field_step(h, q, F, setup, diagnostics=("qc", "qi"), out=out)
+        np.testing.assert_array_equal(h, ht.cpu().numpy())
+        np.testing.assert_array_equal(q, qt_.cpu().numpy())
+        np.testing.assert_array_equal(F, Ft.cpu().numpy())
+        np.testing.assert_array_equal(got["qc"], diag["qc"].cpu().numpy())
+        np.testing.assert_array_equal(got["qi"], diag["qi"].cpu().numpy())
+        assert got["qc"] is out["qc"] or np.shares_memory(got["qc"], out["qc"])
