@@ -60,6 +60,10 @@ def parse(argv=None):
     ap.add_argument("--cpu-sample", type=int, nargs=3, default=(128, 128, 256),
                     metavar=("NX", "NY", "NZ"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="tile requests per arrival rate in the serving episode (0: skip)")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=(100.0, 1000.0),
+                    help="Poisson arrival rates (requests/s) of the serving episode")
     return ap.parse_args(argv)
 
 
@@ -442,6 +446,25 @@ def main(argv=None):
                       "host arrays, transfers pipelined against the step)"}
         del h_host, q_host, F_host, out_host
 
+    # serving: world-coordinate cube tiles (32^3..256^3, weights .4/.3/.2/.1)
+    # from one world (seed 7) under Poisson arrivals, continuous batching over
+    # four CUDA streams; latency = arrival to tile on the host
+    serving = None
+    if args.serve_requests > 0:
+        from steam_b200.serving import TileServer, TileWorld, latency_summary, poisson_trace
+        tw = TileWorld((args.nx, args.ny, args.nz), seed=7, dtype=np_t)
+        tw.drop_world_field()
+        torch.cuda.empty_cache()
+        srv = TileServer(tw, n_slots=4, max_n=min(256, args.nz))
+        srv.serve(poisson_trace(tw, rate=1000.0, n_requests=16, seed=5))  # warm-up
+        serving = {"world": f"{args.nx}x{args.ny}x{args.nz}, seed 7",
+                   "sizes": "32^3/64^3/128^3/256^3 at 0.4/0.3/0.2/0.1",
+                   "slots": 4, "budget_bytes": srv.budget}
+        for rate in args.serve_rates:
+            done = srv.serve(poisson_trace(tw, rate, args.serve_requests, seed=4))
+            serving[f"{rate:g}_req_per_s"] = latency_summary(done)
+        del srv, tw
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(tuple(args.cpu_sample))
@@ -458,7 +481,7 @@ def main(argv=None):
                        "alpha": ALPHA, "C1": C1, "H": H, "Hz": HZ, "seed": 0,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (4.3 GB fields); no flush"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serving": serving,
             "gpu_launches": int(launches), "clocks": clk,
         }
         print(json.dumps(line), flush=True)
