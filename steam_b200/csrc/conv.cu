@@ -277,38 +277,55 @@ struct FusedShape {
   static constexpr int ZT = R * (kFZ / 4);       // z-filter tasks (4 outputs each)
 };
 
+// The fused kernel's filters as kernel-parameter constants: every tap index
+// is a compile-time constant after unrolling, so the multiply-adds read their
+// tap straight from the parameter bank (no shared-memory load per tap).
+// mix is re-indexed by (a, c, b), the pairs enumerated c-major, b-minor.
+template <typename A, int K>
+struct FusedTaps {
+  A z[kFMaxZ][K], y[2][K], x[kFMaxX][K];
+  A mix[kFMaxX * kFMaxPairs];
+  int cx, cy, cz;
+};
+
+template <typename T, typename A, int K>
+static FusedTaps<A, K> fused_taps(const SepParams<T>& p) {
+  FusedTaps<A, K> f;
+  for (int i = 0; i < K; ++i) {
+    f.z[0][i] = (A)p.taps[i];
+    f.z[1][i] = p.nzf > 1 ? (A)p.taps[K + i] : (A)0;
+    f.y[0][i] = (A)p.ytap(0)[i];
+    f.y[1][i] = p.nyf > 1 ? (A)p.ytap(1)[i] : (A)0;
+    f.x[0][i] = (A)p.xtap(0)[i];
+    f.x[1][i] = p.nxf > 1 ? (A)p.xtap(1)[i] : (A)0;
+  }
+  for (int t = 0; t < kFMaxX * kFMaxPairs; ++t) {
+    const int a = t / kFMaxPairs, cb = t % kFMaxPairs;
+    const int c = cb / 2, b = cb % 2;
+    double v = 0.0;
+    for (int q = 0; q < p.npairs; ++q)
+      if (a < p.nxf && p.pair_z[q] == c && p.pair_y[q] == b) v += p.mix[a * p.npairs + q];
+    f.mix[t] = (A)v;
+  }
+  f.cx = p.cx;
+  f.cy = p.cy;
+  f.cz = p.cz;
+  return f;
+}
+
 template <typename T, typename A, int K>
 __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
     const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
-    SepParams<T> p, FusedGeom<T> g, XEpi epi, double* __restrict__ partials) {
+    const __grid_constant__ FusedTaps<A, K> tp, FusedGeom<T> g, XEpi epi,
+    double* __restrict__ partials) {
   using S = FusedShape<K>;
   constexpr int R = S::R, C = S::C, NL = S::NL;
   extern __shared__ unsigned char smem_raw[];
   __shared__ double scratch[32];
-  __shared__ A s_zt[kFMaxZ][K], s_yt[2][K], s_xt[kFMaxX][K];
-  __shared__ A s_mix[kFMaxX * kFMaxPairs];
   __shared__ T s_pre[2][C];
   A* s_in0 = reinterpret_cast<A*>(smem_raw);  // [2][R*C]
   A* s_u = s_in0 + 2 * R * C;                            // [2][R][kFZ]
   const int t = threadIdx.x;
-  const int nzf = p.nzf, nxf = p.nxf, npairs = p.npairs;
-  for (int i = t; i < K; i += kFThreads) {
-    s_zt[0][i] = (A)p.taps[i];
-    s_zt[1][i] = nzf > 1 ? (A)p.taps[K + i] : (A)0;
-    s_yt[0][i] = (A)p.ytap(0)[i];
-    s_yt[1][i] = p.nyf > 1 ? (A)p.ytap(1)[i] : (A)0;
-    s_xt[0][i] = (A)p.xtap(0)[i];
-    s_xt[1][i] = nxf > 1 ? (A)p.xtap(1)[i] : (A)0;
-  }
-  if (t < kFMaxX * kFMaxPairs) {
-    // mix re-indexed by (a, c, b): pairs are enumerated c-major, b-minor
-    const int a = t / kFMaxPairs, cb = t % kFMaxPairs;
-    const int c = cb / 2, b = cb % 2;
-    double v = 0.0;
-    for (int q = 0; q < npairs; ++q)
-      if (a < nxf && p.pair_z[q] == c && p.pair_y[q] == b) v += p.mix[a * npairs + q];
-    s_mix[t] = (A)v;
-  }
   const int zt_i = blockIdx.x % g.nzt;
   const int yt_i = (blockIdx.x / g.nzt) % g.nyt;
   const int64_t xc = blockIdx.x / ((int64_t)g.nzt * g.nyt);
@@ -317,8 +334,8 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
   const int64_t xb = xc * g.chunk;
   const int64_t xe = (xb + g.chunk) < g.nx ? (xb + g.chunk) : g.nx;
   const int64_t count = (xe - xb) + K - 1;  // planes to process
-  const int64_t xin0 = xb - (K - 1 - p.cx);
-  const int padz = K - 1 - p.cz, pady = K - 1 - p.cy;
+  const int64_t xin0 = xb - (K - 1 - tp.cx);
+  const int padz = K - 1 - tp.cz, pady = K - 1 - tp.cy;
   for (int c = t; c < C; c += kFThreads) {
     const int z = z0 - padz + c;
     const bool in_z = z >= 0 && z < g.nz;
@@ -393,7 +410,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
       A a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
 #pragma unroll
       for (int l = 0; l < K; ++l) {
-        const A t0 = s_zt[0][l], t1 = s_zt[1][l];
+        const A t0 = tp.z[0][l], t1 = tp.z[1][l];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
           // out[z] uses staged column z + K - 1 - l
@@ -421,12 +438,12 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
         A v0 = 0, v1 = 0;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-          const A tj = s_yt[b][j];
+          const A tj = tp.y[b][j];
           v0 += tj * col[K - 1 - j];
           v1 += tj * col[K - j];
         }
-        const A m0 = s_mix[0 * kFMaxPairs + c * 2 + b];
-        const A m1 = s_mix[1 * kFMaxPairs + c * 2 + b];
+        const A m0 = tp.mix[0 * kFMaxPairs + c * 2 + b];
+        const A m1 = tp.mix[1 * kFMaxPairs + c * 2 + b];
         w0[0] += m0 * v0;
         w0[1] += m0 * v1;
         w1[0] += m1 * v0;
@@ -443,7 +460,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
 #pragma unroll
         for (int i = 0; i < K; ++i) {
           const int slot = (rr + i + 1) % K;
-          const A c0 = s_xt[0][i], c1 = s_xt[1][i];
+          const A c0 = tp.x[0][i], c1 = tp.x[1][i];
           acc[slot][0] += c0 * w0[0] + c1 * w1[0];
           acc[slot][1] += c0 * w0[1] + c1 * w1[1];
         }
@@ -609,13 +626,13 @@ static int launch_fused(const SepParams<T>& p, int64_t grid, const T* in, T* out
   if (p.kx == 13) {
     STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, A, 13>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fused_conv_kernel<T, A, 13><<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, p, g, epi,
-                                                                      partials);
+    fused_conv_kernel<T, A, 13><<<(unsigned)grid, kFThreads, sm, s>>>(
+        in, out, pre, fused_taps<T, A, 13>(p), g, epi, partials);
   } else {
     STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, A, 25>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fused_conv_kernel<T, A, 25><<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, p, g, epi,
-                                                                      partials);
+    fused_conv_kernel<T, A, 25><<<(unsigned)grid, kFThreads, sm, s>>>(
+        in, out, pre, fused_taps<T, A, 25>(p), g, epi, partials);
   }
   STEAM_LAUNCH_CHECK("conv fused");
   return STEAM_OK;

@@ -143,30 +143,66 @@ __global__ void kernel_build_kernel(int hx, int hy, int hz, T dx, T dy, T dz,
 }
 
 // ---- a17: thermodynamics ------------------------------------------------------
-// A warp owns 32 consecutive columns (contiguous in memory).  Levels are staged
-// 32 at a time through shared memory so that loads and stores are coalesced;
-// each lane then marches its own column with a float64 pressure accumulator.
-constexpr int kThZ = 8;
+// A warp owns 32 consecutive columns (contiguous in memory).  Levels go
+// through shared memory kThZ at a time so that loads and stores are
+// coalesced: each staging instruction moves 32 / kThZ columns x kThZ levels
+// with every lane active (kThZ floats = one 64-byte run per column).  Each
+// lane then marches its own column with a float64 pressure accumulator; the
+// five outputs overwrite the two input slots and three more in place.
+constexpr int kThZ = 16;
 constexpr int kThWarps = 4;
 constexpr int kThPitch = kThZ + 1;
+constexpr int kThArrays = 5;  // h -> T, qt -> qv, qc, qi, p
 
 template <typename T>
 struct ThermoConst {
   T cp, lv, g, t0, t1, dt, c622, es0, ea, eb, ec, dq;
 };
 
+// The float32 form divides by multiplying with the correctly rounded
+// reciprocal (at most one float32 ulp from the quotient) and takes exp from
+// the hardware exp2 outside the Newton loop too: the results stay within a
+// few float32 ulps of the correctly rounded forms, far inside the float32
+// tolerances of T (1e-3 K), the mixing ratios and p.  The float64 form keeps
+// the correctly rounded operations.
+__device__ __forceinline__ float th_div(float a, float b) { return __fmul_rn(a, __frcp_rn(b)); }
+__device__ __forceinline__ double th_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float th_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double th_exp(double x) { return exp(x); }
+
 template <typename T>
 __device__ __forceinline__ T bolton(T Tk, const ThermoConst<T>& k) {
-  return mul_rn(k.es0, d_exp(mul_rn(k.ea, sub_rn(Tk, k.eb)) / sub_rn(Tk, k.ec)));
+  return mul_rn(k.es0, th_exp(th_div(mul_rn(k.ea, sub_rn(Tk, k.eb)), sub_rn(Tk, k.ec))));
+}
+
+// exp(a) for one hypsometric step: the exponent -g dz / (Rd Tv) is small
+// (about -0.012 for 100 m levels), so the Taylor series of exp about 0 to
+// degree 12 is exact to below 2^-60 relative for |a| <= 1/8; larger |a|
+// take exp().
+__device__ __forceinline__ double exp_hyps(double a) {
+  if (!(fabs(a) <= 0.125)) return exp(a);
+  double s = 1.0 / 479001600.0;  // 1/12!
+  s = fma(s, a, 1.0 / 39916800.0);
+  s = fma(s, a, 1.0 / 3628800.0);
+  s = fma(s, a, 1.0 / 362880.0);
+  s = fma(s, a, 1.0 / 40320.0);
+  s = fma(s, a, 1.0 / 5040.0);
+  s = fma(s, a, 1.0 / 720.0);
+  s = fma(s, a, 1.0 / 120.0);
+  s = fma(s, a, 1.0 / 24.0);
+  s = fma(s, a, 1.0 / 6.0);
+  s = fma(s, a, 0.5);
+  s = fma(s, a, 1.0);
+  return fma(s, a, 1.0);
 }
 
 // Inside the Newton iterations the float32 form uses the hardware exp and
-// reciprocal: Newton corrects their few-ulp errors on the next step, and the
-// last step's residual moves T by ~1e-6 K, below a float32 ulp at 280 K.  The
-// float64 form keeps the correctly rounded functions.
+// approximate reciprocal: Newton corrects their few-ulp errors on the next
+// step, and the last step's residual moves T by ~1e-6 K, below a float32 ulp
+// at 280 K.  The float64 form keeps the correctly rounded functions.
 __device__ __forceinline__ float newton_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double newton_exp(double x) { return exp(x); }
-__device__ __forceinline__ float newton_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float newton_rcp(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double newton_rcp(double x) { return 1.0 / x; }
 
 template <typename T>
@@ -181,24 +217,28 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
   extern __shared__ unsigned char th_smem[];
   T* base = reinterpret_cast<T*>(th_smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // sh(a, c, z): array a (h, qt, T, qv, qc, qi, p) of column c, level z
+  // sh(a, c, z): slot a (0: h then T, 1: qt then qv, 2: qc, 3: qi, 4: p) of
+  // column c, level z of the chunk
   auto sh = [&](int a, int c, int z) -> T& {
-    return base[(((size_t)warp * 7 + a) * 32 + c) * kThPitch + z];
+    return base[((warp * kThArrays + a) * 32 + c) * kThPitch + z];
   };
-  const int64_t col0 =
-      ((int64_t)blockIdx.x * kThWarps + warp) * 32;
+  const int64_t col0 = ((int64_t)blockIdx.x * kThWarps + warp) * 32;
   if (col0 >= ncol) return;
   const int ncols = (int)((ncol - col0) < 32 ? (ncol - col0) : 32);
   const int64_t mycol = col0 + lane;
   double p_cur = ps_field ? (lane < ncols ? ps_field[mycol] : 0.0) : ps;
   const double g = 9.81, Rd = 287.04;
+  // staging geometry: lane -> (column group member, level) of a chunk
+  constexpr int kCPI = 32 / kThZ;  // columns per staging instruction
+  const int s_c = lane / kThZ, s_z = lane % kThZ;
   for (int z0 = 0; z0 < nz; z0 += kThZ) {
     const int zc = (nz - z0) < kThZ ? (nz - z0) : kThZ;
-    for (int c = 0; c < ncols; ++c) {
-      if (lane < zc) {
-        const int64_t o = (col0 + c) * nz + z0 + lane;
-        sh(0, c, lane) = h[o];
-        sh(1, c, lane) = qt[o];
+    for (int c0 = 0; c0 < ncols; c0 += kCPI) {
+      const int c = c0 + s_c;
+      if (c < ncols && s_z < zc) {
+        const int64_t o = (col0 + c) * nz + z0 + s_z;
+        sh(0, c, s_z) = h[o];
+        sh(1, c, s_z) = qt[o];
       }
     }
     __syncwarp();
@@ -215,9 +255,9 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
         }
         const T pl = (T)p_cur;
         const T zt = (T)zv[z];
-        const T Td = sub_rn(sub_rn(hl, mul_rn(k.lv, ql)), mul_rn(k.g, zt)) / k.cp;
+        const T Td = th_div(sub_rn(sub_rn(hl, mul_rn(k.lv, ql)), mul_rn(k.g, zt)), k.cp);
         T es = bolton(Td, k);
-        const T qvs = mul_rn(k.c622, es) / sub_rn(pl, es);
+        const T qvs = th_div(mul_rn(k.c622, es), sub_rn(pl, es));
         T Tl = Td, qvl = ql;
         if (ql > qvs) {
           T Tn = Td;
@@ -239,32 +279,33 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
           }
           Tl = Tn;
           const T e = bolton(Tn, k);
-          qvl = mul_rn(k.c622, e) / sub_rn(pl, e);
+          qvl = th_div(mul_rn(k.c622, e), sub_rn(pl, e));
         }
         T cond = sub_rn(ql, qvl);
         cond = cond > (T)0 ? cond : (T)0;
-        T lam = sub_rn(Tl, k.t0) / k.dt;
+        T lam = th_div(sub_rn(Tl, k.t0), k.dt);
         lam = lam < (T)0 ? (T)0 : (lam > (T)1 ? (T)1 : lam);
-        sh(2, lane, zz) = Tl;
-        sh(3, lane, zz) = qvl;
-        sh(4, lane, zz) = mul_rn(lam, cond);
-        sh(5, lane, zz) = mul_rn(sub_rn((T)1, lam), cond);
-        sh(6, lane, zz) = pl;
+        sh(0, lane, zz) = Tl;
+        sh(1, lane, zz) = qvl;
+        sh(2, lane, zz) = mul_rn(lam, cond);
+        sh(3, lane, zz) = mul_rn(sub_rn((T)1, lam), cond);
+        sh(4, lane, zz) = pl;
         if (z < nz - 1) {
           const double Tv = (double)Tl * (1.0 + 0.608 * (double)qvl);
-          p_cur *= exp(-g * dzv[z] / (Rd * Tv));
+          p_cur *= exp_hyps(-g * dzv[z] * __drcp_rn(Rd * Tv));
         }
       }
     }
     __syncwarp();
-    for (int c = 0; c < ncols; ++c) {
-      if (lane < zc) {
-        const int64_t o = (col0 + c) * nz + z0 + lane;
-        To[o] = sh(2, c, lane);
-        qvo[o] = sh(3, c, lane);
-        qco[o] = sh(4, c, lane);
-        qio[o] = sh(5, c, lane);
-        po[o] = sh(6, c, lane);
+    for (int c0 = 0; c0 < ncols; c0 += kCPI) {
+      const int c = c0 + s_c;
+      if (c < ncols && s_z < zc) {
+        const int64_t o = (col0 + c) * nz + z0 + s_z;
+        To[o] = sh(0, c, s_z);
+        qvo[o] = sh(1, c, s_z);
+        qco[o] = sh(2, c, s_z);
+        qio[o] = sh(3, c, s_z);
+        po[o] = sh(4, c, s_z);
       }
     }
     __syncwarp();
@@ -373,8 +414,8 @@ extern "C" int steam_thermo_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
   const double b0 = compose ? bounds[0] : 0.0, b1 = compose ? bounds[1] : 0.0;
   const double b2 = compose ? bounds[2] : 0.0, b3 = compose ? bounds[3] : 0.0;
   const int64_t blocks = (ncol + 32 * kThWarps - 1) / (32 * kThWarps);
-  const size_t sm_f = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(float);
-  const size_t sm_d = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(double);
+  const size_t sm_f = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(float);
+  const size_t sm_d = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(double);
   const double* zv = prof_dev;
   if (dtype == STEAM_F32) {
     STEAM_CUDA(cudaFuncSetAttribute(thermo_kernel<float>,
@@ -436,8 +477,8 @@ extern "C" int steam_thermo(int dtype, int64_t nx, int64_t ny, int64_t nz,
     return fail(STEAM_ERR_CUDA, std::string("steam_thermo: ") + cudaGetErrorString(e));
   }
   const int64_t blocks = (ncol + 32 * kThWarps - 1) / (32 * kThWarps);
-  const size_t sm_f = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(float);
-  const size_t sm_d = (size_t)kThWarps * 7 * 32 * kThPitch * sizeof(double);
+  const size_t sm_f = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(float);
+  const size_t sm_d = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(double);
   if (dtype == STEAM_F32) {
     e = cudaFuncSetAttribute(thermo_kernel<float>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_f);
