@@ -208,8 +208,10 @@ int steam_scalar_pattern(int dtype, int64_t nx, int64_t ny, int64_t nz,
  * demean and clip, then the zero-mean shift mu, solved exactly (bracketed
  * Newton on the piecewise-linear level mean) instead of by 60 bisection
  * sweeps.  pert += delta; with record_applied the increment buffer is left
- * holding pert_after - pert_before.  ledger_out (HOST, may be NULL) receives
- * per level { a0, n_loop, final_demean, mu (NaN if none), n_sweeps }. */
+ * holding pert_after - pert_before, otherwise it is scratch (the sweeps store
+ * the chain's running state there; its contents on return are unspecified).
+ * ledger_out (HOST, may be NULL) receives per level { a0, n_loop,
+ * final_demean, mu (NaN if none), n_sweeps }. */
 size_t steam_bounded_add_workspace_bytes(int64_t nz, int32_t n_rescale);
 int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
                       void* pert, const double* mean_1d, void* increment,

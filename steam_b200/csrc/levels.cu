@@ -449,6 +449,12 @@ struct BAChain {
   const T* cand;  // [nz][kMuCand]
   const T* mean;
   const int* run;  // device flag: the sweep returns at once when it is 0 (NULL: always run)
+  // write-back form (ba_fold_kernel): the increment buffer holds the chain's
+  // first applied[z] steps (and the final clip when fin_stored[z]) already
+  // applied; still[z] marks a level whose last step's scale is not decided
+  const int* applied;
+  const int* fin_stored;
+  const int* still;
   int R;
   T lo, hi;
 };
@@ -685,6 +691,152 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 4)) ba_sweep4
   }
 }
 
+// ---- bounded add sweeps, write-back form -------------------------------------------
+// The increment buffer is the chain's running state: a sweep applies only the
+// steps not yet stored -- at most one whose parameters are now final (the last
+// rescale step of the previous sweep, or the final demean/clip of a level that
+// left the loop) and at most one tentative step (the current rescale step,
+// scale still 1) -- and writes the final part back.  Every sweep therefore
+// costs the same few operations per cell instead of replaying the whole chain
+// from the raw increment.  nz % 4 == 0; a thread owns 4 consecutive levels.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_STATS ? 3 : 4)))
+    ba_fold_kernel(
+    T* __restrict__ d0, T* __restrict__ pert, int record, int64_t nx, int64_t ny, int nz,
+    Win w, BAChain<T> c, double* __restrict__ partials) {
+  if (c.run && *c.run == 0) return;
+  __shared__ double red[4 * kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  // per level: fold step (dm, sc), final clip (dm), tentative step (dm),
+  // mean, mu, candidates; flags as 0/1 in T
+  T* s_fdm = reinterpret_cast<T*>(ba_smem);
+  T* s_fsc = s_fdm + nz;
+  T* s_fon = s_fsc + nz;
+  T* s_cdm = s_fon + nz;
+  T* s_con = s_cdm + nz;
+  T* s_tdm = s_con + nz;
+  T* s_ton = s_tdm + nz;
+  T* s_mean = s_ton + nz;
+  T* s_mu = s_mean + nz;
+  T* s_mon = s_mu + nz;
+  T* s_cand = s_mon + nz;  // [kMuCand][nz]
+  const int R = c.R;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    const int ns = c.nsteps[z], ap = c.applied[z];
+    const int nfin = c.still[z] ? ns - 1 : ns;
+    const bool fold_step = nfin > ap;  // == ap + 1 by construction
+    s_fon[z] = fold_step ? (T)1 : (T)0;
+    s_fdm[z] = fold_step ? c.demean[z * R + ap] : (T)0;
+    s_fsc[z] = fold_step ? c.scale[z * R + ap] : (T)1;
+    const bool fold_fin = c.has_final[z] && !c.fin_stored[z];
+    s_con[z] = fold_fin ? (T)1 : (T)0;
+    s_cdm[z] = c.final_dm[z];
+    const bool tent = ns > nfin;  // the current rescale step, scale 1
+    s_ton[z] = tent ? (T)1 : (T)0;
+    s_tdm[z] = tent ? c.demean[z * R + nfin] : (T)0;
+    s_mean[z] = c.mean[z];
+    s_mon[z] = c.has_mu[z] ? (T)1 : (T)0;
+    s_mu[z] = c.mu[z];
+#pragma unroll
+    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = c.cand[z * kMuCand + k];
+  }
+  __syncthreads();
+  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
+  const int nz4 = nz / 4;
+  const int cpi = kLvThreads / nz4;
+  const int t = threadIdx.x;
+  const bool active = t < cpi * nz4;
+  const int z4 = (t % nz4) * 4;
+  const int cofs = t / nz4;
+  const V4<T> fdm = ld4(s_fdm + z4), fsc = ld4(s_fsc + z4);
+  const V4<T> cdm = ld4(s_cdm + z4), tdm = ld4(s_tdm + z4);
+  const V4<T> mean = ld4(s_mean + z4);
+  // per-level switches as bits: fold step (l), fold final clip (4 + l),
+  // tentative step (8 + l), shift (12 + l)
+  unsigned on = 0;
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    on |= (s_fon[z4 + l] != (T)0 ? 1u : 0u) << l;
+    on |= (s_con[z4 + l] != (T)0 ? 1u : 0u) << (4 + l);
+    on |= (s_ton[z4 + l] != (T)0 ? 1u : 0u) << (8 + l);
+    on |= (s_mon[z4 + l] != (T)0 ? 1u : 0u) << (12 + l);
+  }
+  const bool any_fold = (on & 0xffu) != 0;
+  double acc[Q][4];
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+#pragma unroll
+    for (int l = 0; l < 4; ++l) acc[q][l] = 0.0;
+  const int64_t ncol = nx * ny;
+  if (active) {
+    const int64_t step = (int64_t)gridDim.x * cpi;
+    ColWalk cw;
+    cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
+    for (; cw.col < ncol; cw.advance(step)) {
+      const int64_t i = cw.col * nz + z4;
+      const V4<T> dv = ld4(d0 + i), pv = ld4(pert + i);
+      const bool in_w = w.in(cw.x, cw.y);
+      V4<T> df, pn, dn;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const T p0 = pv.v[l];
+        const T phi = add_rn(p0, mean.v[l]);
+        const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
+        T d = dv.v[l];
+        if (on & (1u << l)) d = mul_rn(clampv(sub_rn(d, fdm.v[l]), clo, chi), fsc.v[l]);
+        if (on & (16u << l)) d = clampv(sub_rn(d, cdm.v[l]), clo, chi);
+        df.v[l] = d;
+        if (on & (256u << l)) d = clampv(sub_rn(d, tdm.v[l]), clo, chi);
+        if (MODE == BA_APPLY) {
+          if (on & (4096u << l)) d = clampv(sub_rn(d, s_mu[z4 + l]), clo, chi);
+          pn.v[l] = add_rn(p0, d);
+          dn.v[l] = sub_rn(pn.v[l], p0);
+        } else if (in_w) {
+          if (MODE == BA_STATS) {
+            acc[0][l] += (double)d;
+            acc[1 % Q][l] += (double)(d < (T)0 ? -d : d);
+          } else {
+#pragma unroll
+            for (int k = 0; k < kMuCand; ++k) {
+              const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
+              const T tv = clampv(raw, clo, chi);
+              acc[2 * k][l] += (double)tv;
+              acc[(2 * k + 1) % Q][l] += (raw > clo && raw < chi) ? 1.0 : 0.0;
+            }
+          }
+        }
+      }
+      if (MODE == BA_APPLY) {
+        st4(pert + i, pn);
+        if (record) st4(d0 + i, dn);
+      } else if (any_fold) {
+        st4(d0 + i, df);
+      }
+    }
+  }
+  if (MODE == BA_APPLY) return;
+  // deterministic reduction: per level, the cpi column slots in order
+  const int nb = gridDim.x;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    __syncthreads();
+    if (active)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) red[cofs * nz + z4 + l] = acc[q][l];
+    __syncthreads();
+    for (int z = t; z < nz; z += kLvThreads) {
+      double sacc = 0.0;
+      for (int cc = 0; cc < cpi; ++cc) sacc += red[cc * nz + z];
+      partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
+    }
+  }
+}
+
+template <typename T>
+static size_t ba_fold_smem_bytes(int64_t nz) {
+  return sizeof(T) * (size_t)nz * (11 + kMuCand);
+}
+
 // ---- projection sweeps (float64 level arithmetic) -----------------------------
 enum { PJ_STATS = 0, PJ_MU = 1, PJ_APPLY = 2 };
 
@@ -899,6 +1051,9 @@ struct BAState {
   int* still;
   int* n_loop;
   int* need;
+  int* applied;     // write-back form: chain steps already stored in the increment
+  int* fin_stored;  // write-back form: final clip already stored
+  int wb;           // the sweeps write back (vectorised path)
   MuSolver<T>* solver;
   // run flags: [0] the first sweep, [1 + k] rescale sweep k (k < R),
   // [1 + R + it] mu sweep it (it < kMuMaxSweeps); [kFlagSweeps] sweeps run
@@ -933,6 +1088,8 @@ __global__ void ba_init_kernel(BAState<T> st, const double* __restrict__ mean_1d
     st.still[z] = 0;
     st.n_loop[z] = 0;
     st.need[z] = 0;
+    st.applied[z] = 0;
+    st.fin_stored[z] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const int nf = ba_flag_count<T>(R);
@@ -973,6 +1130,14 @@ __device__ void ba_prepare_step(BAState<T>& st, int z, int k, int* next_flag) {
   atomicOr(next_flag, 1);
 }
 
+// After a write-back sweep: every final part of the chain is now stored.
+template <typename T>
+__device__ void ba_note_stored(BAState<T>& st, int z) {
+  if (!st.wb) return;
+  st.applied[z] = st.still[z] ? st.nsteps[z] - 1 : st.nsteps[z];
+  st.fin_stored[z] = st.has_final[z];
+}
+
 template <typename T>
 __device__ void ba_count_sweep(BAState<T>& st) {
   if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
@@ -1009,6 +1174,7 @@ __global__ void ba_loop_kernel(BAState<T> st, const double* __restrict__ tot, in
   const int nz = st.nz;
   ba_count_sweep(st);
   for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    ba_note_stored(st, z);
     if (!st.still[z]) continue;
     const double sum_d = tot[z], m_abs = tot[nz + z] / st.N;
     st.cur_mean[z] = sum_d / st.N;
@@ -1057,6 +1223,7 @@ __global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int 
   const int nz = st.nz;
   ba_count_sweep(st);
   for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    ba_note_stored(st, z);
     if (!st.need[z]) continue;
     MuSolver<T> sv = st.solver[z];
     if (sv.done) continue;
@@ -1109,7 +1276,7 @@ static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
   return carve_bytes((size_t)3 * nz, sizeof(int)) +                       // nsteps, has_final, has_mu
          carve_bytes((size_t)nz * (2 * (size_t)R + 4 + kMuCand), elem) +   // chain values
          carve_bytes((size_t)3 * nz, sizeof(double)) +                      // a0, cur_mean, final_d
-         carve_bytes((size_t)4 * nz, sizeof(int)) +                         // active, still, n_loop, need
+         carve_bytes((size_t)6 * nz, sizeof(int)) +  // active, still, n_loop, need, applied, fin_stored
          carve_bytes((size_t)nz * sizeof(MuSolver<double>), 1) +
          carve_bytes((size_t)(2 + R + kMuMaxSweeps), sizeof(int)) +
          carve_bytes((size_t)5 * nz, sizeof(double)) +                      // ledger
@@ -1152,12 +1319,15 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   st.still = c.take<int>(nz);
   st.n_loop = c.take<int>(nz);
   st.need = c.take<int>(nz);
+  st.applied = c.take<int>(nz);
+  st.fin_stored = c.take<int>(nz);
   st.solver = c.take<MuSolver<T>>(nz);
   st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
   st.ledger = c.take<double>((size_t)5 * nz);
   if (!partials || !totals || !st.nsteps || !st.has_final || !st.has_mu || !st.demean ||
       !st.scale || !st.final_dm || !st.mu || !st.mean || !st.cand || !st.a0 || !st.cur_mean ||
-      !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.solver ||
+      !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.applied ||
+      !st.fin_stored || !st.solver ||
       !st.flags || !st.ledger)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
   st.R = R;
@@ -1167,20 +1337,21 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   st.tol_rel = sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49);
   *ledger_dev = st.ledger;
 
-  const size_t ba_sm = ba_smem_bytes<T>(nz, R);
-  STEAM_REQUIRE(ba_sm <= 200 * 1024, "steam_bounded_add: n_rescale * nz too large");
   const bool vec4 = nz % 4 == 0 && nz <= 4 * kLvThreads &&
                     ((uintptr_t)pert % 16 == 0) && ((uintptr_t)inc % 16 == 0);
+  st.wb = vec4 ? 1 : 0;
+  const size_t ba_sm = vec4 ? ba_fold_smem_bytes<T>(nz) : ba_smem_bytes<T>(nz, R);
+  STEAM_REQUIRE(ba_sm <= 200 * 1024, "steam_bounded_add: n_rescale * nz too large");
   const int grid4 = vec4 ? stride_grid((ncol + (kLvThreads / (nz / 4)) - 1) /
                                            (kLvThreads / (nz / 4)), 1, kLvBlocksPerSm)
                          : 0;
   const int sweep_grid = vec4 ? grid4 : grid;
   if (vec4) {
-    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_STATS>,
+    STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_STATS>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_MU>,
+    STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_MU>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep4_kernel<T, BA_APPLY>,
+    STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_APPLY>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
   } else if (m.packed) {
     STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, 1>,
@@ -1207,6 +1378,9 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   ch.mu = st.mu;
   ch.cand = st.cand;
   ch.mean = st.mean;
+  ch.applied = st.applied;
+  ch.fin_stored = st.fin_stored;
+  ch.still = st.still;
   ch.R = R;
   ch.lo = (T)phi_min;
   ch.hi = (T)phi_max;
@@ -1216,8 +1390,8 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
     ch.run = run;
     if (mode == BA_STATS) {
       if (vec4)
-        ba_sweep4_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
-            inc, pert, out, rec, nx, ny, (int)nz, w, ch, partials);
+        ba_fold_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
       else if (m.packed)
         ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
@@ -1226,8 +1400,8 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
     } else if (mode == BA_MU) {
       if (vec4)
-        ba_sweep4_kernel<T, BA_MU><<<grid4, kLvThreads, ba_sm, s>>>(
-            inc, pert, out, rec, nx, ny, (int)nz, w, ch, partials);
+        ba_fold_kernel<T, BA_MU><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
       else if (m.packed)
         ba_sweep_kernel<T, BA_MU, 1><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
@@ -1236,8 +1410,8 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
     } else {
       if (vec4)
-        ba_sweep4_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_sm, s>>>(
-            inc, pert, out, rec, nx, ny, (int)nz, w, ch, partials);
+        ba_fold_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
       else if (m.packed)
         ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
