@@ -936,9 +936,6 @@ def simulate(h_profile, qt_profile, nx, ny, dx, dy, outer_scale, spheroscale,
     """
     check_device(device, "simulate")
     torch = _lib.require_cuda("simulate")
-    if stream_to_disk or _force_tiling is not None:
-        raise NotImplementedError("out-of-core streaming is not part of the device path; "
-                                  "the whole cascade stays resident in HBM")
     seed_was_none = seed is None
     if seed is None:
         seed = int(np.random.SeedSequence().generate_state(1)[0] >> 1)
@@ -1030,12 +1027,44 @@ def simulate(h_profile, qt_profile, nx, ny, dx, dy, outer_scale, spheroscale,
     comp_k = _compensation_profiles(k_values, grids['z_arrays'], sph_profile, z_profile,
                                     anisotropy)
     child_seeds = seed_sequence.spawn(n_classes)
-    (h_pert, qt_pert, flux_field, deficit_h, deficit_qt, deficit_flux, final_grid,
-     run_ledger) = cascade_loop(
-        h_profile, qt_profile, z_profile, grids, C_h_k, C_qt_k, b_h_k, b_qt_k, aspect_k,
-        h_min, h_max, qt_min, qt_max, min_distance_to_ground, sparsity_factors, child_seeds,
-        n_scale_classes_per_dyad=n_scale_classes_per_dyad, turbulon_shape=turbulon_shape,
-        device=device, comp_k=comp_k, ledger=ledger, dtype=dtype, resident=True)
+    store = None
+    if stream_to_disk or _force_tiling is not None:
+        # the reference's out-of-core driver (steam/simulate.py:1240-1412): here
+        # the cascade runs resident and its final fields leave through the store
+        from .streaming import plan_tiling, streamed_cascade_loop
+        if ledger is not None:
+            raise ValueError("simulate: a ledger replay does not stream; drop ledger=")
+        kshape = _turbulon_envelope(1, 1 / (2 * s_x), 1 / (2 * s_y), 1 / (2 * s_z),
+                                    support_factor=SUPPORT_FACTOR, shape=turbulon_shape,
+                                    dtype=np.float64).shape
+        plan = plan_tiling(grids, kshape, budget_bytes=memory_budget, device=device,
+                           force=_force_tiling, save_increments=save_for_refinement)
+        if scratch_dir is None:
+            scratch_dir = (Path(output_path).parent / f".steam_scratch_{Path(output_path).stem}"
+                           if output_path is not None else Path.cwd() / ".steam_scratch")
+        (h_m, qt_m, flux_m, dh_m, dq_m, dF_m, final_grid, run_ledger,
+         store) = streamed_cascade_loop(
+            h_profile, qt_profile, z_profile, grids, C_h_k, C_qt_k, b_h_k, b_qt_k, aspect_k,
+            h_min, h_max, qt_min, qt_max, min_distance_to_ground, sparsity_factors,
+            child_seeds, plan, scratch_dir, n_scale_classes_per_dyad=n_scale_classes_per_dyad,
+            turbulon_shape=turbulon_shape, device=device, comp_k=comp_k, dtype=dtype)
+        tdt = torch_dtype(dtype)
+
+        def back(m):
+            return None if m is None else to_device(np.ascontiguousarray(m), dtype=tdt)[0]
+
+        h_pert, qt_pert, flux_field = back(h_m), back(qt_m), back(flux_m)
+        deficit_h, deficit_qt, deficit_flux = back(dh_m), back(dq_m), back(dF_m)
+        del h_m, qt_m, flux_m, dh_m, dq_m, dF_m
+        store.destroy()
+    else:
+        (h_pert, qt_pert, flux_field, deficit_h, deficit_qt, deficit_flux, final_grid,
+         run_ledger) = cascade_loop(
+            h_profile, qt_profile, z_profile, grids, C_h_k, C_qt_k, b_h_k, b_qt_k, aspect_k,
+            h_min, h_max, qt_min, qt_max, min_distance_to_ground, sparsity_factors,
+            child_seeds, n_scale_classes_per_dyad=n_scale_classes_per_dyad,
+            turbulon_shape=turbulon_shape, device=device, comp_k=comp_k, ledger=ledger,
+            dtype=dtype, resident=True)
     z_final = final_grid['z'].astype(np.float32)
     h_mean_final = np.interp(z_final, z_profile, h_profile).astype(np.float32)
     qt_mean_final = np.interp(z_final, z_profile, qt_profile).astype(np.float32)

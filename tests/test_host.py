@@ -113,3 +113,32 @@ def test_separable_plan_reconstructs_kernel(golden):
             m = sp.mix[a * sp.n_pairs + q]
             rec += m * np.einsum('i,j,k->ijk', X[a], Y[sp.pair_y[q]], Z[sp.pair_z[q]])
     assert np.linalg.norm(rec - K) / np.linalg.norm(K) < 1e-6
+
+
+def test_tile_store_owns_only_its_subtree(tmp_path):
+    from steam_b200.streaming import TileStore
+    st = TileStore(tmp_path)
+    raw = st.create(0, "h", (4, 3, 5))
+    raw[...] = np.arange(60, dtype=np.float32).reshape(5, 4, 3)
+    view = st.open(0, "h")
+    assert view.shape == (4, 3, 5) and view[1, 2, 3] == raw[3, 1, 2]
+    (tmp_path / "keep.txt").write_text("caller data")
+    st.destroy()
+    assert (tmp_path / "keep.txt").exists() and not st.root.exists()
+    foreign = tmp_path / "foreign"
+    foreign.mkdir()
+    (foreign / "x").write_text("x")
+    with pytest.raises(OSError):
+        TileStore(tmp_path, owned_root=foreign)
+
+
+def test_plan_tiling_halo_and_budget():
+    from steam_b200.streaming import plan_tiling
+    grids = {'k': np.array([400.0, 200.0]), 'nx': np.array([64, 128]),
+             'ny': np.array([64, 128]), 'nz': np.array([32, 64])}
+    plan = plan_tiling(grids, (37, 13, 13), budget_bytes=1 << 40)
+    assert plan.horizon == 2 and plan.halo == (19, 7) and plan.tiles == {}
+    forced = plan_tiling(grids, (13, 13, 13), force=(1, 2, 2))
+    assert forced.horizon == 1 and forced.tiles == {1: (2, 2)}
+    with pytest.raises(MemoryError):
+        plan_tiling(grids, (13, 13, 13), budget_bytes=1000)
