@@ -289,6 +289,27 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+# Replicas: one independent workload per rank, timed as the slowest rank
+# ---------------------------------------------------------------------------
+
+def slowest_rank_ms(ms, world, device):
+    """The max over ranks of a per-rank elapsed time (every rank calls it)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(nvox, steps, ms, world):
+    """Whole-job Mvoxels/s: every rank processed ``steps`` workloads of ``nvox``
+    voxels; ``ms`` is the slowest rank's time."""
+    return world * nvox * steps / (ms / 1e3) / 1e6
+
+
+# ---------------------------------------------------------------------------
 # Device arm
 # ---------------------------------------------------------------------------
 
@@ -364,12 +385,9 @@ def main(argv=None):
         dist.barrier()
     ms = t_start.elapsed_time(t_end)
     clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = slowest_rank_ms(ms, world, "cuda")
     ms_per_step = ms / max(args.steps, 1)
-    value = world * nvox * args.steps / (ms / 1e3) / 1e6
+    value = replica_throughput(nvox, args.steps, ms, world)
 
     # one instrumented step: per-entry device time for the roofline
     hp.copy_(h0)
@@ -435,11 +453,8 @@ def main(argv=None):
             e1.record()
             torch.cuda.synchronize()
             total += e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([total], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
-        e2e = {"value": world * nvox * args.e2e_steps / (total / 1e3) / 1e6,
+        total = slowest_rank_ms(total, world, "cuda")
+        e2e = {"value": replica_throughput(nvox, args.e2e_steps, total, world),
                "unit": "Mvoxels/s", "h2d_bytes_per_step": 3 * elem * nvox,
                "d2h_bytes_per_step": 5 * elem * nvox,
                "api": "steam_b200.simulate.field_step (numpy in, numpy out; page-locked "
