@@ -134,6 +134,15 @@ int steam_conv_separable(int dtype, int64_t nx, int64_t ny, int64_t nz,
                          const steam_window_t* window, double* sums_out,
                          void* workspace, size_t workspace_bytes,
                          steam_stream_t stream);
+/* Tuning of the fused separable kernel, which has no counterpart in the
+ * reference (its FFT block length is fixed, steam/utils.py:341): x planes
+ * per CTA for fields of shape (nx, ny, nz), chosen by the host autotuner
+ * (steam_b200/ensemble.py); 0 restores the default (256).  The chunk changes
+ * which CTA computes an output, never the order of its sums, so results are
+ * identical for every chunk.  The workspace query already covers any chunk. */
+int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t chunk);
+int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz);
+
 /* Dense-kernel form (any kernel; direct summation over the taps).  `kernel`
  * is a DEVICE array (kx, ky, kz) of the call's dtype, already folded onto the
  * field period; centres are (k-1)//2 per axis. */

@@ -8,6 +8,10 @@
 //   x-pass: out = sum_a (sum_p mix_ap v_p) (*)_x X_a, with the epilogue.
 #include "common.cuh"
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include <memory>
 #include <vector>
 
@@ -522,10 +526,27 @@ static size_t fused_smem(int k, size_t elem) {
   return elem * ((size_t)2 * R * C + (size_t)kFMaxZ * R * kFZ);
 }
 
-static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz) {
+// x planes per CTA of the fused kernel, per field shape: set by the host's
+// autotuner (steam_conv_set_xchunk), kFChunk otherwise.  The smallest
+// allowed chunk bounds the workspace query.
+constexpr int kFChunkMin = 16;
+static std::mutex g_chunk_mu;
+static std::map<std::tuple<int64_t, int64_t, int64_t>, int> g_chunk;
+
+static int fused_chunk(int64_t nx, int64_t ny, int64_t nz) {
+  std::lock_guard<std::mutex> lock(g_chunk_mu);
+  auto it = g_chunk.find(std::make_tuple(nx, ny, nz));
+  return it == g_chunk.end() ? kFChunk : it->second;
+}
+
+static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz, int chunk) {
   const int64_t nzt = (nz + kFZ - 1) / kFZ, nyt = (ny + kFY - 1) / kFY;
-  const int64_t nxc = (nx + kFChunk - 1) / kFChunk;
+  const int64_t nxc = (nx + chunk - 1) / chunk;
   return nzt * nyt * nxc;
+}
+
+static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz) {
+  return fused_grid(nx, ny, nz, fused_chunk(nx, ny, nz));
 }
 
 // ---- dense direct convolution ----------------------------------------------
@@ -644,7 +665,7 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
                      const double* pre_mul, const T* pre_dev, void* out_v, int epilogue,
                      const steam_window_t* win, double* sums_out, double* totals_dev,
                      void* ws, size_t ws_bytes, cudaStream_t s) {
-  const int64_t grid = fused_grid(nx, ny, nz);
+  const int64_t grid = fused_grid(nx, ny, nz, fused_chunk(nx, ny, nz));
   Carver c(ws, ws_bytes);
   const bool use_pre = pre_div != nullptr || pre_mul != nullptr || pre_dev != nullptr;
   T* pre = c.take<T>((size_t)2 * nz);
@@ -670,7 +691,7 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
   g.nz = (int)nz;
   g.nzt = (int)((nz + kFZ - 1) / kFZ);
   g.nyt = (int)((ny + kFY - 1) / kFY);
-  g.chunk = kFChunk;
+  g.chunk = fused_chunk(nx, ny, nz);
   g.use_pre = use_pre ? 1 : 0;
   XEpi epi;
   epi.mode = epilogue;
@@ -711,7 +732,7 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   if (rc) return rc;
   SepParams<T>& p = *pp;
   const int64_t plane = nx * ny * nz;
-  if (fused_supported(p) && fused_grid(nx, ny, nz) < ((int64_t)1 << 31) &&
+  if (fused_supported(p) && fused_grid(nx, ny, nz, kFChunkMin) < ((int64_t)1 << 31) &&
       ny * nz < ((int64_t)1 << 31))
     return run_fused<T>(nx, ny, nz, p, in_v, pre_div, pre_mul, pre_dev, out_v, epilogue,
                         win, sums_out, totals_dev, ws, ws_bytes, s);
@@ -826,12 +847,13 @@ extern "C" size_t steam_conv_workspace_bytes(int dtype, int64_t nx, int64_t ny,
   bool fused = spec->kx == spec->ky && spec->ky == spec->kz &&
                (spec->kx == 13 || spec->kx == 25) && spec->n_z <= kFMaxZ &&
                spec->n_y <= 2 && spec->n_x <= kFMaxX && spec->n_pairs <= kFMaxPairs &&
-               fused_grid(nx, ny, nz) < ((int64_t)1 << 31) && ny * nz < ((int64_t)1 << 31);
+               fused_grid(nx, ny, nz, kFChunkMin) < ((int64_t)1 << 31) &&
+               ny * nz < ((int64_t)1 << 31);
   for (int q = 0; fused && q < spec->n_pairs; ++q)
     if (spec->pair_z[q] >= 2 || spec->pair_y[q] >= 2) fused = false;
   if (fused)
     return carve_bytes((size_t)2 * nz, elem) +
-           carve_bytes((size_t)fused_grid(nx, ny, nz) * 2, sizeof(double)) +
+           carve_bytes((size_t)fused_grid(nx, ny, nz, kFChunkMin) * 2, sizeof(double)) +
            carve_bytes(2, sizeof(double));
   return multi;
 }
@@ -912,6 +934,22 @@ extern "C" int steam_conv_separable_async(
                                  nullptr, (const double*)pre_dev, out, epilogue, window,
                                  nullptr, sums_dev, workspace, workspace_bytes, s);
   return fail(STEAM_ERR_ARG, "steam_conv_separable_async: bad dtype");
+}
+
+extern "C" int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t chunk) {
+  STEAM_REQUIRE(nx >= 1 && ny >= 1 && nz >= 1, "steam_conv_set_xchunk: empty shape");
+  STEAM_REQUIRE(chunk == 0 || (chunk >= kFChunkMin && chunk <= 4096),
+                "steam_conv_set_xchunk: chunk must be 0 (default) or in [16, 4096]");
+  std::lock_guard<std::mutex> lock(g_chunk_mu);
+  if (chunk == 0)
+    g_chunk.erase(std::make_tuple(nx, ny, nz));
+  else
+    g_chunk[std::make_tuple(nx, ny, nz)] = chunk;
+  return STEAM_OK;
+}
+
+extern "C" int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz) {
+  return fused_chunk(nx, ny, nz);
 }
 
 extern "C" int steam_conv_dense(int dtype, int64_t nx, int64_t ny, int64_t nz,

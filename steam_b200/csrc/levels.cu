@@ -699,14 +699,20 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 4)) ba_sweep4
 // scale still 1) -- and writes the final part back.  Every sweep therefore
 // costs the same few operations per cell instead of replaying the whole chain
 // from the raw increment.  nz % 4 == 0; a thread owns 4 consecutive levels.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_STATS ? 3 : 4)))
-    ba_fold_kernel(
-    T* __restrict__ d0, T* __restrict__ pert, int record, int64_t nx, int64_t ny, int nz,
-    Win w, BAChain<T> c, double* __restrict__ partials) {
-  if (c.run && *c.run == 0) return;
-  __shared__ double red[4 * kLvThreads];
-  extern __shared__ unsigned char ba_smem[];
+// Loads of values other blocks of the same grid wrote in this launch go
+// through L2 (ld.cg), never a stale L1 line.
+template <bool COH, typename V>
+__device__ __forceinline__ V ldc(const V* p) {
+  if (COH) return __ldcg(p);
+  return *p;
+}
+
+template <typename T, int MODE, bool COH>
+__device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__ pert,
+                                             int record, int64_t nx, int64_t ny, int nz,
+                                             const Win& w, const BAChain<T>& c,
+                                             double* __restrict__ partials,
+                                             unsigned char* ba_smem, double* red) {
   // per level: fold step (dm, sc), final clip (dm), tentative step (dm),
   // mean, mu, candidates; flags as 0/1 in T
   T* s_fdm = reinterpret_cast<T*>(ba_smem);
@@ -722,23 +728,23 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_S
   T* s_cand = s_mon + nz;  // [kMuCand][nz]
   const int R = c.R;
   for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-    const int ns = c.nsteps[z], ap = c.applied[z];
-    const int nfin = c.still[z] ? ns - 1 : ns;
+    const int ns = ldc<COH>(c.nsteps + z), ap = ldc<COH>(c.applied + z);
+    const int nfin = ldc<COH>(c.still + z) ? ns - 1 : ns;
     const bool fold_step = nfin > ap;  // == ap + 1 by construction
     s_fon[z] = fold_step ? (T)1 : (T)0;
-    s_fdm[z] = fold_step ? c.demean[z * R + ap] : (T)0;
-    s_fsc[z] = fold_step ? c.scale[z * R + ap] : (T)1;
-    const bool fold_fin = c.has_final[z] && !c.fin_stored[z];
+    s_fdm[z] = fold_step ? ldc<COH>(c.demean + z * R + ap) : (T)0;
+    s_fsc[z] = fold_step ? ldc<COH>(c.scale + z * R + ap) : (T)1;
+    const bool fold_fin = ldc<COH>(c.has_final + z) && !ldc<COH>(c.fin_stored + z);
     s_con[z] = fold_fin ? (T)1 : (T)0;
-    s_cdm[z] = c.final_dm[z];
+    s_cdm[z] = ldc<COH>(c.final_dm + z);
     const bool tent = ns > nfin;  // the current rescale step, scale 1
     s_ton[z] = tent ? (T)1 : (T)0;
-    s_tdm[z] = tent ? c.demean[z * R + nfin] : (T)0;
-    s_mean[z] = c.mean[z];
-    s_mon[z] = c.has_mu[z] ? (T)1 : (T)0;
-    s_mu[z] = c.mu[z];
+    s_tdm[z] = tent ? ldc<COH>(c.demean + z * R + nfin) : (T)0;
+    s_mean[z] = ldc<COH>(c.mean + z);
+    s_mon[z] = ldc<COH>(c.has_mu + z) ? (T)1 : (T)0;
+    s_mu[z] = ldc<COH>(c.mu + z);
 #pragma unroll
-    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = c.cand[z * kMuCand + k];
+    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = ldc<COH>(c.cand + z * kMuCand + k);
   }
   __syncthreads();
   constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
@@ -830,6 +836,16 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_S
       partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
     }
   }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_STATS ? 3 : 4)))
+    ba_fold_kernel(T* __restrict__ d0, T* __restrict__ pert, int record, int64_t nx,
+                   int64_t ny, int nz, Win w, BAChain<T> c, double* __restrict__ partials) {
+  if (c.run && *c.run == 0) return;
+  __shared__ double red[4 * kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  ba_fold_body<T, MODE, false>(d0, pert, record, nx, ny, nz, w, c, partials, ba_smem, red);
 }
 
 template <typename T>
@@ -1058,6 +1074,7 @@ struct BAState {
   // run flags: [0] the first sweep, [1 + k] rescale sweep k (k < R),
   // [1 + R + it] mu sweep it (it < kMuMaxSweeps); [kFlagSweeps] sweeps run
   int* flags;
+  unsigned* bar;  // grid barrier of the persistent phases: arrivals, generation, error
   int R, nz;
   double N, width, tol_rel;
   double* ledger;  // [nz][5]: a0, n_loop, final demean, mu (NaN if none), sweeps
@@ -1095,6 +1112,9 @@ __global__ void ba_init_kernel(BAState<T> st, const double* __restrict__ mean_1d
     const int nf = ba_flag_count<T>(R);
     for (int i = 0; i < nf; ++i) st.flags[i] = 0;
     st.flags[0] = 1;  // the first stats sweep always runs
+    st.bar[0] = 0;
+    st.bar[1] = 0;
+    st.bar[2] = 0;
   }
 }
 
@@ -1168,34 +1188,38 @@ __global__ void ba_a0_kernel(BAState<T> st, const double* __restrict__ tot) {
 }
 
 // After rescale sweep k.
+template <typename T, bool COH = false>
+__device__ void ba_loop_level(BAState<T>& st, const double* tot, int k, int z) {
+  const int nz = st.nz;
+  ba_note_stored(st, z);
+  if (!st.still[z]) return;
+  const double sum_d = ldc<COH>(tot + z), m_abs = ldc<COH>(tot + nz + z) / st.N;
+  st.cur_mean[z] = sum_d / st.N;
+  bool go = true;
+  if (m_abs <= 0.0) {
+    go = false;
+  } else {
+    double sc = st.a0[z] / m_abs;
+    if (sc > 2.0) sc = 2.0;
+    if (fabs(sc - 1.0) < 1e-4) {
+      go = false;
+    } else {
+      st.scale[z * st.R + k] = (T)sc;
+      st.cur_mean[z] = (double)(T)sc * sum_d / st.N;
+    }
+  }
+  if (go && k + 1 < st.R)
+    ba_prepare_step(st, z, k + 1, &st.flags[2 + k]);
+  else
+    ba_leave_loop(st, z);
+}
+
 template <typename T>
 __global__ void ba_loop_kernel(BAState<T> st, const double* __restrict__ tot, int k) {
   if (st.flags[1 + k] == 0) return;
-  const int nz = st.nz;
   ba_count_sweep(st);
-  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
-    ba_note_stored(st, z);
-    if (!st.still[z]) continue;
-    const double sum_d = tot[z], m_abs = tot[nz + z] / st.N;
-    st.cur_mean[z] = sum_d / st.N;
-    bool go = true;
-    if (m_abs <= 0.0) {
-      go = false;
-    } else {
-      double sc = st.a0[z] / m_abs;
-      if (sc > 2.0) sc = 2.0;
-      if (fabs(sc - 1.0) < 1e-4) {
-        go = false;
-      } else {
-        st.scale[z * st.R + k] = (T)sc;
-        st.cur_mean[z] = (double)(T)sc * sum_d / st.N;
-      }
-    }
-    if (go && k + 1 < st.R)
-      ba_prepare_step(st, z, k + 1, &st.flags[2 + k]);
-    else
-      ba_leave_loop(st, z);
-  }
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < st.nz; z += gridDim.x * blockDim.x)
+    ba_loop_level(st, tot, k, z);
 }
 
 // After the loop: every active level starts its shift solve.  Its first
@@ -1217,35 +1241,114 @@ __global__ void ba_mu_init_kernel(BAState<T> st) {
 }
 
 // After mu sweep it.
+template <typename T, bool COH = false>
+__device__ void ba_mu_level(BAState<T>& st, const double* tot, int it, int z) {
+  const int nz = st.nz;
+  ba_note_stored(st, z);
+  if (!st.need[z]) return;
+  MuSolver<T> sv = st.solver[z];
+  if (sv.done) return;
+  double mv[kMuCand], sl[kMuCand], cv[kMuCand];
+  for (int q = 0; q < kMuCand; ++q) {
+    // the candidate actually evaluated is the dtype-rounded one
+    cv[q] = (double)st.cand[z * kMuCand + q];
+    mv[q] = ldc<COH>(tot + (size_t)(2 * q) * nz + z) / st.N;
+    sl[q] = -ldc<COH>(tot + (size_t)(2 * q + 1) * nz + z) / st.N;
+  }
+  if (it == 0 && fabs(mv[0]) <= 1e-9 * st.a0[z]) {
+    st.need[z] = 0;  // the final clip left the level mean-free
+    return;
+  }
+  sv.update(cv, mv, sl);
+  if (!sv.done && it + 1 < kMuMaxSweeps) {
+    double c[kMuCand];
+    sv.candidates(c);
+    for (int q = 0; q < kMuCand; ++q) st.cand[z * kMuCand + q] = (T)c[q];
+    atomicOr(&st.flags[2 + st.R + it], 1);
+  }
+  st.solver[z] = sv;
+}
+
 template <typename T>
 __global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int it) {
   if (st.flags[1 + st.R + it] == 0) return;
-  const int nz = st.nz;
   ba_count_sweep(st);
-  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
-    ba_note_stored(st, z);
-    if (!st.need[z]) continue;
-    MuSolver<T> sv = st.solver[z];
-    if (sv.done) continue;
-    double mv[kMuCand], sl[kMuCand], cv[kMuCand];
-    for (int q = 0; q < kMuCand; ++q) {
-      // the candidate actually evaluated is the dtype-rounded one
-      cv[q] = (double)st.cand[z * kMuCand + q];
-      mv[q] = tot[(size_t)(2 * q) * nz + z] / st.N;
-      sl[q] = -tot[(size_t)(2 * q + 1) * nz + z] / st.N;
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < st.nz; z += gridDim.x * blockDim.x)
+    ba_mu_level(st, tot, it, z);
+}
+
+// ---- persistent phases --------------------------------------------------------------
+// The rescale loop and the shift solve each run as ONE cooperative launch
+// (all blocks co-resident) that iterates sweep -> grid barrier -> reduction ->
+// grid barrier -> per-level update -> grid barrier until no level needs
+// another sweep.  This replaces a fixed launch sequence in which finished
+// iterations still cost an (empty) launch each.  The barrier spins with a
+// bound: a block that waits past kBarSpinLimit polls records an error, and
+// every block leaves at its next barrier.
+constexpr long long kBarSpinLimit = 1ll << 26;  // ~ seconds with the back-off below
+
+__device__ bool grid_barrier(unsigned* bar) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok_s = 1;
+    volatile unsigned* vgen = bar + 1;
+    volatile unsigned* verr = bar + 2;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == g) {
+        if (*verr || ++spins > kBarSpinLimit) {
+          atomicExch(bar + 2, 1u);
+          ok_s = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
     }
-    if (it == 0 && fabs(mv[0]) <= 1e-9 * st.a0[z]) {
-      st.need[z] = 0;  // the final clip left the level mean-free
-      continue;
+    __threadfence();
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_kernel(
+    T* __restrict__ d0, T* __restrict__ pert, int64_t nx, int64_t ny, int nz, Win w,
+    BAChain<T> c, BAState<T> st, double* __restrict__ partials, double* __restrict__ totals,
+    int flag_base, int n_iter) {
+  __shared__ double red[4 * kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
+  const int nb = gridDim.x;
+  c.run = nullptr;
+  for (int it = 0; it < n_iter; ++it) {
+    // read after a barrier: every block sees the same flag
+    if (__ldcg(st.flags + flag_base + it) == 0) break;
+    ba_fold_body<T, MODE, true>(d0, pert, 0, nx, ny, nz, w, c, partials, ba_smem, red);
+    if (!grid_barrier(st.bar)) return;
+    // totals[r] = the r-th row of block partials, summed in a fixed order
+    for (int r = blockIdx.x; r < Q * nz; r += nb) {
+      double acc = 0.0;
+      for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += __ldcg(partials + (size_t)r * nb + i);
+      const double sum = block_sum(acc, red);
+      if (threadIdx.x == 0) totals[r] = sum;
     }
-    sv.update(cv, mv, sl);
-    if (!sv.done && it + 1 < kMuMaxSweeps) {
-      double c[kMuCand];
-      sv.candidates(c);
-      for (int q = 0; q < kMuCand; ++q) st.cand[z * kMuCand + q] = (T)c[q];
-      atomicOr(&st.flags[2 + st.R + it], 1);
+    if (!grid_barrier(st.bar)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += nb * blockDim.x) {
+      if (MODE == BA_MU)
+        ba_mu_level<T, true>(st, totals, it, z);
+      else
+        ba_loop_level<T, true>(st, totals, it, z);
     }
-    st.solver[z] = sv;
+    if (!grid_barrier(st.bar)) return;
   }
 }
 
@@ -1253,7 +1356,8 @@ __global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int 
 template <typename T>
 __global__ void ba_finish_kernel(BAState<T> st) {
   const int nz = st.nz;
-  const int sweeps = st.flags[ba_flag_count<T>(st.R) - 1] + 1;  // + the apply sweep
+  // + the apply sweep; -1 when a persistent phase's grid barrier gave up
+  const int sweeps = st.bar[2] ? -1 : st.flags[ba_flag_count<T>(st.R) - 1] + 1;
   for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
     double mu = __longlong_as_double(0x7ff8000000000000LL);  // NaN: no shift
     if (st.need[z]) {
@@ -1279,6 +1383,7 @@ static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
          carve_bytes((size_t)6 * nz, sizeof(int)) +  // active, still, n_loop, need, applied, fin_stored
          carve_bytes((size_t)nz * sizeof(MuSolver<double>), 1) +
          carve_bytes((size_t)(2 + R + kMuMaxSweeps), sizeof(int)) +
+         carve_bytes(4, sizeof(unsigned)) +
          carve_bytes((size_t)5 * nz, sizeof(double)) +                      // ledger
          carve_bytes((size_t)nz, sizeof(double));                           // mean upload
 }
@@ -1323,12 +1428,13 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   st.fin_stored = c.take<int>(nz);
   st.solver = c.take<MuSolver<T>>(nz);
   st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
+  st.bar = c.take<unsigned>(4);
   st.ledger = c.take<double>((size_t)5 * nz);
   if (!partials || !totals || !st.nsteps || !st.has_final || !st.has_mu || !st.demean ||
       !st.scale || !st.final_dm || !st.mu || !st.mean || !st.cand || !st.a0 || !st.cur_mean ||
       !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.applied ||
       !st.fin_stored || !st.solver ||
-      !st.flags || !st.ledger)
+      !st.flags || !st.bar || !st.ledger)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
   st.R = R;
   st.nz = (int)nz;
@@ -1435,22 +1541,54 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   if ((rc = reduce(2 * (int)nz, &st.flags[0]))) return rc;
   ba_a0_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals);
   STEAM_LAUNCH_CHECK("bounded_add a0");
+  // One persistent cooperative launch per phase on the vectorised path (it
+  // iterates only as long as a level needs another sweep); the fixed launch
+  // sequence otherwise.
+  auto phase = [&](int mode, int flag_base, int n_iter) -> int {
+    auto kern = mode == BA_MU ? ba_phase_kernel<T, BA_MU> : ba_phase_kernel<T, BA_STATS>;
+    STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ba_sm));
+    int per_sm = 0;
+    STEAM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLvThreads, ba_sm));
+    STEAM_REQUIRE(per_sm >= 1, "steam_bounded_add: a persistent phase does not fit an SM");
+    int pgrid = per_sm * sm_count();
+    if (pgrid > grid4) pgrid = grid4;
+    T* d0p = inc;
+    T* pp = pert;
+    int nzi = (int)nz;
+    double* part = partials;
+    double* tot = totals;
+    void* args[] = {&d0p, &pp, &nx, &ny, &nzi, (void*)&w, (void*)&ch, (void*)&st, &part, &tot,
+                    &flag_base, &n_iter};
+    STEAM_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(pgrid), dim3(kLvThreads),
+                                           args, ba_sm, s));
+    count_launch();
+    return STEAM_OK;
+  };
   // demean / clip / rescale-to-A0 loop
-  for (int k = 0; k < R; ++k) {
-    if ((rc = sweep(BA_STATS, &st.flags[1 + k], nullptr, 0))) return rc;
-    if ((rc = reduce(2 * (int)nz, &st.flags[1 + k]))) return rc;
-    ba_loop_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals, k);
-    STEAM_LAUNCH_CHECK("bounded_add loop");
+  if (vec4) {
+    if (R > 0 && (rc = phase(BA_STATS, 1, R))) return rc;
+  } else {
+    for (int k = 0; k < R; ++k) {
+      if ((rc = sweep(BA_STATS, &st.flags[1 + k], nullptr, 0))) return rc;
+      if ((rc = reduce(2 * (int)nz, &st.flags[1 + k]))) return rc;
+      ba_loop_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals, k);
+      STEAM_LAUNCH_CHECK("bounded_add loop");
+    }
   }
   // zero-mean shift
   ba_mu_init_kernel<T><<<lv_blocks, 256, 0, s>>>(st);
   STEAM_LAUNCH_CHECK("bounded_add mu init");
-  for (int it = 0; it < kMuMaxSweeps; ++it) {
-    const int* run = &st.flags[1 + R + it];
-    if ((rc = sweep(BA_MU, run, nullptr, 0))) return rc;
-    if ((rc = reduce(Qmax * (int)nz, run))) return rc;
-    ba_mu_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals, it);
-    STEAM_LAUNCH_CHECK("bounded_add mu");
+  if (vec4) {
+    if ((rc = phase(BA_MU, 1 + R, kMuMaxSweeps))) return rc;
+  } else {
+    for (int it = 0; it < kMuMaxSweeps; ++it) {
+      const int* run = &st.flags[1 + R + it];
+      if ((rc = sweep(BA_MU, run, nullptr, 0))) return rc;
+      if ((rc = reduce(Qmax * (int)nz, run))) return rc;
+      ba_mu_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals, it);
+      STEAM_LAUNCH_CHECK("bounded_add mu");
+    }
   }
   ba_finish_kernel<T><<<lv_blocks, 256, 0, s>>>(st);
   STEAM_LAUNCH_CHECK("bounded_add finish");
@@ -1929,6 +2067,9 @@ static int bounded_add_entry(int64_t nx, int64_t ny, int64_t nz, T* pert,
     STEAM_CUDA(cudaMemcpyAsync(ledger_host, led, sizeof(double) * 5 * nz,
                                cudaMemcpyDeviceToHost, s));
     STEAM_CUDA(cudaStreamSynchronize(s));
+    if (nz > 0 && ledger_host[4] < 0)
+      return fail(STEAM_ERR_CUDA, "steam_bounded_add: a persistent phase's grid barrier "
+                                  "timed out");
   }
   return STEAM_OK;
 }

@@ -1,0 +1,235 @@
+"""Batched ensembles: many independent members in one captured launch graph.
+
+A member is one class step of its own world (its shape, seed, alpha, C1, H,
+Hz): the finest class of a root run over the member's domain, run by a
+``ResidentClass`` on device fields.  ``Ensemble`` spreads the members over a
+few CUDA streams and captures one step of all of them into a single CUDA
+graph: a replay then issues every member's ~400 kernels (noise, the three
+convolutions, patterns, the bounded adds' sweeps and solves, thermodynamics)
+with one launch call, and members of uneven sizes fill the GPU side by side.
+
+``autotune_conv`` is the tile-shape autotuner: for a field shape it times the
+fused convolution at a few x-chunk lengths (planes per CTA; short chunks give
+small members enough CTAs, long ones amortise the halo) and installs the
+fastest for that shape.  The chunk never changes the result.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from . import simulate as sim
+from . import utils as _utils
+from .resident import ResidentClass
+
+CHUNKS = (16, 32, 64, 128, 256)
+_TUNED = {}
+
+
+def member_setup(shape, seed, alpha=1.8, c1=0.1, H=1.0 / 3.0, Hz=5.0 / 9.0,
+                 dtype=np.float32, spheroscale=1000.0):
+    """The ClassSetup of a member: the finest class (k = 200 m, dx = dz =
+    100 m) of a root run over ``shape`` with the member's parameters.  Hz
+    enters through the canonical vertical scale k_z = l_s (k / l_s)^Hz of the
+    advective weight's aspect ratio."""
+    nx, ny, nz = (int(n) for n in shape)
+    height = nz * 100.0
+    zp = np.arange(int(height / 50.0) + 1) * 50.0
+    hp = (340e3 - 20e3 * zp / zp[-1]).astype(np.float32)
+    qp = (0.018 - 0.016 * zp / zp[-1]).astype(np.float32)
+    sph = np.full(zp.size, spheroscale)
+    k = 200.0
+    outer = max(nx, ny) * 100.0
+    grids = sim._compute_all_grids(np.array([k]), nx * 100.0, ny * 100.0, height, (1, 1, 1),
+                                   sph, zp)
+    got = (int(grids['nx'][0]), int(grids['ny'][0]), int(grids['nz'][0]))
+    if got != (nx, ny, nz):
+        raise ValueError(f"member shape {shape} is not a class grid (got {got})")
+    kzl = sim._k_z('piecewise_isotropic_below_spheroscale', outer, sph)
+    C_h = sim._compute_normalization(hp, zp, kzl, np.array([k]), outer, grids,
+                                     hurst_horizontal=H)[0]
+    C_q = sim._compute_normalization(qp, zp, kzl, np.array([k]), outer, grids,
+                                     hurst_horizontal=H)[0]
+    b_h = sim._bound_buffers([C_h], 1, H)[0]
+    b_q = sim._bound_buffers([C_q], 1, H)[0]
+    aspect = np.full(nz, spheroscale * (k / spheroscale) ** Hz / k, np.float32)
+    n_classes = int(round(np.log(outer / 200.0) / np.log(2.0))) + 1
+    key = sim.class_key(np.random.SeedSequence(seed).spawn(n_classes)[-1])
+    return sim.make_class_setup(
+        grids, 0, h_profile=hp, qt_profile=qp, z_profile=zp, C_h=C_h, C_qt=C_q, b_h=b_h,
+        b_qt=b_q, aspect=aspect, bounds=(315 * 1004.0, 355 * 1004.0, 0.0, 0.03), key=key,
+        flux_noise_scale=c1, flux_alpha=alpha, dtype=dtype)
+
+
+def autotune_conv(setup, dtype, chunks=CHUNKS, repeats=3):
+    """Time the fused convolution of ``setup``'s kernel on its shape at each
+    x-chunk, install the fastest; returns {chunk: ms}."""
+    torch = _lib.require_cuda("autotune_conv")
+    lib = _lib.load()
+    shape = tuple(int(n) for n in setup.shape)
+    key = (shape, dtype)
+    if key in _TUNED:
+        return _TUNED[key]
+    plan = setup.plan
+    if plan.kind == 'dense':
+        return {}
+    f = torch.randn(shape, dtype=dtype, device='cuda')
+    out = torch.empty_like(f)
+    times = {}
+    for c in chunks:
+        if c > 2 * shape[0] and c != chunks[0]:
+            continue
+        _lib.check(lib.steam_conv_set_xchunk(*shape, int(c)))
+        _utils.run_plan(plan, f, out)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            _utils.run_plan(plan, f, out)
+        e1.record()
+        e1.synchronize()
+        times[c] = e0.elapsed_time(e1) / repeats
+    best = min(times, key=times.get)
+    _lib.check(lib.steam_conv_set_xchunk(*shape, int(best)))
+    _TUNED[key] = times
+    return times
+
+
+class Member:
+    """One ensemble member: its setup, resident class step and device fields."""
+
+    def __init__(self, shape, seed, alpha=1.8, c1=0.1, H=1.0 / 3.0, Hz=5.0 / 9.0,
+                 dtype=np.float32, init_seed=None):
+        torch = _lib.require_cuda("ensemble member")
+        self.params = dict(shape=tuple(int(n) for n in shape), seed=int(seed), alpha=alpha,
+                           c1=c1, H=H, Hz=Hz)
+        self.setup = member_setup(shape, seed, alpha, c1, H, Hz, dtype)
+        tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+        self.rc = ResidentClass(self.setup, tdt)
+        g = torch.Generator(device='cuda')
+        g.manual_seed(int(seed if init_seed is None else init_seed))
+        self.h0 = 600.0 * torch.randn(shape, generator=g, device='cuda', dtype=tdt)
+        self.q0 = 0.0006 * torch.randn(shape, generator=g, device='cuda', dtype=tdt)
+        self.F0 = 1.0 + 0.1 * torch.rand(shape, generator=g, device='cuda', dtype=tdt)
+        self.h, self.q, self.F = self.h0.clone(), self.q0.clone(), self.F0.clone()
+        self.diag = {k: torch.empty_like(self.h) for k in ("T", "qv", "qc", "qi", "p")}
+
+    @property
+    def voxels(self):
+        nx, ny, nz = self.params['shape']
+        return nx * ny * nz
+
+    def reset(self):
+        self.h.copy_(self.h0)
+        self.q.copy_(self.q0)
+        self.F.copy_(self.F0)
+
+    def step(self):
+        self.rc.step(self.h, self.q, self.F, diagnostics=self.diag)
+
+
+class Ensemble:
+    """Members spread over ``n_streams`` streams; one step of all of them
+    either issued eagerly or replayed from a captured CUDA graph.  Each step
+    starts from the members' initial state (the reset copies are part of it),
+    so every step does the same work."""
+
+    def __init__(self, members, n_streams=4, tune=True):
+        torch = _lib.require_cuda("Ensemble")
+        self.members = list(members)
+        self.streams = [torch.cuda.Stream() for _ in range(max(1, int(n_streams)))]
+        # largest members first, dealt round-robin, so the streams carry
+        # similar work
+        order = sorted(range(len(self.members)), key=lambda i: -self.members[i].voxels)
+        self.lanes = [[] for _ in self.streams]
+        for j, i in enumerate(order):
+            self.lanes[j % len(self.streams)].append(self.members[i])
+        self.tuning = {}
+        if tune:
+            for m in self.members:
+                key = m.params['shape']
+                if key not in self.tuning:
+                    self.tuning[key] = autotune_conv(m.setup, m.rc.dtype)
+        self.graph = None
+        # a first eager step on every stream builds each member's work fields
+        # and its stream's workspace before anything is captured
+        self.step_eager()
+        torch.cuda.synchronize()
+
+    @property
+    def voxels(self):
+        return sum(m.voxels for m in self.members)
+
+    def _issue(self):
+        import torch
+        main = torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(main)
+        for s, lane in zip(self.streams, self.lanes):
+            with torch.cuda.stream(s):
+                for m in lane:
+                    m.reset()
+                    m.step()
+        for s in self.streams:
+            main.wait_stream(s)
+
+    def step_eager(self):
+        self._issue()
+
+    def capture(self):
+        """Capture one step of every member into a CUDA graph."""
+        import torch
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream()
+        with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
+            self._issue()
+        torch.cuda.synchronize()
+        self.graph = g
+        return g
+
+    def step_graph(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def throughput(self, steps=5, graph=True):
+        """Mvoxels/s over ``steps`` ensemble steps (device time)."""
+        import torch
+        run = self.step_graph if graph else self.step_eager
+        run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(steps):
+            run()
+        e1.record()
+        e1.synchronize()
+        host = time.perf_counter() - t0
+        ms = e0.elapsed_time(e1)
+        return {"mvoxels_per_s": self.voxels * steps / (ms / 1e3) / 1e6,
+                "ms_per_step": ms / steps, "host_ms_per_step": 1e3 * host / steps}
+
+
+def config_members(n_members, seed=3, smallest=(64, 64, 64), largest=(256, 256, 128),
+                   dtype=np.float32):
+    """Members with sizes log-uniform between two shapes (x = y, nz at most
+    the largest's), and alpha ~ U[1.5, 1.95], C1 ~ U[0.05, 0.2],
+    H ~ U[0.2, 0.5], Hz ~ U[0.5, 0.6]; member seeds 1000 + j."""
+    rng = np.random.default_rng(seed)
+    lo = np.log(np.prod(smallest))
+    hi = np.log(np.prod(largest))
+    out = []
+    for j in range(n_members):
+        v = np.exp(rng.uniform(lo, hi))
+        # a box with x = y = 2 nz (capped), sizes on multiples of 16
+        nz = int(min(largest[2], max(smallest[2], round((v / 4) ** (1 / 3) / 16) * 16)))
+        nxy = int(max(smallest[0], min(largest[0], round(np.sqrt(v / nz) / 16) * 16)))
+        out.append(Member((nxy, nxy, nz), 1000 + j, alpha=rng.uniform(1.5, 1.95),
+                          c1=rng.uniform(0.05, 0.2), H=rng.uniform(0.2, 0.5),
+                          Hz=rng.uniform(0.5, 0.6), dtype=dtype))
+    return out

@@ -269,6 +269,9 @@ class ResidentClass:
             cl.pattern[name] = PatternLedger(ps[:nz].copy(), ps[nz:].astype(np.int64))
             cl.bounded_add[name] = BoundedAddLedger.from_device(
                 v[self.o_ba[name]:self.o_ba[name] + 5 * nz])
+            if cl.bounded_add[name].n_sweeps < 0:
+                raise RuntimeError(f"resident class step: the {name} bounded add's "
+                                   f"persistent phase timed out at a grid barrier")
         return cl
 
 
