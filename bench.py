@@ -64,6 +64,8 @@ def parse(argv=None):
                     help="tile requests per arrival rate in the serving episode (0: skip)")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=(100.0, 1000.0),
                     help="Poisson arrival rates (requests/s) of the serving episode")
+    ap.add_argument("--ensemble-members", type=int, default=32,
+                    help="members of the batched-ensemble episode (0: skip)")
     return ap.parse_args(argv)
 
 
@@ -480,6 +482,25 @@ def main(argv=None):
             serving[f"{rate:g}_req_per_s"] = latency_summary(done)
         del srv, tw
 
+    # batched ensemble: members of uneven sizes (64^3 .. 256x256x128, log-uniform)
+    # and parameters, over four streams, eagerly and from one captured CUDA
+    # graph; beside it the plain FP64 drop-in (stage by stage, float64) on the
+    # same members
+    ensemble = None
+    if args.ensemble_members > 0:
+        from steam_b200.ensemble import Ensemble, config_members, plain_fp64_throughput
+        members = config_members(args.ensemble_members)
+        ens = Ensemble(members, n_streams=4)
+        ensemble = {"members": len(members), "voxels": ens.voxels,
+                    "eager_fp32": ens.throughput(steps=3, graph=False),
+                    "graph_fp32": ens.throughput(steps=3, graph=True),
+                    "plain_fp64_stagewise": plain_fp64_throughput(members, steps=1)}
+        ensemble["graph_fp32_over_plain_fp64"] = (
+            ensemble["graph_fp32"]["mvoxels_per_s"]
+            / ensemble["plain_fp64_stagewise"]["mvoxels_per_s"])
+        del ens, members
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(tuple(args.cpu_sample))
@@ -497,6 +518,7 @@ def main(argv=None):
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (4.3 GB fields); no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serving": serving,
+            "ensemble": ensemble,
             "gpu_launches": int(launches), "clocks": clk,
         }
         print(json.dumps(line), flush=True)

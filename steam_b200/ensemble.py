@@ -233,3 +233,40 @@ def config_members(n_members, seed=3, smallest=(64, 64, 64), largest=(256, 256, 
                           c1=rng.uniform(0.05, 0.2), H=rng.uniform(0.2, 0.5),
                           Hz=rng.uniform(0.5, 0.6), dtype=dtype))
     return out
+
+
+def plain_fp64_throughput(members, steps=1):
+    """Mvoxels/s of the plain FP64 drop-in on the same members: each member's
+    class step stage by stage (every realized scalar read back to the host
+    between stages, as the reference's stage functions do) in float64, plus
+    the thermodynamic map, one member after another."""
+    import torch
+    from .ledger import ClassLedger
+    from .thermodynamics import recover_diagnostics_device
+    work = []
+    for m in members:
+        p = m.params
+        setup = member_setup(p['shape'], p['seed'], p['alpha'], p['c1'], p['H'], p['Hz'],
+                             dtype=np.float64)
+        h0, q0, F0 = (t.double() for t in (m.h0, m.q0, m.F0))
+        work.append((setup, h0, q0, F0))
+    voxels = sum(m.voxels for m in members)
+
+    def run():
+        for setup, h0, q0, F0 in work:
+            h, q, F = h0.clone(), q0.clone(), F0.clone()
+            sim.run_class(h, q, F, None, None, None, setup, ClassLedger(), resident=False)
+            hlo, hhi, qlo, qhi = setup.bounds
+            recover_diagnostics_device(h, q, setup.z, 101325.0, h_mean=setup.h_mean,
+                                       qt_mean=setup.qt_mean, bounds=[hlo, hhi, qlo, qhi])
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        run()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"mvoxels_per_s": voxels * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps}
