@@ -422,8 +422,19 @@ def main(argv=None):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg.get(name, 2 * elem * nvox) / (per_launch_ms / 1e3) / 1e9
+    # measured DRAM traffic per launch: dram__bytes_read.sum + dram__bytes_write.sum
+    # of each entry's kernels in an ncu capture at 512x512x256 FP32, per voxel;
+    # the kernels stream their fields once, so the traffic scales with voxels
+    # (the convolution figure is the mean of its flux launch and two scalar ones)
+    dram_per_voxel = {"steam_conv_separable_async": 9.67, "steam_thermo_async": 30.1,
+                      "steam_flux_noise_async": 7.42, "steam_scalar_pattern_async": 15.3,
+                      "steam_flux_finish_async": 7.13}
+    traffic = (dram_per_voxel[name] * nvox if args.dtype == "f32" and name in dram_per_voxel
+               else None)
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic / 1e9 if traffic is not None else None,
+                "traffic_unit": "GB per launch (ncu, 512x512x256 capture scaled by voxels)",
                 "per_launch_ms": per_launch_ms,
                 "peak_source": "measured" if peaks else "fallback",
                 "bounded_add_sweeps": ba_sweeps,
