@@ -290,6 +290,7 @@ struct FusedTaps {
   A z[kFMaxZ][K], y[2][K], x[kFMaxX][K];
   A mix[kFMaxX * kFMaxPairs];
   int cx, cy, cz;
+  int sym;  // every z and y filter is even about its centre (K - 1) / 2
 };
 
 template <typename T, typename A, int K>
@@ -314,10 +315,15 @@ static FusedTaps<A, K> fused_taps(const SepParams<T>& p) {
   f.cx = p.cx;
   f.cy = p.cy;
   f.cz = p.cz;
+  bool sym = p.cz == (K - 1) / 2 && p.cy == (K - 1) / 2;
+  for (int i = 0; sym && i < K; ++i)
+    sym = f.z[0][i] == f.z[0][K - 1 - i] && f.z[1][i] == f.z[1][K - 1 - i] &&
+          f.y[0][i] == f.y[0][K - 1 - i] && f.y[1][i] == f.y[1][K - 1 - i];
+  f.sym = sym ? 1 : 0;
   return f;
 }
 
-template <typename T, typename A, int K>
+template <typename T, typename A, int K, bool SYM>
 __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
     const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
     const __grid_constant__ FusedTaps<A, K> tp, FusedGeom<T> g, XEpi epi,
@@ -412,14 +418,32 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
 #pragma unroll
       for (int i = 0; i < K + 3; ++i) win[i] = b[i];
       A a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int l = 0; l < K; ++l) {
-        const A t0 = tp.z[0][l], t1 = tp.z[1][l];
+      if constexpr (SYM) {
+        // even filters: out = t[c] w[m] + sum_d t[c+d] (w[m+d] + w[m-d]), with
+        // the pair sums shared by both z filters
+        constexpr int c = (K - 1) / 2;
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
-          // out[z] uses staged column z + K - 1 - l
-          a0[o] += t0 * win[o + K - 1 - l];
-          a1[o] += t1 * win[o + K - 1 - l];
+          const int m = o + c;
+          a0[o] = tp.z[0][c] * win[m];
+          a1[o] = tp.z[1][c] * win[m];
+#pragma unroll
+          for (int d = 1; d <= c; ++d) {
+            const A ps = win[m + d] + win[m - d];
+            a0[o] += tp.z[0][c + d] * ps;
+            a1[o] += tp.z[1][c + d] * ps;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+          const A t0 = tp.z[0][l], t1 = tp.z[1][l];
+#pragma unroll
+          for (int o = 0; o < 4; ++o) {
+            // out[z] uses staged column z + K - 1 - l
+            a0[o] += t0 * win[o + K - 1 - l];
+            a1[o] += t1 * win[o + K - 1 - l];
+          }
         }
       }
 #pragma unroll
@@ -437,14 +461,33 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
       const A* src = s_u + c * R * kFZ + (2 * yp) * kFZ + zq;
 #pragma unroll
       for (int i = 0; i < K + 1; ++i) col[i] = src[i * kFZ];
+      constexpr int cc = (K - 1) / 2;
+      A ps0[cc + 1], ps1[cc + 1];  // pair sums about rows 2yp and 2yp + 1
+      if constexpr (SYM) {
+        ps0[0] = col[cc];
+        ps1[0] = col[cc + 1];
+#pragma unroll
+        for (int d = 1; d <= cc; ++d) {
+          ps0[d] = col[cc + d] + col[cc - d];
+          ps1[d] = col[cc + 1 + d] + col[cc + 1 - d];
+        }
+      }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         A v0 = 0, v1 = 0;
+        if constexpr (SYM) {
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-          const A tj = tp.y[b][j];
-          v0 += tj * col[K - 1 - j];
-          v1 += tj * col[K - j];
+          for (int d = 0; d <= cc; ++d) {
+            v0 += tp.y[b][cc + d] * ps0[d];
+            v1 += tp.y[b][cc + d] * ps1[d];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < K; ++j) {
+            const A tj = tp.y[b][j];
+            v0 += tj * col[K - 1 - j];
+            v1 += tj * col[K - j];
+          }
         }
         const A m0 = tp.mix[0 * kFMaxPairs + c * 2 + b];
         const A m1 = tp.mix[1 * kFMaxPairs + c * 2 + b];
@@ -645,15 +688,15 @@ static int launch_fused(const SepParams<T>& p, int64_t grid, const T* in, T* out
   const size_t sm = fused_smem(p.kx, sizeof(A));
   STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: filters too long for the fused path");
   if (p.kx == 13) {
-    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, A, 13>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fused_conv_kernel<T, A, 13><<<(unsigned)grid, kFThreads, sm, s>>>(
-        in, out, pre, fused_taps<T, A, 13>(p), g, epi, partials);
+    const FusedTaps<A, 13> tp = fused_taps<T, A, 13>(p);
+    auto kern = tp.sym ? fused_conv_kernel<T, A, 13, true> : fused_conv_kernel<T, A, 13, false>;
+    STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, tp, g, epi, partials);
   } else {
-    STEAM_CUDA(cudaFuncSetAttribute(fused_conv_kernel<T, A, 25>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    fused_conv_kernel<T, A, 25><<<(unsigned)grid, kFThreads, sm, s>>>(
-        in, out, pre, fused_taps<T, A, 25>(p), g, epi, partials);
+    const FusedTaps<A, 25> tp = fused_taps<T, A, 25>(p);
+    auto kern = tp.sym ? fused_conv_kernel<T, A, 25, true> : fused_conv_kernel<T, A, 25, false>;
+    STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, tp, g, epi, partials);
   }
   STEAM_LAUNCH_CHECK("conv fused");
   return STEAM_OK;
