@@ -196,6 +196,9 @@ struct PatternArgs {
   int has_prod;   // 0: no signed amplitude (W alone)
   int has_taper;  // 0: no bound taper
   const double* s_scale_dev;  // non-NULL: s_scale is read here (device), rounded to T
+  // reciprocals of the differencing denominators (the vectorised kernel
+  // multiplies by them: at most one ulp from the quotient)
+  T inv_two_dx, inv_two_dy, inv_two_dz, inv_dz_first, inv_dz_last;
 };
 
 template <typename T, int JM>
@@ -337,8 +340,39 @@ __device__ __forceinline__ T pattern_cell(T r, T rxm, T rxp, T rym, T ryp, T rzm
   return W;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kLvThreads) pattern_vec_kernel(
+template <typename T, bool UNI>
+__device__ __forceinline__ T pattern_cell_fast(T r, T rxm, T rxp, T rym, T ryp, T rzm, T rzp,
+                                               int z, int nz, T prod, T az, T bz, T cz,
+                                               T asp, T ibb, const PatternArgs<T>& a) {
+  const T gx = mul_rn(sub_rn(rxp, rxm), a.inv_two_dx);
+  const T gy = mul_rn(sub_rn(ryp, rym), a.inv_two_dy);
+  const T gh = d_sqrt(add_rn(mul_rn(gx, gx), mul_rn(gy, gy)));
+  T gz;
+  if (z == 0) {
+    gz = mul_rn(sub_rn(rzp, r), a.inv_dz_first);
+  } else if (z == nz - 1) {
+    gz = mul_rn(sub_rn(r, rzm), a.inv_dz_last);
+  } else if (UNI) {
+    gz = mul_rn(sub_rn(rzp, rzm), a.inv_two_dz);
+  } else {
+    gz = add_rn(add_rn(mul_rn(az, rzm), mul_rn(bz, r)), mul_rn(cz, rzp));
+  }
+  gz = gz < (T)0 ? -gz : gz;
+  T W = add_rn(mul_rn(gz, asp), gh);
+  if (a.has_prod) W = mul_rn(W, mul_rn(prod, a.s_scale));
+  if (a.has_taper) {
+    T g = sub_rn(r, a.lo);
+    const T g2 = sub_rn(a.span, g);
+    g = g2 < g ? g2 : g;
+    g = mul_rn(g, ibb);
+    g = g < (T)0 ? (T)0 : (g > (T)1 ? (T)1 : g);
+    W = mul_rn(W, g);
+  }
+  return W;
+}
+
+template <typename T, bool UNI>
+__global__ void __launch_bounds__(kLvThreads, (sizeof(T) == 4 ? 3 : 2)) pattern_vec_kernel(
     const T* __restrict__ pert, const T* __restrict__ vecs, const T* __restrict__ prod,
     int64_t nx, int64_t ny, int nz, Win w, PatternArgs<T> a, T* __restrict__ out,
     double* __restrict__ partials) {
@@ -351,7 +385,7 @@ __global__ void __launch_bounds__(kLvThreads) pattern_vec_kernel(
   const int z4 = (t - cs * nz4) * 4;
   const bool act = cs < cpb;
   // vecs: [0] mean, [1] a, [2] b, [3] c (np.gradient, indexed z-1), [4] aspect, [5] buffer
-  T mz[4], asp[4], bb[4], ca[4], cb[4], cc[4];
+  T mz[4], asp[4], ibb[4], ca[4], cb[4], cc[4];
   T m_lo = (T)0, m_hi = (T)0;
   if (act) {
 #pragma unroll
@@ -359,10 +393,15 @@ __global__ void __launch_bounds__(kLvThreads) pattern_vec_kernel(
       const int z = z4 + l;
       mz[l] = vecs[z];
       asp[l] = vecs[4 * nz + z];
-      bb[l] = vecs[5 * nz + z];
-      ca[l] = z > 0 ? vecs[nz + z - 1] : (T)0;
-      cb[l] = z > 0 ? vecs[2 * nz + z - 1] : (T)0;
-      cc[l] = z > 0 ? vecs[3 * nz + z - 1] : (T)0;
+      const T bb = vecs[5 * nz + z];
+      ibb[l] = (T)1 / (bb > (T)0 ? bb : (T)1e-30);
+      if (!UNI) {
+        ca[l] = z > 0 ? vecs[nz + z - 1] : (T)0;
+        cb[l] = z > 0 ? vecs[2 * nz + z - 1] : (T)0;
+        cc[l] = z > 0 ? vecs[3 * nz + z - 1] : (T)0;
+      } else {
+        ca[l] = cb[l] = cc[l] = (T)0;
+      }
     }
     m_lo = z4 > 0 ? vecs[z4 - 1] : (T)0;
     m_hi = z4 + 4 < nz ? vecs[z4 + 4] : (T)0;
@@ -399,9 +438,10 @@ __global__ void __launch_bounds__(kLvThreads) pattern_vec_kernel(
         const int z = z4 + l;
         const T rzm = l == 0 ? r_lo : r[l - 1];
         const T rzp = l == 3 ? r_hi : r[l + 1];
-        const T Wv = pattern_cell<T>(r[l], add_rn(vxm.v[l], mz[l]), add_rn(vxp.v[l], mz[l]),
-                                     add_rn(vym.v[l], mz[l]), add_rn(vyp.v[l], mz[l]), rzm, rzp,
-                                     z, nz, pr.v[l], ca[l], cb[l], cc[l], asp[l], bb[l], a);
+        const T Wv = pattern_cell_fast<T, UNI>(
+            r[l], add_rn(vxm.v[l], mz[l]), add_rn(vxp.v[l], mz[l]), add_rn(vym.v[l], mz[l]),
+            add_rn(vyp.v[l], mz[l]), rzm, rzp, z, nz, pr.v[l], ca[l], cb[l], cc[l], asp[l],
+            ibb[l], a);
         o.v[l] = Wv;
         if (in_w) {
           acc0[l] += (double)(Wv < (T)0 ? -Wv : Wv);
@@ -1827,8 +1867,12 @@ static int pattern_launch(int64_t nx, int64_t ny, int64_t nz, const T* pert, con
   const LevelMap m = make_map(nz);
   const Win w = make_win(window, nx, ny);
   if (vec) {
-    pattern_vec_kernel<T><<<grid, kLvThreads, 0, s>>>(pert, d_vec, prod, nx, ny, (int)nz, w, a,
-                                                       out, partials);
+    if (a.uniform_z)
+      pattern_vec_kernel<T, true><<<grid, kLvThreads, 0, s>>>(pert, d_vec, prod, nx, ny, (int)nz,
+                                                              w, a, out, partials);
+    else
+      pattern_vec_kernel<T, false><<<grid, kLvThreads, 0, s>>>(pert, d_vec, prod, nx, ny,
+                                                               (int)nz, w, a, out, partials);
   } else if (m.packed)
     pattern_kernel<T, 1><<<grid, kLvThreads, 0, s>>>(
       pert, d_vec, prod, d_vec + nz, d_vec + 2 * nz, d_vec + 3 * nz,
@@ -1874,6 +1918,11 @@ static int pattern_impl(int64_t nx, int64_t ny, int64_t nz, const T* pert,
   a.span = (T)(phi_max - phi_min);
   a.s_scale = (T)s_scale;
   a.s_scale_dev = s_scale_dev;
+  a.inv_two_dx = (T)1 / a.two_dx;
+  a.inv_two_dy = (T)1 / a.two_dy;
+  a.inv_two_dz = a.uniform_z ? (T)1 / a.two_dz : (T)0;
+  a.inv_dz_first = (T)1 / a.dz_first;
+  a.inv_dz_last = (T)1 / a.dz_last;
   a.has_prod = prod != nullptr;
   a.has_taper = bbuf != nullptr;
   int rc;
