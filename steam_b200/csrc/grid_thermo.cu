@@ -159,13 +159,13 @@ struct ThermoConst {
   T cp, lv, g, t0, t1, dt, c622, es0, ea, eb, ec, dq;
 };
 
-// The float32 form divides by multiplying with the correctly rounded
-// reciprocal (at most one float32 ulp from the quotient) and takes exp from
-// the hardware exp2 outside the Newton loop too: the results stay within a
-// few float32 ulps of the correctly rounded forms, far inside the float32
-// tolerances of T (1e-3 K), the mixing ratios and p.  The float64 form keeps
-// the correctly rounded operations.
-__device__ __forceinline__ float th_div(float a, float b) { return __fmul_rn(a, __frcp_rn(b)); }
+// The float32 form divides with the hardware's approximate division (two
+// float32 ulps at most) and takes exp from the hardware exp2 outside the
+// Newton loop too: the results stay within a few float32 ulps of the
+// correctly rounded forms, far inside the float32 tolerances of T (1e-3 K),
+// the mixing ratios and p.  The float64 form keeps the correctly rounded
+// operations.
+__device__ __forceinline__ float th_div(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double th_div(double a, double b) { return a / b; }
 __device__ __forceinline__ float th_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double th_exp(double x) { return exp(x); }
@@ -291,8 +291,18 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
         sh(3, lane, zz) = mul_rn(sub_rn((T)1, lam), cond);
         sh(4, lane, zz) = pl;
         if (z < nz - 1) {
-          const double Tv = (double)Tl * (1.0 + 0.608 * (double)qvl);
-          p_cur *= exp_hyps(-g * dzv[z] * __drcp_rn(Rd * Tv));
+          // the float32 form forms the small exponent in float32 (relative
+          // error ~1e-7 of a ~1e-2 exponent, ~1e-9 of p per level); p itself
+          // accumulates in float64 in both forms
+          double a_h;
+          if (sizeof(T) == 4) {
+            const float Tv = __fmul_rn((float)Tl, __fadd_rn(1.0f, __fmul_rn(0.608f, (float)qvl)));
+            a_h = (double)__fdividef((float)(-g * dzv[z]), __fmul_rn((float)Rd, Tv));
+          } else {
+            const double Tv = (double)Tl * (1.0 + 0.608 * (double)qvl);
+            a_h = -g * dzv[z] / (Rd * Tv);
+          }
+          p_cur *= exp_hyps(a_h);
         }
       }
     }
