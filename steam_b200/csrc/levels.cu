@@ -808,67 +808,101 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     on |= (s_mon[z4 + l] != (T)0 ? 1u : 0u) << (12 + l);
   }
   const bool any_fold = (on & 0xffu) != 0;
-  double acc[Q][4];
+  // sums in float64; the shift sweep's in-range counts as integers (exact)
+  constexpr int QS = MODE == BA_MU ? kMuCand : 2;
+  double acc[QS][4];
+  unsigned cnt[MODE == BA_MU ? kMuCand : 1][4];
 #pragma unroll
-  for (int q = 0; q < Q; ++q)
+  for (int q = 0; q < QS; ++q)
 #pragma unroll
     for (int l = 0; l < 4; ++l) acc[q][l] = 0.0;
+#pragma unroll
+  for (int q = 0; q < (MODE == BA_MU ? kMuCand : 1); ++q)
+#pragma unroll
+    for (int l = 0; l < 4; ++l) cnt[q][l] = 0u;
   const int64_t ncol = nx * ny;
+  auto process = [&](const ColWalk& cw, const V4<T>& dv, const V4<T>& pv) {
+    const int64_t i = cw.col * nz + z4;
+    const bool in_w = w.in(cw.x, cw.y);
+    V4<T> df, pn, dn;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const T p0 = pv.v[l];
+      const T phi = add_rn(p0, mean.v[l]);
+      const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
+      T d = dv.v[l];
+      if (on & (1u << l)) d = mul_rn(clampv(sub_rn(d, fdm.v[l]), clo, chi), fsc.v[l]);
+      if (on & (16u << l)) d = clampv(sub_rn(d, cdm.v[l]), clo, chi);
+      df.v[l] = d;
+      if (on & (256u << l)) d = clampv(sub_rn(d, tdm.v[l]), clo, chi);
+      if (MODE == BA_APPLY) {
+        if (on & (4096u << l)) d = clampv(sub_rn(d, s_mu[z4 + l]), clo, chi);
+        pn.v[l] = add_rn(p0, d);
+        dn.v[l] = sub_rn(pn.v[l], p0);
+      } else if (in_w) {
+        if (MODE == BA_STATS) {
+          acc[0][l] += (double)d;
+          acc[1 % QS][l] += (double)(d < (T)0 ? -d : d);
+        } else {
+#pragma unroll
+          for (int k = 0; k < kMuCand; ++k) {
+            const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
+            const T tv = clampv(raw, clo, chi);
+            acc[k][l] += (double)tv;
+            cnt[k % (MODE == BA_MU ? kMuCand : 1)][l] += (raw > clo && raw < chi) ? 1u : 0u;
+          }
+        }
+      }
+    }
+    if (MODE == BA_APPLY) {
+      st4(pert + i, pn);
+      if (record) st4(d0 + i, dn);
+    } else if (any_fold) {
+      st4(d0 + i, df);
+    }
+  };
   if (active) {
     const int64_t step = (int64_t)gridDim.x * cpi;
     ColWalk cw;
     cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
-    for (; cw.col < ncol; cw.advance(step)) {
-      const int64_t i = cw.col * nz + z4;
-      const V4<T> dv = ld4(d0 + i), pv = ld4(pert + i);
-      const bool in_w = w.in(cw.x, cw.y);
-      V4<T> df, pn, dn;
+    // two columns in flight per thread where registers allow
+    constexpr int U = MODE == BA_APPLY ? 2 : 1;
+    while (cw.col + (U - 1) * step < ncol) {
+      ColWalk u[U];
+      V4<T> dv[U], pv[U];
+      u[0] = cw;
 #pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        const T p0 = pv.v[l];
-        const T phi = add_rn(p0, mean.v[l]);
-        const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
-        T d = dv.v[l];
-        if (on & (1u << l)) d = mul_rn(clampv(sub_rn(d, fdm.v[l]), clo, chi), fsc.v[l]);
-        if (on & (16u << l)) d = clampv(sub_rn(d, cdm.v[l]), clo, chi);
-        df.v[l] = d;
-        if (on & (256u << l)) d = clampv(sub_rn(d, tdm.v[l]), clo, chi);
-        if (MODE == BA_APPLY) {
-          if (on & (4096u << l)) d = clampv(sub_rn(d, s_mu[z4 + l]), clo, chi);
-          pn.v[l] = add_rn(p0, d);
-          dn.v[l] = sub_rn(pn.v[l], p0);
-        } else if (in_w) {
-          if (MODE == BA_STATS) {
-            acc[0][l] += (double)d;
-            acc[1 % Q][l] += (double)(d < (T)0 ? -d : d);
-          } else {
+      for (int k = 1; k < U; ++k) {
+        u[k] = u[k - 1];
+        u[k].advance(step);
+      }
 #pragma unroll
-            for (int k = 0; k < kMuCand; ++k) {
-              const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
-              const T tv = clampv(raw, clo, chi);
-              acc[2 * k][l] += (double)tv;
-              acc[(2 * k + 1) % Q][l] += (raw > clo && raw < chi) ? 1.0 : 0.0;
-            }
-          }
-        }
+      for (int k = 0; k < U; ++k) {
+        dv[k] = ld4(d0 + u[k].col * nz + z4);
+        pv[k] = ld4(pert + u[k].col * nz + z4);
       }
-      if (MODE == BA_APPLY) {
-        st4(pert + i, pn);
-        if (record) st4(d0 + i, dn);
-      } else if (any_fold) {
-        st4(d0 + i, df);
-      }
+#pragma unroll
+      for (int k = 0; k < U; ++k) process(u[k], dv[k], pv[k]);
+      cw = u[U - 1];
+      cw.advance(step);
     }
+    for (; cw.col < ncol; cw.advance(step))
+      process(cw, ld4(d0 + cw.col * nz + z4), ld4(pert + cw.col * nz + z4));
   }
   if (MODE == BA_APPLY) return;
   // deterministic reduction: per level, the cpi column slots in order
   const int nb = gridDim.x;
+  // partial rows: stats {sum d, sum |d|}; shift {mean_k, count_k} per candidate
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     __syncthreads();
     if (active)
 #pragma unroll
-      for (int l = 0; l < 4; ++l) red[cofs * nz + z4 + l] = acc[q][l];
+      for (int l = 0; l < 4; ++l)
+        red[cofs * nz + z4 + l] =
+            MODE == BA_MU ? ((q & 1) ? (double)cnt[(q >> 1) % (MODE == BA_MU ? kMuCand : 1)][l]
+                                     : acc[(q >> 1) % QS][l])
+                          : acc[q % QS][l];
     __syncthreads();
     for (int z = t; z < nz; z += kLvThreads) {
       double sacc = 0.0;
