@@ -502,9 +502,12 @@ def main(argv=None):
         from steam_b200.ensemble import Ensemble, config_members, plain_fp64_throughput
         members = config_members(args.ensemble_members)
         ens = Ensemble(members, n_streams=4)
+        eager = ens.throughput(steps=3, graph=False)
+        ens.check()
+        graph = ens.throughput(steps=3, graph=True)
+        ens.check()
         ensemble = {"members": len(members), "voxels": ens.voxels,
-                    "eager_fp32": ens.throughput(steps=3, graph=False),
-                    "graph_fp32": ens.throughput(steps=3, graph=True),
+                    "eager_fp32": eager, "graph_fp32": graph,
                     "plain_fp64_stagewise": plain_fp64_throughput(members, steps=1)}
         ensemble["graph_fp32_over_plain_fp64"] = (
             ensemble["graph_fp32"]["mvoxels_per_s"]

@@ -475,7 +475,9 @@ __global__ void __launch_bounds__(kLvThreads, (sizeof(T) == 4 ? 3 : 2)) pattern_
 //   if has_mu[z]:       d = clip(d - mu[z], caps)
 // with caps = (lo - phi, hi - phi), phi = pert + mean.
 constexpr int kMuCand = 4;
-enum { BA_STATS = 0, BA_MU = 1, BA_APPLY = 2 };
+// BA_SUMS: the first sweep, sum d and sum |d| of the raw increment (no chain
+// step is set yet, so the perturbation is not read)
+enum { BA_STATS = 0, BA_MU = 1, BA_APPLY = 2, BA_SUMS = 3 };
 
 template <typename T>
 struct BAChain {
@@ -588,149 +590,6 @@ __global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
   if (MODE != BA_APPLY) store_level_partials<Q, JM>(m, acc, red, partials);
 }
 
-// Vectorised form of the sweep for nz % 4 == 0: a thread owns 4 consecutive
-// levels, loads 16 bytes per field per column, and issues two columns' loads
-// before any arithmetic.  Same chain, same results as ba_sweep_kernel.
-constexpr int kBaU = 1;  // columns loaded ahead per thread
-
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 4)) ba_sweep4_kernel(
-    const T* __restrict__ d0, T* __restrict__ pert, T* __restrict__ inc_out,
-    int record, int64_t nx, int64_t ny, int nz, Win w, BAChain<T> c,
-    double* __restrict__ partials) {
-  if (c.run && *c.run == 0) return;
-  extern __shared__ unsigned char ba_smem[];
-  __shared__ double red[4 * kLvThreads];  // [cpi][nz] with cpi * nz == 4 * 256 / 4 ... <= 1024
-  const int R = c.R;
-  T* s_dm = reinterpret_cast<T*>(ba_smem);
-  T* s_sc = s_dm + (size_t)R * nz;
-  T* s_fin = s_sc + (size_t)R * nz;
-  T* s_mu = s_fin + nz;
-  T* s_mean = s_mu + nz;
-  T* s_cand = s_mean + nz;
-  int* s_ns = reinterpret_cast<int*>(s_cand + (size_t)kMuCand * nz);
-  int* s_hf = s_ns + nz;
-  int* s_hm = s_hf + nz;
-  for (int i = threadIdx.x; i < R * nz; i += blockDim.x) {
-    const int z = i % nz, st = i / nz;
-    s_dm[i] = c.demean[z * R + st];
-    s_sc[i] = c.scale[z * R + st];
-  }
-  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-    s_fin[z] = c.final_dm[z];
-    s_mu[z] = c.mu[z];
-    s_mean[z] = c.mean[z];
-    s_ns[z] = c.nsteps[z];
-    s_hf[z] = c.has_final[z];
-    s_hm[z] = c.has_mu[z];
-#pragma unroll
-    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = c.cand[z * kMuCand + k];
-  }
-  __syncthreads();
-  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
-  const int nz4 = nz / 4;
-  const int cpi = kLvThreads / nz4;  // columns per block-iteration
-  const int t = threadIdx.x;
-  const bool active = t < cpi * nz4;
-  const int z4 = (t % nz4) * 4;
-  const int cofs = t / nz4;
-  double acc[Q][4];
-#pragma unroll
-  for (int q = 0; q < Q; ++q)
-#pragma unroll
-    for (int l = 0; l < 4; ++l) acc[q][l] = 0.0;
-  const int64_t ncol = nx * ny;
-  int nsmax = 0;
-#pragma unroll
-  for (int l = 0; l < 4; ++l) nsmax = s_ns[z4 + l] > nsmax ? s_ns[z4 + l] : nsmax;
-  auto process = [&](int64_t col, int64_t x, int64_t y, const V4<T>& dv, const V4<T>& pv) {
-    const int64_t i = col * nz + z4;
-    V4<T> pn, dn;
-    const bool in_w = w.in(x, y);
-#pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const int zl = z4 + l;
-      const T p0 = pv.v[l];
-      T d = dv.v[l];
-      const T phi = add_rn(p0, s_mean[zl]);
-      const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
-      const int nsl = s_ns[zl];
-      for (int st = 0; st < nsmax; ++st) {
-        if (st < nsl) {
-          d = clampv(sub_rn(d, s_dm[st * nz + zl]), clo, chi);
-          d = mul_rn(d, s_sc[st * nz + zl]);
-        }
-      }
-      if (s_hf[zl]) d = clampv(sub_rn(d, s_fin[zl]), clo, chi);
-      if (MODE == BA_APPLY) {
-        if (s_hm[zl]) d = clampv(sub_rn(d, s_mu[zl]), clo, chi);
-        pn.v[l] = add_rn(p0, d);
-        dn.v[l] = sub_rn(pn.v[l], p0);
-      } else if (in_w) {
-        if (MODE == BA_STATS) {
-          acc[0][l] += (double)d;
-          acc[1 % Q][l] += (double)(d < (T)0 ? -d : d);
-        } else {
-#pragma unroll
-          for (int k = 0; k < kMuCand; ++k) {
-            const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
-            const T tv = clampv(raw, clo, chi);
-            acc[2 * k][l] += (double)tv;
-            acc[(2 * k + 1) % Q][l] += (raw > clo && raw < chi) ? 1.0 : 0.0;
-          }
-        }
-      }
-    }
-    if (MODE == BA_APPLY) {
-      st4(pert + i, pn);
-      if (record) st4(inc_out + i, dn);
-    }
-  };
-  if (active) {
-    const int64_t step = (int64_t)gridDim.x * cpi;
-    ColWalk cw;
-    cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
-    constexpr int U = MODE == BA_MU ? 1 : kBaU;
-    while (cw.col + (U - 1) * step < ncol) {
-      ColWalk u[U];
-      V4<T> dv[U], pv[U];
-      u[0] = cw;
-#pragma unroll
-      for (int k = 1; k < U; ++k) {
-        u[k] = u[k - 1];
-        u[k].advance(step);
-      }
-#pragma unroll
-      for (int k = 0; k < U; ++k) {
-        dv[k] = ld4(d0 + u[k].col * nz + z4);
-        pv[k] = ld4(pert + u[k].col * nz + z4);
-      }
-#pragma unroll
-      for (int k = 0; k < U; ++k) process(u[k].col, u[k].x, u[k].y, dv[k], pv[k]);
-      cw = u[U - 1];
-      cw.advance(step);
-    }
-    for (; cw.col < ncol; cw.advance(step))
-      process(cw.col, cw.x, cw.y, ld4(d0 + cw.col * nz + z4), ld4(pert + cw.col * nz + z4));
-  }
-  if (MODE == BA_APPLY) return;
-  // deterministic reduction: per level, the cpi column slots in order
-  const int nb = gridDim.x;
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    __syncthreads();
-    if (active)
-#pragma unroll
-      for (int l = 0; l < 4; ++l) red[cofs * nz + z4 + l] = acc[q][l];
-    __syncthreads();
-    for (int z = t; z < nz; z += kLvThreads) {
-      double sacc = 0.0;
-      for (int cc = 0; cc < cpi; ++cc) sacc += red[cc * nz + z];
-      partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
-    }
-  }
-}
-
 // ---- bounded add sweeps, write-back form -------------------------------------------
 // The increment buffer is the chain's running state: a sweep applies only the
 // steps not yet stored -- at most one whose parameters are now final (the last
@@ -741,6 +600,42 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 4)) ba_sweep4
 // from the raw increment.  nz % 4 == 0; a thread owns 4 consecutive levels.
 // Loads of values other blocks of the same grid wrote in this launch go
 // through L2 (ld.cg), never a stale L1 line.
+// Shared-memory ring of the statistics and shift sweeps: kBaStages columns
+// per thread, 4 elements of the increment and 4 of the perturbation each.
+constexpr int kBaStages = 4;
+
+// per-level parameters at the front of the fold kernels' dynamic shared
+// memory (rounded up to 16 bytes; the cp.async ring follows)
+template <typename T>
+__host__ __device__ constexpr size_t ba_fold_param_bytes(int64_t nz) {
+  return (sizeof(T) * (size_t)nz * (11 + kMuCand) + 15) / 16 * 16;
+}
+
+// 4 elements (16 or 32 bytes) global -> shared, asynchronously (L2 only)
+template <typename T>
+__device__ __forceinline__ void cp_async_v4(T* sdst, const T* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+#pragma unroll
+  for (int b = 0; b < (int)sizeof(T) / 4; ++b)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s + 16 * b),
+                 "l"(reinterpret_cast<const char*>(gsrc) + 16 * b)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ V4<T> lds4(const T* p) {
+  return ld4(p);
+}
+
 template <bool COH, typename V>
 __device__ __forceinline__ V ldc(const V* p) {
   if (COH) return __ldcg(p);
@@ -808,6 +703,10 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     on |= (s_mon[z4 + l] != (T)0 ? 1u : 0u) << (12 + l);
   }
   const bool any_fold = (on & 0xffu) != 0;
+  // a statistics sweep with no clip step on this thread's levels (the first
+  // sweep, and levels that left the loop with their final clip stored) never
+  // reads the perturbation
+  const bool need_p = MODE == BA_SUMS ? false : (MODE != BA_STATS || (on & 0xfffu) != 0);
   // sums in float64; the shift sweep's in-range counts as integers (exact)
   constexpr int QS = MODE == BA_MU ? kMuCand : 2;
   double acc[QS][4];
@@ -824,6 +723,15 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   auto process = [&](const ColWalk& cw, const V4<T>& dv, const V4<T>& pv) {
     const int64_t i = cw.col * nz + z4;
     const bool in_w = w.in(cw.x, cw.y);
+    if constexpr (MODE == BA_SUMS) {
+      if (in_w)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          acc[0][l] += (double)dv.v[l];
+          acc[1][l] += (double)(dv.v[l] < (T)0 ? -dv.v[l] : dv.v[l]);
+        }
+      return;
+    }
     V4<T> df, pn, dn;
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
@@ -861,12 +769,12 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
       st4(d0 + i, df);
     }
   };
-  if (active) {
+  if (active && MODE == BA_APPLY) {
     const int64_t step = (int64_t)gridDim.x * cpi;
     ColWalk cw;
     cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
-    // two columns in flight per thread where registers allow
-    constexpr int U = MODE == BA_APPLY ? 2 : 1;
+    // two columns in flight per thread
+    constexpr int U = 2;
     while (cw.col + (U - 1) * step < ncol) {
       ColWalk u[U];
       V4<T> dv[U], pv[U];
@@ -888,6 +796,39 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     }
     for (; cw.col < ncol; cw.advance(step))
       process(cw, ld4(d0 + cw.col * nz + z4), ld4(pert + cw.col * nz + z4));
+  } else if (active) {
+    // statistics and shift sweeps: the thread's own 16-byte pieces of the
+    // next kBaStages - 1 columns stream into its slots of a shared-memory
+    // ring by cp.async while it works on the current column, so the loads in
+    // flight do not depend on registers (a thread reads back only what it
+    // copied itself: no block barrier)
+    const int64_t step = (int64_t)gridDim.x * cpi;
+    ColWalk cw, front;
+    cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
+    front = cw;
+    T* ring = reinterpret_cast<T*>(ba_smem + ba_fold_param_bytes<T>(nz));
+    auto slot = [&](int s, int f) { return ring + ((size_t)(s * 2 + f) * kLvThreads + t) * 4; };
+    auto issue = [&](int s) {
+      if (front.col < ncol) {
+        const size_t off = (size_t)front.col * nz + z4;
+        cp_async_v4(slot(s, 0), d0 + off);
+        if (need_p) cp_async_v4(slot(s, 1), pert + off);
+      }
+      cp_async_commit();  // one group per column, empty past the end
+      front.advance(step);
+    };
+#pragma unroll
+    for (int s = 0; s < kBaStages - 1; ++s) issue(s);
+    int cur = 0;
+    for (; cw.col < ncol; cw.advance(step)) {
+      issue(cur == 0 ? kBaStages - 1 : cur - 1);
+      cp_async_wait<kBaStages - 1>();
+      const V4<T> dv = lds4(slot(cur, 0));
+      const V4<T> pv = need_p ? lds4(slot(cur, 1)) : V4<T>{};
+      process(cw, dv, pv);
+      cur = cur + 1 == kBaStages ? 0 : cur + 1;
+    }
+    cp_async_wait<0>();
   }
   if (MODE == BA_APPLY) return;
   // deterministic reduction: per level, the cpi column slots in order
@@ -924,7 +865,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_S
 
 template <typename T>
 static size_t ba_fold_smem_bytes(int64_t nz) {
-  return sizeof(T) * (size_t)nz * (11 + kMuCand);
+  return ba_fold_param_bytes<T>(nz) + (size_t)kBaStages * 2 * kLvThreads * 4 * sizeof(T);
 }
 
 // ---- projection sweeps (float64 level arithmetic) -----------------------------
@@ -1527,12 +1468,15 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
                          : 0;
   const int sweep_grid = vec4 ? grid4 : grid;
   if (vec4) {
+    STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_SUMS>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
     STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_STATS>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
     STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_MU>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
     STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_APPLY>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ba_fold_param_bytes<T>(nz)));
   } else if (m.packed) {
     STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_STATS, 1>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
@@ -1568,7 +1512,17 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
 
   auto sweep = [&](int mode, const int* run, T* out, int rec) -> int {
     ch.run = run;
-    if (mode == BA_STATS) {
+    if (mode == BA_SUMS) {
+      if (vec4)
+        ba_fold_kernel<T, BA_SUMS><<<grid4, kLvThreads, ba_sm, s>>>(
+            inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
+      else if (m.packed)
+        ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+      else
+        ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
+            inc, pert, out, rec, nx, ny, m, w, ch, partials);
+    } else if (mode == BA_STATS) {
       if (vec4)
         ba_fold_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
             inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
@@ -1590,7 +1544,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
     } else {
       if (vec4)
-        ba_fold_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_sm, s>>>(
+        ba_fold_kernel<T, BA_APPLY><<<grid4, kLvThreads, ba_fold_param_bytes<T>(nz), s>>>(
             inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
       else if (m.packed)
         ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
@@ -1611,7 +1565,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   ba_init_kernel<T><<<lv_blocks, 256, 0, s>>>(st, mean_dev);
   STEAM_LAUNCH_CHECK("bounded_add init");
   // sweep 0: a0 = mean|d|, mean d
-  if ((rc = sweep(BA_STATS, &st.flags[0], nullptr, 0))) return rc;
+  if ((rc = sweep(BA_SUMS, &st.flags[0], nullptr, 0))) return rc;
   if ((rc = reduce(2 * (int)nz, &st.flags[0]))) return rc;
   ba_a0_kernel<T><<<lv_blocks, 256, 0, s>>>(st, totals);
   STEAM_LAUNCH_CHECK("bounded_add a0");

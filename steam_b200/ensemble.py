@@ -196,6 +196,14 @@ class Ensemble:
             self.capture()
         self.graph.replay()
 
+    def check(self):
+        """Wait for the device and read every member's ledger; raises if a
+        member's step failed (a persistent phase that timed out at a grid
+        barrier).  Returns the members' ``ClassLedger``s."""
+        import torch
+        torch.cuda.synchronize()
+        return [m.rc.class_ledger(wait=False) for m in self.members]
+
     def throughput(self, steps=5, graph=True):
         """Mvoxels/s over ``steps`` ensemble steps (device time)."""
         import torch

@@ -254,9 +254,13 @@ class ResidentClass:
             result[k] = host_out[k].numpy()
         return result
 
-    def class_ledger(self, cl=None):
-        """The step's ledger as a ``ClassLedger`` (waits for the step)."""
-        self.ledger_ready.synchronize()
+    def class_ledger(self, cl=None, wait=True):
+        """The step's ledger as a ``ClassLedger``.  ``wait``: wait for the
+        step's ledger copy first; a caller that replayed the step from a CUDA
+        graph (whose event records do not reach this event) synchronises the
+        device itself and passes False."""
+        if wait:
+            self.ledger_ready.synchronize()
         v = self.ledger_host.numpy().copy()
         nz = self.shape[2]
         fl = v[self.o_fl:self.o_fl + 10]

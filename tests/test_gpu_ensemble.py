@@ -18,9 +18,11 @@ def test_graph_replay_equals_eager_steps():
     ens.step_eager()
     torch.cuda.synchronize()
     eager = [(m.h.clone(), m.q.clone(), m.F.clone(), m.diag["qc"].clone()) for m in members]
+    led_eager = [(cl.flux.realized.total, cl.flux.n_clipped) for cl in ens.check()]
     for m in members:  # scramble, so the replay must recompute everything
         for t in (m.h, m.q, m.F, m.diag["qc"]):
             t.fill_(-7.0)
+        m.rc.ledger_host.zero_()
     ens.capture()
     for _ in range(2):
         ens.step_graph()
@@ -28,6 +30,8 @@ def test_graph_replay_equals_eager_steps():
     for m, ref in zip(members, eager):
         for a, b in zip((m.h, m.q, m.F, m.diag["qc"]), ref):
             assert bool((a == b).all())
+    # the replayed steps' ledgers (copied back inside the graph) are the eager ones
+    assert [(cl.flux.realized.total, cl.flux.n_clipped) for cl in ens.check()] == led_eager
     # members differ from one another (their own seeds and parameters)
     assert not np.allclose(members[0].F.cpu().numpy().mean(), members[1].F.cpu().numpy().mean(),
                            rtol=0, atol=0)
