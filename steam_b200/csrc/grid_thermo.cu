@@ -157,6 +157,8 @@ constexpr int kThArrays = 5;  // h -> T, qt -> qv, qc, qi, p
 template <typename T>
 struct ThermoConst {
   T cp, lv, g, t0, t1, dt, c622, es0, ea, eb, ec, dq;
+  // float32 path: ea log2(e), 1/cp, 1/dt, dq c622
+  T ea2, inv_cp, inv_dt, dqc;
 };
 
 // The float32 form divides with the hardware's approximate division (two
@@ -175,16 +177,32 @@ __device__ __forceinline__ T bolton(T Tk, const ThermoConst<T>& k) {
   return mul_rn(k.es0, th_exp(th_div(mul_rn(k.ea, sub_rn(Tk, k.eb)), sub_rn(Tk, k.ec))));
 }
 
+// the hardware's approximate reciprocal and base-2 exponential (PTX
+// rcp.approx / ex2.approx: about 1 and 2 float32 ulps)
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Bolton's saturation vapour pressure in the float32 form:
+// es0 2^(ea log2(e) (T - eb) / (T - ec))
+__device__ __forceinline__ float bolton_f(float Tk, const ThermoConst<float>& k) {
+  return k.es0 * ex2_approx(k.ea2 * (Tk - k.eb) * rcp_approx(Tk - k.ec));
+}
+
 // exp(a) for one hypsometric step: the exponent -g dz / (Rd Tv) is small
 // (about -0.012 for 100 m levels), so the Taylor series of exp about 0 to
-// degree 12 is exact to below 2^-60 relative for |a| <= 1/8; larger |a|
-// take exp().
+// degree 9 is exact to below 2^-61 relative for |a| <= 1/16 (the remainder
+// is at most |a|^10 / 10! e^|a|); larger |a| take exp().
 __device__ __forceinline__ double exp_hyps(double a) {
-  if (!(fabs(a) <= 0.125)) return exp(a);
-  double s = 1.0 / 479001600.0;  // 1/12!
-  s = fma(s, a, 1.0 / 39916800.0);
-  s = fma(s, a, 1.0 / 3628800.0);
-  s = fma(s, a, 1.0 / 362880.0);
+  if (!(fabs(a) <= 0.0625)) return exp(a);
+  double s = 1.0 / 362880.0;  // 1/9!
   s = fma(s, a, 1.0 / 40320.0);
   s = fma(s, a, 1.0 / 5040.0);
   s = fma(s, a, 1.0 / 720.0);
@@ -196,14 +214,94 @@ __device__ __forceinline__ double exp_hyps(double a) {
   return fma(s, a, 1.0);
 }
 
-// Inside the Newton iterations the float32 form uses the hardware exp and
-// approximate reciprocal: Newton corrects their few-ulp errors on the next
-// step, and the last step's residual moves T by ~1e-6 K, below a float32 ulp
-// at 280 K.  The float64 form keeps the correctly rounded functions.
-__device__ __forceinline__ float newton_exp(float x) { return __expf(x); }
+// Inside the Newton iterations the float64 form keeps the correctly rounded
+// functions.
 __device__ __forceinline__ double newton_exp(double x) { return exp(x); }
-__device__ __forceinline__ float newton_rcp(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double newton_rcp(double x) { return 1.0 / x; }
+
+// Saturation adjustment of one cell: T and qv from h, qt at pressure p.
+// Newton on f(T) = cp T + Lv qvs(T, p) + g z - h, 5 iterations from the dry
+// temperature, when qt exceeds the saturation mixing ratio there.
+// float32: fused multiply-adds and the approximate reciprocal and exp2; the
+// two reciprocals 1/(T - 29.65) and 1/(p - es) are shared between the Bolton
+// exponent, qvs and dqvs/dT = dq c622 p es / ((T - 29.65)^2 (p - es)^2).
+__device__ __forceinline__ void saturate(float hl, float ql, float pl, float gz,
+                                         const ThermoConst<float>& k, float& Tl, float& qvl) {
+  const float Td = __fmul_rn(__fsub_rn(__fsub_rn(hl, __fmul_rn(k.lv, ql)), gz), k.inv_cp);
+  const float es = bolton_f(Td, k);
+  const float qvs = k.c622 * es * rcp_approx(pl - es);
+  Tl = Td;
+  qvl = ql;
+  if (ql > qvs) {
+    const float gzh = gz - hl, cpl = k.dqc * pl;
+    float Tn = Td;
+#pragma unroll 1
+    for (int it = 0; it < 5; ++it) {
+      const float i1 = rcp_approx(Tn - k.ec);
+      const float e = k.es0 * ex2_approx(k.ea2 * (Tn - k.eb) * i1);
+      const float i2 = rcp_approx(pl - e);
+      const float q = k.c622 * e * i2;
+      const float f = fmaf(k.cp, Tn, fmaf(k.lv, q, gzh));
+      const float u = i1 * i2;
+      const float dq = cpl * e * u * u;
+      Tn = fmaf(-f, rcp_approx(fmaf(k.lv, dq, k.cp)), Tn);
+    }
+    Tl = Tn;
+    const float e = bolton_f(Tn, k);
+    qvl = k.c622 * e * rcp_approx(pl - e);
+  }
+}
+
+// float64: the correctly rounded operations, in the reference's order.
+__device__ __forceinline__ void saturate(double hl, double ql, double pl, double gz,
+                                         const ThermoConst<double>& k, double& Tl,
+                                         double& qvl) {
+  const double Td = th_div(sub_rn(sub_rn(hl, mul_rn(k.lv, ql)), gz), k.cp);
+  const double es = bolton(Td, k);
+  const double qvs = th_div(mul_rn(k.c622, es), sub_rn(pl, es));
+  Tl = Td;
+  qvl = ql;
+  if (ql > qvs) {
+    double Tn = Td;
+#pragma unroll 1
+    for (int it = 0; it < 5; ++it) {
+      const double i1 = newton_rcp(sub_rn(Tn, k.ec));
+      const double e = mul_rn(k.es0, newton_exp(mul_rn(mul_rn(k.ea, sub_rn(Tn, k.eb)), i1)));
+      const double i2 = newton_rcp(sub_rn(pl, e));
+      const double q = mul_rn(mul_rn(k.c622, e), i2);
+      const double f = sub_rn(add_rn(add_rn(mul_rn(k.cp, Tn), mul_rn(k.lv, q)), gz), hl);
+      const double de = mul_rn(mul_rn(k.dq, e), mul_rn(i1, i1));
+      const double dq = mul_rn(mul_rn(mul_rn(k.c622, pl), mul_rn(i2, i2)), de);
+      Tn = sub_rn(Tn, mul_rn(f, newton_rcp(add_rn(k.cp, mul_rn(k.lv, dq)))));
+    }
+    Tl = Tn;
+    const double e = bolton(Tn, k);
+    qvl = th_div(mul_rn(k.c622, e), sub_rn(pl, e));
+  }
+}
+
+// the ice fraction ramp (T - 235.15) / 38, unclamped
+__device__ __forceinline__ float ice_ramp(float Tl, const ThermoConst<float>& k) {
+  return (Tl - k.t0) * k.inv_dt;
+}
+__device__ __forceinline__ double ice_ramp(double Tl, const ThermoConst<double>& k) {
+  return th_div(sub_rn(Tl, k.t0), k.dt);
+}
+
+// the hypsometric exponent -g dz / (Rd Tv) of the step to the next level:
+// float32 from ghyp dz = -g dz / Rd and the approximate reciprocal (relative
+// error ~1e-7 of a ~1e-2 exponent, ~1e-9 of p per level), float64 exact; p
+// itself accumulates in float64 in both forms
+__device__ __forceinline__ double hyps_exponent(float Tl, float qvl, float ghdz,
+                                                const ThermoConst<float>&) {
+  const float Tv = __fmul_rn(Tl, __fadd_rn(1.0f, __fmul_rn(0.608f, qvl)));
+  return (double)(ghdz * rcp_approx(Tv));
+}
+__device__ __forceinline__ double hyps_exponent(double Tl, double qvl, double gdz,
+                                                const ThermoConst<double>&) {
+  const double Tv = Tl * (1.0 + 0.608 * qvl);
+  return gdz / (287.04 * Tv);
+}
 
 template <typename T>
 __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
@@ -222,17 +320,27 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
   auto sh = [&](int a, int c, int z) -> T& {
     return base[((warp * kThArrays + a) * 32 + c) * kThPitch + z];
   };
+  // the chunk's per-level constants, per warp: g z, mean h, mean qt and the
+  // hypsometric numerator (-g dz / Rd in float32, -g dz in float64)
+  T* lv = base + (size_t)kThWarps * kThArrays * 32 * kThPitch + warp * 4 * kThZ;
   const int64_t col0 = ((int64_t)blockIdx.x * kThWarps + warp) * 32;
   if (col0 >= ncol) return;
   const int ncols = (int)((ncol - col0) < 32 ? (ncol - col0) : 32);
   const int64_t mycol = col0 + lane;
   double p_cur = ps_field ? (lane < ncols ? ps_field[mycol] : 0.0) : ps;
-  const double g = 9.81, Rd = 287.04;
   // staging geometry: lane -> (column group member, level) of a chunk
   constexpr int kCPI = 32 / kThZ;  // columns per staging instruction
   const int s_c = lane / kThZ, s_z = lane % kThZ;
   for (int z0 = 0; z0 < nz; z0 += kThZ) {
     const int zc = (nz - z0) < kThZ ? (nz - z0) : kThZ;
+    if (lane < zc) {
+      const int z = z0 + lane;
+      lv[lane] = mul_rn(k.g, (T)zv[z]);
+      lv[kThZ + lane] = (T)hm[z];
+      lv[2 * kThZ + lane] = (T)qm[z];
+      lv[3 * kThZ + lane] =
+          sizeof(T) == 4 ? (T)(-9.81 * dzv[z] / 287.04) : (T)(-9.81 * dzv[z]);
+    }
     for (int c0 = 0; c0 < ncols; c0 += kCPI) {
       const int c = c0 + s_c;
       if (c < ncols && s_z < zc) {
@@ -248,62 +356,24 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
         T hl = sh(0, lane, zz), ql = sh(1, lane, zz);
         if (compose) {
           // _compose_output without a deficit: state + mean, clamped to bounds
-          hl = add_rn(hl, (T)hm[z]);
-          ql = add_rn(ql, (T)qm[z]);
+          hl = add_rn(hl, lv[kThZ + zz]);
+          ql = add_rn(ql, lv[2 * kThZ + zz]);
           hl = hl < hlo ? hlo : (hl > hhi ? hhi : hl);
           ql = ql < qlo ? qlo : (ql > qhi ? qhi : ql);
         }
         const T pl = (T)p_cur;
-        const T zt = (T)zv[z];
-        const T Td = th_div(sub_rn(sub_rn(hl, mul_rn(k.lv, ql)), mul_rn(k.g, zt)), k.cp);
-        T es = bolton(Td, k);
-        const T qvs = th_div(mul_rn(k.c622, es), sub_rn(pl, es));
-        T Tl = Td, qvl = ql;
-        if (ql > qvs) {
-          T Tn = Td;
-#pragma unroll 1
-          for (int it = 0; it < 5; ++it) {
-            // f(T) = cp T + Lv qvs(T, p) + g z - h and its derivative, with the
-            // two reciprocals 1/(T - 29.65) and 1/(p - es) shared between the
-            // Bolton exponent, qvs, des/dT and dqvs/dT
-            const T i1 = newton_rcp(sub_rn(Tn, k.ec));
-            const T e = mul_rn(k.es0, newton_exp(mul_rn(mul_rn(k.ea, sub_rn(Tn, k.eb)), i1)));
-            const T i2 = newton_rcp(sub_rn(pl, e));
-            const T q = mul_rn(mul_rn(k.c622, e), i2);
-            const T f = sub_rn(add_rn(add_rn(mul_rn(k.cp, Tn), mul_rn(k.lv, q)),
-                                      mul_rn(k.g, zt)),
-                               hl);
-            const T de = mul_rn(mul_rn(k.dq, e), mul_rn(i1, i1));
-            const T dq = mul_rn(mul_rn(mul_rn(k.c622, pl), mul_rn(i2, i2)), de);
-            Tn = sub_rn(Tn, mul_rn(f, newton_rcp(add_rn(k.cp, mul_rn(k.lv, dq)))));
-          }
-          Tl = Tn;
-          const T e = bolton(Tn, k);
-          qvl = th_div(mul_rn(k.c622, e), sub_rn(pl, e));
-        }
+        T Tl, qvl;
+        saturate(hl, ql, pl, lv[zz], k, Tl, qvl);
         T cond = sub_rn(ql, qvl);
         cond = cond > (T)0 ? cond : (T)0;
-        T lam = th_div(sub_rn(Tl, k.t0), k.dt);
+        T lam = ice_ramp(Tl, k);
         lam = lam < (T)0 ? (T)0 : (lam > (T)1 ? (T)1 : lam);
         sh(0, lane, zz) = Tl;
         sh(1, lane, zz) = qvl;
         sh(2, lane, zz) = mul_rn(lam, cond);
         sh(3, lane, zz) = mul_rn(sub_rn((T)1, lam), cond);
         sh(4, lane, zz) = pl;
-        if (z < nz - 1) {
-          // the float32 form forms the small exponent in float32 (relative
-          // error ~1e-7 of a ~1e-2 exponent, ~1e-9 of p per level); p itself
-          // accumulates in float64 in both forms
-          double a_h;
-          if (sizeof(T) == 4) {
-            const float Tv = __fmul_rn((float)Tl, __fadd_rn(1.0f, __fmul_rn(0.608f, (float)qvl)));
-            a_h = (double)__fdividef((float)(-g * dzv[z]), __fmul_rn((float)Rd, Tv));
-          } else {
-            const double Tv = (double)Tl * (1.0 + 0.608 * (double)qvl);
-            a_h = -g * dzv[z] / (Rd * Tv);
-          }
-          p_cur *= exp_hyps(a_h);
-        }
+        if (z < nz - 1) p_cur *= exp_hyps(hyps_exponent(Tl, qvl, lv[3 * kThZ + zz], k));
       }
     }
     __syncwarp();
@@ -336,6 +406,10 @@ static ThermoConst<T> thermo_const() {
   k.eb = (T)273.15;
   k.ec = (T)29.65;
   k.dq = (T)4302.6;
+  k.ea2 = (T)(17.67 * 1.4426950408889634);
+  k.inv_cp = (T)(1.0 / 1004.0);
+  k.inv_dt = (T)(1.0 / (273.15 - 235.15));
+  k.dqc = (T)(4302.6 * 0.622);
   return k;
 }
 
@@ -424,8 +498,10 @@ extern "C" int steam_thermo_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
   const double b0 = compose ? bounds[0] : 0.0, b1 = compose ? bounds[1] : 0.0;
   const double b2 = compose ? bounds[2] : 0.0, b3 = compose ? bounds[3] : 0.0;
   const int64_t blocks = (ncol + 32 * kThWarps - 1) / (32 * kThWarps);
-  const size_t sm_f = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(float);
-  const size_t sm_d = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(double);
+  const size_t sm_f = ((size_t)kThWarps * kThArrays * 32 * kThPitch + kThWarps * 4 * kThZ) *
+                      sizeof(float);
+  const size_t sm_d = ((size_t)kThWarps * kThArrays * 32 * kThPitch + kThWarps * 4 * kThZ) *
+                      sizeof(double);
   const double* zv = prof_dev;
   if (dtype == STEAM_F32) {
     STEAM_CUDA(cudaFuncSetAttribute(thermo_kernel<float>,
@@ -487,8 +563,10 @@ extern "C" int steam_thermo(int dtype, int64_t nx, int64_t ny, int64_t nz,
     return fail(STEAM_ERR_CUDA, std::string("steam_thermo: ") + cudaGetErrorString(e));
   }
   const int64_t blocks = (ncol + 32 * kThWarps - 1) / (32 * kThWarps);
-  const size_t sm_f = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(float);
-  const size_t sm_d = (size_t)kThWarps * kThArrays * 32 * kThPitch * sizeof(double);
+  const size_t sm_f = ((size_t)kThWarps * kThArrays * 32 * kThPitch + kThWarps * 4 * kThZ) *
+                      sizeof(float);
+  const size_t sm_d = ((size_t)kThWarps * kThArrays * 32 * kThPitch + kThWarps * 4 * kThZ) *
+                      sizeof(double);
   if (dtype == STEAM_F32) {
     e = cudaFuncSetAttribute(thermo_kernel<float>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_f);

@@ -187,11 +187,13 @@ class ResidentClass:
                   surface_pressure=101325.0):
         """One class step on host arrays, with the transfers pipelined.
 
-        h, qt, flux (numpy, updated in place) are uploaded on a copy stream
-        in the order the step needs them (F first; h and qt while the flux
-        advance runs), and each result is downloaded as soon as it is final
-        (F while the scalars run, h while qt runs, qt and the diagnostics
-        last), so copies overlap compute in both directions.  ``out`` maps
+        h, qt, flux (numpy, updated in place) are uploaded on one copy
+        stream in the order the step needs them (F first; h and qt while the
+        flux advance runs), and each result is downloaded on a second copy
+        stream as soon as it is final (F while h and qt are still going up and
+        the scalars run, h while qt runs, qt and the diagnostics last), so the
+        two directions of the link run at the same time and both overlap
+        compute.  ``out`` maps
         diagnostic names to host arrays to fill; page-locked arrays (e.g.
         ``torch.empty(..., pin_memory=True).numpy()``) let every copy run
         asynchronously at full PCIe bandwidth.  Returns the diagnostics."""
@@ -203,18 +205,19 @@ class ResidentClass:
         if self.io is None:
             self.io = {k: torch.empty(shape, dtype=self.dtype, device='cuda')
                        for k in ('h', 'qt', 'F', 'T', 'qv', 'qc', 'qi', 'p')}
-            self.copy_stream = torch.cuda.Stream()
-        io, cp = self.io, self.copy_stream
+            self.up_stream = torch.cuda.Stream()
+            self.down_stream = torch.cuda.Stream()
+        io, up, cp = self.io, self.up_stream, self.down_stream
         main = torch.cuda.current_stream()
         src = {k: torch.from_numpy(np.ascontiguousarray(a, dtype=self.np_t))
                for k, a in (('F', flux), ('h', h), ('qt', qt))}
-        cp.wait_stream(main)  # the device buffers are free once earlier work is done
+        up.wait_stream(main)  # the device buffers are free once earlier work is done
         ready = {}
-        with torch.cuda.stream(cp):
+        with torch.cuda.stream(up):
             for k in ('F', 'h', 'qt'):
                 io[k].copy_(src[k], non_blocking=True)
                 ready[k] = torch.cuda.Event()
-                ready[k].record(cp)
+                ready[k].record(up)
         main.wait_event(ready['F'])
         done = {}
         diag_dev = {k: io[k] for k in ('T', 'qv', 'qc', 'qi', 'p')} if diagnostics else None
@@ -247,6 +250,7 @@ class ResidentClass:
                 for k in diagnostics:
                     host_out[k].copy_(io[k], non_blocking=True)
         cp.synchronize()
+        up.synchronize()
         for k, host in (('F', flux), ('h', h), ('qt', qt)):
             if '_' + k in host_out:
                 host[...] = host_out['_' + k].numpy()
