@@ -348,9 +348,13 @@ int steam_pattern_norm_async(int dtype, int64_t nz, const double* level_sums_dev
 
 /* steam_bounded_add with the level means on the device (mean_dev, nz
  * doubles) and its ledger written to ledger_dev (DEVICE, [nz][5], may be
- * NULL).  The launch sequence is fixed (one stats sweep, n_rescale rescale
- * sweeps, 48 shift sweeps, one apply sweep); sweeps whose phase has ended
- * exit at once. */
+ * NULL).  With nz % 4 == 0 and 16-byte aligned fields the rescale loop and
+ * the shift solve each run as ONE cooperative launch that sweeps while any
+ * level needs another sweep; its grid barriers wait a bounded time, and a
+ * barrier that gives up ends the launch and marks the ledger's sweep count
+ * -1 (the host raises).  Otherwise the launch sequence is fixed (one stats
+ * sweep, n_rescale rescale sweeps, 48 shift sweeps, one apply sweep) and
+ * sweeps whose phase has ended exit at once. */
 int steam_bounded_add_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
                             const double* mean_dev, void* increment, double phi_min,
                             double phi_max, const steam_window_t* window, int32_t n_rescale,
