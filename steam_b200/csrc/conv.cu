@@ -323,7 +323,7 @@ static FusedTaps<A, K> fused_taps(const SepParams<T>& p) {
   return f;
 }
 
-template <typename T, typename A, int K, bool SYM>
+template <typename T, typename A, int K, bool SYM, bool PRE>
 __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
     const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
     const __grid_constant__ FusedTaps<A, K> tp, FusedGeom<T> g, XEpi epi,
@@ -349,8 +349,8 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
   for (int c = t; c < C; c += kFThreads) {
     const int z = z0 - padz + c;
     const bool in_z = z >= 0 && z < g.nz;
-    s_pre[0][c] = (in_z && g.use_pre) ? pre[z] : (T)1;
-    s_pre[1][c] = (in_z && g.use_pre) ? pre[g.nz + z] : (T)1;
+    s_pre[0][c] = (in_z && PRE) ? pre[z] : (T)1;
+    s_pre[1][c] = (in_z && PRE) ? pre[g.nz + z] : (T)1;
   }
   // this thread's staged elements e = t + i*kFThreads: their offset within
   // an input plane (-1 for zero padding) and their staged column
@@ -364,51 +364,69 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
     goff[i] = v ? (int)(wrapi(y0 - pady + r, g.ny) * g.nz + z) : -1;
   }
   const int64_t plane_elems = g.ny * (int64_t)g.nz;
+  // the prologue's per-level divisor and multiplier of each staged element
+  // (loop invariant: the element's staged column is fixed per thread)
+  __syncthreads();  // s_pre is complete
+  T pdiv[NL], pmul[NL];
+#pragma unroll
+  for (int i = 0; i < NL; ++i) {
+    const int e = t + i * kFThreads;
+    const int c = e % C;
+    pdiv[i] = PRE ? s_pre[0][c] : (T)1;
+    pmul[i] = PRE ? s_pre[1][c] : (T)1;
+  }
   T ld[NL];
-  auto issue_loads = [&](int64_t k) {
-    const T* base = in + wrapi(xin0 + k, g.nx) * plane_elems;
+  // input plane pointer, advanced one plane per iteration with the wrap in x
+  int64_t xi = wrapi(xin0, g.nx);
+  auto issue_loads = [&]() {
+    const T* base = in + xi * plane_elems;
 #pragma unroll
     for (int i = 0; i < NL; ++i) ld[i] = goff[i] >= 0 ? base[goff[i]] : (T)0;
+    xi = xi + 1 == g.nx ? 0 : xi + 1;
   };
   auto commit_loads = [&](A* dst) {
 #pragma unroll
     for (int i = 0; i < NL; ++i) {
       const int e = t + i * kFThreads;
       if (e < R * C) {
-        const int c = e % C;  // C is a compile-time constant
         T v = ld[i];
-        if (g.use_pre) v = mul_rn(v / s_pre[0][c], s_pre[1][c]);
+        if (PRE) v = mul_rn(v / pdiv[i], pmul[i]);
         dst[e] = (A)v;
       }
     }
   };
-  // output points of this thread: rows 2*yp, 2*yp+1 at column zq
+  // output points of this thread: rows 2*yp, 2*yp+1 at column zq; their
+  // offsets within an output plane and whether they lie inside the array
   const int zq = t % kFZ, yp = t / kFZ;
   const int64_t oy0 = y0 + 2 * yp;
   const bool okz = z0 + zq < g.nz;
-  // output rows oy0, oy0 + 1 (each valid when inside the array)
-#define OY(m) (oy0 + (m))
-#define OK(m) (okz && OY(m) < g.ny)
+  const bool ok0 = okz && oy0 < g.ny, ok1 = okz && oy0 + 1 < g.ny;
+  const int64_t o0 = oy0 * g.nz + z0 + zq, o1 = o0 + g.nz;
+  const bool iny0 = oy0 >= epi.wy0 && oy0 < epi.wy1;
+  const bool iny1 = oy0 + 1 >= epi.wy0 && oy0 + 1 < epi.wy1;
   A acc[K][2];
 #pragma unroll
   for (int sl = 0; sl < K; ++sl) acc[sl][0] = acc[sl][1] = (A)0;
   double s_f = 0.0, s_clip = 0.0;
   __syncthreads();
-  issue_loads(0);
+  issue_loads();
   commit_loads(s_in0);
   __syncthreads();
   const bool flux_epi = epi.mode == STEAM_EPI_FLUX;
-  for (int64_t k = 0; k < count; ++k) {
+  const int count_i = (int)count;
+  int rph = 0;  // ring phase: k mod K
+  for (int k = 0; k < count_i; ++k) {
     A* s_in = s_in0 + (k & 1) * R * C;
-    if (k + 1 < count) issue_loads(k + 1);
-    // the flux under the output plane this iteration completes, loaded now so
-    // that the load overlaps the plane's filters
-    T fprev[2] = {(T)0, (T)0};
-    if (flux_epi && k >= K - 1) {
-      const int64_t x = xb + (k - (K - 1));
-#pragma unroll
-      for (int m = 0; m < 2; ++m)
-        if (OK(m)) fprev[m] = out[(x * g.ny + OY(m)) * g.nz + z0 + zq];
+    if (k + 1 < count_i) issue_loads();
+    // the output plane this iteration completes (when j >= 0)
+    const int j = k - (K - 1);
+    const int64_t x = xb + j;
+    T* outp = out + (j >= 0 ? x : 0) * plane_elems;
+    // the flux under it, loaded now so that the load overlaps the filters
+    T fprev0 = (T)0, fprev1 = (T)0;
+    if (flux_epi && j >= 0) {
+      if (ok0) fprev0 = outp[o0];
+      if (ok1) fprev1 = outp[o1];
     }
     // ---- z filters, 4 outputs per task: u_c[r][z4 .. z4+3]
     for (int task = t; task < S::ZT; task += kFThreads) {
@@ -483,10 +501,10 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
           }
         } else {
 #pragma unroll
-          for (int j = 0; j < K; ++j) {
-            const A tj = tp.y[b][j];
-            v0 += tj * col[K - 1 - j];
-            v1 += tj * col[K - j];
+          for (int jj = 0; jj < K; ++jj) {
+            const A tj = tp.y[b][jj];
+            v0 += tj * col[K - 1 - jj];
+            v1 += tj * col[K - jj];
           }
         }
         const A m0 = tp.mix[0 * kFMaxPairs + c * 2 + b];
@@ -497,10 +515,9 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
         w1[1] += m1 * v1;
       }
     }
-    // ---- fold into the ring: plane k feeds output j = k + i - (K-1) in slot
-    //      j mod K; output k - (K-1) is then complete and leaves the ring
-    const int rph = (int)(k % K);
-    const int64_t j = k - (K - 1);
+    // ---- fold into the ring: plane k feeds output j + i in slot (k + i + 1)
+    //      mod K; output j is then complete and leaves the ring
+    const bool in_wx = x >= epi.wx0 && x < epi.wx1;
 #pragma unroll
     for (int rr = 0; rr < K; ++rr) {
       if (rr == rph) {
@@ -513,24 +530,28 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
         }
         const int es = (rr + 1) % K;
         if (j >= 0) {
-          const int64_t x = xb + j;
-#pragma unroll
-          for (int m = 0; m < 2; ++m) {
-            if (OK(m)) {
-              const int64_t o = (x * g.ny + OY(m)) * g.nz + z0 + zq;
-              if (flux_epi) {
-                T f = add_rn(fprev[m], (T)acc[es][m]);
-                if (f < (T)0) {
-                  s_clip += 1.0;
-                  f = (T)0;
-                }
-                out[o] = f;
-                if (x >= epi.wx0 && x < epi.wx1 && OY(m) >= epi.wy0 && OY(m) < epi.wy1)
-                  s_f += (double)f;
-              } else {
-                out[o] = (T)acc[es][m];
+          if (flux_epi) {
+            T f0 = add_rn(fprev0, (T)acc[es][0]);
+            T f1 = add_rn(fprev1, (T)acc[es][1]);
+            if (ok0) {
+              if (f0 < (T)0) {
+                s_clip += 1.0;
+                f0 = (T)0;
               }
+              outp[o0] = f0;
+              if (in_wx && iny0) s_f += (double)f0;
             }
+            if (ok1) {
+              if (f1 < (T)0) {
+                s_clip += 1.0;
+                f1 = (T)0;
+              }
+              outp[o1] = f1;
+              if (in_wx && iny1) s_f += (double)f1;
+            }
+          } else {
+            if (ok0) outp[o0] = (T)acc[es][0];
+            if (ok1) outp[o1] = (T)acc[es][1];
           }
         }
         // a slot leaving the ring is cleared whether or not its output lies
@@ -539,11 +560,10 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
         acc[es][1] = (A)0;
       }
     }
-    if (k + 1 < count) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
+    rph = rph + 1 == K ? 0 : rph + 1;
+    if (k + 1 < count_i) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
     __syncthreads();
   }
-#undef OY
-#undef OK
   if (epi.mode == STEAM_EPI_FLUX) {
     double t0 = block_sum(s_f, scratch);
     double t1 = block_sum(s_clip, scratch);
@@ -689,12 +709,18 @@ static int launch_fused(const SepParams<T>& p, int64_t grid, const T* in, T* out
   STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: filters too long for the fused path");
   if (p.kx == 13) {
     const FusedTaps<A, 13> tp = fused_taps<T, A, 13>(p);
-    auto kern = tp.sym ? fused_conv_kernel<T, A, 13, true> : fused_conv_kernel<T, A, 13, false>;
+    auto kern = tp.sym ? (g.use_pre ? fused_conv_kernel<T, A, 13, true, true>
+                                    : fused_conv_kernel<T, A, 13, true, false>)
+                       : (g.use_pre ? fused_conv_kernel<T, A, 13, false, true>
+                                    : fused_conv_kernel<T, A, 13, false, false>);
     STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, tp, g, epi, partials);
   } else {
     const FusedTaps<A, 25> tp = fused_taps<T, A, 25>(p);
-    auto kern = tp.sym ? fused_conv_kernel<T, A, 25, true> : fused_conv_kernel<T, A, 25, false>;
+    auto kern = tp.sym ? (g.use_pre ? fused_conv_kernel<T, A, 25, true, true>
+                                    : fused_conv_kernel<T, A, 25, true, false>)
+                       : (g.use_pre ? fused_conv_kernel<T, A, 25, false, true>
+                                    : fused_conv_kernel<T, A, 25, false, false>);
     STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<(unsigned)grid, kFThreads, sm, s>>>(in, out, pre, tp, g, epi, partials);
   }
