@@ -7,6 +7,7 @@
 //   y-pass: v_p = u_c (*)_y Y_b     (TY x TZ tiles of one x-plane)
 //   x-pass: out = sum_a (sum_p mix_ap v_p) (*)_x X_a, with the epilogue.
 #include "common.cuh"
+#include <type_traits>
 
 #include <map>
 #include <mutex>
@@ -285,6 +286,9 @@ struct FusedShape {
 // is a compile-time constant after unrolling, so the multiply-adds read their
 // tap straight from the parameter bank (no shared-memory load per tap).
 // mix is re-indexed by (a, c, b), the pairs enumerated c-major, b-minor.
+__device__ __forceinline__ float fma_a(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_a(double a, double b, double c) { return fma(a, b, c); }
+
 template <typename A, int K>
 struct FusedTaps {
   A z[kFMaxZ][K], y[2][K], x[kFMaxX][K];
@@ -324,10 +328,11 @@ static FusedTaps<A, K> fused_taps(const SepParams<T>& p) {
 }
 
 template <typename T, typename A, int K, bool SYM, bool PRE>
-__global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
+__global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
     const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
     const __grid_constant__ FusedTaps<A, K> tp, FusedGeom<T> g, XEpi epi,
     double* __restrict__ partials) {
+  static_assert(K <= 25, "the ring dispatch covers K <= 25");
   using S = FusedShape<K>;
   constexpr int R = S::R, C = S::C, NL = S::NL;
   extern __shared__ unsigned char smem_raw[];
@@ -364,17 +369,9 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
     goff[i] = v ? (int)(wrapi(y0 - pady + r, g.ny) * g.nz + z) : -1;
   }
   const int64_t plane_elems = g.ny * (int64_t)g.nz;
-  // the prologue's per-level divisor and multiplier of each staged element
-  // (loop invariant: the element's staged column is fixed per thread)
-  __syncthreads();  // s_pre is complete
-  T pdiv[NL], pmul[NL];
-#pragma unroll
-  for (int i = 0; i < NL; ++i) {
-    const int e = t + i * kFThreads;
-    const int c = e % C;
-    pdiv[i] = PRE ? s_pre[0][c] : (T)1;
-    pmul[i] = PRE ? s_pre[1][c] : (T)1;
-  }
+  // staged column of this thread's first element; element i sits at column
+  // (c_base + i * kFThreads) mod C
+  const int c_base = t % C;
   T ld[NL];
   // input plane pointer, advanced one plane per iteration with the wrap in x
   int64_t xi = wrapi(xin0, g.nx);
@@ -390,7 +387,11 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
       const int e = t + i * kFThreads;
       if (e < R * C) {
         T v = ld[i];
-        if (PRE) v = mul_rn(v / pdiv[i], pmul[i]);
+        if (PRE) {
+          int c = c_base + (i * kFThreads) % C;  // compile-time offset
+          c = c >= C ? c - C : c;
+          v = mul_rn(v / s_pre[0][c], s_pre[1][c]);
+        }
         dst[e] = (A)v;
       }
     }
@@ -518,48 +519,63 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
     // ---- fold into the ring: plane k feeds output j + i in slot (k + i + 1)
     //      mod K; output j is then complete and leaves the ring
     const bool in_wx = x >= epi.wx0 && x < epi.wx1;
+    // the ring step for phase rr (a compile-time constant, so every slot
+    // index is static); accumulated with two fused multiply-adds per slot
+    auto ring_step = [&](auto rr_c) {
+      constexpr int rr = decltype(rr_c)::value;
 #pragma unroll
-    for (int rr = 0; rr < K; ++rr) {
-      if (rr == rph) {
-#pragma unroll
-        for (int i = 0; i < K; ++i) {
-          const int slot = (rr + i + 1) % K;
-          const A c0 = tp.x[0][i], c1 = tp.x[1][i];
-          acc[slot][0] += c0 * w0[0] + c1 * w1[0];
-          acc[slot][1] += c0 * w0[1] + c1 * w1[1];
-        }
-        const int es = (rr + 1) % K;
-        if (j >= 0) {
-          if (flux_epi) {
-            T f0 = add_rn(fprev0, (T)acc[es][0]);
-            T f1 = add_rn(fprev1, (T)acc[es][1]);
-            if (ok0) {
-              if (f0 < (T)0) {
-                s_clip += 1.0;
-                f0 = (T)0;
-              }
-              outp[o0] = f0;
-              if (in_wx && iny0) s_f += (double)f0;
-            }
-            if (ok1) {
-              if (f1 < (T)0) {
-                s_clip += 1.0;
-                f1 = (T)0;
-              }
-              outp[o1] = f1;
-              if (in_wx && iny1) s_f += (double)f1;
-            }
-          } else {
-            if (ok0) outp[o0] = (T)acc[es][0];
-            if (ok1) outp[o1] = (T)acc[es][1];
-          }
-        }
-        // a slot leaving the ring is cleared whether or not its output lies
-        // in this chunk (planes before the chunk only feed the halo)
-        acc[es][0] = (A)0;
-        acc[es][1] = (A)0;
+      for (int i = 0; i < K; ++i) {
+        const int slot = (rr + i + 1) % K;
+        const A c0 = tp.x[0][i], c1 = tp.x[1][i];
+        acc[slot][0] = fma_a(c1, w1[0], fma_a(c0, w0[0], acc[slot][0]));
+        acc[slot][1] = fma_a(c1, w1[1], fma_a(c0, w0[1], acc[slot][1]));
       }
+      constexpr int es = (rr + 1) % K;
+      if (j >= 0) {
+        if (flux_epi) {
+          T f0 = add_rn(fprev0, (T)acc[es][0]);
+          T f1 = add_rn(fprev1, (T)acc[es][1]);
+          if (ok0) {
+            if (f0 < (T)0) {
+              s_clip += 1.0;
+              f0 = (T)0;
+            }
+            outp[o0] = f0;
+            if (in_wx && iny0) s_f += (double)f0;
+          }
+          if (ok1) {
+            if (f1 < (T)0) {
+              s_clip += 1.0;
+              f1 = (T)0;
+            }
+            outp[o1] = f1;
+            if (in_wx && iny1) s_f += (double)f1;
+          }
+        } else {
+          if (ok0) outp[o0] = (T)acc[es][0];
+          if (ok1) outp[o1] = (T)acc[es][1];
+        }
+      }
+      // a slot leaving the ring is cleared whether or not its output lies
+      // in this chunk (planes before the chunk only feed the halo)
+      acc[es][0] = (A)0;
+      acc[es][1] = (A)0;
+    };
+#define STEAM_RING_CASE(n)                                  \
+  case n:                                                   \
+    if constexpr (n < K) ring_step(std::integral_constant<int, n>{}); \
+    break;
+    switch (rph) {
+      STEAM_RING_CASE(0) STEAM_RING_CASE(1) STEAM_RING_CASE(2) STEAM_RING_CASE(3)
+      STEAM_RING_CASE(4) STEAM_RING_CASE(5) STEAM_RING_CASE(6) STEAM_RING_CASE(7)
+      STEAM_RING_CASE(8) STEAM_RING_CASE(9) STEAM_RING_CASE(10) STEAM_RING_CASE(11)
+      STEAM_RING_CASE(12) STEAM_RING_CASE(13) STEAM_RING_CASE(14) STEAM_RING_CASE(15)
+      STEAM_RING_CASE(16) STEAM_RING_CASE(17) STEAM_RING_CASE(18) STEAM_RING_CASE(19)
+      STEAM_RING_CASE(20) STEAM_RING_CASE(21) STEAM_RING_CASE(22) STEAM_RING_CASE(23)
+      STEAM_RING_CASE(24)
+      default: break;
     }
+#undef STEAM_RING_CASE
     rph = rph + 1 == K ? 0 : rph + 1;
     if (k + 1 < count_i) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
     __syncthreads();
