@@ -75,36 +75,52 @@ inline size_t carve_bytes(size_t count, size_t elem) {
 // (key0, key1).  Round 0 sees the raw 64-bit world indices of x and z, so an
 // index outside [0, 2^32) (a negative z below a nest's ground) multiplies
 // modulo 2^64 exactly as the reference's uint64 arithmetic does; every word
-// is 32-bit from round 1 on.
+// is 32-bit from round 1 on.  The key schedule (key0 + r W0, key1 + r W1 for
+// rounds r = 1..9) is the same at every site, so it is built once on the
+// host and reaches the kernels as parameters.
 // ---------------------------------------------------------------------------
+struct PhiloxKey {
+  uint32_t k0[10], k1[10];  // round keys; [0] is the raw key
+  uint32_t k2;              // the counter's fourth word
+};
+
+__host__ __device__ inline PhiloxKey philox_key(uint32_t key0, uint32_t key1, uint32_t key2) {
+  PhiloxKey k;
+  uint32_t a = key0, b = key1;
+  for (int r = 0; r < 10; ++r) {
+    k.k0[r] = a;
+    k.k1[r] = b;
+    a += 0x9E3779B9u;
+    b += 0xBB67AE85u;
+  }
+  k.k2 = key2;
+  return k;
+}
+
 __device__ __forceinline__ void philox_site(int64_t ix, uint32_t iy, int64_t iz,
-                                            uint32_t key0, uint32_t key1,
-                                            uint32_t key2, uint32_t& r0,
+                                            const PhiloxKey& K, uint32_t& r0,
                                             uint32_t& r1) {
   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
-  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
   uint32_t c0, c1, c2, c3;
   {
     unsigned long long p0 = (unsigned long long)M0 * (unsigned long long)ix;
     unsigned long long p1 = (unsigned long long)M1 * (unsigned long long)iz;
-    c0 = (uint32_t)(p1 >> 32) ^ iy ^ key0;
+    c0 = (uint32_t)(p1 >> 32) ^ iy ^ K.k0[0];
     c1 = (uint32_t)p1;
-    c2 = (uint32_t)(p0 >> 32) ^ key2 ^ key1;
+    c2 = (uint32_t)(p0 >> 32) ^ K.k2 ^ K.k1[0];
     c3 = (uint32_t)p0;
   }
-  uint32_t k0 = key0, k1 = key1;
 #pragma unroll
   for (int r = 1; r < 10; ++r) {
-    k0 += W0;
-    k1 += W1;
-    uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
-    uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
-    uint32_t n0 = hi1 ^ c1 ^ k0;
-    uint32_t n2 = hi0 ^ c3 ^ k1;
+    // 32 x 32 -> 64-bit products: high and low words from one multiply
+    const unsigned long long q0 = (unsigned long long)M0 * c0;
+    const unsigned long long q1 = (unsigned long long)M1 * c2;
+    const uint32_t n0 = (uint32_t)(q1 >> 32) ^ c1 ^ K.k0[r];
+    const uint32_t n2 = (uint32_t)(q0 >> 32) ^ c3 ^ K.k1[r];
+    c1 = (uint32_t)q1;
+    c3 = (uint32_t)q0;
     c0 = n0;
-    c1 = lo1;
     c2 = n2;
-    c3 = lo0;
   }
   r0 = c0;
   r1 = c1;

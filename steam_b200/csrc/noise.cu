@@ -20,7 +20,7 @@ struct RegionDev {
   int64_t ox, oy, oz;
   int64_t wx, wy;
   int32_t sx, sy, sz;
-  uint32_t k0, k1, k2;
+  PhiloxKey key;
 };
 
 static RegionDev to_dev(const steam_region_t& r) {
@@ -36,9 +36,7 @@ static RegionDev to_dev(const steam_region_t& r) {
   d.sx = r.sparsity[0];
   d.sy = r.sparsity[1];
   d.sz = r.sparsity[2];
-  d.k0 = r.key[0];
-  d.k1 = r.key[1];
-  d.k2 = r.key[2];
+  d.key = philox_key(r.key[0], r.key[1], r.key[2]);
   return d;
 }
 
@@ -67,7 +65,7 @@ __device__ __forceinline__ T region_gamma(const RegionDev& r, int64_t x,
   if (!divisible(gx, r.sx) || !divisible(gy, r.sy) || !divisible(gz, r.sz))
     return (T)0;
   uint32_t r0, r1;
-  philox_site(gx, (uint32_t)gy, gz, r.k0, r.k1, r.k2, r0, r1);
+  philox_site(gx, (uint32_t)gy, gz, r.key, r0, r1);
   return levy_draw<T>((T)lattice_uniform(r0), (T)lattice_uniform(r1), lp);
 }
 
@@ -82,7 +80,7 @@ __device__ __forceinline__ float region_gamma<float>(const RegionDev& r, int64_t
   if (!divisible(gx, r.sx) || !divisible(gy, r.sy) || !divisible(gz, r.sz))
     return 0.0f;
   uint32_t r0, r1;
-  philox_site(gx, (uint32_t)gy, gz, r.k0, r.k1, r.k2, r0, r1);
+  philox_site(gx, (uint32_t)gy, gz, r.key, r0, r1);
   return levy_draw_f32(lattice_uniform(r0), lattice_uniform(r1), lp);
 }
 
@@ -90,8 +88,7 @@ __global__ void keyed_uniforms_kernel(const int64_t* __restrict__ ix,
                                       const int64_t* __restrict__ iy,
                                       const int64_t* __restrict__ iz,
                                       int64_t ny, int64_t nz, int64_t n,
-                                      uint32_t k0, uint32_t k1, uint32_t k2,
-                                      float* __restrict__ lane0,
+                                      PhiloxKey key, float* __restrict__ lane0,
                                       float* __restrict__ lane1) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -100,7 +97,7 @@ __global__ void keyed_uniforms_kernel(const int64_t* __restrict__ ix,
     int64_t b = col % ny;
     int64_t a = col / ny;
     uint32_t r0, r1;
-    philox_site(ix[a], (uint32_t)iy[b], iz[c], k0, k1, k2, r0, r1);
+    philox_site(ix[a], (uint32_t)iy[b], iz[c], key, r0, r1);
     lane0[i] = lattice_uniform(r0);
     lane1[i] = lattice_uniform(r1);
   }
@@ -145,9 +142,16 @@ __global__ void __launch_bounds__(256) flux_noise_kernel(
   const int zt = threadIdx.x - cofs * zlanes;
   double s_flux = 0.0, s_abs = 0.0, s_nnz = 0.0;
   if (cofs < cols_per_iter) {
-    for (uint32_t col = blockIdx.x * cols_per_iter + cofs; col < ncol;
-         col += gridDim.x * cols_per_iter) {
-      const uint32_t x = col / ny, y = col - x * ny;
+    // columns visited with a fixed stride: x and y advance without a division
+    const uint32_t c_step = gridDim.x * cols_per_iter;
+    const uint32_t sx = c_step / ny, sy = c_step - sx * ny;
+    uint32_t col = blockIdx.x * cols_per_iter + cofs;
+    uint32_t x = col / ny, y = col - x * ny;
+    for (; col < ncol; col += c_step, x += sx, y += sy) {
+      if (y >= ny) {
+        y -= ny;
+        x += 1;
+      }
       const bool in_win = x >= a.wx0 && x < a.wx1 && y >= a.wy0 && y < a.wy1;
       const int64_t base = (int64_t)col * nz;
       for (int z = zt; z < nz; z += zlanes) {
@@ -198,7 +202,7 @@ extern "C" int steam_keyed_uniforms(const int64_t* world_ix, int64_t nx,
                 "steam_keyed_uniforms: null pointer");
   int grid = stride_grid(n, 256, 16);
   keyed_uniforms_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(
-      world_ix, world_iy, world_iz, ny, nz, n, key0, key1, key2, lane0, lane1);
+      world_ix, world_iy, world_iz, ny, nz, n, philox_key(key0, key1, key2), lane0, lane1);
   STEAM_LAUNCH_CHECK("steam_keyed_uniforms");
   return STEAM_OK;
 }
