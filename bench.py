@@ -426,9 +426,9 @@ def main(argv=None):
     # of each entry's kernels in an ncu capture at 512x512x256 FP32, per voxel;
     # the kernels stream their fields once, so the traffic scales with voxels
     # (the convolution figure is the mean of its flux launch and two scalar ones)
-    dram_per_voxel = {"steam_conv_separable_async": 9.67, "steam_thermo_async": 30.1,
-                      "steam_flux_noise_async": 7.42, "steam_scalar_pattern_async": 15.3,
-                      "steam_flux_finish_async": 7.13}
+    dram_per_voxel = {"steam_conv_separable_async": 9.45, "steam_thermo_async": 30.24,
+                      "steam_flux_noise_async": 7.40, "steam_scalar_pattern_async": 14.68,
+                      "steam_flux_finish_async": 7.12}
     traffic = (dram_per_voxel[name] * nvox if args.dtype == "f32" and name in dram_per_voxel
                else None)
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
