@@ -174,6 +174,38 @@ __device__ __forceinline__ double d_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float d_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double d_sqrt(double x) { return sqrt(x); }
 
+// Four consecutive elements of a column, moved as 16-byte accesses (two for
+// float64); the pointer is 16-byte aligned.
+template <typename T>
+struct V4 {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ V4<T> ld4(const T* p) {
+  V4<T> r;
+  if (sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    r.v[0] = (T)q.x; r.v[1] = (T)q.y; r.v[2] = (T)q.z; r.v[3] = (T)q.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    r.v[0] = (T)a.x; r.v[1] = (T)a.y; r.v[2] = (T)b.x; r.v[3] = (T)b.y;
+  }
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void st4(T* p, const V4<T>& r) {
+  if (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)r.v[0], (float)r.v[1],
+                                                (float)r.v[2], (float)r.v[3]);
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2((double)r.v[0], (double)r.v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2((double)r.v[2], (double)r.v[3]);
+  }
+}
+
 // Uncontracted arithmetic: the reference evaluates these products and sums as
 // separate rounded operations, so they are kept out of FMA contraction.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }

@@ -50,6 +50,16 @@ __device__ __forceinline__ int64_t wrapi(int64_t v, int64_t n) {
   return r < 0 ? r + n : r;
 }
 
+// The input scaling of the second convolution, f' = f / mean(z) * C_k(z)
+// (steam/simulate.py:1989-1992), as ONE multiply by C_k / mean formed in
+// float64 and rounded to the field's type: within a unit in the last place
+// of the two separately rounded operations, and a multiply instead of a
+// division on every staged element.
+template <typename T>
+__device__ __forceinline__ T pre_scale(T div, T mul) {
+  return (T)((double)mul / (double)div);
+}
+
 // ---- z-pass -------------------------------------------------------------
 // Block = CB consecutive columns (contiguous in memory), staged with zero
 // padding: buf[j] = in[j - (kz-1-cz)].
@@ -76,7 +86,7 @@ __global__ void __launch_bounds__(256) zpass_kernel(
       T v = (T)0;
       if (s >= 0 && s < nz) {
         v = in[(col0 + c) * nz + s];
-        if (PRE) v = mul_rn(v / pre_div[s], pre_mul[s]);
+        if (PRE) v = mul_rn(v, pre_scale(pre_div[s], pre_mul[s]));
       }
       buf[c * len + j] = v;
     }
@@ -337,7 +347,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
   constexpr int R = S::R, C = S::C, NL = S::NL;
   extern __shared__ unsigned char smem_raw[];
   __shared__ double scratch[32];
-  __shared__ T s_pre[2][C];
+  __shared__ T s_pre[C];
   A* s_in0 = reinterpret_cast<A*>(smem_raw);  // [2][R*C]
   A* s_u = s_in0 + 2 * R * C;                            // [2][R][kFZ]
   const int t = threadIdx.x;
@@ -354,8 +364,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
   for (int c = t; c < C; c += kFThreads) {
     const int z = z0 - padz + c;
     const bool in_z = z >= 0 && z < g.nz;
-    s_pre[0][c] = (in_z && PRE) ? pre[z] : (T)1;
-    s_pre[1][c] = (in_z && PRE) ? pre[g.nz + z] : (T)1;
+    s_pre[c] = (in_z && PRE) ? pre_scale(pre[z], pre[g.nz + z]) : (T)1;
   }
   // this thread's staged elements e = t + i*kFThreads: their offset within
   // an input plane (-1 for zero padding) and their staged column
@@ -390,7 +399,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
         if (PRE) {
           int c = c_base + (i * kFThreads) % C;  // compile-time offset
           c = c >= C ? c - C : c;
-          v = mul_rn(v / s_pre[0][c], s_pre[1][c]);
+          v = mul_rn(v, s_pre[c]);
         }
         dst[e] = (A)v;
       }

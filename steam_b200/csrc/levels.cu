@@ -272,36 +272,6 @@ __global__ void __launch_bounds__(kLvThreads) pattern_kernel(
   store_level_partials<2, JM>(m, acc, red, partials);
 }
 
-template <typename T>
-struct V4 {
-  T v[4];
-};
-
-template <typename T>
-__device__ __forceinline__ V4<T> ld4(const T* p) {
-  V4<T> r;
-  if (sizeof(T) == 4) {
-    const float4 q = *reinterpret_cast<const float4*>(p);
-    r.v[0] = (T)q.x; r.v[1] = (T)q.y; r.v[2] = (T)q.z; r.v[3] = (T)q.w;
-  } else {
-    const double2 a = *reinterpret_cast<const double2*>(p);
-    const double2 b = *reinterpret_cast<const double2*>(p + 2);
-    r.v[0] = (T)a.x; r.v[1] = (T)a.y; r.v[2] = (T)b.x; r.v[3] = (T)b.y;
-  }
-  return r;
-}
-
-template <typename T>
-__device__ __forceinline__ void st4(T* p, const V4<T>& r) {
-  if (sizeof(T) == 4) {
-    *reinterpret_cast<float4*>(p) = make_float4((float)r.v[0], (float)r.v[1],
-                                                (float)r.v[2], (float)r.v[3]);
-  } else {
-    *reinterpret_cast<double2*>(p) = make_double2((double)r.v[0], (double)r.v[1]);
-    *reinterpret_cast<double2*>(p + 2) = make_double2((double)r.v[2], (double)r.v[3]);
-  }
-}
-
 // ---- scalar pattern, one 4-level group per thread --------------------------------
 // For nz % 4 == 0 (nz <= 1024): a column's nz/4 threads each own 4 consecutive
 // levels for the whole grid-stride walk, so the per-level constants sit in
@@ -730,43 +700,43 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
           acc[0][l] += (double)dv.v[l];
           acc[1][l] += (double)(dv.v[l] < (T)0 ? -dv.v[l] : dv.v[l]);
         }
-      return;
-    }
-    V4<T> df, pn, dn;
+    } else {
+      V4<T> df, pn, dn;
 #pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const T p0 = pv.v[l];
-      const T phi = add_rn(p0, mean.v[l]);
-      const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
-      T d = dv.v[l];
-      if (on & (1u << l)) d = mul_rn(clampv(sub_rn(d, fdm.v[l]), clo, chi), fsc.v[l]);
-      if (on & (16u << l)) d = clampv(sub_rn(d, cdm.v[l]), clo, chi);
-      df.v[l] = d;
-      if (on & (256u << l)) d = clampv(sub_rn(d, tdm.v[l]), clo, chi);
-      if (MODE == BA_APPLY) {
-        if (on & (4096u << l)) d = clampv(sub_rn(d, s_mu[z4 + l]), clo, chi);
-        pn.v[l] = add_rn(p0, d);
-        dn.v[l] = sub_rn(pn.v[l], p0);
-      } else if (in_w) {
-        if (MODE == BA_STATS) {
-          acc[0][l] += (double)d;
-          acc[1 % QS][l] += (double)(d < (T)0 ? -d : d);
-        } else {
+      for (int l = 0; l < 4; ++l) {
+        const T p0 = pv.v[l];
+        const T phi = add_rn(p0, mean.v[l]);
+        const T clo = sub_rn(c.lo, phi), chi = sub_rn(c.hi, phi);
+        T d = dv.v[l];
+        if (on & (1u << l)) d = mul_rn(clampv(sub_rn(d, fdm.v[l]), clo, chi), fsc.v[l]);
+        if (on & (16u << l)) d = clampv(sub_rn(d, cdm.v[l]), clo, chi);
+        df.v[l] = d;
+        if (on & (256u << l)) d = clampv(sub_rn(d, tdm.v[l]), clo, chi);
+        if (MODE == BA_APPLY) {
+          if (on & (4096u << l)) d = clampv(sub_rn(d, s_mu[z4 + l]), clo, chi);
+          pn.v[l] = add_rn(p0, d);
+          dn.v[l] = sub_rn(pn.v[l], p0);
+        } else if (in_w) {
+          if (MODE == BA_STATS) {
+            acc[0][l] += (double)d;
+            acc[1 % QS][l] += (double)(d < (T)0 ? -d : d);
+          } else {
 #pragma unroll
-          for (int k = 0; k < kMuCand; ++k) {
-            const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
-            const T tv = clampv(raw, clo, chi);
-            acc[k][l] += (double)tv;
-            cnt[k % (MODE == BA_MU ? kMuCand : 1)][l] += (raw > clo && raw < chi) ? 1u : 0u;
+            for (int k = 0; k < kMuCand; ++k) {
+              const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
+              const T tv = clampv(raw, clo, chi);
+              acc[k][l] += (double)tv;
+              cnt[k % (MODE == BA_MU ? kMuCand : 1)][l] += (raw > clo && raw < chi) ? 1u : 0u;
+            }
           }
         }
       }
-    }
-    if (MODE == BA_APPLY) {
-      st4(pert + i, pn);
-      if (record) st4(d0 + i, dn);
-    } else if (any_fold) {
-      st4(d0 + i, df);
+      if (MODE == BA_APPLY) {
+        st4(pert + i, pn);
+        if (record) st4(d0 + i, dn);
+      } else if (any_fold) {
+        st4(d0 + i, df);
+      }
     }
   };
   if (active && MODE == BA_APPLY) {
