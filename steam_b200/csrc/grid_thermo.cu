@@ -331,6 +331,25 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
   // staging geometry: lane -> (column group member, level) of a chunk
   constexpr int kCPI = 32 / kThZ;  // columns per staging instruction
   const int s_c = lane / kThZ, s_z = lane % kThZ;
+  // the h and qt values this lane stages for a chunk, loaded one chunk ahead
+  // so that the loads of chunk z0 + kThZ are in flight while chunk z0 is
+  // computed
+  constexpr int kPer = 32 / kCPI;  // staging instructions per chunk
+  T nh[kPer], nq[kPer];
+  auto fetch = [&](int z0f) {
+    const int zcf = (nz - z0f) < kThZ ? (nz - z0f) : kThZ;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int c = i * kCPI + s_c;
+      nh[i] = nq[i] = (T)0;
+      if (c < ncols && s_z < zcf) {
+        const int64_t o = (col0 + c) * nz + z0f + s_z;
+        nh[i] = h[o];
+        nq[i] = qt[o];
+      }
+    }
+  };
+  fetch(0);
   for (int z0 = 0; z0 < nz; z0 += kThZ) {
     const int zc = (nz - z0) < kThZ ? (nz - z0) : kThZ;
     if (lane < zc) {
@@ -341,14 +360,15 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
       lv[3 * kThZ + lane] =
           sizeof(T) == 4 ? (T)(-9.81 * dzv[z] / 287.04) : (T)(-9.81 * dzv[z]);
     }
-    for (int c0 = 0; c0 < ncols; c0 += kCPI) {
-      const int c = c0 + s_c;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int c = i * kCPI + s_c;
       if (c < ncols && s_z < zc) {
-        const int64_t o = (col0 + c) * nz + z0 + s_z;
-        sh(0, c, s_z) = h[o];
-        sh(1, c, s_z) = qt[o];
+        sh(0, c, s_z) = nh[i];
+        sh(1, c, s_z) = nq[i];
       }
     }
+    if (z0 + kThZ < nz) fetch(z0 + kThZ);
     __syncwarp();
     if (lane < ncols) {
       for (int zz = 0; zz < zc; ++zz) {
