@@ -551,9 +551,11 @@ __global__ void __launch_bounds__(kLvThreads) ba_sweep_kernel(
 #pragma unroll
       for (int k = 0; k < kMuCand; ++k) {
         const T raw = sub_rn(d, s_cand[k * nz + z]);
-        const T tv = clampv(raw, clo, chi);
-        acc[2 * k][j] += (double)tv;
-        acc[(2 * k + 1) % Q][j] += (raw > clo && raw < chi) ? 1.0 : 0.0;
+        const bool in = raw > clo && raw < chi;
+        // inside the caps the cell's value d - mu enters as d (the solver
+        // subtracts mu times the inside count); outside, the cap
+        acc[2 * k][j] += (double)(in ? d : clampv(raw, clo, chi));
+        acc[(2 * k + 1) % Q][j] += in ? 1.0 : 0.0;
       }
     }
   });
@@ -578,7 +580,7 @@ constexpr int kBaStages = 4;
 // memory (rounded up to 16 bytes; the cp.async ring follows)
 template <typename T>
 __host__ __device__ constexpr size_t ba_fold_param_bytes(int64_t nz) {
-  return (sizeof(T) * (size_t)nz * (11 + kMuCand) + 15) / 16 * 16;
+  return (sizeof(T) * (size_t)nz * (13 + kMuCand) + 15) / 16 * 16;
 }
 
 // 4 elements (16 or 32 bytes) global -> shared, asynchronously (L2 only)
@@ -631,6 +633,8 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   T* s_mu = s_mean + nz;
   T* s_mon = s_mu + nz;
   T* s_cand = s_mon + nz;  // [kMuCand][nz]
+  T* s_cmin = s_cand + kMuCand * nz;  // smallest and largest candidate
+  T* s_cmax = s_cmin + nz;
   const int R = c.R;
   for (int z = threadIdx.x; z < nz; z += blockDim.x) {
     const int ns = ldc<COH>(c.nsteps + z), ap = ldc<COH>(c.applied + z);
@@ -648,8 +652,16 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     s_mean[z] = ldc<COH>(c.mean + z);
     s_mon[z] = ldc<COH>(c.has_mu + z) ? (T)1 : (T)0;
     s_mu[z] = ldc<COH>(c.mu + z);
+    T cmin = ldc<COH>(c.cand + z * kMuCand), cmax = cmin;
 #pragma unroll
-    for (int k = 0; k < kMuCand; ++k) s_cand[k * nz + z] = ldc<COH>(c.cand + z * kMuCand + k);
+    for (int k = 0; k < kMuCand; ++k) {
+      const T ck = ldc<COH>(c.cand + z * kMuCand + k);
+      s_cand[k * nz + z] = ck;
+      cmin = ck < cmin ? ck : cmin;
+      cmax = ck > cmax ? ck : cmax;
+    }
+    s_cmin[z] = cmin;
+    s_cmax[z] = cmax;
   }
   __syncthreads();
   constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
@@ -721,12 +733,31 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
             acc[0][l] += (double)d;
             acc[1 % QS][l] += (double)(d < (T)0 ? -d : d);
           } else {
+            // d - mu over the candidates spans [d - cmax, d - cmin]: a cell
+            // inside the caps (or beyond one cap) for all of them takes one
+            // conversion; only a cell with a cap inside that span is
+            // evaluated per candidate
+            constexpr int KC = MODE == BA_MU ? kMuCand : 1;
+            const T lo_all = sub_rn(d, s_cmax[z4 + l]), hi_all = sub_rn(d, s_cmin[z4 + l]);
+            if (lo_all > clo && hi_all < chi) {
+              const double x = (double)d;
 #pragma unroll
-            for (int k = 0; k < kMuCand; ++k) {
-              const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
-              const T tv = clampv(raw, clo, chi);
-              acc[k][l] += (double)tv;
-              cnt[k % (MODE == BA_MU ? kMuCand : 1)][l] += (raw > clo && raw < chi) ? 1u : 0u;
+              for (int k = 0; k < kMuCand; ++k) {
+                acc[k][l] += x;
+                cnt[k % KC][l] += 1u;
+              }
+            } else if (lo_all >= chi || hi_all <= clo) {
+              const double x = (double)(lo_all >= chi ? chi : clo);
+#pragma unroll
+              for (int k = 0; k < kMuCand; ++k) acc[k][l] += x;
+            } else {
+#pragma unroll
+              for (int k = 0; k < kMuCand; ++k) {
+                const T raw = sub_rn(d, s_cand[k * nz + z4 + l]);
+                const bool in = raw > clo && raw < chi;
+                acc[k][l] += (double)(in ? d : clampv(raw, clo, chi));
+                cnt[k % KC][l] += in ? 1u : 0u;
+              }
             }
           }
         }
@@ -1237,8 +1268,11 @@ __device__ void ba_mu_level(BAState<T>& st, const double* tot, int it, int z) {
   for (int q = 0; q < kMuCand; ++q) {
     // the candidate actually evaluated is the dtype-rounded one
     cv[q] = (double)st.cand[z * kMuCand + q];
-    mv[q] = ldc<COH>(tot + (size_t)(2 * q) * nz + z) / st.N;
-    sl[q] = -ldc<COH>(tot + (size_t)(2 * q + 1) * nz + z) / st.N;
+    // the sweeps sum d over the cells inside the caps and the cap elsewhere:
+    // the level mean at this candidate is (sum - mu * inside count) / N
+    const double inside = ldc<COH>(tot + (size_t)(2 * q + 1) * nz + z);
+    mv[q] = (ldc<COH>(tot + (size_t)(2 * q) * nz + z) - cv[q] * inside) / st.N;
+    sl[q] = -inside / st.N;
   }
   if (it == 0 && fabs(mv[0]) <= 1e-9 * st.a0[z]) {
     st.need[z] = 0;  // the final clip left the level mean-free
@@ -1429,7 +1463,8 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   *ledger_dev = st.ledger;
 
   const bool vec4 = nz % 4 == 0 && nz <= 4 * kLvThreads &&
-                    ((uintptr_t)pert % 16 == 0) && ((uintptr_t)inc % 16 == 0);
+                    ((uintptr_t)pert % 16 == 0) && ((uintptr_t)inc % 16 == 0) &&
+                    ba_fold_smem_bytes<T>(nz) <= 200 * 1024;
   st.wb = vec4 ? 1 : 0;
   const size_t ba_sm = vec4 ? ba_fold_smem_bytes<T>(nz) : ba_smem_bytes<T>(nz, R);
   STEAM_REQUIRE(ba_sm <= 200 * 1024, "steam_bounded_add: n_rescale * nz too large");

@@ -328,8 +328,12 @@ def test_bounded_add_larger_levels(steam):
     p_o, i_o = pert.copy(), inc.copy()
     O.bounded_amplitude_add(p_o, mean, i_o, 0.0, 0.03, record_applied=True)
     p_g, i_g = pert.copy(), inc.copy()
-    sim._bounded_amplitude_add(p_g, mean, i_g, 0.0, 0.03, record_applied=True)
-    np.testing.assert_allclose(p_g, p_o, rtol=0, atol=5e-9)
+    led = sim._bounded_amplitude_add(p_g, mean, i_g, 0.0, 0.03, record_applied=True)
+    # the device solver stops once the shift is bracketed to a0 2^-20 (the
+    # float32 staircase of the level mean); a cell then differs by at most
+    # that plus a rounding at each end
+    atol = np.ldexp(float(np.max(led.a0)), -20) + 2 * float(np.spacing(np.float32(0.03)))
+    np.testing.assert_allclose(p_g, p_o, rtol=0, atol=atol)
 
 
 def test_projection_against_oracle(steam):
