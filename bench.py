@@ -64,7 +64,7 @@ def parse(argv=None):
                     help="tile requests per arrival rate in the serving episode (0: skip)")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=(100.0, 1000.0),
                     help="Poisson arrival rates (requests/s) of the serving episode")
-    ap.add_argument("--ensemble-members", type=int, default=32,
+    ap.add_argument("--ensemble-members", type=int, default=256,
                     help="members of the batched-ensemble episode (0: skip)")
     return ap.parse_args(argv)
 
