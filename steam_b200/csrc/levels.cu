@@ -467,6 +467,9 @@ struct BAChain {
   const int* applied;
   const int* fin_stored;
   const int* still;
+  // write-back form: per group of 4 levels, whether this sweep stores the
+  // group's pending steps (written by block 0 of a statistics or shift sweep)
+  int* grp;
   int R;
   T lo, hi;
 };
@@ -689,6 +692,15 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   // sweep, and levels that left the loop with their final clip stored) never
   // reads the perturbation
   const bool need_p = MODE == BA_SUMS ? false : (MODE != BA_STATS || (on & 0xfffu) != 0);
+  // a statistics sweep has nothing to do for 4 levels none of which is still
+  // in the rescale loop (their sums are not read, and steps they have pending
+  // stay pending: no later step joins them, and the apply sweep applies
+  // them): it reads and writes nothing for them
+  const bool work = active && !(MODE == BA_STATS && (on & 0xf00u) == 0u);
+  if ((MODE == BA_STATS || MODE == BA_MU) && blockIdx.x == 0)
+    for (int g = threadIdx.x; g < nz / 4; g += blockDim.x)
+      c.grp[g] = MODE == BA_STATS && (s_ton[4 * g] != (T)0 || s_ton[4 * g + 1] != (T)0 ||
+                                       s_ton[4 * g + 2] != (T)0 || s_ton[4 * g + 3] != (T)0);
   // sums in float64; the shift sweep's in-range counts as integers (exact)
   constexpr int QS = MODE == BA_MU ? kMuCand : 2;
   double acc[QS][4];
@@ -765,7 +777,7 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
       if (MODE == BA_APPLY) {
         st4(pert + i, pn);
         if (record) st4(d0 + i, dn);
-      } else if (any_fold) {
+      } else if (MODE == BA_STATS && any_fold) {
         st4(d0 + i, df);
       }
     }
@@ -797,7 +809,7 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     }
     for (; cw.col < ncol; cw.advance(step))
       process(cw, ld4(d0 + cw.col * nz + z4), ld4(pert + cw.col * nz + z4));
-  } else if (active) {
+  } else if (work) {
     // statistics and shift sweeps: the thread's own 16-byte pieces of the
     // next kBaStages - 1 columns stream into its slots of a shared-memory
     // ring by cp.async while it works on the current column, so the loads in
@@ -1085,6 +1097,7 @@ struct BAState {
   int* need;
   int* applied;     // write-back form: chain steps already stored in the increment
   int* fin_stored;  // write-back form: final clip already stored
+  int* grp;         // write-back form: the last sweep stored group z / 4
   int wb;           // the sweeps write back (vectorised path)
   MuSolver<T>* solver;
   // run flags: [0] the first sweep, [1 + k] rescale sweep k (k < R),
@@ -1169,7 +1182,10 @@ __device__ void ba_prepare_step(BAState<T>& st, int z, int k, int* next_flag) {
 // After a write-back sweep: every final part of the chain is now stored.
 template <typename T>
 __device__ void ba_note_stored(BAState<T>& st, int z) {
-  if (!st.wb) return;
+  // only a statistics sweep that processed the level's group stores its
+  // pending steps; a shift sweep stores nothing (the apply sweep applies
+  // whatever is still pending)
+  if (!st.wb || !__ldcg(st.grp + (z >> 2))) return;
   st.applied[z] = st.still[z] ? st.nsteps[z] - 1 : st.nsteps[z];
   st.fin_stored[z] = st.has_final[z];
 }
@@ -1404,7 +1420,9 @@ static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
          carve_bytes((size_t)(2 + R + kMuMaxSweeps), sizeof(int)) +
          carve_bytes(4, sizeof(unsigned)) +
          carve_bytes((size_t)5 * nz, sizeof(double)) +                      // ledger
-         carve_bytes((size_t)nz, sizeof(double));                           // mean upload
+         carve_bytes((size_t)nz, sizeof(double)) +                          // mean upload
+         carve_bytes((size_t)nz / 4 + 1, sizeof(int)) +                     // grp
+         (size_t)32 * 256;  // the 256-byte alignment of every separate carve
 }
 
 // Enqueues the whole bounded add on stream s: no host synchronisation and no
@@ -1445,6 +1463,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   st.need = c.take<int>(nz);
   st.applied = c.take<int>(nz);
   st.fin_stored = c.take<int>(nz);
+  st.grp = c.take<int>(nz / 4 + 1);
   st.solver = c.take<MuSolver<T>>(nz);
   st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
   st.bar = c.take<unsigned>(4);
@@ -1452,7 +1471,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   if (!partials || !totals || !st.nsteps || !st.has_final || !st.has_mu || !st.demean ||
       !st.scale || !st.final_dm || !st.mu || !st.mean || !st.cand || !st.a0 || !st.cur_mean ||
       !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.applied ||
-      !st.fin_stored || !st.solver ||
+      !st.fin_stored || !st.grp || !st.solver ||
       !st.flags || !st.bar || !st.ledger)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
   st.R = R;
@@ -1510,6 +1529,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   ch.applied = st.applied;
   ch.fin_stored = st.fin_stored;
   ch.still = st.still;
+  ch.grp = st.grp;
   ch.R = R;
   ch.lo = (T)phi_min;
   ch.hi = (T)phi_max;
