@@ -117,6 +117,8 @@ __global__ void levy_field_kernel(RegionDev r, LevyParams<T> lp,
   }
 }
 
+constexpr int kNoiseZLanes = 64;
+
 struct NoiseArgs {
   double scale, shift;
   int32_t n_zero, zero_bottom, zero_top;
@@ -136,7 +138,10 @@ __global__ void __launch_bounds__(256) flux_noise_kernel(
   const uint32_t ncol = (uint32_t)(r.nx * r.ny);
   const uint32_t ny = (uint32_t)r.ny;
   const int nz = (int)r.nz;
-  const int zlanes = nz < (int)blockDim.x ? nz : (int)blockDim.x;
+  // up to kNoiseZLanes threads per column, each taking every kNoiseZLanes-th
+  // level, so the per-column work (walk, wrap, window, the x and y words of
+  // the Philox counter) is shared by several cells
+  const int zlanes = nz < kNoiseZLanes ? nz : kNoiseZLanes;
   const int cols_per_iter = (int)blockDim.x / zlanes;
   const int cofs = threadIdx.x / zlanes;
   const int zt = threadIdx.x - cofs * zlanes;
@@ -276,7 +281,7 @@ static int flux_noise_launch(int dtype, const steam_region_t* region, double alp
   if (n == 0) return STEAM_OK;
   STEAM_REQUIRE(flux && product, std::string(who) + ": null field pointer");
   STEAM_REQUIRE(r.nx * r.ny < ((int64_t)1 << 32), std::string(who) + ": more than 2^32 columns");
-  const int64_t cols_per_block = r.nz < 256 ? 256 / r.nz : 1;
+  const int64_t cols_per_block = 256 / (r.nz < kNoiseZLanes ? r.nz : kNoiseZLanes);
   int grid = stride_grid((r.nx * r.ny + cols_per_block - 1) / cols_per_block, 1,
                          kNoiseBlocksPerSm);
   Carver c(workspace, workspace_bytes);
