@@ -117,7 +117,7 @@ __global__ void levy_field_kernel(RegionDev r, LevyParams<T> lp,
   }
 }
 
-constexpr int kNoiseZLanes = 64;
+constexpr int kNoiseZLanes = 32;
 
 struct NoiseArgs {
   double scale, shift;
