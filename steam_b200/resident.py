@@ -104,7 +104,7 @@ class ResidentClass:
         return self.work
 
     def step(self, hp, qp, F, diagnostics=None, surface_pressure=101325.0, ready=None,
-             done=None):
+             done=None, before_thermo=(), copy_ledger=True):
         """Enqueue one class step on the resident fields (mutated in place)
         and, with ``diagnostics`` (a dict of tensors T, qv, qc, qi, p), the
         composition + thermodynamics.  Returns without waiting on the GPU.
@@ -112,7 +112,11 @@ class ResidentClass:
         ``ready`` maps 'h' / 'qt' to CUDA events the step waits for before it
         first reads that field (an upload still in flight on another
         stream); ``done``, a dict, receives events recorded when F, h, qt and
-        the diagnostics are final."""
+        the diagnostics are final; the thermodynamics waits for the events in
+        ``before_thermo`` (copies still reading the diagnostic buffers).
+        ``copy_ledger=False`` leaves the ledger block on the device (a caller
+        that copies it on its own stream); ``done['end']`` then marks the
+        step's end."""
         import torch
         lib, cs, code = self.lib, self.setup, self.code
         nx, ny, nz = self.shape
@@ -171,6 +175,8 @@ class ResidentClass:
                 done[name].record()
         if diagnostics is not None:
             d = diagnostics
+            for ev in before_thermo:
+                torch.cuda.current_stream().wait_event(ev)
             _lib.check(lib.steam_thermo_async(
                 code, nx, ny, nz, _lib.ptr(hp), _lib.ptr(qp), _lib.ptr(self.prof), 1,
                 _lib.dvec(self.bounds), float(surface_pressure), None, _lib.ptr(d["T"]),
@@ -179,12 +185,16 @@ class ResidentClass:
             if done is not None:
                 done['diag'] = torch.cuda.Event()
                 done['diag'].record()
-        self.ledger_host.copy_(L, non_blocking=True)
-        self.ledger_ready.record()
+        if copy_ledger:
+            self.ledger_host.copy_(L, non_blocking=True)
+            self.ledger_ready.record()
+        elif done is not None:
+            done['end'] = torch.cuda.Event()
+            done['end'].record()
         return self
 
     def host_step(self, h, qt, flux, diagnostics=('qc', 'qi'), out=None,
-                  surface_pressure=101325.0):
+                  surface_pressure=101325.0, wait=True):
         """One class step on host arrays, with the transfers pipelined.
 
         h, qt, flux (numpy, updated in place) are uploaded on one copy
@@ -193,10 +203,19 @@ class ResidentClass:
         stream as soon as it is final (F while h and qt are still going up and
         the scalars run, h while qt runs, qt and the diagnostics last), so the
         two directions of the link run at the same time and both overlap
-        compute.  ``out`` maps
-        diagnostic names to host arrays to fill; page-locked arrays (e.g.
-        ``torch.empty(..., pin_memory=True).numpy()``) let every copy run
-        asynchronously at full PCIe bandwidth.  Returns the diagnostics."""
+        compute.  ``out`` maps diagnostic names to host arrays to fill;
+        page-locked arrays (e.g. ``torch.empty(..., pin_memory=True).numpy()``)
+        let every copy run asynchronously at full PCIe bandwidth.  Returns the
+        diagnostics.
+
+        ``wait=False`` returns a ``PendingHostStep`` at once, without waiting
+        for the downloads: a following call on the same arrays orders itself
+        after them (each upload waits for the download of the same array, the
+        thermodynamics for the previous diagnostic downloads), so the uploads
+        of step k + 1 overlap the downloads of step k.  Only for host arrays
+        the copies can fill directly (C-contiguous, of the step's dtype);
+        others make the call wait.  The step's ledger comes with the pending
+        step (``result()[1]``), not from ``class_ledger``."""
         import torch
         shape = self.shape
         for name, a in (('h', h), ('qt', qt), ('flux', flux)):
@@ -207,23 +226,31 @@ class ResidentClass:
                        for k in ('h', 'qt', 'F', 'T', 'qv', 'qc', 'qi', 'p')}
             self.up_stream = torch.cuda.Stream()
             self.down_stream = torch.cuda.Stream()
+            self.downloaded = None
         io, up, cp = self.io, self.up_stream, self.down_stream
+        prev = self.downloaded
         main = torch.cuda.current_stream()
         src = {k: torch.from_numpy(np.ascontiguousarray(a, dtype=self.np_t))
                for k, a in (('F', flux), ('h', h), ('qt', qt))}
-        up.wait_stream(main)  # the device buffers are free once earlier work is done
+        up.wait_stream(main)  # the previous step's compute is done with the buffers
         ready = {}
         with torch.cuda.stream(up):
             for k in ('F', 'h', 'qt'):
+                if prev is not None:
+                    up.wait_event(prev[k])  # its download of this array is complete
                 io[k].copy_(src[k], non_blocking=True)
                 ready[k] = torch.cuda.Event()
                 ready[k].record(up)
         main.wait_event(ready['F'])
         done = {}
         diag_dev = {k: io[k] for k in ('T', 'qv', 'qc', 'qi', 'p')} if diagnostics else None
+        before = (prev['diag'],) if prev is not None and 'diag' in prev else ()
+        # the main stream carries compute only: every device-to-host copy,
+        # the ledger's included, goes on the download stream
         self.step(io['h'], io['qt'], io['F'], diagnostics=diag_dev,
-                  surface_pressure=surface_pressure, ready=ready, done=done)
-        result = {}
+                  surface_pressure=surface_pressure, ready=ready, done=done,
+                  before_thermo=before, copy_ledger=False)
+        ledger = torch.empty(self.ledger.numel(), dtype=torch.float64, pin_memory=True)
         if out is None:
             out = {}
         host_out = {}
@@ -232,31 +259,36 @@ class ResidentClass:
                 host_out[k] = torch.from_numpy(out[k])
             else:
                 host_out[k] = torch.empty(shape, dtype=self.dtype, pin_memory=True)
+        dl = {}
         with torch.cuda.stream(cp):
-            for ev, pairs in (('F', (('F', flux),)), ('h', (('h', h),)), ('qt', (('qt', qt),))):
-                cp.wait_event(done[ev])
-                for k, host in pairs:
-                    dst = host if isinstance(host, np.ndarray) else None
-                    t = torch.from_numpy(dst) if dst is not None and dst.dtype == self.np_t \
-                        and dst.flags.c_contiguous else None
-                    if t is not None:
-                        t.copy_(io[k], non_blocking=True)
-                    else:
-                        host_out['_' + k] = torch.empty(shape, dtype=self.dtype,
-                                                        pin_memory=True)
-                        host_out['_' + k].copy_(io[k], non_blocking=True)
+            for k, host in (('F', flux), ('h', h), ('qt', qt)):
+                cp.wait_event(done[k])
+                t = torch.from_numpy(host) if isinstance(host, np.ndarray) and \
+                    host.dtype == self.np_t and host.flags.c_contiguous else None
+                if t is not None:
+                    t.copy_(io[k], non_blocking=True)
+                else:
+                    host_out['_' + k] = torch.empty(shape, dtype=self.dtype, pin_memory=True)
+                    host_out['_' + k].copy_(io[k], non_blocking=True)
+                dl[k] = torch.cuda.Event()
+                dl[k].record(cp)
             if diagnostics:
                 cp.wait_event(done['diag'])
                 for k in diagnostics:
                     host_out[k].copy_(io[k], non_blocking=True)
-        cp.synchronize()
-        up.synchronize()
-        for k, host in (('F', flux), ('h', h), ('qt', qt)):
-            if '_' + k in host_out:
-                host[...] = host_out['_' + k].numpy()
-        for k in (diagnostics or ()):
-            result[k] = host_out[k].numpy()
-        return result
+                dl['diag'] = torch.cuda.Event()
+                dl['diag'].record(cp)
+            cp.wait_event(done['end'])
+            ledger.copy_(self.ledger, non_blocking=True)
+            ledger_ready = torch.cuda.Event()
+            ledger_ready.record(cp)
+        self.downloaded = dl
+        pending = PendingHostStep(self, (('F', flux), ('h', h), ('qt', qt)), host_out,
+                                  tuple(diagnostics or ()), ledger, ledger_ready)
+        staged = any(k.startswith('_') for k in host_out)
+        if wait or staged:
+            return pending.result()[0] if wait else pending.wait_now()
+        return pending
 
     def class_ledger(self, cl=None, wait=True):
         """The step's ledger as a ``ClassLedger``.  ``wait``: wait for the
@@ -265,7 +297,10 @@ class ResidentClass:
         device itself and passes False."""
         if wait:
             self.ledger_ready.synchronize()
-        v = self.ledger_host.numpy().copy()
+        return self.parse_ledger(self.ledger_host.numpy().copy(), cl)
+
+    def parse_ledger(self, v, cl=None):
+        """A ``ClassLedger`` from a host copy of the step's ledger block."""
         nz = self.shape[2]
         fl = v[self.o_fl:self.o_fl + 10]
         cl = ClassLedger() if cl is None else cl
@@ -281,6 +316,42 @@ class ResidentClass:
                 raise RuntimeError(f"resident class step: the {name} bounded add's "
                                    f"persistent phase timed out at a grid barrier")
         return cl
+
+
+class PendingHostStep:
+    """A host step whose downloads may still be in flight (``host_step`` with
+    ``wait=False``).  ``result()`` waits for them and returns (diagnostics,
+    ClassLedger) of this step."""
+
+    def __init__(self, rc, fields, host_out, names, ledger, ledger_ready):
+        self._rc = rc
+        self._fields = fields
+        self._host_out = host_out
+        self._names = names
+        self._ledger = ledger
+        self._ledger_ready = ledger_ready
+        self._done = None
+
+    def _finish(self):
+        if self._done is None:
+            self._rc.down_stream.synchronize()
+            self._rc.up_stream.synchronize()
+            for k, host in self._fields:
+                if '_' + k in self._host_out:
+                    host[...] = self._host_out['_' + k].numpy()
+            diag = {k: self._host_out[k].numpy() for k in self._names}
+            self._ledger_ready.synchronize()
+            self._done = (diag, self._rc.parse_ledger(self._ledger.numpy().copy()))
+        return self._done
+
+    def wait_now(self):
+        """Finish now (the call that staged a host array needs its results
+        written back before anything else reads them) and return self."""
+        self._finish()
+        return self
+
+    def result(self):
+        return self._finish()
 
 
 _CACHE = {}

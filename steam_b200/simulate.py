@@ -1139,7 +1139,7 @@ def make_class_setup(grids, i, *, h_profile, qt_profile, z_profile, C_h, C_qt, b
 
 
 def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=101325.0,
-               diagnostics=('qc', 'qi'), ledger=None, out=None):
+               diagnostics=('qc', 'qi'), ledger=None, out=None, wait=True):
     """One size class plus the thermodynamic map to condensate.
 
     Advances the flux, adds the h and qt increments (pattern, second
@@ -1150,6 +1150,12 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
     (diagnostics dict, ClassLedger).  With numpy arrays, ``out`` (a dict of
     host arrays) receives the diagnostics; page-locked arrays let the
     pipelined transfers run at full PCIe bandwidth.
+
+    ``wait=False`` (host arrays only) returns a ``PendingHostStep`` before the
+    downloads finish; its ``result()`` gives (diagnostics, ClassLedger).  A
+    following call on the same arrays is ordered after those downloads and
+    its uploads overlap them, so a loop of steps keeps both directions of the
+    link busy.  Read the arrays only after ``result()``.
     """
     from .ledger import ClassLedger
     from .thermodynamics import recover_diagnostics_device
@@ -1160,9 +1166,10 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
         from .resident import resident_for
         np_t = np.asarray(h_perturbation).dtype
         rc = resident_for(setup, torch.float64 if np_t == np.float64 else torch.float32)
-        diag = rc.host_step(h_perturbation, qt_perturbation, flux, diagnostics=diagnostics,
-                            out=out, surface_pressure=surface_pressure)
-        return diag, rc.class_ledger()
+        pending = rc.host_step(h_perturbation, qt_perturbation, flux,
+                               diagnostics=diagnostics, out=out,
+                               surface_pressure=surface_pressure, wait=False)
+        return pending.result() if wait else pending
     hp, h_host = to_device(h_perturbation)
     qp, q_host = to_device(qt_perturbation, dtype=hp.dtype)
     F, f_host = to_device(flux, dtype=hp.dtype)

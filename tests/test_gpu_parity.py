@@ -549,6 +549,50 @@ def test_resident_step_matches_stage_by_stage(steam, dtype, shape, window):
         assert bs.n_sweeps == br.n_sweeps
 
 
+def test_field_step_pipelined_steps_match_resident_steps(steam):
+    """field_step with wait=False, three steps in a row on the same page-locked
+    arrays (each step's uploads overlapping the previous step's downloads),
+    gives the bits and ledgers of three resident steps on device tensors."""
+    import torch
+    from steam_b200 import simulate as sim
+    from steam_b200.resident import ResidentClass
+    nx, ny, nz = 32, 24, 20
+    sim_, zp, hp, qp, grids, C_h, C_q = _one_class_setup(nx, ny, nz)
+    setup = sim.make_class_setup(
+        grids, 0, h_profile=hp, qt_profile=qp, z_profile=zp, C_h=C_h[0], C_qt=C_q[0],
+        b_h=sim._bound_buffers(C_h, 1)[0], b_qt=sim._bound_buffers(C_q, 1)[0],
+        aspect=np.ones(nz, np.float32), bounds=(315 * 1004.0, 355 * 1004.0, 0.0, 0.03),
+        key=O.class_key(np.random.SeedSequence(9)), flux_noise_scale=0.1, dtype=np.float32)
+    rng = np.random.default_rng(6)
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+        t.copy_(torch.from_numpy(a))
+        return t.numpy()
+    h = pinned((800.0 * rng.standard_normal((nx, ny, nz))).astype(np.float32))
+    q = pinned((0.0008 * rng.standard_normal((nx, ny, nz))).astype(np.float32))
+    F = pinned((1.0 + 0.2 * rng.random((nx, ny, nz))).astype(np.float32))
+    ht, qt_, Ft = (torch.as_tensor(a.copy(), device='cuda') for a in (h, q, F))
+    rc = ResidentClass(setup, torch.float32)
+    want = []
+    for _ in range(3):
+        diag = {k: torch.empty_like(ht) for k in ("T", "qv", "qc", "qi", "p")}
+        rc.step(ht, qt_, Ft, diagnostics=diag)
+        want.append((diag["qc"].cpu().numpy(), diag["qi"].cpu().numpy(),
+                     rc.class_ledger().flux.realized.total))
+    outs = [{k: pinned(np.zeros((nx, ny, nz), np.float32)) for k in ("qc", "qi")}
+            for _ in range(3)]
+    pend = [sim.field_step(h, q, F, setup, out=o, wait=False) for o in outs]
+    got = [p.result() for p in pend]
+    for (d, led), (qc, qi, realized) in zip(got, want):
+        np.testing.assert_array_equal(d["qc"], qc)
+        np.testing.assert_array_equal(d["qi"], qi)
+        assert led.flux.realized.total == realized
+    np.testing.assert_array_equal(h, ht.cpu().numpy())
+    np.testing.assert_array_equal(q, qt_.cpu().numpy())
+    np.testing.assert_array_equal(F, Ft.cpu().numpy())
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_field_step_host_arrays_match_resident_tensors(steam, dtype):
     """field_step on numpy arrays (pipelined copies on a second stream) gives
