@@ -223,8 +223,9 @@ __device__ __forceinline__ double newton_rcp(double x) { return 1.0 / x; }
 // Newton on f(T) = cp T + Lv qvs(T, p) + g z - h, 5 iterations from the dry
 // temperature, when qt exceeds the saturation mixing ratio there.
 // float32: fused multiply-adds and the approximate reciprocal and exp2; the
-// two reciprocals 1/(T - 29.65) and 1/(p - es) are shared between the Bolton
-// exponent, qvs and dqvs/dT = dq c622 p es / ((T - 29.65)^2 (p - es)^2).
+// reciprocal 1/(T - 29.65) is shared between the Bolton exponent and
+// dqvs/dT = dq c622 p es / ((T - 29.65)^2 (p - es)^2), and the step needs
+// one more reciprocal, of its denominator.
 __device__ __forceinline__ void saturate(float hl, float ql, float pl, float gz,
                                          const ThermoConst<float>& k, float& Tl, float& qvl) {
   const float Td = __fmul_rn(__fsub_rn(__fsub_rn(hl, __fmul_rn(k.lv, ql)), gz), k.inv_cp);
@@ -233,18 +234,20 @@ __device__ __forceinline__ void saturate(float hl, float ql, float pl, float gz,
   Tl = Td;
   qvl = ql;
   if (ql > qvs) {
-    const float gzh = gz - hl, cpl = k.dqc * pl;
+    // the Newton step f / f' with numerator and denominator both multiplied
+    // by (p - es)^2, which takes the reciprocal of (p - es) out of the loop:
+    //   f (p - es)^2  = ((cp T + g z - h)(p - es) + Lv c622 es)(p - es)
+    //   f'(p - es)^2  = cp (p - es)^2 + Lv dq c622 p es / (T - 29.65)^2
+    const float gzh = gz - hl, lvc = k.lv * k.c622, lvdq = k.lv * k.dqc * pl;
     float Tn = Td;
 #pragma unroll 1
     for (int it = 0; it < 5; ++it) {
       const float i1 = rcp_approx(Tn - k.ec);
       const float e = k.es0 * ex2_approx(k.ea2 * (Tn - k.eb) * i1);
-      const float i2 = rcp_approx(pl - e);
-      const float q = k.c622 * e * i2;
-      const float f = fmaf(k.cp, Tn, fmaf(k.lv, q, gzh));
-      const float u = i1 * i2;
-      const float dq = cpl * e * u * u;
-      Tn = fmaf(-f, rcp_approx(fmaf(k.lv, dq, k.cp)), Tn);
+      const float pe = pl - e;
+      const float num = fmaf(fmaf(k.cp, Tn, gzh), pe, lvc * e) * pe;
+      const float den = fmaf(k.cp * pe, pe, lvdq * e * i1 * i1);
+      Tn = fmaf(-num, rcp_approx(den), Tn);
     }
     Tl = Tn;
     const float e = bolton_f(Tn, k);
