@@ -26,7 +26,7 @@ from . import simulate as sim
 from . import utils as _utils
 from .resident import ResidentClass
 
-CHUNKS = (16, 32, 64, 128, 256)
+CHUNKS = (16, 32, 64, 128, 256, 384, 512)
 _TUNED = {}
 
 
