@@ -109,6 +109,47 @@ def factor_kernel(kernel, tol):
     return Px, Py, Pz, core, err
 
 
+def _sparse_core_rotation(core):
+    """Rotations Ry, Rz of the y and z factor bases that make the core's
+    (y 1, z 1) slice vanish, or None.
+
+    With G_a[b, c] = core[a, b, c], the slice after rotating by unit vectors y
+    (y column 1) and z (z column 1) is y^T G_a z.  A z for which G_0 z and
+    G_1 z are parallel (a zero of the quadratic form det[G_0 z, G_1 z]) and a
+    y orthogonal to both make it zero for every a.  The turbulon kernels,
+    sums of separable terms g(x) g(y) g(z) (3 - x^2 - y^2 - z^2), have one:
+    their y and z filter pairs then drop from 4 to 3.  Orthogonal rotations
+    leave the factorisation's conditioning unchanged."""
+    G = [core[a] for a in range(core.shape[0])]
+    if len(G) == 1:
+        z = np.array([0.0, 1.0])
+    else:
+        M = np.empty((2, 2))
+        for i in range(2):
+            for j in range(2):
+                u, v = G[0][:, i], G[1][:, j]
+                M[i, j] = u[0] * v[1] - u[1] * v[0]
+        w, V = np.linalg.eigh(0.5 * (M + M.T))
+        scale = max(float(np.max(np.abs(w))), 1e-300)
+        if float(np.min(np.abs(w))) <= 1e-12 * scale:
+            z = V[:, int(np.argmin(np.abs(w)))]
+        elif w[0] * w[1] < 0:
+            z = np.sqrt(abs(w[1])) * V[:, 0] + np.sqrt(abs(w[0])) * V[:, 1]
+        else:
+            return None
+    z = z / np.linalg.norm(z)
+    g = max((Ga @ z for Ga in G), key=np.linalg.norm)
+    if np.linalg.norm(g) == 0.0:
+        return None
+    y = np.array([-g[1], g[0]]) / np.linalg.norm(g)
+    Ry = np.column_stack([[y[1], -y[0]], y])
+    Rz = np.column_stack([[z[1], -z[0]], z])
+    rot = np.einsum('abc,bB,cC->aBC', core, Ry, Rz)
+    if np.max(np.abs(rot[:, 1, 1])) > 1e-13 * max(float(np.max(np.abs(core))), 1e-300):
+        return None
+    return Ry, Rz
+
+
 def plan_from_factors(Px, Py, Pz, core, kshape, field_shape, err=0.0):
     """Separable plan from explicit factors (x: Px[:, a], ...), or None when
     the factor counts exceed the kernels' limits."""
@@ -131,6 +172,16 @@ def plan_from_factors(Px, Py, Pz, core, kshape, field_shape, err=0.0):
                 P[:, j] = e
         return P
 
+    pairs = [(c, b) for c in range(rz) for b in range(ry)]
+    if ry == 2 and rz == 2:
+        rot = _sparse_core_rotation(core)
+        if rot is not None:
+            Ry, Rz = rot
+            Py, Pz = Py @ Ry, Pz @ Rz
+            core = np.einsum('abc,bB,cC->aBC', core, Ry, Rz)
+            core[:, 1, 1] = 0.0
+            pairs = [(0, 0), (0, 1), (1, 0)]
+    npairs = len(pairs)
     Px, Py, Pz = even(Px), even(Py), even(Pz)
     spec = _lib.SepConv()
     spec.kz, spec.ky, spec.kx = kz, ky, kx
@@ -138,13 +189,11 @@ def plan_from_factors(Px, Py, Pz, core, kshape, field_shape, err=0.0):
     spec.cy = effective_centre(ky, ny)
     spec.cx = effective_centre(kx, nx)
     spec.n_z, spec.n_y, spec.n_x, spec.n_pairs = rz, ry, rx, npairs
-    for c in range(rz):
-        for b in range(ry):
-            q = c * ry + b
-            spec.pair_z[q] = c
-            spec.pair_y[q] = b
-            for a in range(rx):
-                spec.mix[a * npairs + q] = float(core[a, b, c])
+    for q, (c, b) in enumerate(pairs):
+        spec.pair_z[q] = c
+        spec.pair_y[q] = b
+        for a in range(rx):
+            spec.mix[a * npairs + q] = float(core[a, b, c])
     return ConvPlan(
         kind='separable', shape=(kx, ky, kz), spec=spec,
         z_taps=_lib.dvec(Pz.T.ravel()), y_taps=_lib.dvec(Py.T.ravel()),
