@@ -99,6 +99,28 @@ def test_factorisation_of_turbulon_kernels(golden):
     assert U.plan_convolution(rnd, (16, 16, 16), np.float32).kind == 'dense'
 
 
+def test_turbulon_plan_has_three_filter_pairs():
+    """A float64 turbulon kernel, a sum of separable terms
+    g g g (3 - x^2 - y^2 - z^2), gets y and z bases in which one of the four
+    (z filter, y filter) pairs vanishes; the 3-pair network still equals the
+    kernel to roundoff.  A float32-rounded kernel keeps all four pairs."""
+    for args in ((1, 0.5, 0.5, 0.5), (1, 0.5, 0.5, 0.25), (2, 0.5, 0.5, 0.5)):
+        K = O.turbulon_envelope(*args, dtype=np.float64)
+        plan = U.plan_convolution(K, (64, 64, 32), np.float64)
+        sp = plan.spec
+        assert plan.kind == 'separable' and sp.n_pairs == 3
+        assert sorted((sp.pair_z[q], sp.pair_y[q]) for q in range(3)) == [(0, 0), (0, 1), (1, 0)]
+        Z = np.ctypeslib.as_array(plan.z_taps)[:sp.n_z * sp.kz].reshape(sp.n_z, sp.kz)
+        Y = np.ctypeslib.as_array(plan.y_taps)[:sp.n_y * sp.ky].reshape(sp.n_y, sp.ky)
+        X = np.ctypeslib.as_array(plan.x_taps)[:sp.n_x * sp.kx].reshape(sp.n_x, sp.kx)
+        rec = np.zeros_like(K)
+        for a in range(sp.n_x):
+            for q in range(sp.n_pairs):
+                rec += sp.mix[a * sp.n_pairs + q] * np.einsum(
+                    'i,j,k->ijk', X[a], Y[sp.pair_y[q]], Z[sp.pair_z[q]])
+        assert np.linalg.norm(rec - K) / np.linalg.norm(K) < 1e-12
+
+
 def test_separable_plan_reconstructs_kernel(golden):
     """The separable network given to the device equals the kernel."""
     K = golden["kern_s1"].astype(np.float64)
