@@ -866,8 +866,11 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   }
 }
 
+// The bounded add's first sweep (BA_SUMS) and apply sweep (BA_APPLY) as
+// launches of their own; its statistics and shift sweeps run inside
+// ba_phase_kernel.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : (MODE == BA_STATS ? 3 : 4)))
+__global__ void __launch_bounds__(kLvThreads, 4)
     ba_fold_kernel(T* __restrict__ d0, T* __restrict__ pert, int record, int64_t nx,
                    int64_t ny, int nz, Win w, BAChain<T> c, double* __restrict__ partials) {
   if (c.run && *c.run == 0) return;
@@ -1494,10 +1497,6 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   if (vec4) {
     STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_SUMS>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-    STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_STATS>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
-    STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_MU>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
     STEAM_CUDA(cudaFuncSetAttribute(ba_fold_kernel<T, BA_APPLY>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ba_fold_param_bytes<T>(nz)));
@@ -1548,20 +1547,16 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
         ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
     } else if (mode == BA_STATS) {
-      if (vec4)
-        ba_fold_kernel<T, BA_STATS><<<grid4, kLvThreads, ba_sm, s>>>(
-            inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
-      else if (m.packed)
+      // (the vectorised path runs its statistics and shift sweeps inside
+      // ba_phase_kernel)
+      if (m.packed)
         ba_sweep_kernel<T, BA_STATS, 1><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
       else
         ba_sweep_kernel<T, BA_STATS, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
     } else if (mode == BA_MU) {
-      if (vec4)
-        ba_fold_kernel<T, BA_MU><<<grid4, kLvThreads, ba_sm, s>>>(
-            inc, pert, rec, nx, ny, (int)nz, w, ch, partials);
-      else if (m.packed)
+      if (m.packed)
         ba_sweep_kernel<T, BA_MU, 1><<<grid, kLvThreads, ba_sm, s>>>(
             inc, pert, out, rec, nx, ny, m, w, ch, partials);
       else
