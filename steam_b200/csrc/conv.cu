@@ -347,6 +347,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
     const __grid_constant__ FusedTaps<A, K> tp, FusedGeom<T> g, XEpi epi,
     double* __restrict__ partials) {
   static_assert(K <= 25, "the ring dispatch covers K <= 25");
+  static_assert((K + 3) % 4 == 0, "the z window moves in groups of 4");
   using S = FusedShape<K>;
   constexpr int R = S::R, C = S::C, NL = S::NL;
   extern __shared__ unsigned char smem_raw[];
@@ -445,10 +446,16 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
     // ---- z filters, 4 outputs per task: u_c[r][z4 .. z4+3]
     for (int task = t; task < S::ZT; task += kFThreads) {
       const int r = task / (kFZ / 4), z4 = (task % (kFZ / 4)) * 4;
-      const A* b = s_in + r * C + z4;
+      const A* b = s_in + r * C + z4;  // 16-byte aligned: C and z4 are multiples of 4
       A win[K + 3];
 #pragma unroll
-      for (int i = 0; i < K + 3; ++i) win[i] = b[i];
+      for (int i = 0; i < K + 3; i += 4) {
+        const V4<A> q = ld4(b + i);
+        win[i] = q.v[0];
+        win[i + 1] = q.v[1];
+        win[i + 2] = q.v[2];
+        win[i + 3] = q.v[3];
+      }
       A a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
       if constexpr (SYM) {
         // even filters: out = t[c] w[m] + sum_d t[c+d] (w[m+d] + w[m-d]), with
@@ -478,11 +485,8 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
           }
         }
       }
-#pragma unroll
-      for (int o = 0; o < 4; ++o) {
-        s_u[(r)*kFZ + z4 + o] = a0[o];
-        s_u[R * kFZ + r * kFZ + z4 + o] = a1[o];
-      }
+      st4(s_u + r * kFZ + z4, V4<A>{{a0[0], a0[1], a0[2], a0[3]}});
+      st4(s_u + R * kFZ + r * kFZ + z4, V4<A>{{a1[0], a1[1], a1[2], a1[3]}});
     }
     __syncthreads();
     // ---- y filters for rows 2yp, 2yp+1 at column zq, then the mixing
