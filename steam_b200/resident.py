@@ -96,7 +96,7 @@ class ResidentClass:
         w = setup.window
         cols = nx * ny if w is None else (w[1] - w[0]) * (w[3] - w[2])
         self.cells = float(cols * nz)
-        if nx * ny * nz >= (1 << 26) and setup.plan.kind != 'dense':
+        if nx * ny * nz >= (1 << 28) and setup.plan.kind != 'dense':
             # a field this large amortises timing its convolution's tile
             # lengths once (the tile never changes a result)
             from .ensemble import autotune_conv
