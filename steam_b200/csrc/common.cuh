@@ -206,6 +206,24 @@ __device__ __forceinline__ void st4(T* p, const V4<T>& r) {
   }
 }
 
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// one 4-byte element global -> shared through L1; src_bytes 0 writes a zero
+// (the source is then not read)
+__device__ __forceinline__ void cp_async4_zfill(void* sdst, const void* gsrc, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc),
+               "r"(src_bytes)
+               : "memory");
+}
+
 // Uncontracted arithmetic: the reference evaluates these products and sums as
 // separate rounded operations, so they are kept out of FMA contraction.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }

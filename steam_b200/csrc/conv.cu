@@ -342,7 +342,7 @@ static FusedTaps<A, K> fused_taps(const SepParams<T>& p) {
 }
 
 template <typename T, typename A, int K, bool SYM, bool PRE, bool P3>
-__global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
+__global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2) : (K <= 13 ? 2 : 1))) fused_conv_kernel(
     const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ pre,
     const __grid_constant__ FusedTaps<A, K> tp, FusedGeom<T> g, XEpi epi,
     double* __restrict__ partials) {
@@ -386,27 +386,45 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
   // staged column of this thread's first element; element i sits at column
   // (c_base + i * kFThreads) mod C
   const int c_base = t % C;
+  // Staging of the next plane: float32 in float32 arithmetic copies it
+  // straight into shared memory with cp.async (no registers held across the
+  // plane's filters); a conversion to float64 goes through registers.
+  constexpr bool kAsync = std::is_same<T, A>::value && sizeof(T) == 4;
   T ld[NL];
   // input plane pointer, advanced one plane per iteration with the wrap in x
   int64_t xi = wrapi(xin0, g.nx);
-  auto issue_loads = [&]() {
+  auto issue_loads = [&](A* dst) {
     const T* base = in + xi * plane_elems;
+    if constexpr (kAsync) {
 #pragma unroll
-    for (int i = 0; i < NL; ++i) ld[i] = goff[i] >= 0 ? base[goff[i]] : (T)0;
+      for (int i = 0; i < NL; ++i) {
+        const int e = t + i * kFThreads;
+        if (e < R * C)
+          cp_async4_zfill(dst + e, goff[i] >= 0 ? base + goff[i] : base, goff[i] >= 0 ? 4 : 0);
+      }
+      cp_async_commit();
+    } else {
+#pragma unroll
+      for (int i = 0; i < NL; ++i) ld[i] = goff[i] >= 0 ? base[goff[i]] : (T)0;
+    }
     xi = xi + 1 == g.nx ? 0 : xi + 1;
   };
   auto commit_loads = [&](A* dst) {
+    if constexpr (kAsync) cp_async_wait<0>();
 #pragma unroll
     for (int i = 0; i < NL; ++i) {
       const int e = t + i * kFThreads;
       if (e < R * C) {
-        T v = ld[i];
-        if (PRE) {
-          int c = c_base + (i * kFThreads) % C;  // compile-time offset
-          c = c >= C ? c - C : c;
-          v = mul_rn(v, s_pre[c]);
+        int c = c_base + (i * kFThreads) % C;  // compile-time offset
+        c = c >= C ? c - C : c;
+        if constexpr (kAsync) {
+          // the thread's own copies are complete: scale them in place
+          if (PRE) dst[e] = mul_rn(dst[e], s_pre[c]);
+        } else {
+          T v = ld[i];
+          if (PRE) v = mul_rn(v, s_pre[c]);
+          dst[e] = (A)v;
         }
-        dst[e] = (A)v;
       }
     }
   };
@@ -424,7 +442,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
   for (int sl = 0; sl < K; ++sl) acc[sl][0] = acc[sl][1] = (A)0;
   double s_f = 0.0, s_clip = 0.0;
   __syncthreads();
-  issue_loads();
+  issue_loads(s_in0);
   commit_loads(s_in0);
   __syncthreads();
   const bool flux_epi = epi.mode == STEAM_EPI_FLUX;
@@ -432,7 +450,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 && !PRE 
   int rph = 0;  // ring phase: k mod K
   for (int k = 0; k < count_i; ++k) {
     A* s_in = s_in0 + (k & 1) * R * C;
-    if (k + 1 < count_i) issue_loads();
+    if (k + 1 < count_i) issue_loads(s_in0 + ((k + 1) & 1) * R * C);
     // the output plane this iteration completes (when j >= 0)
     const int j = k - (K - 1);
     const int64_t x = xb + j;

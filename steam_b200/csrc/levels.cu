@@ -597,15 +597,6 @@ __device__ __forceinline__ void cp_async_v4(T* sdst, const T* gsrc) {
                  : "memory");
 }
 
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 template <typename T>
 __device__ __forceinline__ V4<T> lds4(const T* p) {
   return ld4(p);
