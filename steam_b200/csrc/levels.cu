@@ -439,7 +439,9 @@ __global__ void __launch_bounds__(kLvThreads, (sizeof(T) == 4 ? 3 : 2)) pattern_
 }
 
 // ---- bounded add sweeps --------------------------------------------------------
-// Per-level chain, replayed from the raw increment on every sweep:
+// Per-level chain (the replay form, ba_sweep_kernel, for any layout, applies
+// it from the raw increment on every sweep; the write-back form below keeps
+// its running state in the increment):
 //   for s < nsteps[z]:  d = clip(d - demean[z,s], caps) * scale[z,s]
 //   if has_final[z]:    d = clip(d - final_dm[z], caps)
 //   if has_mu[z]:       d = clip(d - mu[z], caps)
@@ -1310,8 +1312,8 @@ __global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int 
 // The rescale loop and the shift solve each run as ONE cooperative launch
 // (all blocks co-resident) that iterates sweep -> grid barrier -> reduction ->
 // grid barrier -> per-level update -> grid barrier until no level needs
-// another sweep.  This replaces a fixed launch sequence in which finished
-// iterations still cost an (empty) launch each.  The barrier spins with a
+// another sweep (a fixed launch sequence would spend an empty launch on each
+// iteration a phase does not need).  The barrier spins with a
 // bound: a block that waits past kBarSpinLimit polls records an error, and
 // every block leaves at its next barrier.
 constexpr long long kBarSpinLimit = 1ll << 26;  // ~ seconds with the back-off below
@@ -1420,9 +1422,12 @@ static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
 }
 
 // Enqueues the whole bounded add on stream s: no host synchronisation and no
-// host decision between sweeps.  Sweeps whose phase has ended return at once
-// (their run flag is 0), so the launch sequence is fixed: one stats sweep,
-// R rescale sweeps, kMuMaxSweeps shift sweeps, one apply sweep.  mean_dev
+// host decision between sweeps.  Vectorised layouts (nz % 4 == 0, 16-byte
+// aligned fields): the first sweep, one persistent cooperative launch for the
+// rescale loop and one for the shift solve, the apply sweep.  Other layouts:
+// a fixed sequence (one stats sweep, R rescale sweeps, kMuMaxSweeps shift
+// sweeps, one apply sweep) in which sweeps whose phase has ended return at
+// once (their run flag is 0).  mean_dev
 // (device, nz doubles) is the level mean profile; the ledger ends in
 // st.ledger (device, [nz][5]).
 template <typename T>
