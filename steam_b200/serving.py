@@ -21,6 +21,7 @@ host buffer of its slot; latency is arrival to download complete.
 from __future__ import annotations
 
 import ctypes
+import gc
 import time
 from collections import deque
 
@@ -205,6 +206,17 @@ class TileServer:
         admitting each at its arrival time as slots and budget allow.
         Returns the requests with 'start', 'done', 'latency' (seconds) and,
         with ``keep``, 'tile' (host array)."""
+        # the host loop is the server's critical path: no collection pauses
+        # while requests are in flight
+        gc_was = gc.isenabled()
+        gc.disable()
+        try:
+            return self._serve(requests, keep)
+        finally:
+            if gc_was:
+                gc.enable()
+
+    def _serve(self, requests, keep):
         pending = deque(sorted(requests, key=lambda r: r['arrival']))
         free = list(self.slots)
         busy = []
