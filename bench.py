@@ -435,6 +435,10 @@ def main(argv=None):
                 "traffic_unit": "GB per launch (ncu, 512x512x256 capture scaled by voxels)",
                 "per_launch_ms": per_launch_ms,
                 "peak_source": "measured" if peaks else "fallback",
+                # the convolutions, noise and thermodynamics issue hundreds of
+                # instructions per voxel: their limiter is instruction issue
+                # (ncu issue-active 55-76 %), not DRAM, hence the low fraction
+                "limiter": "instruction issue (FP32/FP64 pipes), not DRAM",
                 "bounded_add_sweeps": ba_sweeps,
                 "breakdown_ms_per_step": {k: round(v[0] / max(args.steps, 1), 3)
                                           for k, v in sorted(calls.items(),
