@@ -424,9 +424,9 @@ def main(argv=None):
     # of each entry's kernels in an ncu capture at 512x512x256 FP32, per voxel;
     # the kernels stream their fields once, so the traffic scales with voxels
     # (the convolution figure is the mean of its flux launch and two scalar ones)
-    dram_per_voxel = {"steam_conv_separable_async": 9.15, "steam_thermo_async": 29.74,
-                      "steam_flux_noise_async": 7.38, "steam_scalar_pattern_async": 14.70,
-                      "steam_flux_finish_async": 7.11}
+    dram_per_voxel = {"steam_conv_separable_async": 9.25, "steam_thermo_async": 29.77,
+                      "steam_flux_noise_async": 7.45, "steam_scalar_pattern_async": 14.60,
+                      "steam_flux_finish_async": 7.13}
     traffic = (dram_per_voxel[name] * nvox if args.dtype == "f32" and name in dram_per_voxel
                else None)
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
