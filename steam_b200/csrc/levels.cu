@@ -376,7 +376,8 @@ __global__ void __launch_bounds__(kLvThreads, (sizeof(T) == 4 ? 3 : 2)) pattern_
     m_lo = z4 > 0 ? vecs[z4 - 1] : (T)0;
     m_hi = z4 + 4 < nz ? vecs[z4 + 4] : (T)0;
   }
-  double acc0[4] = {0, 0, 0, 0}, acc1[4] = {0, 0, 0, 0};
+  double acc0[4] = {0, 0, 0, 0};
+  unsigned acc1[4] = {0u, 0u, 0u, 0u};  // nonzero counts, exact as integers
   const int64_t ncol = nx * ny;
   const int64_t step = (int64_t)gridDim.x * cpb;
   ColWalk cw;
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(kLvThreads, (sizeof(T) == 4 ? 3 : 2)) pattern_
         o.v[l] = Wv;
         if (in_w) {
           acc0[l] += (double)(Wv < (T)0 ? -Wv : Wv);
-          acc1[l] += Wv != (T)0 ? 1.0 : 0.0;
+          acc1[l] += Wv != (T)0 ? 1u : 0u;
         }
       }
       st4(out + base, o);
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(kLvThreads, (sizeof(T) == 4 ? 3 : 2)) pattern_
     __syncthreads();
     if (act)
 #pragma unroll
-      for (int l = 0; l < 4; ++l) red[cs * nz + z4 + l] = q == 0 ? acc0[l] : acc1[l];
+      for (int l = 0; l < 4; ++l) red[cs * nz + z4 + l] = q == 0 ? acc0[l] : (double)acc1[l];
     __syncthreads();
     for (int z = t; z < nz; z += blockDim.x) {
       double sacc = 0.0;
