@@ -145,7 +145,8 @@ __global__ void __launch_bounds__(256) flux_noise_kernel(
   const int cols_per_iter = (int)blockDim.x / zlanes;
   const int cofs = threadIdx.x / zlanes;
   const int zt = threadIdx.x - cofs * zlanes;
-  double s_flux = 0.0, s_abs = 0.0, s_nnz = 0.0;
+  double s_flux = 0.0, s_abs = 0.0;
+  unsigned s_nnz = 0u;  // nonzero count, exact as an integer
   if (cofs < cols_per_iter) {
     // columns visited with a fixed stride: x and y advance without a division
     const uint32_t c_step = gridDim.x * cols_per_iter;
@@ -172,14 +173,14 @@ __global__ void __launch_bounds__(256) flux_noise_kernel(
         if (in_win) {
           s_flux += (double)f;
           s_abs += (double)(e < (T)0 ? -e : e);
-          s_nnz += (e != (T)0) ? 1.0 : 0.0;
+          s_nnz += (e != (T)0) ? 1u : 0u;
         }
       }
     }
   }
   double t0 = block_sum(s_flux, scratch);
   double t1 = block_sum(s_abs, scratch);
-  double t2 = block_sum(s_nnz, scratch);
+  double t2 = block_sum((double)s_nnz, scratch);
   if (threadIdx.x == 0) {
     partials[0 * gridDim.x + blockIdx.x] = t0;
     partials[1 * gridDim.x + blockIdx.x] = t1;
