@@ -715,8 +715,9 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
       if (in_w)
 #pragma unroll
         for (int l = 0; l < 4; ++l) {
-          acc[0][l] += (double)dv.v[l];
-          acc[1][l] += (double)(dv.v[l] < (T)0 ? -dv.v[l] : dv.v[l]);
+          const double x = (double)dv.v[l];  // one conversion; |x| is exact
+          acc[0][l] += x;
+          acc[1][l] += fabs(x);
         }
     } else {
       V4<T> df, pn, dn;
@@ -736,8 +737,9 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
           dn.v[l] = sub_rn(pn.v[l], p0);
         } else if (in_w) {
           if (MODE == BA_STATS) {
-            acc[0][l] += (double)d;
-            acc[1 % QS][l] += (double)(d < (T)0 ? -d : d);
+            const double x = (double)d;
+            acc[0][l] += x;
+            acc[1 % QS][l] += fabs(x);
           } else {
             // d - mu over the candidates spans [d - cmax, d - cmin]: a cell
             // inside the caps (or beyond one cap) for all of them takes one
