@@ -255,10 +255,12 @@ __device__ __forceinline__ float sinpi_scaled(double a, float v) {
 }
 
 // The two powers fac = x1^fexp and tail = x2^texp are taken together as one
-// exp2 of fexp log2(x1) + texp log2(x2): the exponent carries the log2
-// errors (one float32 ulp of each logarithm), so the product keeps a relative
-// error of ~4e-8 |exponent| -- a few float32 ulps at the far tail, ~1e-7 for
-// typical draws -- and one exp2 replaces two full pow evaluations.
+// exp2 of fexp log2(x1) + texp log2(x2), with the hardware's approximate
+// log2 (2^-22 absolute on [0.5, 2], 2 ulps elsewhere): the exponent carries
+// those errors, so the product keeps a relative error of ~1e-7 |exponent|
+// (measured: 1e-7 - 4e-7 relative L2 of the draws against float64), and one
+// exp2 replaces two full pow evaluations.  R = -log(u1) keeps the accurate
+// logarithm: near u1 = 1 it needs relative accuracy of a value near 0.
 __device__ __forceinline__ float levy_draw_f32(float u0, float u1,
                                                const LevyParams<float>& p) {
   const float eps = 1e-6f;
@@ -268,7 +270,7 @@ __device__ __forceinline__ float levy_draw_f32(float u0, float u1,
   const float x1 = __fmul_rn(c > eps ? c : eps, p.am1);
   const float c2 = sinpi_scaled(p.am1_d, v);
   const float x2 = (c2 > eps ? c2 : eps) / R;
-  const float e = fmaf(p.fexp, log2f(x1), p.texp * log2f(x2));
+  const float e = fmaf(p.fexp, __log2f(x1), p.texp * __log2f(x2));
   return __fmul_rn(__fmul_rn(sinpi_scaled(p.alpha_d, v), p.sign), exp2f(e));
 }
 
