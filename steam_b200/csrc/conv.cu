@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
   constexpr int R = S::R, C = S::C, NL = S::NL;
   extern __shared__ unsigned char smem_raw[];
   __shared__ double scratch[32];
-  __shared__ T s_pre[C];
+  __shared__ __align__(16) T s_pre[C];  // read 4 at a time by the z pass
   A* s_in0 = reinterpret_cast<A*>(smem_raw);  // [2][R*C]
   A* s_u = s_in0 + 2 * R * C;                            // [2][R][kFZ]
   const int t = threadIdx.x;
@@ -418,8 +418,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
         int c = c_base + (i * kFThreads) % C;  // compile-time offset
         c = c >= C ? c - C : c;
         if constexpr (kAsync) {
-          // the thread's own copies are complete: scale them in place
-          if (PRE) dst[e] = mul_rn(dst[e], s_pre[c]);
+          // (the z pass applies the scaling as it reads the slab)
         } else {
           T v = ld[i];
           if (PRE) v = mul_rn(v, s_pre[c]);
@@ -473,6 +472,15 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
         win[i + 1] = q.v[1];
         win[i + 2] = q.v[2];
         win[i + 3] = q.v[3];
+        if constexpr (kAsync && PRE) {
+          // the slab holds the raw input: scale by the factors of columns
+          // z4 + i .. z4 + i + 3, the same multiply the staging would do
+          const V4<T> f = ld4(s_pre + z4 + i);
+          win[i] = mul_rn(win[i], f.v[0]);
+          win[i + 1] = mul_rn(win[i + 1], f.v[1]);
+          win[i + 2] = mul_rn(win[i + 2], f.v[2]);
+          win[i + 3] = mul_rn(win[i + 3], f.v[3]);
+        }
       }
       A a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
       if constexpr (SYM) {
