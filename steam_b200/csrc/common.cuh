@@ -244,13 +244,27 @@ __device__ __forceinline__ double d_sinpi(double x) { return sinpi(x); }
 // The literal float32 evaluation loses most digits where the cosines near
 // their zeros feed the negative powers (0.4-1.7 % relative L2 over the draws
 // against float64); this form keeps every factor to a few float32 ulps.
+// sin(pi r) for |r| <= 1/2 as r P(r^2), P the Taylor series of sin(pi r)/r
+// through r^10 (the next term is below 2^-28 relative there): within 3
+// float32 ulps, and relative accuracy is kept as r -> 0.
+__device__ __forceinline__ float sinpi_half(float r) {
+  const float s = r * r;
+  float p = -7.370430945714348e-03f;     // -pi^11 / 11!
+  p = fmaf(p, s, 8.214588661112823e-02f);  //  pi^9 / 9!
+  p = fmaf(p, s, -5.992645293207921e-01f); // -pi^7 / 7!
+  p = fmaf(p, s, 2.550164039877345e+00f);  //  pi^5 / 5!
+  p = fmaf(p, s, -5.167712780049970e+00f); // -pi^3 / 3!
+  p = fmaf(p, s, 3.141592653589793e+00f);  //  pi
+  return r * p;
+}
+
 // sin(pi * a * v) with the product formed in float64 and reduced by its
 // nearest integer n exactly, so the float32 sine sees an exact small argument:
 // sin(pi a v) = (-1)^n sin(pi (a v - n)).
 __device__ __forceinline__ float sinpi_scaled(double a, float v) {
   const double av = a * (double)v;
   const double n = rint(av);
-  const float s = sinpif((float)(av - n));
+  const float s = sinpi_half((float)(av - n));
   return ((long long)n & 1) ? -s : s;
 }
 
@@ -266,7 +280,7 @@ __device__ __forceinline__ float levy_draw_f32(float u0, float u1,
   const float eps = 1e-6f;
   const float v = 1.0f - u0;
   const float R = -logf(u1 > eps ? u1 : eps);
-  const float c = sinpif(v);
+  const float c = sinpi_half(v > 0.5f ? 1.0f - v : v);  // sin(pi v) = sin(pi (1 - v)), exact
   const float x1 = __fmul_rn(c > eps ? c : eps, p.am1);
   const float c2 = sinpi_scaled(p.am1_d, v);
   const float x2 = (c2 > eps ? c2 : eps) / R;
