@@ -283,7 +283,8 @@ __device__ __forceinline__ float levy_draw_f32(float u0, float u1,
   const float c = sinpi_half(v > 0.5f ? 1.0f - v : v);  // sin(pi v) = sin(pi (1 - v)), exact
   const float x1 = __fmul_rn(c > eps ? c : eps, p.am1);
   const float c2 = sinpi_scaled(p.am1_d, v);
-  const float x2 = (c2 > eps ? c2 : eps) / R;
+  // the approximate quotient (2 ulps; R <= 14) only feeds the approximate log2
+  const float x2 = __fdividef(c2 > eps ? c2 : eps, R);
   const float e = fmaf(p.fexp, __log2f(x1), p.texp * __log2f(x2));
   return __fmul_rn(__fmul_rn(sinpi_scaled(p.alpha_d, v), p.sign), exp2f(e));
 }
