@@ -61,8 +61,10 @@ def parse(argv=None):
                     metavar=("NX", "NY", "NZ"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=200,
-                    help="tile requests per arrival rate in the serving episode (0: skip)")
-    ap.add_argument("--serve-rates", type=float, nargs="+", default=(100.0, 1000.0),
+                    help="tile requests per arrival rate in the serving episode, at most "
+                         "2 s of arrivals and at least 20 (0: skip)")
+    ap.add_argument("--serve-rates", type=float, nargs="+",
+                    default=(10.0, 100.0, 1000.0, 2000.0),
                     help="Poisson arrival rates (requests/s) of the serving episode")
     ap.add_argument("--ensemble-members", type=int, default=256,
                     help="members of the batched-ensemble episode (0: skip)")
@@ -497,7 +499,8 @@ def main(argv=None):
                    "sizes": "32^3/64^3/128^3/256^3 at 0.4/0.3/0.2/0.1",
                    "slots": 4, "budget_bytes": srv.budget}
         for rate in args.serve_rates:
-            done = srv.serve(poisson_trace(tw, rate, args.serve_requests, seed=4))
+            nreq = min(args.serve_requests, max(20, int(2.0 * rate)))
+            done = srv.serve(poisson_trace(tw, rate, nreq, seed=4))
             serving[f"{rate:g}_req_per_s"] = latency_summary(done)
         del srv, tw
 

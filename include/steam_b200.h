@@ -156,6 +156,17 @@ int steam_conv_dense(int dtype, int64_t nx, int64_t ny, int64_t nz,
 int steam_scale(int dtype, int64_t n, void* field, double scale, int32_t fill,
                 steam_stream_t stream);
 
+/* ---- a11 apply on a served tile ------------------------------------------
+ * out[i][j][k] = box[x0+i][y0+j][z0+k] * scale (fill != 0: = scale) for the
+ * (ox, oy, oz) window of an (nx, ny, nz) box (z fastest); out is contiguous.
+ * The volume-mean restore of steam/simulate.py:2208-2215 (scale rounded to the
+ * dtype first, as steam_scale) applied only to the cells a tile returns, so a
+ * tile server needs no whole-box pass and no strided copy. */
+int steam_tile_extract(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* box,
+                       int64_t x0, int64_t y0, int64_t z0, int64_t ox, int64_t oy,
+                       int64_t oz, double scale, int32_t fill, void* out,
+                       steam_stream_t stream);
+
 /* ---- level-weighted accumulate ------------------------------------------
  * acc += coef[z] * (a - b), or coef[z] * a when b is NULL: the compensation
  * deficit update of cascade_loop (steam/simulate.py:1917, 2024).  coef is a

@@ -73,6 +73,9 @@ _SIGNATURES = {
     "steam_conv_dense": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i32,
                                         c_i32, c_i32, c_vp, c_vp, c_vp]),
     "steam_scale": (ctypes.c_int, [ctypes.c_int, c_i64, c_vp, c_dbl, c_i32, c_vp]),
+    "steam_tile_extract": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i64,
+                                          c_i64, c_i64, c_i64, c_i64, c_i64, c_dbl, c_i32,
+                                          c_vp, c_vp]),
     "steam_accumulate_levels": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                                c_vp, c_vp, c_dp, c_vp]),
     "steam_level_sums_workspace_bytes": (c_size, [c_i64]),

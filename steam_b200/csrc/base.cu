@@ -72,6 +72,24 @@ __global__ void scale_kernel(int64_t n, T* __restrict__ f, T s, int fill) {
   }
 }
 
+// One warp per output row (i, j): out[i][j][:] = box[x0 + i][y0 + j][z0 + :] * s
+// (or s with fill), z the fastest axis on both sides.
+template <typename T>
+__global__ void tile_extract_kernel(int64_t ny, int64_t nz, const T* __restrict__ box,
+                                    int64_t x0, int64_t y0, int64_t z0, int64_t ox,
+                                    int64_t oy, int64_t oz, T s, int fill,
+                                    T* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       row < ox * oy; row += warps) {
+    const int64_t i = row / oy, j = row - i * oy;
+    const T* src = box + ((x0 + i) * ny + (y0 + j)) * nz + z0;
+    T* dst = out + row * oz;
+    for (int64_t k = lane; k < oz; k += 32) dst[k] = fill ? s : src[k] * s;
+  }
+}
+
 template <typename T>
 __global__ void accumulate_levels_kernel(int64_t n, int64_t nz, T* __restrict__ acc,
                                          const T* __restrict__ a,
@@ -229,5 +247,32 @@ extern "C" int steam_scale(int dtype, int64_t n, void* field, double scale,
   else
     return fail(STEAM_ERR_ARG, "steam_scale: bad dtype");
   STEAM_LAUNCH_CHECK("steam_scale");
+  return STEAM_OK;
+}
+
+extern "C" int steam_tile_extract(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                  const void* box, int64_t x0, int64_t y0, int64_t z0,
+                                  int64_t ox, int64_t oy, int64_t oz, double scale,
+                                  int32_t fill, void* out, steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0 && ox >= 0 && oy >= 0 && oz >= 0,
+                "steam_tile_extract: negative size");
+  STEAM_REQUIRE(x0 >= 0 && y0 >= 0 && z0 >= 0 && x0 + ox <= nx && y0 + oy <= ny &&
+                    z0 + oz <= nz,
+                "steam_tile_extract: window outside the box");
+  if (ox == 0 || oy == 0 || oz == 0) return STEAM_OK;
+  STEAM_REQUIRE(box != nullptr && out != nullptr, "steam_tile_extract: null array");
+  cudaStream_t s = (cudaStream_t)stream;
+  int grid = stride_grid(ox * oy, 8, 8);
+  if (dtype == STEAM_F32)
+    tile_extract_kernel<float><<<grid, 256, 0, s>>>(ny, nz, (const float*)box, x0, y0, z0,
+                                                    ox, oy, oz, (float)scale, fill,
+                                                    (float*)out);
+  else if (dtype == STEAM_F64)
+    tile_extract_kernel<double><<<grid, 256, 0, s>>>(ny, nz, (const double*)box, x0, y0,
+                                                     z0, ox, oy, oz, scale, fill,
+                                                     (double*)out);
+  else
+    return fail(STEAM_ERR_ARG, "steam_tile_extract: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_tile_extract");
   return STEAM_OK;
 }

@@ -150,6 +150,10 @@ class _Slot:
         self.sums = torch.zeros(8, dtype=torch.float64, device='cuda')
         ws = max(world.workspace_bytes((nbox, nbox, zbox)), 1)
         self.ws = torch.empty(ws, dtype=torch.uint8, device='cuda')
+        # the tile's cells, contiguous, then page-locked: both sized once here so
+        # serving allocates nothing (a first allocation on a stream blocks the
+        # host loop for tens of ms)
+        self.out = torch.empty(max_n ** 3, dtype=world.dtype, device='cuda')
         self.host = torch.empty(max_n ** 3, dtype=world.dtype, pin_memory=True)
         self.event = torch.cuda.Event()
         self.request = None
@@ -186,9 +190,12 @@ class TileServer:
             stream = _lib.stream()
             _lib.check(w.lib.steam_scale(w.code, cnt, _lib.ptr(F), 1.0, 1, stream))
             w.advance(F, product, borig, box, slot.sums, zb, zt, slot.ws, stream)
-            _lib.check(w.lib.steam_scale(w.code, cnt, _lib.ptr(F), w.factor, w.fill, stream))
-            host = slot.host[:n ** 3].view(n, n, n)
-            host.copy_(F[HALO:HALO + n, HALO:HALO + n, zoff:zoff + n], non_blocking=True)
+            # the world restore on the tile's cells only, into the contiguous buffer
+            out = slot.out[:n ** 3]
+            _lib.check(w.lib.steam_tile_extract(
+                w.code, box[0], box[1], box[2], _lib.ptr(F), HALO, HALO, zoff, n, n, n,
+                w.factor, w.fill, _lib.ptr(out), stream))
+            slot.host[:n ** 3].copy_(out, non_blocking=True)
             slot.event.record(slot.stream)
         slot.request = req
 
@@ -252,11 +259,13 @@ class TileServer:
                     free.append(slot)
                     out.append(req)
                     progressed = True
-            if not progressed:
-                if busy or (pending and pending[0]['arrival'] <= now):
-                    time.sleep(20e-6)
-                elif pending:
-                    time.sleep(max(0.0, min(1e-3, pending[0]['arrival'] - now)))
+            if not progressed and not busy and pending:
+                # idle until the next arrival: sleep only when it is more than
+                # 2 ms away (a sleep can overshoot on a loaded host); with
+                # tiles in flight the loop polls without sleeping
+                wait = pending[0]['arrival'] - now
+                if wait > 2e-3:
+                    time.sleep(wait - 1e-3)
         return out
 
 

@@ -49,3 +49,31 @@ def test_tiles_in_a_mix_equal_alone():
     assert s['p99_ms'] >= s['p50_ms'] > 0
     # the budget admits at most three 32^3 boxes at once, yet all complete
     assert srv.in_flight_bytes == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("fill", [0, 1])
+def test_tile_extract_window_times_scale(dtype, fill):
+    """steam_tile_extract: an odd window of a box, rounded scale applied (or
+    filled), written contiguously; the host refuses a window past the box."""
+    import ctypes
+    import torch
+    from steam_b200 import _lib
+    lib = _lib.load()
+    code = _lib.STEAM_F32 if dtype == np.float32 else _lib.STEAM_F64
+    tdt = torch.float32 if dtype == np.float32 else torch.float64
+    g = torch.Generator(device='cuda').manual_seed(3)
+    box = torch.rand((37, 29, 45), generator=g, device='cuda', dtype=tdt) * 3
+    x0, y0, z0, ox, oy, oz = 5, 2, 7, 31, 27, 33
+    scale = 1.0 + 1.0 / 3.0
+    out = torch.full((ox * oy * oz,), -1.0, device='cuda', dtype=tdt)
+    _lib.check(lib.steam_tile_extract(code, 37, 29, 45, _lib.ptr(box), x0, y0, z0, ox, oy, oz,
+                                      scale, fill, _lib.ptr(out), _lib.stream()))
+    torch.cuda.synchronize()
+    s = np.asarray(scale, dtype=dtype)
+    want = (np.full((ox, oy, oz), s, dtype=dtype) if fill else
+            box.cpu().numpy()[x0:x0 + ox, y0:y0 + oy, z0:z0 + oz] * s)
+    np.testing.assert_array_equal(out.cpu().numpy().reshape(ox, oy, oz), want)
+    with pytest.raises(Exception):
+        _lib.check(lib.steam_tile_extract(code, 37, 29, 45, _lib.ptr(box), x0, y0, 13, ox, oy,
+                                          oz, scale, fill, _lib.ptr(out), _lib.stream()))
