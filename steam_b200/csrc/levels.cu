@@ -1074,6 +1074,9 @@ struct MuSolver {
 
 // Most mu sweeps a solve may take (the bracket at least halves per sweep).
 constexpr int kMuMaxSweeps = 48;
+// column groups (one block's pass of the vectorised sweep) per persistent
+// phase block and sweep, at least
+constexpr int kPhaseMinGroups = 32;
 
 // Writable view of the chain the sweeps replay, plus the solver's state.
 template <typename T>
@@ -1600,6 +1603,16 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
     STEAM_REQUIRE(per_sm >= 1, "steam_bounded_add: a persistent phase does not fit an SM");
     int pgrid = per_sm * sm_count();
     if (pgrid > grid4) pgrid = grid4;
+    // A phase is persistent and spends much of its time at grid barriers, so
+    // its blocks hold their SMs' slots for the whole loop.  Size it by the
+    // work, at least kPhaseMinGroups column groups per block and sweep: a
+    // large field still takes every slot, while a small one (an ensemble
+    // member) leaves the other SMs to concurrent streams and pays for fewer
+    // arrivals at each barrier.
+    const int64_t cpb = kLvThreads / (nz / 4);
+    const int64_t groups = (ncol + cpb - 1) / cpb;
+    const int64_t want = (groups + kPhaseMinGroups - 1) / kPhaseMinGroups;
+    if (want < pgrid) pgrid = want > 1 ? (int)want : 1;
     T* d0p = inc;
     T* pp = pert;
     int nzi = (int)nz;

@@ -4,9 +4,11 @@ A member is one class step of its own world (its shape, seed, alpha, C1, H,
 Hz): the finest class of a root run over the member's domain, run by a
 ``ResidentClass`` on device fields.  ``Ensemble`` spreads the members over a
 few CUDA streams and captures one step of all of them into a single CUDA
-graph: a replay then issues every member's ~400 kernels (noise, the three
-convolutions, patterns, the bounded adds' sweeps and solves, thermodynamics)
-with one launch call, and members of uneven sizes fill the GPU side by side.
+graph: a replay then issues every member's 32 library launches (noise, the
+three convolutions, patterns, the bounded adds' sweeps and persistent solve
+phases, thermodynamics) with one launch call, and members of uneven sizes fill
+the GPU side by side (a bounded add's persistent phase is sized by its
+member's work, so a small member's phase leaves most SMs to the others).
 
 ``autotune_conv`` is the tile-shape autotuner: for a field shape it times the
 fused convolution at a few x-chunk lengths (planes per CTA; short chunks give
