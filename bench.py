@@ -431,6 +431,24 @@ def main(argv=None):
                       "steam_flux_finish_async": 7.13}
     traffic = (dram_per_voxel[name] * nvox if args.dtype == "f32" and name in dram_per_voxel
                else None)
+    # the instruction-issue roofline beside it: warp instructions per voxel of
+    # each entry's kernels in the same ncu capture (512x512x256 FP32;
+    # smsp__inst_executed.sum / voxels; the convolution figure is the mean of
+    # its flux launch and two scalar ones) against 4 warp instructions per
+    # cycle per SM at the SM clock sampled during the timed region
+    inst_per_voxel = {"steam_conv_separable_async": 7.577, "steam_thermo_async": 8.480,
+                      "steam_flux_noise_async": 7.781, "steam_scalar_pattern_async": 2.716,
+                      "steam_flux_finish_async": 0.107}
+    issue = None
+    if args.dtype == "f32" and name in inst_per_voxel:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+        if mhz:
+            ach = inst_per_voxel[name] * nvox / (per_launch_ms / 1e3) / 1e9
+            pk = sms * 4 * mhz * 1e6 / 1e9
+            issue = {"achieved": ach, "peak": pk, "unit": "G warp instructions/s",
+                     "frac": ach / pk, "inst_per_voxel": inst_per_voxel[name],
+                     "sm_mhz": mhz, "sms": sms}
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic / 1e9 if traffic is not None else None,
@@ -441,6 +459,7 @@ def main(argv=None):
                 # instructions per voxel: their limiter is instruction issue
                 # (ncu issue-active 55-76 %), not DRAM, hence the low fraction
                 "limiter": "instruction issue (FP32/FP64 pipes), not DRAM",
+                "issue": issue,
                 "bounded_add_sweeps": ba_sweeps,
                 "breakdown_ms_per_step": {k: round(v[0] / max(args.steps, 1), 3)
                                           for k, v in sorted(calls.items(),
