@@ -354,7 +354,9 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
   __shared__ double scratch[32];
   __shared__ __align__(16) T s_pre[C];  // read 4 at a time by the z pass
   A* s_in0 = reinterpret_cast<A*>(smem_raw);  // [2][R*C]
-  A* s_u = s_in0 + 2 * R * C;                            // [2][R][kFZ]
+  // the z filters' output, double-buffered by plane parity so that one
+  // barrier per plane suffices: [2 parity][kFMaxZ][R][kFZ]
+  A* s_u0 = s_in0 + 2 * R * C;
   const int t = threadIdx.x;
   const int zt_i = blockIdx.x % g.nzt;
   const int yt_i = (blockIdx.x / g.nzt) % g.nyt;
@@ -444,12 +446,18 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
   issue_loads(s_in0);
   commit_loads(s_in0);
   __syncthreads();
+  if (count > 1) issue_loads(s_in0 + R * C);
   const bool flux_epi = epi.mode == STEAM_EPI_FLUX;
   const int count_i = (int)count;
   int rph = 0;  // ring phase: k mod K
   for (int k = 0; k < count_i; ++k) {
+    // One barrier per plane.  Before it: the z pass of plane k (reads slab
+    // k, writes s_u[k & 1]) and the arrival of slab k + 1.  After it: the
+    // loads of slab k + 2 into slab k's buffer (every z read of it is done),
+    // the y pass of plane k (reads s_u[k & 1], which is next written by the z
+    // pass of plane k + 2, after the next barrier) and the ring step.
     A* s_in = s_in0 + (k & 1) * R * C;
-    if (k + 1 < count_i) issue_loads(s_in0 + ((k + 1) & 1) * R * C);
+    A* s_u = s_u0 + (k & 1) * kFMaxZ * R * kFZ;
     // the output plane this iteration completes (when j >= 0)
     const int j = k - (K - 1);
     const int64_t x = xb + j;
@@ -514,7 +522,9 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
       st4(s_u + r * kFZ + z4, V4<A>{{a0[0], a0[1], a0[2], a0[3]}});
       st4(s_u + R * kFZ + r * kFZ + z4, V4<A>{{a1[0], a1[1], a1[2], a1[3]}});
     }
+    if (k + 1 < count_i) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
     __syncthreads();
+    if (k + 2 < count_i) issue_loads(s_in);
     // ---- y filters for rows 2yp, 2yp+1 at column zq, then the mixing
     A w0[2] = {0, 0}, w1[2] = {0, 0};
 #pragma unroll
@@ -621,8 +631,6 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
     }
 #undef STEAM_RING_CASE
     rph = rph + 1 == K ? 0 : rph + 1;
-    if (k + 1 < count_i) commit_loads(s_in0 + ((k + 1) & 1) * R * C);
-    __syncthreads();
   }
   if (epi.mode == STEAM_EPI_FLUX) {
     double t0 = block_sum(s_f, scratch);
@@ -646,7 +654,7 @@ static bool fused_supported(const SepParams<T>& p) {
 
 static size_t fused_smem(int k, size_t elem) {
   const int R = kFY + k - 1, C = kFZ + k - 1;
-  return elem * ((size_t)2 * R * C + (size_t)kFMaxZ * R * kFZ);
+  return elem * ((size_t)2 * R * C + (size_t)2 * kFMaxZ * R * kFZ);
 }
 
 // x planes per CTA of the fused kernel, per field shape: set by the host's
