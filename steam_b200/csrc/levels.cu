@@ -663,11 +663,43 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   __syncthreads();
   constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
   const int nz4 = nz / 4;
-  const int cpi = kLvThreads / nz4;
   const int t = threadIdx.x;
-  const bool active = t < cpi * nz4;
-  const int z4 = (t % nz4) * 4;
-  const int cofs = t / nz4;
+  // A statistics sweep works only on the groups of 4 levels with a level
+  // still in the rescale loop.  When some groups have left it, the block's
+  // threads are dealt over the remaining groups alone (more columns per
+  // block step) instead of idling on the groups that are done: s_act lists
+  // the groups in the loop, s_gix maps a group to its place in that list
+  // (-1: out of the loop).
+  int ng = nz4;     // groups dealt over the threads
+  int nact = nz4;   // groups with work
+  const int* act = nullptr;
+  const int* gix = nullptr;
+  if constexpr (MODE == BA_STATS) {
+    __shared__ int s_act[kLvThreads], s_gix[kLvThreads], s_nact;
+    if (t == 0) {
+      int n = 0;
+      for (int g = 0; g < nz4; ++g) {
+        const bool in = s_ton[4 * g] != (T)0 || s_ton[4 * g + 1] != (T)0 ||
+                        s_ton[4 * g + 2] != (T)0 || s_ton[4 * g + 3] != (T)0;
+        s_gix[g] = in ? n : -1;
+        if (in) s_act[n++] = g;
+      }
+      s_nact = n;
+    }
+    __syncthreads();
+    nact = s_nact;
+    if (nact < nz4) {
+      ng = nact > 0 ? nact : 1;
+      act = s_act;
+      gix = s_gix;
+    }
+  }
+  const bool compact = act != nullptr;
+  const int cpi = kLvThreads / ng;
+  const bool active = t < cpi * ng && nact > 0;
+  const int gi = t % ng;
+  const int z4 = (compact ? (nact > 0 ? act[gi] : 0) : gi) * 4;
+  const int cofs = t / ng;
   const V4<T> fdm = ld4(s_fdm + z4), fsc = ld4(s_fsc + z4);
   const V4<T> cdm = ld4(s_cdm + z4), tdm = ld4(s_tdm + z4);
   const V4<T> mean = ld4(s_mean + z4);
@@ -843,20 +875,25 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   // deterministic reduction: per level, the cpi column slots in order
   const int nb = gridDim.x;
   // partial rows: stats {sum d, sum |d|}; shift {mean_k, count_k} per candidate
+  // (dealt over the groups in the loop: slot [cofs][gi][l], and 0 for the
+  // levels of groups out of it, whose sums are not read)
+  const int rw = compact ? 4 * ng : nz;  // red row width
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     __syncthreads();
     if (active)
 #pragma unroll
       for (int l = 0; l < 4; ++l)
-        red[cofs * nz + z4 + l] =
+        red[cofs * rw + (compact ? 4 * gi : z4) + l] =
             MODE == BA_MU ? ((q & 1) ? (double)cnt[(q >> 1) % (MODE == BA_MU ? kMuCand : 1)][l]
                                      : acc[(q >> 1) % QS][l])
                           : acc[q % QS][l];
     __syncthreads();
     for (int z = t; z < nz; z += kLvThreads) {
       double sacc = 0.0;
-      for (int cc = 0; cc < cpi; ++cc) sacc += red[cc * nz + z];
+      const int col = compact ? (gix[z >> 2] >= 0 ? 4 * gix[z >> 2] + (z & 3) : -1) : z;
+      if (col >= 0)
+        for (int cc = 0; cc < cpi; ++cc) sacc += red[cc * rw + col];
       partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
     }
   }
