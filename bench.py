@@ -427,7 +427,7 @@ def main(argv=None):
     # the kernels stream their fields once, so the traffic scales with voxels
     # (the convolution figure is the mean of its flux launch and two scalar ones)
     dram_per_voxel = {"steam_conv_separable_async": 9.24, "steam_thermo_async": 29.77,
-                      "steam_flux_noise_async": 7.45, "steam_scalar_pattern_async": 14.60,
+                      "steam_flux_noise_async": 7.45, "steam_scalar_pattern_async": 14.96,
                       "steam_flux_finish_async": 7.13}
     traffic = (dram_per_voxel[name] * nvox if args.dtype == "f32" and name in dram_per_voxel
                else None)
@@ -437,7 +437,7 @@ def main(argv=None):
     # its flux launch and two scalar ones) against 4 warp instructions per
     # cycle per SM at the SM clock sampled during the timed region
     inst_per_voxel = {"steam_conv_separable_async": 7.801, "steam_thermo_async": 8.480,
-                      "steam_flux_noise_async": 7.781, "steam_scalar_pattern_async": 2.716,
+                      "steam_flux_noise_async": 7.781, "steam_scalar_pattern_async": 2.497,
                       "steam_flux_finish_async": 0.107}
     issue = None
     if args.dtype == "f32" and name in inst_per_voxel:
