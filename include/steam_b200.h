@@ -191,11 +191,13 @@ int steam_level_sums(int dtype, int64_t nx, int64_t ny, int64_t nz,
  * steam_level_sums without (workspace, workspace_bytes): the scratch is one
  * static device array of steam_level_sums_noalloc_scratch_bytes() (4 MiB) that
  * every GPU loading this library holds until exit.  Limit: nz <= 1024
- * (STEAM_ERR_UNSUPPORTED above that); any nx, ny.  The first call on a device
- * resolves the array's address on that device, so make it before any stream
- * capture.  All calls share the one array: calls whose work overlaps on the
- * GPU (other streams, other host threads) race on it; serialise them.
- * sums_out is written before return (the call synchronises its stream). */
+ * (STEAM_ERR_UNSUPPORTED above that); any nx, ny.  The array's address is per
+ * CUDA context (the context that loaded this library's module); every call
+ * looks it up in the calling thread's current context.  All calls share the
+ * one array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race on it; serialise them.  sums_out is written before return:
+ * the call copies into host memory and synchronises its stream, so it must
+ * never be called while a stream is being captured. */
 size_t steam_level_sums_noalloc_scratch_bytes(void);
 int steam_level_sums_noalloc(int dtype, int64_t nx, int64_t ny, int64_t nz,
                              const void* field, const steam_window_t* window,

@@ -10,7 +10,6 @@
 
 #include <cmath>
 #include <limits>
-#include <mutex>
 #include <vector>
 
 namespace steam {
@@ -2287,32 +2286,23 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;  // 4 MiB per device
 constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
-constexpr int kNoAllocMaxDevices = 64;
-
 // In host code this name is only a handle for the runtime; the device address
-// comes from cudaGetSymbolAddress below, once per device.
+// comes from cudaGetSymbolAddress below.
 __device__ __align__(256) double g_level_sums_scratch[kNoAllocScratchDoubles];
 
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of the scratch array on the current device.  The first call
-// on a device resolves it (with that device current) and caches it.
+// Device address of the scratch array in the calling thread's current
+// context.  The address belongs to the context that loaded this module: a
+// host application may switch between its own contexts, and after
+// cudaDeviceReset the module is loaded again at another address, so the
+// address is looked up on every call (a table lookup once the module is
+// loaded) rather than remembered per device.
 int noalloc_scratch(double** out) {
-  int dev = -1;
-  STEAM_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
-    return fail(STEAM_ERR_UNSUPPORTED, "steam_level_sums_noalloc: device ordinal above 63");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_level_sums_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return fail(STEAM_ERR_CUDA, std::string("steam_level_sums_noalloc: cudaGetSymbolAddress: ") +
-                                      cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
-  }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_level_sums_scratch);
+  if (e != cudaSuccess || p == nullptr)
+    return fail(STEAM_ERR_CUDA, std::string("steam_level_sums_noalloc: cudaGetSymbolAddress: ") +
+                                    cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
   return STEAM_OK;
 }
 

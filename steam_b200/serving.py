@@ -199,10 +199,18 @@ class TileServer:
             slot.event.record(slot.stream)
         slot.request = req
 
+    def check_request(self, req):
+        """Refuse a request this server cannot hold, before it takes a slot."""
+        n = int(req['n'])
+        if not 1 <= n <= self.max_n:
+            raise ValueError(f"tile size {n} outside [1, {self.max_n}] (the server's max_n)")
+        self.world.tile_box(req['origin'], n)  # raises ValueError on a bad z range
+
     def tile(self, origin, n):
         """One tile, alone (synchronous); returns a host array."""
         slot = self.slots[0]
         req = {'origin': origin, 'n': int(n)}
+        self.check_request(req)
         self._launch(slot, req)
         slot.event.synchronize()
         slot.request = None
@@ -224,6 +232,8 @@ class TileServer:
                 gc.enable()
 
     def _serve(self, requests, keep):
+        for req in requests:
+            self.check_request(req)
         pending = deque(sorted(requests, key=lambda r: r['arrival']))
         free = list(self.slots)
         busy = []
@@ -241,8 +251,12 @@ class TileServer:
                 slot = free.pop()
                 req['start'] = now
                 req['bytes'] = need
+                try:
+                    self._launch(slot, req)
+                except BaseException:
+                    free.append(slot)
+                    raise
                 self.in_flight_bytes += need
-                self._launch(slot, req)
                 busy.append(slot)
                 progressed = True
             for slot in list(busy):

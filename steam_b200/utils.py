@@ -288,7 +288,7 @@ def _flux_epilogue_dense(flux_t, conv_t, window):
     flux_t.clamp_(min=0)
     inner = flux_t if window is None else flux_t[window[0]:window[1], window[2]:window[3]]
     return (float(inner.sum(dtype=flux_t.new_zeros(()).double().dtype).item()),
-            float(inner.numel() // flux_t.shape[2]), float(n_clipped))
+            float(inner.numel()), float(n_clipped))
 
 
 def convolve_device(field_t, kernel, out=None, tol=None):

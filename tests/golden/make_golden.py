@@ -1,17 +1,27 @@
-"""Generate tests/golden/reference_fixtures.npz by running the reference.
+"""Generate the golden fixtures by running the reference.
 
 The reference implementation (thomasdewitt/STEAM, pure Python + numba) is
-imported read-only from its source tree -- default /root/reference, or the
-path given as the first argument -- with two shims: a one-line ``netCDF4``
-import stub (the package imports netCDF4 at module load; nothing here writes
-NetCDF) and a scratch NUMBA_CACHE_DIR so that no shipped numba cache is read.
+imported read-only from its source tree, whose path is the required first
+argument, with two shims: a one-line ``netCDF4`` import stub (the package
+imports netCDF4 at module load; nothing here writes NetCDF) and a scratch
+NUMBA_CACHE_DIR so that no shipped numba cache is read.
 
-Every fixture is small: inputs and the reference's outputs for the hot-path
-stages at toy sizes.  The tests compare the oracle (and, on a GPU, the CUDA
-path) against these arrays; the reference itself is never needed at test
-time.
+Two files:
 
-Run: python tests/golden/make_golden.py [/path/to/reference]
+* ``reference_fixtures.npz``: inputs and the reference's outputs for the
+  hot-path stages at toy sizes (``--part unit``);
+* ``c0_class_step.npz``: the reference's own single class step at the
+  128 x 128 x 64 configuration (``tests/config_cases.py``; seed 0, alpha 1.8,
+  C1 0.1, H 1/3, Hz 5/9), for the Mexican-hat and the Morlet turbulon, through
+  its ``cascade_loop`` on the finest class's grid and its
+  ``recover_diagnostics``: the ledger scalars in full, the fields' per-level
+  mean and RMS in full, and a fixed sample of 16,384 cells of every field
+  (``--part c0``).
+
+The tests compare the oracle (and, on a GPU, the CUDA path) against these
+arrays; the reference itself is never needed at test time.
+
+Run: python tests/golden/make_golden.py /path/to/reference [--part unit|c0|all]
 """
 
 from __future__ import annotations
@@ -46,8 +56,66 @@ def _import_reference(ref_root: Path):
 
 
 def main(argv):
-    ref_root = Path(argv[1]) if len(argv) > 1 else Path("/root/reference")
-    sim, noise, utils, thermo, kat_mod = _import_reference(ref_root)
+    import argparse
+    ap = argparse.ArgumentParser(description="generate the golden fixtures")
+    ap.add_argument("reference", type=Path, help="source tree of thomasdewitt/STEAM")
+    ap.add_argument("--part", choices=("unit", "c0", "all"), default="all")
+    args = ap.parse_args(argv[1:])
+    mods = _import_reference(args.reference)
+    if args.part in ("unit", "all"):
+        unit_fixtures(*mods)
+    if args.part in ("c0", "all"):
+        c0_fixtures(*mods)
+
+
+def c0_fixtures(sim, noise, utils, thermo, kat_mod):
+    """The reference's single class step at 128 x 128 x 64."""
+    sys.path.insert(0, str(HERE.parent))
+    import config_cases as cc
+
+    case = cc.build(sim, cc.C0)
+    shape = case['shape']
+    idx = cc.sample_index(int(np.prod(shape)))
+    fx = {"idx": idx.astype(np.int64), "input_seed": np.int64(2026)}
+    zero_comp = [np.ones(shape[2], np.float32)]
+    for tshape in ('mexican_hat', 'morlet_omega0_6'):
+        tag = 'mh' if tshape == 'mexican_hat' else 'mo'
+        h, q, F = cc.inputs(shape)
+        out = sim.cascade_loop(
+            case['hp'], case['qp'], case['zp'], case['grids'], case['C_h'], case['C_q'],
+            case['b_h'], case['b_q'], [case['aspect']], *cc.BOUNDS, 1, (1, 1, 1),
+            [case['seed']], h_perturbation=h, qt_perturbation=q, flux=F,
+            flux_noise_scale=cc.C1, turbulon_shape=tshape, comp_k=zero_comp)
+        h_o, q_o, F_o = out[0], out[1], out[2]
+        led = out[7].classes[0]
+        hm, qm = case['h_mean'], case['qt_mean']
+        diag = thermo.recover_diagnostics(np.clip(h_o + hm, cc.BOUNDS[0], cc.BOUNDS[1]),
+                                          np.clip(q_o + qm, cc.BOUNDS[2], cc.BOUNDS[3]),
+                                          case['z'], cc.SURFACE_PRESSURE, device='cpu')
+        fields = {"flux": F_o, "h": h_o, "qt": q_o, "qc": diag['qc'], "qi": diag['qi'],
+                  "T": diag['T']}
+        for name, f in fields.items():
+            fx[f"{tag}_{name}_sample"] = np.asarray(f).reshape(-1)[idx].astype(np.float32)
+            fx[f"{tag}_{name}_levels"] = cc.level_stats(f)
+        fl = led.flux
+        fx[f"{tag}_flux_ledger"] = np.array([
+            fl.entering.total, fl.entering.count, fl.noise_abs.total, fl.noise_abs.count,
+            fl.realized.total, fl.realized.count, fl.n_clipped], dtype=np.float64)
+        for name in ('h', 'qt'):
+            pl = led.pattern[name]
+            fx[f"{tag}_{name}_pattern"] = np.stack([np.asarray(pl.level_total, np.float64),
+                                                    np.asarray(pl.level_count, np.float64)])
+            ba = led.bounded_add[name]
+            fx[f"{tag}_{name}_ba_a0"] = np.asarray(ba.a0, np.float64)
+            fx[f"{tag}_{name}_ba_mu"] = np.asarray(ba.mu, np.float64)
+            fx[f"{tag}_{name}_ba_n_loop"] = np.asarray(ba.n_loop, np.int32)
+            fx[f"{tag}_{name}_ba_final_demean"] = np.asarray(ba.final_demean, np.float64)
+    out_path = HERE / "c0_class_step.npz"
+    np.savez_compressed(out_path, **fx)
+    print(f"wrote {out_path} ({out_path.stat().st_size} bytes, {len(fx)} arrays)")
+
+
+def unit_fixtures(sim, noise, utils, thermo, kat_mod):
     fx = {}
 
     # -- Philox known answers (Random123 vectors carried by the reference tests)

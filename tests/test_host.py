@@ -164,3 +164,22 @@ def test_plan_tiling_halo_and_budget():
     assert forced.horizon == 1 and forced.tiles == {1: (2, 2)}
     with pytest.raises(MemoryError):
         plan_tiling(grids, (13, 13, 13), budget_bytes=1000)
+
+
+def test_tile_server_refuses_oversize_and_bad_requests_before_a_slot():
+    """A request larger than the server's max_n, or outside the world's z
+    range, is a ValueError at admission; the budget count is untouched."""
+    from types import SimpleNamespace
+
+    from steam_b200 import serving
+
+    world = SimpleNamespace(shape=(64, 64, 32), n_zero=2)
+    world.tile_box = lambda origin, n: serving.TileWorld.tile_box(world, origin, n)
+    server = SimpleNamespace(max_n=16, world=world, in_flight_bytes=0)
+    check = serving.TileServer.check_request
+    check(server, {'origin': (0, 0, 0), 'n': 16})
+    with pytest.raises(ValueError, match="max_n"):
+        check(server, {'origin': (0, 0, 0), 'n': 32})
+    with pytest.raises(ValueError, match="outside"):
+        check(server, {'origin': (0, 0, 20), 'n': 16})
+    assert server.in_flight_bytes == 0

@@ -5,10 +5,14 @@ reference's own numpy arithmetic must match to float32 roundoff; the FFT-based
 stages agree to the reference's own FFT accuracy.
 """
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
 from oracle import steam_oracle as O
+
+REPO = Path(__file__).resolve().parents[1]
 
 
 def rel_l2(a, b):
@@ -153,3 +157,30 @@ def test_thermodynamics(golden):
     out = O.recover_diagnostics(golden["th_h"], golden["th_qt"], golden["th_z"], 101325.0)
     for k in ("T", "qv", "qc", "qi", "p"):
         np.testing.assert_allclose(out[k], golden[f"th_{k}"], rtol=1e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("tshape,tag", [("mexican_hat", "mh"), ("morlet_omega0_6", "mo")])
+def test_oracle_c0_class_step_against_reference_run(tshape, tag):
+    """The float32-mode oracle against the reference's own class step at
+    128 x 128 x 64 (seed 0; tests/golden/c0_class_step.npz): sampled cells of
+    every field, per-level statistics and the ledger.  The pattern's level
+    sums and every integer count are equal; fields agree to float32
+    rounding (the FFT libraries differ)."""
+    import config_cases as cc
+    from steam_b200 import simulate as S
+    with np.load(REPO / "tests" / "golden" / "c0_class_step.npz") as g:
+        g = {k: g[k] for k in g.files}
+    case = cc.build(S, cc.C0)
+    fields, rec = cc.oracle_step(O, case, *cc.inputs(cc.C0), tshape, np.float32)
+    idx = g["idx"]
+    for name, f in fields.items():
+        assert cc.rel_l2(f.reshape(-1)[idx], g[f"{tag}_{name}_sample"]) < 2e-6, name
+        assert cc.rel_l2(cc.level_stats(f), g[f"{tag}_{name}_levels"]) < 1e-6, name
+    fl = g[f"{tag}_flux_ledger"]
+    r = rec['flux']
+    assert r['n_clipped'] == fl[6]
+    for name in ("h", "qt"):
+        pat = g[f"{tag}_{name}_pattern"]
+        np.testing.assert_array_equal(rec[name]['level_count'], pat[1])
+        np.testing.assert_allclose(rec[name]['level_total'], pat[0], rtol=1e-12)
+        np.testing.assert_allclose(rec[name]['a0'], g[f"{tag}_{name}_ba_a0"], rtol=1e-5)

@@ -58,6 +58,7 @@ def _assert_same(got, want):
     ((64, 48, 256), None),            # one level per thread, grid not capped
     ((40, 33, 96), (3, 31, 5, 30)),   # windowed means
     ((20, 16, 1000), None),           # several levels per thread, grid capped
+    ((4, 4, 1024), None),             # the maximum nz: tightest grid cap, every slot used
 ])
 def test_noalloc_matches_workspace_entry_twice(dtype_name, shape, win):
     torch = _lib.require_cuda("test")
@@ -84,3 +85,18 @@ def test_noalloc_rejects_too_many_levels():
     assert rc == 4
     assert b"1024" in lib.steam_last_error()
     assert lib.steam_level_sums_noalloc_scratch_bytes() == 4 << 20
+
+
+@pytest.mark.parametrize("shape", [(0, 5, 8), (5, 0, 8), (3, 3, 0)])
+def test_noalloc_empty_extents_match_workspace_entry(shape):
+    """An empty column set gives zero sums and the window's cell count per
+    level; an empty z extent writes nothing.  Both entry points agree."""
+    torch = _lib.require_cuda("test")
+    lib = _lib.load()
+    f = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    nz = shape[2]
+    want = _workspace_sums(lib, torch, f, None)
+    got = _noalloc_sums(lib, f, None)
+    np.testing.assert_array_equal(got, want)
+    if nz:
+        np.testing.assert_array_equal(got[:, :3], 0.0)
