@@ -56,6 +56,10 @@ def parse(argv=None):
     ap.add_argument("--ny", type=int, default=2048)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--dtype", choices=("f32", "f64"), default="f32")
+    ap.add_argument("--shape", choices=("mexican_hat", "morlet_omega0_6"),
+                    default="mexican_hat",
+                    help="turbulon shape: the Mexican hat factors into separable "
+                         "filters; the Morlet runs the FFT convolution")
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-sample", type=int, nargs=3, default=(128, 128, 256),
                     metavar=("NX", "NY", "NZ"))
@@ -77,11 +81,12 @@ def parse(argv=None):
 # Workload setup (host, shared by both arms)
 # ---------------------------------------------------------------------------
 
-def config_dict(shape, world):
+def config_dict(shape, world, turbulon_shape="mexican_hat"):
     """The workload's config, the same for both arms."""
     return {"workload": f"field step at {shape[0]}x{shape[1]}x{shape[2]} "
                         f"(finest class of the {shape[0]}x{shape[1]}x{shape[2]} domain, "
                         f"k=200 m, dx=dz=100 m) + condensate",
+            "turbulon": turbulon_shape,
             "alpha": ALPHA, "C1": C1, "H": H, "Hz": HZ, "seed": 0,
             "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (4.3 GB fields); no flush"}
@@ -291,7 +296,7 @@ def run_reference(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": args.dtype.replace("f", "f"), "data": "synthetic (seeded)",
         "impl": "reference",
-        "config": config_dict((args.nx, args.ny, args.nz), world),
+        "config": config_dict((args.nx, args.ny, args.nz), world, args.shape),
         "cpu_baseline": {"value": value, "unit": "Mvoxels/s", "cores": threads,
                          "kind": "port",
                          "sample": f"the oracle's class step + condensate on a {nx}x{ny}x{nz} "
@@ -311,7 +316,7 @@ def run_reference(args, rank, world):
 # Error of the benched float32 step against float64
 # ---------------------------------------------------------------------------
 
-def float64_error(torch, sim, w, h0, q0, F0, F, hp, qp, diag, clip_band=1e-3):
+def float64_error(torch, sim, w, h0, q0, F0, F, hp, qp, diag, turbulon_shape, clip_band=1e-3):
     """Run the same class step in float64 on the device from the same inputs
     and return the float32 result's error against it: log-flux relative L2
     over the cells clear of the clip (F > clip_band in both), the count of
@@ -323,7 +328,7 @@ def float64_error(torch, sim, w, h0, q0, F0, F, hp, qp, diag, clip_band=1e-3):
         w['grids'], 0, h_profile=w['hp'], qt_profile=w['qp'], z_profile=w['zp'],
         C_h=w['C_h'], C_qt=w['C_q'], b_h=w['b_h'], b_qt=w['b_q'], aspect=w['aspect'],
         bounds=BOUNDS, key=w['key'], flux_noise_scale=C1, flux_alpha=ALPHA,
-        dtype=np.float64)
+        turbulon_shape=turbulon_shape, dtype=np.float64)
     h64, q64, F64 = h0.double(), q0.double(), F0.double()
     d64 = {k: torch.empty_like(h64) for k in ("T", "qv", "qc", "qi", "p")}
     r64 = _resident.ResidentClass(setup64, torch.float64)
@@ -417,7 +422,8 @@ def main(argv=None):
     setup = sim.make_class_setup(
         w['grids'], 0, h_profile=w['hp'], qt_profile=w['qp'], z_profile=w['zp'],
         C_h=w['C_h'], C_qt=w['C_q'], b_h=w['b_h'], b_qt=w['b_q'], aspect=w['aspect'],
-        bounds=BOUNDS, key=w['key'], flux_noise_scale=C1, flux_alpha=ALPHA, dtype=np_t)
+        bounds=BOUNDS, key=w['key'], flux_noise_scale=C1, flux_alpha=ALPHA,
+        turbulon_shape=args.shape, dtype=np_t)
     from steam_b200.resident import resident_for
 
     gen = torch.Generator(device="cuda")
@@ -479,6 +485,8 @@ def main(argv=None):
     # 3 fields of traffic, and two scalar convolutions, 2 fields each)
     alg = {
         "steam_conv_separable_async": 7 * elem * nvox / 3,  # mean over the three launches
+        "steam_conv_fft_async": 7 * elem * nvox / 3,        # the same three launches
+        "steam_conv_direct_async": 7 * elem * nvox / 3,
         "steam_flux_noise_async": 2 * elem * nvox,          # read flux, write product
         "steam_flux_finish_async": 2 * elem * nvox,         # read and write flux
         "steam_scalar_pattern_async": 3 * elem * nvox,      # read pert + product, write W
@@ -547,7 +555,7 @@ def main(argv=None):
             diag.pop(k)
         resident.work = None
         torch.cuda.empty_cache()
-        error = float64_error(torch, sim, w, h0, q0, F0, F, hp, qp, diag)
+        error = float64_error(torch, sim, w, h0, q0, F0, F, hp, qp, diag, args.shape)
         torch.cuda.empty_cache()
 
     # end to end through the public host-array API, pinned host buffers
@@ -640,7 +648,7 @@ def main(argv=None):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.dtype, "data": "synthetic (seeded state and noise)",
-            "config": config_dict(shape, world),
+            "config": config_dict(shape, world, args.shape),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "error": error,
             "serving": serving,
             "ensemble": ensemble,

@@ -143,12 +143,59 @@ int steam_conv_separable(int dtype, int64_t nx, int64_t ny, int64_t nz,
 int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t chunk);
 int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz);
 
-/* Dense-kernel form (any kernel; direct summation over the taps).  `kernel`
- * is a DEVICE array (kx, ky, kz) of the call's dtype, already folded onto the
- * field period; centres are (k-1)//2 per axis. */
-int steam_conv_dense(int dtype, int64_t nx, int64_t ny, int64_t nz,
-                     const void* kernel, int32_t kx, int32_t ky, int32_t kz,
-                     const void* in, void* out, steam_stream_t stream);
+/* ---- a9/a10 for kernels without a separable form -----------------------
+ * The Morlet turbulon (steam/turbulons.py:40-48) and any kernel whose Tucker
+ * factorisation is not exact to the dtype's tolerance.  Same semantics as
+ * convolve_fft_xy_oa_z (steam/utils.py:293-427): x and y circular over the
+ * field's period, z linear with zero padding; the kernel is NOT folded onto
+ * the period: (cx, cy) are the centres the fold implies (k//2 - (1 if n even)
+ * for an axis longer than its period n, (k-1)//2 otherwise) and cz =
+ * (kz-1)//2.  Prologue and epilogues as steam_conv_separable: pre_div /
+ * pre_mul (HOST, per level, may be NULL) or pre_dev (DEVICE [2][nz] of the
+ * call's dtype) scale the input by pre[1][z] / pre[0][z]; STEAM_EPI_FLUX
+ * makes out = max(out + conv, 0) with { sum out over the window, cells,
+ * clip count } in sums_out (HOST, 3 doubles) or { sum, clip count } in
+ * sums_dev (DEVICE, 2 doubles).
+ *
+ * Kernel spectrum (replaces steam/utils.py:367-375): the kernel (DEVICE
+ * float64, C order (kx, ky, kz), each extent <= 25) zero-padded to 32^3 and
+ * transformed in float64 on the device, stored as complex float32
+ * [17][32][32] in the order the FFT kernel reads it. */
+size_t steam_conv_fft_spectrum_bytes(void);
+int steam_conv_fft_spectrum(const double* kernel_dev, int32_t kx, int32_t ky, int32_t kz,
+                            void* spectrum_dev, steam_stream_t stream);
+
+/* Float32 overlap-save FFT convolution on 32^3 cubes (kernel extents <= 25):
+ * forward transforms, the spectrum product and the inverse transforms of a
+ * cube in one CTA's shared memory, prologue and epilogue fused. */
+size_t steam_conv_fft_workspace_bytes(int64_t nx, int64_t ny, int64_t nz);
+int steam_conv_fft(int64_t nx, int64_t ny, int64_t nz, int32_t kx, int32_t ky, int32_t kz,
+                   int32_t cx, int32_t cy, const void* spectrum_dev, const void* in,
+                   const double* pre_div, const double* pre_mul, void* out, int32_t epilogue,
+                   const steam_window_t* window, double* sums_out, void* workspace,
+                   size_t workspace_bytes, steam_stream_t stream);
+int steam_conv_fft_async(int64_t nx, int64_t ny, int64_t nz, int32_t kx, int32_t ky,
+                         int32_t kz, int32_t cx, int32_t cy, const void* spectrum_dev,
+                         const void* in, const void* pre_dev, void* out, int32_t epilogue,
+                         const steam_window_t* window, double* sums_dev, void* workspace,
+                         size_t workspace_bytes, steam_stream_t stream);
+
+/* Direct summation over the kernel's taps (float64 fields, where the FFT's
+ * float32 arithmetic is not wanted, or kernels longer than 25 taps).
+ * kernel_dev is a DEVICE array (kx, ky, kz) of the call's dtype; float64
+ * accumulation. */
+size_t steam_conv_direct_workspace_bytes(int64_t nx, int64_t ny, int64_t nz);
+int steam_conv_direct(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* kernel_dev,
+                      int32_t kx, int32_t ky, int32_t kz, int32_t cx, int32_t cy,
+                      const void* in, const double* pre_div, const double* pre_mul, void* out,
+                      int32_t epilogue, const steam_window_t* window, double* sums_out,
+                      void* workspace, size_t workspace_bytes, steam_stream_t stream);
+int steam_conv_direct_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                            const void* kernel_dev, int32_t kx, int32_t ky, int32_t kz,
+                            int32_t cx, int32_t cy, const void* in, const void* pre_dev,
+                            void* out, int32_t epilogue, const steam_window_t* window,
+                            double* sums_dev, void* workspace, size_t workspace_bytes,
+                            steam_stream_t stream);
 
 /* ---- a11 apply: scalar rescale ----------------------------------------
  * field *= scale (the volume-mean restore of steam/simulate.py:2208-2215;

@@ -70,8 +70,24 @@ _SIGNATURES = {
                                             c_vp]),
     "steam_conv_set_xchunk": (ctypes.c_int, [c_i64, c_i64, c_i64, c_i32]),
     "steam_conv_get_xchunk": (ctypes.c_int, [c_i64, c_i64, c_i64]),
-    "steam_conv_dense": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i32,
-                                        c_i32, c_i32, c_vp, c_vp, c_vp]),
+    "steam_conv_fft_spectrum_bytes": (c_size, []),
+    "steam_conv_fft_spectrum": (ctypes.c_int, [c_vp, c_i32, c_i32, c_i32, c_vp, c_vp]),
+    "steam_conv_fft_workspace_bytes": (c_size, [c_i64, c_i64, c_i64]),
+    "steam_conv_fft": (ctypes.c_int, [c_i64, c_i64, c_i64, c_i32, c_i32, c_i32, c_i32, c_i32,
+                                      c_vp, c_vp, c_dp, c_dp, c_vp, c_i32,
+                                      ctypes.POINTER(Window), c_dp, c_vp, c_size, c_vp]),
+    "steam_conv_fft_async": (ctypes.c_int, [c_i64, c_i64, c_i64, c_i32, c_i32, c_i32, c_i32,
+                                            c_i32, c_vp, c_vp, c_vp, c_vp, c_i32,
+                                            ctypes.POINTER(Window), c_vp, c_vp, c_size, c_vp]),
+    "steam_conv_direct_workspace_bytes": (c_size, [c_i64, c_i64, c_i64]),
+    "steam_conv_direct": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i32,
+                                         c_i32, c_i32, c_i32, c_i32, c_vp, c_dp, c_dp, c_vp,
+                                         c_i32, ctypes.POINTER(Window), c_dp, c_vp, c_size,
+                                         c_vp]),
+    "steam_conv_direct_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
+                                               c_i32, c_i32, c_i32, c_i32, c_i32, c_vp, c_vp,
+                                               c_vp, c_i32, ctypes.POINTER(Window), c_vp, c_vp,
+                                               c_size, c_vp]),
     "steam_scale": (ctypes.c_int, [ctypes.c_int, c_i64, c_vp, c_dbl, c_i32, c_vp]),
     "steam_tile_extract": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i64,
                                           c_i64, c_i64, c_i64, c_i64, c_i64, c_dbl, c_i32,

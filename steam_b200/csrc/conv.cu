@@ -1,6 +1,6 @@
 // Circular-x/y, linear-z convolution on a separable network of 1D filters
-// (the turbulon kernels are sums of a few separable terms), plus a dense
-// direct-summation form for arbitrary kernels.
+// (the turbulon kernels are sums of a few separable terms).  Kernels without
+// such a form go to fftconv.cu.
 //
 // Three passes, each a coalesced stencil over the z-fastest layout:
 //   z-pass: u_c = f (*)_z Z_c       (columns staged in shared memory)
@@ -680,37 +680,6 @@ static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz) {
   return fused_grid(nx, ny, nz, fused_chunk(nx, ny, nz));
 }
 
-// ---- dense direct convolution ----------------------------------------------
-template <typename T>
-__global__ void dense_conv_kernel(const T* __restrict__ in, int64_t nx,
-                                  int64_t ny, int64_t nz,
-                                  const T* __restrict__ K, int kx, int ky,
-                                  int kz, int cx, int cy, int cz,
-                                  T* __restrict__ out) {
-  const int64_t n = nx * ny * nz;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t z = i % nz;
-    int64_t col = i / nz;
-    int64_t y = col % ny;
-    int64_t x = col / ny;
-    double acc = 0.0;
-    for (int a = 0; a < kx; ++a) {
-      int64_t xs = wrapi(x - a + cx, nx);
-      for (int b = 0; b < ky; ++b) {
-        int64_t ys = wrapi(y - b + cy, ny);
-        const T* src = in + (xs * ny + ys) * nz;
-        const T* kk = K + ((int64_t)a * ky + b) * kz;
-        for (int c = 0; c < kz; ++c) {
-          int64_t zs = z - c + cz;
-          if (zs >= 0 && zs < nz) acc += (double)kk[c] * (double)src[zs];
-        }
-      }
-    }
-    out[i] = (T)acc;
-  }
-}
-
 template <typename T>
 static int fill_params(const steam_sepconv_t* s, const double* zt,
                        const double* yt, const double* xt, SepParams<T>& p) {
@@ -1122,34 +1091,4 @@ extern "C" int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t
 
 extern "C" int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz) {
   return fused_chunk(nx, ny, nz);
-}
-
-extern "C" int steam_conv_dense(int dtype, int64_t nx, int64_t ny, int64_t nz,
-                                const void* kernel, int32_t kx, int32_t ky,
-                                int32_t kz, const void* in, void* out,
-                                steam_stream_t stream) {
-  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0,
-                "steam_conv_dense: negative extent");
-  STEAM_REQUIRE(kx >= 1 && ky >= 1 && kz >= 1,
-                "steam_conv_dense: kernel extents must be >= 1");
-  STEAM_REQUIRE(kx <= nx && ky <= ny,
-                "steam_conv_dense: fold the kernel onto the field period first");
-  const int64_t n = nx * ny * nz;
-  if (n == 0) return STEAM_OK;
-  STEAM_REQUIRE(kernel && in && out, "steam_conv_dense: null pointer");
-  cudaStream_t s = (cudaStream_t)stream;
-  int grid = stride_grid(n, 256, 8);
-  const int cx = (kx - 1) / 2, cy = (ky - 1) / 2, cz = (kz - 1) / 2;
-  if (dtype == STEAM_F32)
-    dense_conv_kernel<float><<<grid, 256, 0, s>>>(
-        (const float*)in, nx, ny, nz, (const float*)kernel, kx, ky, kz, cx, cy,
-        cz, (float*)out);
-  else if (dtype == STEAM_F64)
-    dense_conv_kernel<double><<<grid, 256, 0, s>>>(
-        (const double*)in, nx, ny, nz, (const double*)kernel, kx, ky, kz, cx,
-        cy, cz, (double*)out);
-  else
-    return fail(STEAM_ERR_ARG, "steam_conv_dense: bad dtype");
-  STEAM_LAUNCH_CHECK("steam_conv_dense");
-  return STEAM_OK;
 }

@@ -22,6 +22,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
+from . import utils as _utils
 from .ledger import (BoundedAddLedger, ClassLedger, FluxAdvanceLedger, MeanReduction,
                      PatternLedger)
 
@@ -36,16 +37,14 @@ def _off(t, n_doubles):
 class ResidentClass:
     """Device-resident constants, work fields and ledger block of one class.
 
-    ``setup`` is a ``simulate.ClassSetup`` whose convolution plan is
-    separable (every turbulon kernel is)."""
+    ``setup`` is a ``simulate.ClassSetup``; its convolution plan may be of
+    any kind (separable, FFT or direct)."""
 
     def __init__(self, setup, dtype=None):
         torch = _lib.require_cuda("resident class step")
         from . import simulate as sim
         self.lib = _lib.load()
         self.setup = setup
-        if setup.plan.kind == 'dense':
-            raise NotImplementedError("resident class step: the kernel does not factor")
         self.dtype = dtype if dtype is not None else torch.float32
         self.np_t = np.float64 if self.dtype == torch.float64 else np.float32
         self.code = _lib.STEAM_F64 if self.dtype == torch.float64 else _lib.STEAM_F32
@@ -96,7 +95,9 @@ class ResidentClass:
         w = setup.window
         cols = nx * ny if w is None else (w[1] - w[0]) * (w[3] - w[2])
         self.cells = float(cols * nz)
-        if nx * ny * nz >= (1 << 28) and setup.plan.kind != 'dense':
+        from . import utils as _utils
+        _utils.prepare_plan(setup.plan, dev, self.dtype)
+        if nx * ny * nz >= (1 << 28) and setup.plan.kind == 'separable':
             # a field this large amortises timing its convolution's tile
             # lengths once (the tile never changes a result)
             from .ensemble import autotune_conv
@@ -136,7 +137,7 @@ class ResidentClass:
         plan = cs.plan
         ws = _lib.WORKSPACE.get(max(
             lib.steam_flux_noise_workspace_bytes(),
-            lib.steam_conv_workspace_bytes(code, nx, ny, nz, ctypes.byref(plan.spec)),
+            _utils.plan_workspace_bytes(plan, code, self.shape),
             lib.steam_scalar_pattern_workspace_bytes(nx, ny, nz),
             lib.steam_bounded_add_workspace_bytes(nz, N_RESCALE)))
         wsp, wsn = _lib.ptr(ws), ws.numel()
@@ -145,10 +146,8 @@ class ResidentClass:
             code, ctypes.byref(self.region), self.alpha, self.pcs, self.shift, int(cs.n_zero),
             int(bool(cs.zero_bottom)), int(bool(cs.zero_top)), _lib.ptr(F), _lib.ptr(product),
             win, _off(L, self.o_ns), wsp, wsn, stream))
-        _lib.check(lib.steam_conv_separable_async(
-            code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps, plan.x_taps,
-            _lib.ptr(product), None, _lib.ptr(F), _lib.STEAM_EPI_FLUX, win, _off(L, self.o_cs),
-            wsp, wsn, stream))
+        _utils.run_plan_async(plan, product, F, None, _lib.STEAM_EPI_FLUX, cs.window,
+                              _off(L, self.o_cs), ws, stream)
         _lib.check(lib.steam_flux_finish_async(
             code, F.numel(), _lib.ptr(F), _off(L, self.o_ns), _off(L, self.o_cs), self.cells,
             _off(L, self.o_fl), stream))
@@ -167,10 +166,8 @@ class ResidentClass:
                 float(lo), float(hi), _lib.ptr(W), win, ps, wsp, wsn, stream))
             _lib.check(lib.steam_pattern_norm_async(
                 code, nz, ps, _lib.ptr(self.mul[name]), _lib.ptr(self.pre[name]), stream))
-            _lib.check(lib.steam_conv_separable_async(
-                code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps,
-                plan.x_taps, _lib.ptr(W), _lib.ptr(self.pre[name]), _lib.ptr(inc),
-                _lib.STEAM_EPI_STORE, win, None, wsp, wsn, stream))
+            _utils.run_plan_async(plan, W, inc, self.pre[name], _lib.STEAM_EPI_STORE,
+                                  cs.window, None, ws, stream)
             _lib.check(lib.steam_bounded_add_async(
                 code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
                 float(lo), float(hi), win, N_RESCALE, 0, _off(L, self.o_ba[name]), wsp, wsn,

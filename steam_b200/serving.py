@@ -78,19 +78,14 @@ class TileWorld:
             int(zero_bottom), int(zero_top), _lib.ptr(F), _lib.ptr(product), None,
             _lib.ptr(sums), _lib.ptr(ws), ws.numel(), stream))
         plan = _utils.plan_convolution(self.kernel, box, self.np_t)
-        if plan.kind == 'dense':
-            raise NotImplementedError("TileWorld: the kernel does not factor for this box")
-        _lib.check(lib.steam_conv_separable_async(
-            self.code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps,
-            plan.x_taps, _lib.ptr(product), None, _lib.ptr(F), _lib.STEAM_EPI_FLUX, None,
-            ctypes.c_void_p(sums.data_ptr() + 24), _lib.ptr(ws), ws.numel(), stream))
+        _utils.run_plan_async(plan, product, F, None, _lib.STEAM_EPI_FLUX, None,
+                              ctypes.c_void_p(sums.data_ptr() + 24), ws, stream)
 
     def workspace_bytes(self, box):
         lib = self.lib
         plan = _utils.plan_convolution(self.kernel, box, self.np_t)
         return max(lib.steam_flux_noise_workspace_bytes(),
-                   lib.steam_conv_workspace_bytes(self.code, box[0], box[1], box[2],
-                                                  ctypes.byref(plan.spec)))
+                   _utils.plan_workspace_bytes(plan, self.code, box))
 
     def _world_ledger(self):
         """The restore factor realized over the whole world (one advance)."""

@@ -678,7 +678,7 @@ def run_class(hp, qp, F, dh, dq, dF, cs, cl, increment_dir=None, index=0, reside
     torch = _lib.require_cuda("cascade_loop")
     need_inc = cs.deficit is not None or increment_dir is not None
     if (resident and not need_inc and cl.flux is None and not cl.pattern
-            and not cl.bounded_add and cs.plan.kind != 'dense'):
+            and not cl.bounded_add):
         # measure mode: the resident step keeps every scalar on the device
         from .resident import resident_for
         resident_for(cs, F.dtype).step(hp, qp, F).class_ledger(cl)
@@ -1161,7 +1161,7 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
     from .thermodynamics import recover_diagnostics_device
     torch = _lib.require_cuda("field_step")
     if (not is_tensor(h_perturbation) and ledger is None and setup.deficit is None
-            and setup.plan.kind != 'dense' and np.ndim(surface_pressure) == 0):
+            and np.ndim(surface_pressure) == 0):
         # host arrays: the resident step with pipelined transfers
         from .resident import resident_for
         np_t = np.asarray(h_perturbation).dtype
@@ -1175,8 +1175,7 @@ def field_step(h_perturbation, qt_perturbation, flux, setup, surface_pressure=10
     F, f_host = to_device(flux, dtype=hp.dtype)
     cl = ClassLedger() if ledger is None else ledger
     diag = {}
-    resident = (ledger is None and setup.deficit is None and setup.plan.kind != 'dense'
-                and np.ndim(surface_pressure) == 0)
+    resident = ledger is None and setup.deficit is None and np.ndim(surface_pressure) == 0
     if resident:
         from .resident import resident_for
         rc = resident_for(setup, hp.dtype)

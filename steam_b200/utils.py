@@ -3,10 +3,14 @@
 ``convolve_fft_xy_oa_z`` keeps the reference's semantics -- x and y circular
 over the full array period, z linear with zero padding, the kernel centred at
 (k-1)//2 after being folded onto a narrower field -- but not its method.  A
-turbulon kernel is a sum of a few separable terms, so the convolution runs as
-three coalesced 1D stencil passes on the device (z, then y, then x) over a
-Tucker factorisation of the kernel taken on the host in float64.  A kernel
-that does not factor into a few terms runs as a dense direct sum.
+turbulon kernel that is a sum of a few separable terms (the Mexican hat)
+runs as three coalesced 1D stencil passes on the device (z, then y, then x)
+over a Tucker factorisation of the kernel taken on the host in float64.  A
+kernel without such a form (the Morlet turbulon) runs, for float32 fields,
+as an overlap-save FFT convolution on 32^3 cubes with its spectrum built on
+the device, and for float64 fields (or kernels longer than 25 taps) as a
+direct sum over its taps.  Neither folds the kernel: a kernel longer than
+the period is applied with the centre the fold implies (``effective_centre``).
 """
 
 from __future__ import annotations
@@ -32,28 +36,6 @@ MAX_TAPS = 1536
 FACTOR_TOL = {np.float32: 1e-6, np.float64: 1e-12}
 
 
-def fold_kernel_to_field(kernel, field_shape):
-    """Periodise a kernel wider than the field on x and y (steam/utils.py:222-242)."""
-    result = kernel
-    for axis in (0, 1):
-        n_field = field_shape[axis]
-        n_kern = result.shape[axis]
-        if n_kern <= n_field:
-            continue
-        shape = list(result.shape)
-        shape[axis] = n_field
-        folded = np.zeros(shape, dtype=result.dtype)
-        center = n_kern // 2
-        for i in range(n_kern):
-            dst = [slice(None)] * 3
-            src = [slice(None)] * 3
-            dst[axis] = (i - center) % n_field
-            src[axis] = i
-            folded[tuple(dst)] += result[tuple(src)]
-        result = np.roll(folded, n_field // 2, axis=axis)
-    return result
-
-
 def effective_centre(k: int, n: int) -> int:
     """Centre tap of a kernel axis convolved circularly over period n.
 
@@ -74,17 +56,24 @@ def _mode_basis(unfolded, tol_abs):
     return U[:, :max(r, 1)]
 
 
+FFT_MAX_TAPS = 25  # longest kernel axis of the 32^3-cube FFT convolution
+
+
 @dataclass
 class ConvPlan:
-    """A kernel prepared for one field period (nx, ny) and dtype."""
+    """A kernel prepared for one field period (nx, ny) and dtype.
+
+    ``kind``: 'separable' (Tucker factors), 'fft' (float32 fields, kernel
+    spectrum on the device) or 'direct' (sum over the taps)."""
     kind: str
     shape: tuple
     spec: object = None
     z_taps: object = None
     y_taps: object = None
     x_taps: object = None
-    dense: object = None           # folded kernel (host ndarray)
-    dense_dev: object = None       # folded kernel on the device
+    kernel: object = None          # the unfolded kernel (host float64), fft / direct
+    centre: tuple = (0, 0)         # (cx, cy) for the unfolded kernel, fft / direct
+    device_data: dict = None       # per (device, dtype): kernel / spectrum tensors
     error: float = 0.0             # relative Frobenius error of the factorisation
 
 
@@ -200,6 +189,18 @@ def plan_from_factors(Px, Py, Pz, core, kshape, field_shape, err=0.0):
         x_taps=_lib.dvec(Px.T.ravel()), error=err)
 
 
+def _fused_separable(plan):
+    """Whether the library runs a separable plan as its fused single-pass
+    kernel: a cubic 13 or 25-tap support, at most 2 z, 2 y and 2 x filters and
+    4 (z, y) filter pairs drawn from the first two of each."""
+    sp = plan.spec
+    if not (sp.kx == sp.ky == sp.kz and sp.kx in (13, 25)):
+        return False
+    if sp.n_z > 2 or sp.n_y > 2 or sp.n_x > 2 or sp.n_pairs > 4:
+        return False
+    return all(sp.pair_z[q] < 2 and sp.pair_y[q] < 2 for q in range(sp.n_pairs))
+
+
 _PLAN_CACHE: dict = {}
 
 
@@ -217,78 +218,132 @@ def plan_convolution(kernel, field_shape, dtype=np.float32, tol=None):
     if plan is not None:
         return plan
     Px, Py, Pz, core, err = factor_kernel(kernel, tol)
-    plan = None
+    sep = None
     if err <= tol:
-        plan = plan_from_factors(Px, Py, Pz, core, kernel.shape, (nx, ny), err)
-    if plan is None:
-        folded = fold_kernel_to_field(np.asarray(kernel, dtype=np.float64), (nx, ny))
-        plan = ConvPlan(kind='dense', shape=folded.shape, dense=folded)
+        sep = plan_from_factors(Px, Py, Pz, core, kernel.shape, (nx, ny), err)
+    k64 = np.ascontiguousarray(kernel, dtype=np.float64)
+    fft_ok = dtype == np.float32 and max(k64.shape) <= FFT_MAX_TAPS
+    # the fused separable kernel is the fastest form; a separable plan beyond
+    # it runs as three passes through HBM with one intermediate field per
+    # filter (pair), which the FFT convolution beats
+    if sep is not None and (_fused_separable(sep) or not fft_ok):
+        plan = sep
+    else:
+        plan = ConvPlan(kind='fft' if fft_ok else 'direct', shape=k64.shape, kernel=k64,
+                        centre=(effective_centre(k64.shape[0], nx),
+                                effective_centre(k64.shape[1], ny)),
+                        device_data={}, error=0.0)
     if len(_PLAN_CACHE) > 256:
         _PLAN_CACHE.clear()
     _PLAN_CACHE[key] = plan
     return plan
 
 
-def run_plan(plan, field_t, out_t, pre_div=None, pre_mul=None,
-             epilogue=_lib.STEAM_EPI_STORE, window=None):
-    """Launch a planned convolution on device tensors; returns the epilogue
-    sums (flux epilogue) or None."""
+def prepare_plan(plan, device, dtype):
+    """The plan's kernel (direct) or spectrum (fft) on ``device``, built once
+    per (device, dtype) on the current stream; call it before capturing a
+    graph that runs the plan.  Returns the tensors the launches read."""
     import torch
+    if plan.kind == 'separable':
+        return None
+    key = (torch.device(device), dtype)
+    data = plan.device_data.get(key)
+    if data is not None:
+        return data
+    lib = _lib.load()
+    k64 = torch.as_tensor(plan.kernel, device=device).contiguous()
+    if plan.kind == 'fft':
+        spec = torch.empty(lib.steam_conv_fft_spectrum_bytes(), dtype=torch.uint8, device=device)
+        kx, ky, kz = plan.shape
+        _lib.check(lib.steam_conv_fft_spectrum(_lib.ptr(k64), kx, ky, kz, _lib.ptr(spec),
+                                               _lib.stream()))
+        data = (spec, k64)  # the float64 kernel stays alive while the build may run
+    else:
+        data = (k64.to(dtype).contiguous(),)
+    plan.device_data[key] = data
+    return data
+
+
+def _device_data(plan, field_t):
+    return prepare_plan(plan, field_t.device, field_t.dtype)
+
+
+def plan_workspace_bytes(plan, code, shape):
+    """Workspace of one launch of ``plan`` on a field of ``shape``."""
+    lib = _lib.load()
+    nx, ny, nz = (int(n) for n in shape)
+    if plan.kind == 'separable':
+        return lib.steam_conv_workspace_bytes(code, nx, ny, nz, ctypes.byref(plan.spec))
+    if plan.kind == 'fft':
+        return lib.steam_conv_fft_workspace_bytes(nx, ny, nz)
+    return lib.steam_conv_direct_workspace_bytes(nx, ny, nz)
+
+
+def run_plan_async(plan, field_t, out_t, pre_dev=None, epilogue=_lib.STEAM_EPI_STORE,
+                   window=None, sums_dev=None, workspace=None, stream=None):
+    """Enqueue a planned convolution with its scalars on the device:
+    ``pre_dev`` a [2][nz] device tensor (or pointer) of the field's dtype,
+    ``sums_dev`` a device pointer to 2 doubles for the flux epilogue."""
     lib = _lib.load()
     nx, ny, nz = (int(n) for n in field_t.shape)
     code = _lib.dtype_code(field_t)
-    if plan.kind == 'dense':
-        if epilogue != _lib.STEAM_EPI_STORE or pre_div is not None or pre_mul is not None:
-            tmp_in = field_t
-            if pre_div is not None or pre_mul is not None:
-                d = torch.as_tensor(np.asarray(pre_div if pre_div is not None else np.ones(nz)),
-                                    dtype=field_t.dtype, device=field_t.device)
-                m = torch.as_tensor(np.asarray(pre_mul if pre_mul is not None else np.ones(nz)),
-                                    dtype=field_t.dtype, device=field_t.device)
-                tmp_in = (field_t / d) * m
-            conv = torch.empty_like(field_t)
-            _dense(lib, plan, tmp_in, conv, code)
-            if epilogue == _lib.STEAM_EPI_STORE:
-                out_t.copy_(conv)
-                return None
-            return _flux_epilogue_dense(out_t, conv, window)
-        _dense(lib, plan, field_t, out_t, code)
-        return None
-    nbytes = lib.steam_conv_workspace_bytes(code, nx, ny, nz, ctypes.byref(plan.spec))
-    ws = _lib.WORKSPACE.get(nbytes)
+    stream = _lib.stream() if stream is None else stream
+    if workspace is None:
+        workspace = _lib.WORKSPACE.get(plan_workspace_bytes(plan, code, field_t.shape))
+    wsp, wsn = _lib.ptr(workspace), workspace.numel()
+    pre = _lib.ptr(pre_dev) if hasattr(pre_dev, 'data_ptr') else pre_dev
+    win = _lib.window_arg(window)
+    if plan.kind == 'separable':
+        _lib.check(lib.steam_conv_separable_async(
+            code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps, plan.x_taps,
+            _lib.ptr(field_t), pre, _lib.ptr(out_t), epilogue, win, sums_dev, wsp, wsn, stream))
+        return
+    data = _device_data(plan, field_t)
+    kx, ky, kz = plan.shape
+    cx, cy = plan.centre
+    if plan.kind == 'fft':
+        _lib.check(lib.steam_conv_fft_async(
+            nx, ny, nz, kx, ky, kz, cx, cy, _lib.ptr(data[0]), _lib.ptr(field_t), pre,
+            _lib.ptr(out_t), epilogue, win, sums_dev, wsp, wsn, stream))
+    else:
+        _lib.check(lib.steam_conv_direct_async(
+            code, nx, ny, nz, _lib.ptr(data[0]), kx, ky, kz, cx, cy, _lib.ptr(field_t), pre,
+            _lib.ptr(out_t), epilogue, win, sums_dev, wsp, wsn, stream))
+
+
+def run_plan(plan, field_t, out_t, pre_div=None, pre_mul=None,
+             epilogue=_lib.STEAM_EPI_STORE, window=None):
+    """Launch a planned convolution on device tensors; returns the epilogue
+    sums (flux epilogue: sum F over the window, cells, clip count) or None."""
+    lib = _lib.load()
+    nx, ny, nz = (int(n) for n in field_t.shape)
+    code = _lib.dtype_code(field_t)
+    ws = _lib.WORKSPACE.get(plan_workspace_bytes(plan, code, field_t.shape))
     sums = _lib.dout(3)
     pd = _lib.dvec(pre_div) if pre_div is not None else None
     pm = _lib.dvec(pre_mul) if pre_mul is not None else None
-    _lib.check(lib.steam_conv_separable(
-        code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps, plan.x_taps,
-        _lib.ptr(field_t), pd, pm, _lib.ptr(out_t), epilogue, _lib.window_arg(window),
-        sums, _lib.ptr(ws), ws.numel(), _lib.stream()))
+    win = _lib.window_arg(window)
+    if plan.kind == 'separable':
+        _lib.check(lib.steam_conv_separable(
+            code, nx, ny, nz, ctypes.byref(plan.spec), plan.z_taps, plan.y_taps, plan.x_taps,
+            _lib.ptr(field_t), pd, pm, _lib.ptr(out_t), epilogue, win, sums, _lib.ptr(ws),
+            ws.numel(), _lib.stream()))
+    else:
+        data = _device_data(plan, field_t)
+        kx, ky, kz = plan.shape
+        cx, cy = plan.centre
+        if plan.kind == 'fft':
+            _lib.check(lib.steam_conv_fft(
+                nx, ny, nz, kx, ky, kz, cx, cy, _lib.ptr(data[0]), _lib.ptr(field_t), pd, pm,
+                _lib.ptr(out_t), epilogue, win, sums, _lib.ptr(ws), ws.numel(), _lib.stream()))
+        else:
+            _lib.check(lib.steam_conv_direct(
+                code, nx, ny, nz, _lib.ptr(data[0]), kx, ky, kz, cx, cy, _lib.ptr(field_t), pd,
+                pm, _lib.ptr(out_t), epilogue, win, sums, _lib.ptr(ws), ws.numel(),
+                _lib.stream()))
     if epilogue == _lib.STEAM_EPI_FLUX:
         return (sums[0], sums[1], sums[2])
     return None
-
-
-def _dense(lib, plan, field_t, out_t, code):
-    import torch
-    key = (field_t.dtype, field_t.device)
-    if plan.dense_dev is None or plan.dense_dev[0] != key:
-        plan.dense_dev = (key, torch.as_tensor(plan.dense, dtype=field_t.dtype,
-                                               device=field_t.device).contiguous())
-    kdev = plan.dense_dev[1]
-    nx, ny, nz = (int(n) for n in field_t.shape)
-    kx, ky, kz = plan.shape
-    _lib.check(lib.steam_conv_dense(code, nx, ny, nz, _lib.ptr(kdev), kx, ky, kz,
-                                    _lib.ptr(field_t), _lib.ptr(out_t), _lib.stream()))
-
-
-def _flux_epilogue_dense(flux_t, conv_t, window):
-    """F = max(F + conv, 0) with the flux epilogue's sums, for the dense path."""
-    flux_t.add_(conv_t)
-    n_clipped = int((flux_t < 0).sum().item())
-    flux_t.clamp_(min=0)
-    inner = flux_t if window is None else flux_t[window[0]:window[1], window[2]:window[3]]
-    return (float(inner.sum(dtype=flux_t.new_zeros(()).double().dtype).item()),
-            float(inner.numel()), float(n_clipped))
 
 
 def convolve_device(field_t, kernel, out=None, tol=None):

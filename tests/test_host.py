@@ -96,7 +96,16 @@ def test_factorisation_of_turbulon_kernels(golden):
     plan = U.plan_convolution(golden["kern_s1"], (64, 64, 32), np.float32)
     assert plan.kind == 'separable' and plan.spec.n_pairs == 4
     rnd = np.random.default_rng(3).standard_normal((7, 7, 7))
-    assert U.plan_convolution(rnd, (16, 16, 16), np.float32).kind == 'dense'
+    assert U.plan_convolution(rnd, (16, 16, 16), np.float32).kind == 'fft'
+    assert U.plan_convolution(rnd, (16, 16, 16), np.float64).kind == 'direct'
+    morlet = O.turbulon_envelope(1, 0.5, 0.5, 0.5, shape='morlet_omega0_6', dtype=np.float64)
+    # the Morlet turbulon factors to Tucker rank 3 at float32 tolerance, beyond
+    # the fused separable kernel: the FFT form; at float64 tolerance it does not
+    assert U.plan_convolution(morlet, (64, 64, 32), np.float32).kind == 'fft'
+    assert U.plan_convolution(morlet, (64, 64, 32), np.float64).kind == 'direct'
+    wide = np.random.default_rng(4).standard_normal((27, 5, 5))
+    p = U.plan_convolution(wide, (16, 16, 16), np.float32)
+    assert p.kind == 'direct' and p.centre == (U.effective_centre(27, 16), 2)
 
 
 def test_turbulon_plan_has_three_filter_pairs():
