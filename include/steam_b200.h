@@ -214,6 +214,19 @@ int steam_tile_extract(int dtype, int64_t nx, int64_t ny, int64_t nz, const void
                        int64_t oz, double scale, int32_t fill, void* out,
                        steam_stream_t stream);
 
+/* ---- output composition ---------------------------------------------------
+ * field = clamp(field + add[z], lo, hi): the mean-profile add and bound clamp
+ * of _compose_output (steam/simulate.py:3586-3598).  add is a HOST per-level
+ * vector. */
+int steam_add_levels_clamp(int dtype, int64_t nx, int64_t ny, int64_t nz, void* field,
+                           const double* add, double lo, double hi, steam_stream_t stream);
+
+/* ---- z-major slab ---------------------------------------------------------
+ * out[z][x][y] = field[x][y][z0 + z] for z < dz: the level-major layout the
+ * streamed output writes (steam/streaming.py:1462-1692), on the device. */
+int steam_slab_zmajor(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* field,
+                      int64_t z0, int64_t dz, void* out, steam_stream_t stream);
+
 /* ---- level-weighted accumulate ------------------------------------------
  * acc += coef[z] * (a - b), or coef[z] * a when b is NULL: the compensation
  * deficit update of cascade_loop (steam/simulate.py:1917, 2024).  coef is a
@@ -415,6 +428,14 @@ int steam_pattern_norm_async(int dtype, int64_t nz, const double* level_sums_dev
  * -1 (the host raises).  Otherwise the launch sequence is fixed (one stats
  * sweep, n_rescale rescale sweeps, 48 shift sweeps, one apply sweep) and
  * sweeps whose phase has ended exit at once. */
+/* The persistent phases' grid barrier: how many polls (with a short sleep
+ * each) a block waits for the others before it gives up, records the error
+ * and leaves (the ledger's sweep count becomes -1; the synchronous entry
+ * returns STEAM_ERR_CUDA).  0 restores the default (2^26 polls, seconds).
+ * Applies to calls enqueued after it, process-wide.  No counterpart in the
+ * reference, whose bounded add has no device-side wait. */
+int steam_set_barrier_spin_limit(int64_t polls);
+
 int steam_bounded_add_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
                             const double* mean_dev, void* increment, double phi_min,
                             double phi_max, const steam_window_t* window, int32_t n_rescale,

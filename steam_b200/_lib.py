@@ -94,6 +94,10 @@ _SIGNATURES = {
                                           c_vp, c_vp]),
     "steam_accumulate_levels": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                                c_vp, c_vp, c_dp, c_vp]),
+    "steam_add_levels_clamp": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_dp,
+                                              c_dbl, c_dbl, c_vp]),
+    "steam_slab_zmajor": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i64, c_i64,
+                                         c_vp, c_vp]),
     "steam_level_sums_workspace_bytes": (c_size, [c_i64]),
     "steam_level_sums": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                         ctypes.POINTER(Window), c_dp, c_vp, c_size, c_vp]),
@@ -109,6 +113,7 @@ _SIGNATURES = {
     "steam_bounded_add": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_dp,
                                          c_vp, c_dbl, c_dbl, ctypes.POINTER(Window), c_i32,
                                          c_i32, c_dp, c_vp, c_size, c_vp]),
+    "steam_set_barrier_spin_limit": (ctypes.c_int, [c_i64]),
     "steam_project_bounds": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_dp,
                                             c_dbl, c_dbl, ctypes.POINTER(Window), c_dp,
                                             c_vp, c_size, c_vp]),

@@ -144,6 +144,65 @@ extern "C" int steam_accumulate_levels(int dtype, int64_t nx, int64_t ny,
   return fail(STEAM_ERR_ARG, "steam_accumulate_levels: bad dtype");
 }
 
+// ---- output composition: add a level profile and clamp -------------------------
+template <typename T>
+__global__ void add_levels_clamp_kernel(int64_t n, int64_t nz, T* __restrict__ f,
+                                        const T* __restrict__ add, T lo, T hi) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T v = f[i] + add[i % nz];
+    v = v < lo ? lo : v;
+    f[i] = v > hi ? hi : v;
+  }
+}
+
+template <typename T>
+static int add_levels_clamp_impl(int64_t n, int64_t nz, void* f, const double* add, double lo,
+                                 double hi, cudaStream_t s) {
+  T* dadd = nullptr;
+  STEAM_CUDA(cudaMallocAsync((void**)&dadd, sizeof(T) * nz, s));
+  std::vector<T> h(nz);
+  for (int64_t z = 0; z < nz; ++z) h[z] = (T)add[z];
+  cudaError_t e = cudaMemcpyAsync(dadd, h.data(), sizeof(T) * nz, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // h dies with this frame
+  if (e == cudaSuccess) {
+    add_levels_clamp_kernel<T><<<stride_grid(n, 1024), 256, 0, s>>>(n, nz, (T*)f, dadd, (T)lo,
+                                                                    (T)hi);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(dadd, s);
+  if (e != cudaSuccess)
+    return fail(STEAM_ERR_CUDA, std::string("steam_add_levels_clamp: ") + cudaGetErrorString(e));
+  return STEAM_OK;
+}
+
+// ---- z-major slab of a field (x, y, z) -> (z, x, y) ----------------------------
+// The field as a matrix [nx*ny columns][nz levels]; a 32 x 32 tile goes
+// through shared memory so both the reads (along z) and the writes (along
+// the columns) are coalesced.
+template <typename T>
+__global__ void __launch_bounds__(256) slab_zmajor_kernel(const T* __restrict__ f, int64_t ncol,
+                                                          int64_t nz, int64_t z0, int64_t dz,
+                                                          T* __restrict__ out) {
+  __shared__ T tile[32][33];
+  const int64_t ctiles = (ncol + 31) / 32, ztiles = (dz + 31) / 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int64_t t = blockIdx.x; t < ctiles * ztiles; t += gridDim.x) {
+    const int64_t c0 = (t / ztiles) * 32, zt0 = (t % ztiles) * 32;
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const int64_t c = c0 + r, z = zt0 + tx;
+      if (c < ncol && z < dz) tile[r][tx] = f[c * nz + z0 + z];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const int64_t z = zt0 + r, c = c0 + tx;
+      if (c < ncol && z < dz) out[z * ncol + c] = tile[tx][r];
+    }
+  }
+}
+
 // ---- flux advance, device-side finish ---------------------------------------------
 // The volume-mean restore of the flux advance (steam/simulate.py:2204-2218)
 // with its scalars read from device memory: every thread derives the same
@@ -274,5 +333,43 @@ extern "C" int steam_tile_extract(int dtype, int64_t nx, int64_t ny, int64_t nz,
   else
     return fail(STEAM_ERR_ARG, "steam_tile_extract: bad dtype");
   STEAM_LAUNCH_CHECK("steam_tile_extract");
+  return STEAM_OK;
+}
+
+extern "C" int steam_add_levels_clamp(int dtype, int64_t nx, int64_t ny, int64_t nz, void* field,
+                                      const double* add, double lo, double hi,
+                                      steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_add_levels_clamp: negative extent");
+  STEAM_REQUIRE(lo <= hi, "steam_add_levels_clamp: lower bound above the upper");
+  const int64_t n = nx * ny * nz;
+  if (n == 0) return STEAM_OK;
+  STEAM_REQUIRE(field && add, "steam_add_levels_clamp: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32) return add_levels_clamp_impl<float>(n, nz, field, add, lo, hi, s);
+  if (dtype == STEAM_F64) return add_levels_clamp_impl<double>(n, nz, field, add, lo, hi, s);
+  return fail(STEAM_ERR_ARG, "steam_add_levels_clamp: bad dtype");
+}
+
+extern "C" int steam_slab_zmajor(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                 const void* field, int64_t z0, int64_t dz, void* out,
+                                 steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0 && dz >= 0,
+                "steam_slab_zmajor: negative extent");
+  STEAM_REQUIRE(z0 >= 0 && z0 + dz <= nz, "steam_slab_zmajor: levels outside the field");
+  const int64_t ncol = nx * ny;
+  if (ncol * dz == 0) return STEAM_OK;
+  STEAM_REQUIRE(field && out, "steam_slab_zmajor: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t tiles = ((ncol + 31) / 32) * ((dz + 31) / 32);
+  const int grid = stride_grid(tiles, 1, 8);
+  if (dtype == STEAM_F32)
+    slab_zmajor_kernel<float><<<grid, 256, 0, s>>>((const float*)field, ncol, nz, z0, dz,
+                                                   (float*)out);
+  else if (dtype == STEAM_F64)
+    slab_zmajor_kernel<double><<<grid, 256, 0, s>>>((const double*)field, ncol, nz, z0, dz,
+                                                    (double*)out);
+  else
+    return fail(STEAM_ERR_ARG, "steam_slab_zmajor: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_slab_zmajor");
   return STEAM_OK;
 }

@@ -8,6 +8,8 @@
 // partials are reduced in a fixed order, so sums are reproducible.
 #include "common.cuh"
 
+#include <atomic>
+
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -1153,6 +1155,7 @@ struct BAState {
   // [1 + R + it] mu sweep it (it < kMuMaxSweeps); [kFlagSweeps] sweeps run
   int* flags;
   unsigned* bar;  // grid barrier of the persistent phases: arrivals, generation, error
+  long long spin_limit;  // polls a block waits at that barrier before it gives up
   int R, nz;
   double N, width, tol_rel;
   double* ledger;  // [nz][5]: a0, n_loop, final demean, mu (NaN if none), sweeps
@@ -1370,8 +1373,9 @@ __global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int 
 // bound: a block that waits past kBarSpinLimit polls records an error, and
 // every block leaves at its next barrier.
 constexpr long long kBarSpinLimit = 1ll << 26;  // ~ seconds with the back-off below
+std::atomic<long long> g_bar_spin_limit{kBarSpinLimit};
 
-__device__ bool grid_barrier(unsigned* bar) {
+__device__ bool grid_barrier(unsigned* bar, long long spin_limit) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1388,7 +1392,7 @@ __device__ bool grid_barrier(unsigned* bar) {
     } else {
       long long spins = 0;
       while (*vgen == g) {
-        if (*verr || ++spins > kBarSpinLimit) {
+        if (*verr || ++spins > spin_limit) {
           atomicExch(bar + 2, 1u);
           ok_s = 0;
           break;
@@ -1416,7 +1420,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_
     // read after a barrier: every block sees the same flag
     if (__ldcg(st.flags + flag_base + it) == 0) break;
     ba_fold_body<T, MODE, true>(d0, pert, 0, nx, ny, nz, w, c, partials, ba_smem, red);
-    if (!grid_barrier(st.bar)) return;
+    if (!grid_barrier(st.bar, st.spin_limit)) return;
     // totals[r] = the r-th row of block partials, summed in a fixed order
     for (int r = blockIdx.x; r < Q * nz; r += nb) {
       double acc = 0.0;
@@ -1424,7 +1428,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_
       const double sum = block_sum(acc, red);
       if (threadIdx.x == 0) totals[r] = sum;
     }
-    if (!grid_barrier(st.bar)) return;
+    if (!grid_barrier(st.bar, st.spin_limit)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
     for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += nb * blockDim.x) {
       if (MODE == BA_MU)
@@ -1432,7 +1436,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_
       else
         ba_loop_level<T, true>(st, totals, it, z);
     }
-    if (!grid_barrier(st.bar)) return;
+    if (!grid_barrier(st.bar, st.spin_limit)) return;
   }
 }
 
@@ -1528,6 +1532,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
   st.R = R;
   st.nz = (int)nz;
+  st.spin_limit = g_bar_spin_limit.load();
   st.N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
   st.width = phi_max - phi_min;
   st.tol_rel = sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49);
@@ -2216,6 +2221,16 @@ extern "C" int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
     return fail(STEAM_ERR_ARG, "steam_bounded_add: bad dtype");
   if (rc) return rc;
   if (!ledger_out) STEAM_CUDA(cudaStreamSynchronize(s));
+  else if (nz > 0 && ledger_out[4] < 0)
+    return fail(STEAM_ERR_CUDA,
+                "steam_bounded_add: a persistent phase gave up at a grid barrier (its blocks "
+                "waited past the spin limit); the perturbation is partly updated");
+  return STEAM_OK;
+}
+
+extern "C" int steam_set_barrier_spin_limit(int64_t polls) {
+  STEAM_REQUIRE(polls >= 0, "steam_set_barrier_spin_limit: negative poll count");
+  g_bar_spin_limit.store(polls == 0 ? kBarSpinLimit : (long long)polls);
   return STEAM_OK;
 }
 

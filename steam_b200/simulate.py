@@ -561,14 +561,12 @@ def compose_output_device(state_t, deficit_t, mean_1d, phi_min, phi_max, window=
         _accumulate(deficit_t, state_t, None, ones)
         projection = project_device(deficit_t, mean_1d, phi_min, phi_max, window)
         out = deficit_t
-    m = torch.as_tensor(np.asarray(mean_1d, dtype=np_t), device=out.device)
-    _accumulate(out, _broadcast_levels(m, out), None, ones)
-    out.clamp_(min=float(np_t(phi_min)), max=float(np_t(phi_max)))
+    nx, ny, nz = (int(n) for n in out.shape)
+    mean = np.asarray(mean_1d, dtype=np_t).astype(np.float64)
+    _lib.check(_lib.load().steam_add_levels_clamp(
+        _lib.dtype_code(out), nx, ny, nz, _lib.ptr(out), _lib.dvec(mean),
+        float(np_t(phi_min)), float(np_t(phi_max)), _lib.stream()))
     return out, projection
-
-
-def _broadcast_levels(m, like):
-    return m.view(1, 1, -1).expand(like.shape).contiguous()
 
 
 def _compose_output(state, deficit, mean_1d, phi_min, phi_max, window=None,

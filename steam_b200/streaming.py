@@ -174,6 +174,9 @@ def write_field(store, index, name, field_t, slab_levels=8):
     slab = max(1, min(int(slab_levels), nz))
     bufs = [torch.empty((slab, nx, ny), dtype=field_t.dtype, pin_memory=True)
             for _ in range(2)]
+    zmaj = torch.empty((slab, nx, ny), dtype=field_t.dtype, device=field_t.device)
+    lib = _lib.load()
+    code = _lib.dtype_code(field_t)
     done = [torch.cuda.Event(), torch.cuda.Event()]
     side = torch.cuda.Stream()
     side.wait_stream(torch.cuda.current_stream())
@@ -183,9 +186,11 @@ def write_field(store, index, name, field_t, slab_levels=8):
         z0 = starts[k]
         z1 = min(nz, z0 + slab)
         with torch.cuda.stream(side):
-            # the (x, y, z) -> (z, x, y) reorder runs on the device
-            view = field_t[:, :, z0:z1].permute(2, 0, 1).contiguous()
-            bufs[k % 2][:z1 - z0].copy_(view, non_blocking=True)
+            # the (x, y, z) -> (z, x, y) reorder runs on the device; the copy
+            # of slab k - 1 out of zmaj precedes this launch on the same stream
+            _lib.check(lib.steam_slab_zmajor(code, nx, ny, nz, _lib.ptr(field_t), z0, z1 - z0,
+                                             _lib.ptr(zmaj), _lib.stream()))
+            bufs[k % 2][:z1 - z0].copy_(zmaj[:z1 - z0], non_blocking=True)
             done[k % 2].record(side)
 
     issue(0)
