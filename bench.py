@@ -603,7 +603,6 @@ def main(argv=None):
     if args.serve_requests > 0:
         from steam_b200.serving import TileServer, TileWorld, latency_summary, poisson_trace
         tw = TileWorld((args.nx, args.ny, args.nz), seed=7, dtype=np_t)
-        tw.drop_world_field()
         torch.cuda.empty_cache()
         srv = TileServer(tw, n_slots=4, max_n=min(256, args.nz))
         srv.serve(poisson_trace(tw, rate=1000.0, n_requests=16, seed=5))  # warm-up

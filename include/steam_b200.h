@@ -292,8 +292,12 @@ int steam_scalar_pattern(int dtype, int64_t nx, int64_t ny, int64_t nz,
  * sweeps.  pert += delta; with record_applied the increment buffer is left
  * holding pert_after - pert_before, otherwise it is scratch (the sweeps store
  * the chain's running state there; its contents on return are unspecified).
- * ledger_out (HOST, may be NULL) receives per level { a0, n_loop,
- * final_demean, mu (NaN if none), n_sweeps }. */
+ * ledger_out (HOST, may be NULL) receives per level a record of
+ * steam_bounded_add_ledger_doubles(n_rescale) doubles: { a0, n_loop,
+ * final_demean, mu (NaN if none), n_sweeps, chain steps, final clip set,
+ * demean[n_rescale], scale[n_rescale] } -- the last four the per-level chain
+ * that steam_bounded_add_replay applies. */
+size_t steam_bounded_add_ledger_doubles(int32_t n_rescale);
 size_t steam_bounded_add_workspace_bytes(int64_t nz, int32_t n_rescale);
 int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
                       void* pert, const double* mean_1d, void* increment,
@@ -428,6 +432,36 @@ int steam_pattern_norm_async(int dtype, int64_t nz, const double* level_sums_dev
  * -1 (the host raises).  Otherwise the launch sequence is fixed (one stats
  * sweep, n_rescale rescale sweeps, 48 shift sweeps, one apply sweep) and
  * sweeps whose phase has ended exit at once. */
+/* Apply-only replay of a recorded projection (the replay branch of
+ * _project_onto_bounds, steam/simulate.py:3462-3488): levels whose recorded
+ * mu (HOST, nz doubles) is not NaN become clip(pert + mean - mu, lo, hi) -
+ * mean; the others are left bit-identical.  Workspace as steam_project_bounds. */
+int steam_project_bounds_replay(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
+                                const double* mean_1d, double phi_min, double phi_max,
+                                const double* mu, void* workspace, size_t workspace_bytes,
+                                steam_stream_t stream);
+
+/* Apply-only replay of a recorded bounded add (the APPLY-ONLY branch of
+ * _bounded_amplitude_add, steam/simulate.py:3196-3213, and
+ * _bounded_amplitude_add_cuda's replay): per level, the recorded demeans,
+ * clips, scales, final demean and shift are applied to the increment with no
+ * reduction, then pert += delta (with record_applied the increment is left
+ * holding pert_after - pert_before).  Any subset of the columns of the field
+ * that recorded the ledger -- a tile of the world -- replays to the same
+ * values there, bit for bit.  ledger (HOST [nz][ledger_doubles]) and mean_1d
+ * (HOST) in the synchronous form, both DEVICE in the async one. */
+size_t steam_bounded_add_replay_workspace_bytes(int64_t nz, int32_t n_rescale);
+int steam_bounded_add_replay(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
+                             const double* mean_1d, void* increment, double phi_min,
+                             double phi_max, int32_t n_rescale, int32_t record_applied,
+                             const double* ledger, void* workspace, size_t workspace_bytes,
+                             steam_stream_t stream);
+int steam_bounded_add_replay_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
+                                   const double* mean_dev, void* increment, double phi_min,
+                                   double phi_max, int32_t n_rescale, int32_t record_applied,
+                                   const double* ledger_dev, void* workspace,
+                                   size_t workspace_bytes, steam_stream_t stream);
+
 /* The persistent phases' grid barrier: how many polls (with a short sleep
  * each) a block waits for the others before it gives up, records the error
  * and leaves (the ledger's sweep count becomes -1; the synchronous entry

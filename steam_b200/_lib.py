@@ -114,6 +114,17 @@ _SIGNATURES = {
                                          c_vp, c_dbl, c_dbl, ctypes.POINTER(Window), c_i32,
                                          c_i32, c_dp, c_vp, c_size, c_vp]),
     "steam_set_barrier_spin_limit": (ctypes.c_int, [c_i64]),
+    "steam_bounded_add_ledger_doubles": (c_size, [c_i32]),
+    "steam_project_bounds_replay": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
+                                                   c_dp, c_dbl, c_dbl, c_dp, c_vp, c_size,
+                                                   c_vp]),
+    "steam_bounded_add_replay_workspace_bytes": (c_size, [c_i64, c_i32]),
+    "steam_bounded_add_replay": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_dp,
+                                                c_vp, c_dbl, c_dbl, c_i32, c_i32, c_dp, c_vp,
+                                                c_size, c_vp]),
+    "steam_bounded_add_replay_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
+                                                      c_vp, c_vp, c_dbl, c_dbl, c_i32, c_i32,
+                                                      c_vp, c_vp, c_size, c_vp]),
     "steam_project_bounds": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_dp,
                                             c_dbl, c_dbl, ctypes.POINTER(Window), c_dp,
                                             c_vp, c_size, c_vp]),

@@ -1158,8 +1158,14 @@ struct BAState {
   long long spin_limit;  // polls a block waits at that barrier before it gives up
   int R, nz;
   double N, width, tol_rel;
-  double* ledger;  // [nz][5]: a0, n_loop, final demean, mu (NaN if none), sweeps
+  double* ledger;  // [nz][ba_ledger_width(R)], see ba_finish_kernel
 };
+
+// Per-level ledger record: a0, n_loop, final demean, mu (NaN if none), sweeps
+// of the whole solve, then the chain the apply sweep replays -- its step
+// count, whether the final clip is set, the steps' demeans [R] and scales [R]
+// (each the working dtype's value, exact in float64).
+__host__ __device__ inline int ba_ledger_width(int R) { return 7 + 2 * R; }
 
 template <typename T>
 __host__ __device__ inline int ba_flag_count(int R) {
@@ -1454,12 +1460,19 @@ __global__ void ba_finish_kernel(BAState<T> st) {
       st.mu[z] = (T)mu;
     }
     if (st.ledger) {
-      double* l = st.ledger + 5 * (size_t)z;
+      const int R = st.R;
+      double* l = st.ledger + (size_t)ba_ledger_width(R) * z;
       l[0] = st.a0[z];
       l[1] = st.n_loop[z];
       l[2] = st.active[z] ? st.final_d[z] : 0.0;
       l[3] = mu;
       l[4] = sweeps;
+      l[5] = st.nsteps[z];
+      l[6] = st.has_final[z];
+      for (int k = 0; k < R; ++k) {
+        l[7 + k] = (double)st.demean[(size_t)z * R + k];
+        l[7 + R + k] = (double)st.scale[(size_t)z * R + k];
+      }
     }
   }
 }
@@ -1472,7 +1485,7 @@ static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
          carve_bytes((size_t)nz * sizeof(MuSolver<double>), 1) +
          carve_bytes((size_t)(2 + R + kMuMaxSweeps), sizeof(int)) +
          carve_bytes(4, sizeof(unsigned)) +
-         carve_bytes((size_t)5 * nz, sizeof(double)) +                      // ledger
+         carve_bytes((size_t)ba_ledger_width(R) * nz, sizeof(double)) +     // ledger
          carve_bytes((size_t)nz, sizeof(double)) +                          // mean upload
          carve_bytes((size_t)nz / 4 + 1, sizeof(int)) +                     // grp
          (size_t)32 * 256;  // the 256-byte alignment of every separate carve
@@ -1523,7 +1536,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   st.solver = c.take<MuSolver<T>>(nz);
   st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
   st.bar = c.take<unsigned>(4);
-  st.ledger = c.take<double>((size_t)5 * nz);
+  st.ledger = c.take<double>((size_t)ba_ledger_width(R) * nz);
   if (!partials || !totals || !st.nsteps || !st.has_final || !st.has_mu || !st.demean ||
       !st.scale || !st.final_dm || !st.mu || !st.mean || !st.cand || !st.a0 || !st.cur_mean ||
       !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.applied ||
@@ -1706,6 +1719,157 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   STEAM_LAUNCH_CHECK("bounded_add finish");
   // apply (always runs)
   if ((rc = sweep(BA_APPLY, nullptr, inc, record))) return rc;
+  return STEAM_OK;
+}
+
+// ---- apply-only replay of a recorded bounded add -------------------------------
+// steam/simulate.py:3196-3213 (the APPLY-ONLY branch): given the per-level
+// chain a solve recorded, the increment is taken through the same demeans,
+// clips, scales, final demean and shift with no reduction at all, so any
+// subset of the columns (a tile of the world that recorded it) replays to
+// the same bits as the solve produced there.
+template <typename T>
+__global__ void ba_chain_from_ledger_kernel(BAState<T> st, const double* __restrict__ led,
+                                            const double* __restrict__ mean_dev) {
+  const int nz = st.nz, R = st.R, W = ba_ledger_width(R);
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
+    const double* l = led + (size_t)W * z;
+    st.nsteps[z] = (int)l[5];
+    st.has_final[z] = (int)l[6];
+    st.final_dm[z] = (T)l[2];
+    const bool hm = !isnan(l[3]);
+    st.has_mu[z] = hm ? 1 : 0;
+    st.mu[z] = hm ? (T)l[3] : (T)0;
+    st.mean[z] = (T)mean_dev[z];
+    for (int k = 0; k < kMuCand; ++k) st.cand[(size_t)z * kMuCand + k] = (T)0;
+    for (int k = 0; k < R; ++k) {
+      st.demean[(size_t)z * R + k] = (T)l[7 + k];
+      st.scale[(size_t)z * R + k] = (T)l[7 + R + k];
+    }
+  }
+}
+
+static size_t ba_replay_bytes(int64_t nz, int R, size_t elem) {
+  return carve_bytes((size_t)3 * nz, sizeof(int)) +
+         carve_bytes((size_t)nz * (2 * (size_t)R + 3 + kMuCand), elem) +
+         carve_bytes((size_t)nz, sizeof(double)) +                       // mean upload
+         carve_bytes((size_t)ba_ledger_width(R) * nz, sizeof(double)) +  // ledger upload
+         (size_t)16 * 256;
+}
+
+template <typename T>
+static int bounded_add_replay_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
+                                   const double* mean, int mean_on_device, T* inc,
+                                   double phi_min, double phi_max, int R, int record,
+                                   const double* led, int led_on_device, void* ws,
+                                   size_t ws_bytes, cudaStream_t s) {
+  Carver c(ws, ws_bytes);
+  BAState<T> st{};
+  st.nsteps = c.take<int>(nz);
+  st.has_final = c.take<int>(nz);
+  st.has_mu = c.take<int>(nz);
+  st.demean = c.take<T>((size_t)nz * (R > 0 ? R : 1));
+  st.scale = c.take<T>((size_t)nz * (R > 0 ? R : 1));
+  st.final_dm = c.take<T>(nz);
+  st.mu = c.take<T>(nz);
+  st.mean = c.take<T>(nz);
+  st.cand = c.take<T>((size_t)nz * kMuCand);
+  const double* mean_dev = mean;
+  const double* led_dev = led;
+  if (!mean_on_device) {
+    double* up = c.take<double>(nz);
+    if (!up) return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_replay: workspace too small");
+    STEAM_CUDA(cudaMemcpyAsync(up, mean, sizeof(double) * nz, cudaMemcpyHostToDevice, s));
+    mean_dev = up;
+  }
+  if (!led_on_device) {
+    double* up = c.take<double>((size_t)ba_ledger_width(R) * nz);
+    if (!up) return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_replay: workspace too small");
+    STEAM_CUDA(cudaMemcpyAsync(up, led, sizeof(double) * ba_ledger_width(R) * nz,
+                               cudaMemcpyHostToDevice, s));
+    led_dev = up;
+  }
+  if (!st.nsteps || !st.has_final || !st.has_mu || !st.demean || !st.scale || !st.final_dm ||
+      !st.mu || !st.mean || !st.cand)
+    return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_replay: workspace too small");
+  st.R = R;
+  st.nz = (int)nz;
+  const int lv_blocks = (int)((nz + 255) / 256);
+  ba_chain_from_ledger_kernel<T><<<lv_blocks, 256, 0, s>>>(st, led_dev, mean_dev);
+  STEAM_LAUNCH_CHECK("bounded_add replay chain");
+  BAChain<T> ch{};
+  ch.nsteps = st.nsteps;
+  ch.demean = st.demean;
+  ch.scale = st.scale;
+  ch.has_final = st.has_final;
+  ch.final_dm = st.final_dm;
+  ch.has_mu = st.has_mu;
+  ch.mu = st.mu;
+  ch.cand = st.cand;
+  ch.mean = st.mean;
+  ch.run = nullptr;
+  ch.R = R;
+  ch.lo = (T)phi_min;
+  ch.hi = (T)phi_max;
+  const LevelMap m = make_map(nz);
+  const int grid = level_grid(nx * ny, m);
+  const Win w = make_win(nullptr, nx, ny);
+  const size_t ba_sm = ba_smem_bytes<T>(nz, R);
+  STEAM_REQUIRE(ba_sm <= 200 * 1024, "steam_bounded_add_replay: n_rescale * nz too large");
+  if (m.packed) {
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, 1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    ba_sweep_kernel<T, BA_APPLY, 1><<<grid, kLvThreads, ba_sm, s>>>(
+        inc, pert, inc, record, nx, ny, m, w, ch, nullptr);
+  } else {
+    STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, kLvMaxJ>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
+    ba_sweep_kernel<T, BA_APPLY, kLvMaxJ><<<grid, kLvThreads, ba_sm, s>>>(
+        inc, pert, inc, record, nx, ny, m, w, ch, nullptr);
+  }
+  STEAM_LAUNCH_CHECK("bounded_add replay");
+  return STEAM_OK;
+}
+
+// Apply-only replay of a recorded projection (steam/simulate.py:3462-3488):
+// the levels with a recorded shift become clip(field - mu, lo, hi), the rest
+// stay bit-identical.
+template <typename T>
+static int project_replay_impl(int64_t nx, int64_t ny, int64_t nz, T* pert,
+                               const double* mean_1d, double lo, double hi,
+                               const double* mu_in, void* ws, size_t ws_bytes,
+                               cudaStream_t s) {
+  const LevelMap m = make_map(nz);
+  const int grid = level_grid(nx * ny, m);
+  const Win w = make_win(nullptr, nx, ny);
+  Carver c(ws, ws_bytes);
+  double* d_mean = c.take<double>(nz);
+  int* d_active = c.take<int>(nz);
+  double* d_mu = c.take<double>(nz);
+  if (!d_mean || !d_active || !d_mu)
+    return fail(STEAM_ERR_WORKSPACE, "steam_project_bounds_replay: workspace too small");
+  std::vector<double> h_mean(mean_1d, mean_1d + nz), h_mu(nz, 0.0);
+  std::vector<int> active(nz, 0);
+  bool any = false;
+  for (int64_t z = 0; z < nz; ++z) {
+    if (std::isnan(mu_in[z])) continue;
+    active[z] = 1;
+    h_mu[z] = mu_in[z];
+    any = true;
+  }
+  if (!any) return STEAM_OK;
+  int rc;
+  if ((rc = upload(d_mean, h_mean, s))) return rc;
+  if ((rc = upload(d_active, active, s))) return rc;
+  if ((rc = upload(d_mu, h_mu, s))) return rc;
+  if (m.packed)
+    proj_sweep_kernel<T, PJ_APPLY, 1><<<grid, kLvThreads, 0, s>>>(
+        pert, d_mean, lo, hi, d_active, d_mu, nullptr, nx, ny, m, w, nullptr);
+  else
+    proj_sweep_kernel<T, PJ_APPLY, kLvMaxJ><<<grid, kLvThreads, 0, s>>>(
+        pert, d_mean, lo, hi, d_active, d_mu, nullptr, nx, ny, m, w, nullptr);
+  STEAM_LAUNCH_CHECK("project replay sweep");
+  STEAM_CUDA(cudaStreamSynchronize(s));
   return STEAM_OK;
 }
 
@@ -2181,16 +2345,16 @@ static int bounded_add_entry(int64_t nx, int64_t ny, int64_t nz, T* pert,
   int rc = bounded_add_enqueue<T>(nx, ny, nz, pert, mean_dev, inc, phi_min, phi_max, window, R,
                                   record, c, &led, s);
   if (rc) return rc;
+  const size_t led_bytes = sizeof(double) * ba_ledger_width(R) * nz;
   if (ledger_dev)
-    STEAM_CUDA(cudaMemcpyAsync(ledger_dev, led, sizeof(double) * 5 * nz,
-                               cudaMemcpyDeviceToDevice, s));
+    STEAM_CUDA(cudaMemcpyAsync(ledger_dev, led, led_bytes, cudaMemcpyDeviceToDevice, s));
   if (ledger_host) {
-    STEAM_CUDA(cudaMemcpyAsync(ledger_host, led, sizeof(double) * 5 * nz,
-                               cudaMemcpyDeviceToHost, s));
+    STEAM_CUDA(cudaMemcpyAsync(ledger_host, led, led_bytes, cudaMemcpyDeviceToHost, s));
     STEAM_CUDA(cudaStreamSynchronize(s));
     if (nz > 0 && ledger_host[4] < 0)
-      return fail(STEAM_ERR_CUDA, "steam_bounded_add: a persistent phase's grid barrier "
-                                  "timed out");
+      return fail(STEAM_ERR_CUDA, "steam_bounded_add: a persistent phase gave up at a grid "
+                                  "barrier (its blocks waited past the spin limit); the "
+                                  "perturbation is partly updated");
   }
   return STEAM_OK;
 }
@@ -2221,10 +2385,6 @@ extern "C" int steam_bounded_add(int dtype, int64_t nx, int64_t ny, int64_t nz,
     return fail(STEAM_ERR_ARG, "steam_bounded_add: bad dtype");
   if (rc) return rc;
   if (!ledger_out) STEAM_CUDA(cudaStreamSynchronize(s));
-  else if (nz > 0 && ledger_out[4] < 0)
-    return fail(STEAM_ERR_CUDA,
-                "steam_bounded_add: a persistent phase gave up at a grid barrier (its blocks "
-                "waited past the spin limit); the perturbation is partly updated");
   return STEAM_OK;
 }
 
@@ -2403,4 +2563,78 @@ extern "C" int steam_level_sums_noalloc(int dtype, int64_t nx, int64_t ny, int64
                              cudaMemcpyDeviceToHost, s));
   STEAM_CUDA(cudaStreamSynchronize(s));
   return STEAM_OK;
+}
+
+extern "C" size_t steam_bounded_add_ledger_doubles(int32_t n_rescale) {
+  return n_rescale < 0 ? 0 : (size_t)ba_ledger_width(n_rescale);
+}
+
+extern "C" size_t steam_bounded_add_replay_workspace_bytes(int64_t nz, int32_t n_rescale) {
+  return ba_replay_bytes(nz, n_rescale, sizeof(double));
+}
+
+static int replay_entry(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
+                        const double* mean, int mean_dev, void* increment, double phi_min,
+                        double phi_max, int32_t n_rescale, int32_t record,
+                        const double* ledger, int led_dev, void* ws, size_t ws_bytes,
+                        steam_stream_t stream, const char* who) {
+  int rc = bounded_add_check(nx, ny, nz, n_rescale, phi_min, phi_max, nullptr, who);
+  if (rc) return rc;
+  if (nx * ny * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(pert && increment && mean && ledger, std::string(who) + ": null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    return bounded_add_replay_impl<float>(nx, ny, nz, (float*)pert, mean, mean_dev,
+                                          (float*)increment, phi_min, phi_max, n_rescale,
+                                          record, ledger, led_dev, ws, ws_bytes, s);
+  if (dtype == STEAM_F64)
+    return bounded_add_replay_impl<double>(nx, ny, nz, (double*)pert, mean, mean_dev,
+                                           (double*)increment, phi_min, phi_max, n_rescale,
+                                           record, ledger, led_dev, ws, ws_bytes, s);
+  return fail(STEAM_ERR_ARG, std::string(who) + ": bad dtype");
+}
+
+extern "C" int steam_bounded_add_replay(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                        void* pert, const double* mean_1d, void* increment,
+                                        double phi_min, double phi_max, int32_t n_rescale,
+                                        int32_t record_applied, const double* ledger,
+                                        void* workspace, size_t workspace_bytes,
+                                        steam_stream_t stream) {
+  int rc = replay_entry(dtype, nx, ny, nz, pert, mean_1d, 0, increment, phi_min, phi_max,
+                        n_rescale, record_applied, ledger, 0, workspace, workspace_bytes,
+                        stream, "steam_bounded_add_replay");
+  if (rc) return rc;
+  STEAM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  return STEAM_OK;
+}
+
+extern "C" int steam_bounded_add_replay_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                              void* pert, const double* mean_dev,
+                                              void* increment, double phi_min,
+                                              double phi_max, int32_t n_rescale,
+                                              int32_t record_applied, const double* ledger_dev,
+                                              void* workspace, size_t workspace_bytes,
+                                              steam_stream_t stream) {
+  return replay_entry(dtype, nx, ny, nz, pert, mean_dev, 1, increment, phi_min, phi_max,
+                      n_rescale, record_applied, ledger_dev, 1, workspace, workspace_bytes,
+                      stream, "steam_bounded_add_replay_async");
+}
+
+extern "C" int steam_project_bounds_replay(int dtype, int64_t nx, int64_t ny, int64_t nz,
+                                           void* pert, const double* mean_1d, double phi_min,
+                                           double phi_max, const double* mu, void* workspace,
+                                           size_t workspace_bytes, steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_project_bounds_replay: negative extent");
+  STEAM_REQUIRE(nz <= kLvThreads * kLvMaxJ, "steam_project_bounds_replay: nz above 1024");
+  STEAM_REQUIRE(phi_max > phi_min, "steam_project_bounds_replay: phi_max must exceed phi_min");
+  if (nx * ny * nz == 0) return STEAM_OK;
+  STEAM_REQUIRE(pert && mean_1d && mu, "steam_project_bounds_replay: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == STEAM_F32)
+    return project_replay_impl<float>(nx, ny, nz, (float*)pert, mean_1d, phi_min, phi_max, mu,
+                                      workspace, workspace_bytes, s);
+  if (dtype == STEAM_F64)
+    return project_replay_impl<double>(nx, ny, nz, (double*)pert, mean_1d, phi_min, phi_max,
+                                       mu, workspace, workspace_bytes, s);
+  return fail(STEAM_ERR_ARG, "steam_project_bounds_replay: bad dtype");
 }

@@ -75,32 +75,76 @@ class FluxAdvanceLedger:
 
 
 class BoundedAddLedger:
-    """Per-level results of one bounded-add solve (steam/ledger.py:145-194).
+    """Per-level results of one bounded-add solve (steam/ledger.py:145-194):
+    the target amplitude a0, the loop's demeans and scales, the loop length
+    n_loop and rescale count n_scale, the final demean and the zero-mean
+    shift mu (NaN where none was needed) -- the sequence that replays the
+    solve with no reduction (steam/simulate.py:3196-3213) -- plus how many
+    field sweeps the device solve took.
 
-    The device solve records the target amplitude a0, the loop length, the
-    final demean and the zero-mean shift mu (NaN where none was needed), plus
-    how many field sweeps the solve took.
+    ``demean`` and ``scale`` (nz, n_rescale) hold the values the device's
+    chain applied, in the working dtype (exact in float64); a step that was
+    not rescaled carries scale 1, which multiplies exactly.
     """
 
-    __slots__ = ('a0', 'n_loop', 'final_demean', 'mu', 'n_sweeps')
+    __slots__ = ('a0', 'demean', 'scale', 'n_loop', 'n_scale', 'final_demean', 'mu',
+                 'n_sweeps', 'n_steps', 'has_final')
 
-    def __init__(self, nz):
+    def __init__(self, nz, n_rescale=10):
         self.a0 = np.zeros(nz, dtype=np.float64)
+        self.demean = np.zeros((nz, n_rescale), dtype=np.float64)
+        self.scale = np.ones((nz, n_rescale), dtype=np.float64)
         self.n_loop = np.zeros(nz, dtype=np.int32)
+        self.n_scale = np.zeros(nz, dtype=np.int32)
         self.final_demean = np.zeros(nz, dtype=np.float64)
         self.mu = np.full(nz, np.nan, dtype=np.float64)
         self.n_sweeps = 0
+        self.n_steps = np.zeros(nz, dtype=np.int32)
+        self.has_final = np.zeros(nz, dtype=np.int32)
+
+    @staticmethod
+    def record_doubles(n_rescale):
+        """Doubles per level of the device record (the C-ABI's
+        steam_bounded_add_ledger_doubles)."""
+        return 7 + 2 * int(n_rescale)
 
     @classmethod
-    def from_device(cls, packed):
-        packed = np.asarray(packed, dtype=np.float64).reshape(-1, 5)
-        out = cls(packed.shape[0])
+    def from_device(cls, packed, n_rescale=10):
+        R = int(n_rescale)
+        packed = np.asarray(packed, dtype=np.float64).reshape(-1, cls.record_doubles(R))
+        out = cls(packed.shape[0], R)
         out.a0[:] = packed[:, 0]
         out.n_loop[:] = packed[:, 1].astype(np.int32)
         out.final_demean[:] = packed[:, 2]
         out.mu[:] = packed[:, 3]
         out.n_sweeps = int(packed[0, 4]) if packed.shape[0] else 0
+        out.n_steps[:] = packed[:, 5].astype(np.int32)
+        out.has_final[:] = packed[:, 6].astype(np.int32)
+        out.demean[:] = packed[:, 7:7 + R]
+        out.scale[:] = packed[:, 7 + R:7 + 2 * R]
+        steps = np.arange(R)[None, :]
+        out.n_scale[:] = np.count_nonzero((out.scale != 1.0) & (steps < out.n_steps[:, None]),
+                                          axis=1)
         return out
+
+    def to_device(self):
+        """The packed per-level record the replay entry points read."""
+        nz, R = self.demean.shape
+        packed = np.zeros((nz, self.record_doubles(R)), dtype=np.float64)
+        packed[:, 0] = self.a0
+        packed[:, 1] = self.n_loop
+        packed[:, 2] = self.final_demean
+        packed[:, 3] = self.mu
+        packed[:, 4] = self.n_sweeps
+        packed[:, 5] = self.n_steps
+        packed[:, 6] = self.has_final
+        packed[:, 7:7 + R] = self.demean
+        packed[:, 7 + R:7 + 2 * R] = self.scale
+        return packed
+
+    @property
+    def n_rescale(self):
+        return self.demean.shape[1]
 
     @property
     def clip_only(self):

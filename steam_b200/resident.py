@@ -74,11 +74,14 @@ class ResidentClass:
         h_min, h_max, qt_min, qt_max = setup.bounds
         self.bounds = [float(self.np_t(v)) for v in (h_min, h_max, qt_min, qt_max)]
         # ledger block: noise sums [3] | conv sums [2] | flux ledger [10] |
-        # pattern sums h, qt [2][nz] each | bounded-add ledger h, qt [nz][5] each
+        # pattern sums h, qt [2][nz] each | bounded-add ledger h, qt [nz][W]
+        # each (W = BoundedAddLedger.record_doubles(N_RESCALE))
+        W = BoundedAddLedger.record_doubles(N_RESCALE)
+        self.ba_width = W
         self.o_ns, self.o_cs, self.o_fl = 0, 3, 5
         self.o_ps = {'h': 15, 'qt': 15 + 2 * nz}
-        self.o_ba = {'h': 15 + 4 * nz, 'qt': 15 + 9 * nz}
-        n_led = 15 + 14 * nz
+        self.o_ba = {'h': 15 + 4 * nz, 'qt': 15 + 4 * nz + W * nz}
+        n_led = 15 + 4 * nz + 2 * W * nz
         self.ledger = torch.zeros(n_led, **f64)
         self.ledger_host = torch.empty(n_led, dtype=torch.float64, pin_memory=True)
         self.ledger_ready = torch.cuda.Event()
@@ -109,8 +112,49 @@ class ResidentClass:
             self.work = tuple(torch.empty_like(like) for _ in range(3))
         return self.work
 
+    def workspace_bytes(self):
+        """Scratch one step takes from the stream's workspace."""
+        lib, code = self.lib, self.code
+        nx, ny, nz = self.shape
+        return max(lib.steam_flux_noise_workspace_bytes(),
+                   _utils.plan_workspace_bytes(self.setup.plan, code, self.shape),
+                   lib.steam_scalar_pattern_workspace_bytes(nx, ny, nz),
+                   lib.steam_bounded_add_workspace_bytes(nz, N_RESCALE),
+                   lib.steam_bounded_add_replay_workspace_bytes(nz, N_RESCALE))
+
+    def set_origin(self, origin, world_shape):
+        """Place this class's box at ``origin`` of a world of ``world_shape``
+        (the world-keyed noise is evaluated at world coordinates)."""
+        from . import simulate as sim
+        cs = self.setup
+        region = sim.NoiseRegion(cs.region.key, tuple(int(v) for v in origin),
+                                 tuple(int(v) for v in world_shape))
+        self.region = sim._region_struct(region, self.shape, cs.sparsity)
+
+    def replay_block(self, world_block, world_cells, world_nz):
+        """This class's ledger layout filled from the ledger block of a class
+        over more levels (``world_nz``; the same layout there): the flux
+        sums, and the per-level pattern sums and bounded-add chains of this
+        class's levels, which are the world's first nz.  For a box of the
+        world that starts at its ground; the result is what ``step(...,
+        replay=)`` reads."""
+        import torch
+        nz, W = self.shape[2], self.ba_width
+        if world_nz < nz:
+            raise ValueError(f"replay: the world has {world_nz} levels, this class {nz}")
+        blk = torch.zeros_like(self.ledger)
+        blk[:15] = world_block[:15]
+        for name in ('h', 'qt'):
+            w0 = 15 if name == 'h' else 15 + 2 * world_nz
+            o = self.o_ps[name]
+            blk[o:o + nz] = world_block[w0:w0 + nz]
+            blk[o + nz:o + 2 * nz] = world_block[w0 + world_nz:w0 + world_nz + nz]
+            wb = 15 + 4 * world_nz + (0 if name == 'h' else W * world_nz)
+            blk[self.o_ba[name]:self.o_ba[name] + W * nz] = world_block[wb:wb + W * nz]
+        return ReplayBlock(blk, float(world_cells))
+
     def step(self, hp, qp, F, diagnostics=None, surface_pressure=101325.0, ready=None,
-             done=None, before_thermo=(), copy_ledger=True):
+             done=None, before_thermo=(), copy_ledger=True, replay=None, work=None):
         """Enqueue one class step on the resident fields (mutated in place)
         and, with ``diagnostics`` (a dict of tensors T, qv, qc, qi, p), the
         composition + thermodynamics.  Returns without waiting on the GPU.
@@ -122,7 +166,17 @@ class ResidentClass:
         ``before_thermo`` (copies still reading the diagnostic buffers).
         ``copy_ledger=False`` leaves the ledger block on the device (a caller
         that copies it on its own stream); ``done['end']`` then marks the
-        step's end."""
+        step's end.
+
+        ``replay`` (a ``ReplayBlock``, see ``replay_block``) makes the step
+        apply-only: the flux restore and the signed-amplitude scale come from
+        its flux sums and cell count, the second convolution's per-level
+        normalisation from its pattern sums, and each bounded add replays its
+        recorded chain -- no realized scalar of this field is used, so a box
+        cut from a larger field gives that field's values on every cell far
+        enough from the box's sides (the kernel's support plus the pattern
+        stencil).  ``work``: three field-shaped tensors (the product, the
+        pattern and the increment) to use instead of this class's own."""
         import torch
         lib, cs, code = self.lib, self.setup, self.code
         nx, ny, nz = self.shape
@@ -130,16 +184,14 @@ class ResidentClass:
             if tuple(t.shape) != self.shape or t.dtype != self.dtype or not t.is_contiguous():
                 raise ValueError("resident class step: fields must be contiguous "
                                  f"{self.shape} {self.dtype} CUDA tensors")
-        product, W, inc = self._work(F)
+        product, W, inc = self._work(F) if work is None else work
         stream = _lib.stream()
         win = _lib.window_arg(cs.window)
         L = self.ledger
         plan = cs.plan
-        ws = _lib.WORKSPACE.get(max(
-            lib.steam_flux_noise_workspace_bytes(),
-            _utils.plan_workspace_bytes(plan, code, self.shape),
-            lib.steam_scalar_pattern_workspace_bytes(nx, ny, nz),
-            lib.steam_bounded_add_workspace_bytes(nz, N_RESCALE)))
+        ws = _lib.WORKSPACE.get(self.workspace_bytes())
+        src = L if replay is None else replay.block
+        cells = self.cells if replay is None else replay.cells
         wsp, wsn = _lib.ptr(ws), ws.numel()
         # flux advance
         _lib.check(lib.steam_flux_noise_async(
@@ -149,7 +201,7 @@ class ResidentClass:
         _utils.run_plan_async(plan, product, F, None, _lib.STEAM_EPI_FLUX, cs.window,
                               _off(L, self.o_cs), ws, stream)
         _lib.check(lib.steam_flux_finish_async(
-            code, F.numel(), _lib.ptr(F), _off(L, self.o_ns), _off(L, self.o_cs), self.cells,
+            code, F.numel(), _lib.ptr(F), _off(src, self.o_ns), _off(src, self.o_cs), cells,
             _off(L, self.o_fl), stream))
         if done is not None:
             done['F'] = torch.cuda.Event()
@@ -165,13 +217,20 @@ class ResidentClass:
                 _off(L, self.o_fl + 7), float(cs.dx), float(cs.dy), _lib.dvec(self.z), 1,
                 float(lo), float(hi), _lib.ptr(W), win, ps, wsp, wsn, stream))
             _lib.check(lib.steam_pattern_norm_async(
-                code, nz, ps, _lib.ptr(self.mul[name]), _lib.ptr(self.pre[name]), stream))
+                code, nz, _off(src, self.o_ps[name]), _lib.ptr(self.mul[name]),
+                _lib.ptr(self.pre[name]), stream))
             _utils.run_plan_async(plan, W, inc, self.pre[name], _lib.STEAM_EPI_STORE,
                                   cs.window, None, ws, stream)
-            _lib.check(lib.steam_bounded_add_async(
-                code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
-                float(lo), float(hi), win, N_RESCALE, 0, _off(L, self.o_ba[name]), wsp, wsn,
-                stream))
+            if replay is None:
+                _lib.check(lib.steam_bounded_add_async(
+                    code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
+                    float(lo), float(hi), win, N_RESCALE, 0, _off(L, self.o_ba[name]), wsp,
+                    wsn, stream))
+            else:
+                _lib.check(lib.steam_bounded_add_replay_async(
+                    code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
+                    float(lo), float(hi), N_RESCALE, 0, _off(replay.block, self.o_ba[name]),
+                    wsp, wsn, stream))
             if done is not None:
                 done[name] = torch.cuda.Event()
                 done[name].record()
@@ -313,11 +372,23 @@ class ResidentClass:
             ps = v[self.o_ps[name]:self.o_ps[name] + 2 * nz]
             cl.pattern[name] = PatternLedger(ps[:nz].copy(), ps[nz:].astype(np.int64))
             cl.bounded_add[name] = BoundedAddLedger.from_device(
-                v[self.o_ba[name]:self.o_ba[name] + 5 * nz])
+                v[self.o_ba[name]:self.o_ba[name] + self.ba_width * nz], N_RESCALE)
             if cl.bounded_add[name].n_sweeps < 0:
                 raise RuntimeError(f"resident class step: the {name} bounded add's "
                                    f"persistent phase timed out at a grid barrier")
         return cl
+
+
+class ReplayBlock:
+    """A ledger block in a ResidentClass's layout plus the cell count its
+    flux sums were taken over: the realized scalars an apply-only step
+    uses."""
+
+    __slots__ = ('block', 'cells')
+
+    def __init__(self, block, cells):
+        self.block = block
+        self.cells = float(cells)
 
 
 class PendingHostStep:

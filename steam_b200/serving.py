@@ -1,26 +1,36 @@
-"""Serving world-coordinate tiles of the flux field with continuous batching.
+"""Serving world-coordinate tiles of the full class step with continuous batching.
 
-A ``TileWorld`` is one class of a STEAM world: its grid, its Philox key, its
-turbulon kernel and its world ledger -- the flux advance's realized restore
-factor, measured once over the whole world (the measure/apply split of
-steam/ledger.py:115-142 and of the tiled driver steam/streaming.py:850-1447,
-where per-class scalars are realized over the domain and applied per tile).
-A tile request (world origin, cube size n) is computed from its own box: the
-tile plus the kernel's halo of 6 cells per side (12 s + 1 = 13 taps at
-sparsity 1; steam/streaming.py:707 uses the same 6 s + 1 halo), with the
-world-keyed noise evaluated at world coordinates, so a tile equals the same
-cells of the whole-world field bit for bit, alone or in any mix.
+A ``TileWorld`` is one class of a STEAM world -- the finest class (k = 200 m,
+dx = dz = 100 m) of a root run over the world's shape with its seed and
+parameters -- stepped once from rest (h' = qt' = 0, F = 1) over the whole
+world: the flux advance, both scalar branches with the second convolution and
+the bounded add, and the thermodynamic map to condensate.  What that step
+realized over the whole world -- the flux restore and signed-amplitude
+scale, the pattern's per-level sums, both bounded adds' per-level chains --
+is its world ledger (the measure/apply split of steam/ledger.py:46-270 and of
+the tiled driver steam/streaming.py:1139-1280), kept on the device.
+
+A tile request (world origin, cube size n) is computed apply-only from a box
+of the world: the tile plus a halo of 7 cells per side in x and y (the
+kernel's half width 6 and one for the pattern's stencil: the kernel//2 + 1
+rule of steam/streaming.py:707), and in z every level from the ground to
+7 above the tile (the thermodynamic column march starts at the surface).
+The box's step evaluates the world-keyed noise at world coordinates and
+takes every realized scalar from the world ledger, so each field of the
+tile (h', qt', F, qc, qi) equals the same cells of the world's step bit for
+bit, alone or in any mix.
 
 ``TileServer`` admits requests as they arrive: a request starts when one of
-its CUDA streams is free and the bytes of all requests in flight stay under a
-device-memory budget (by default half of the HBM free at start); requests in
-flight overlap on the device.  Each tile is downloaded into a page-locked
-host buffer of its slot; latency is arrival to download complete.
+its CUDA-stream slots is free and the bytes of all requests in flight stay
+under a device-memory budget (by default half of the HBM free at start);
+requests in flight overlap on the device.  Each tile's five fields land in a
+page-locked host buffer of its slot with one copy; latency is arrival to
+that copy's completion.  Every device buffer a request touches is sized and
+allocated before the first request is admitted (``prepare``).
 """
 
 from __future__ import annotations
 
-import ctypes
 import gc
 import time
 from collections import deque
@@ -31,127 +41,110 @@ from . import _lib
 from . import simulate as sim
 from . import utils as _utils
 
-HALO = 6  # (13 - 1) / 2: the sparsity-1 turbulon kernel's half width
+HALO = 7   # the sparsity-1 kernel's half width (6) + the pattern stencil (1)
+FIELDS = ('h', 'qt', 'flux', 'qc', 'qi')
 
 
 class TileWorld:
-    """One class of a world: the finest class of a root run over
-    ``shape`` (dx = dz = 100 m, turbulon size k = 200 m) with seed ``seed``."""
+    """One class of a world over ``shape`` (seed, alpha, C1, H, Hz), stepped
+    once from rest; its world ledger stays on the device.  ``keep_fields``
+    keeps the world's own step (for checking tiles against it)."""
 
-    def __init__(self, shape, seed=7, alpha=sim.FLUX_ALPHA, c1=0.1, n_per_dyad=1,
-                 dtype=np.float32, min_distance_to_ground=1):
+    def __init__(self, shape, seed=7, alpha=sim.FLUX_ALPHA, c1=0.1, H=1.0 / 3.0,
+                 Hz=5.0 / 9.0, dtype=np.float32, keep_fields=False):
         torch = _lib.require_cuda("TileWorld")
+        from .ensemble import member_setup
+        from .resident import ResidentClass
         self.lib = _lib.load()
         self.shape = tuple(int(n) for n in shape)
-        nx, ny, nz = self.shape
         self.np_t = np.dtype(dtype).type
         self.dtype = torch.float64 if self.np_t == np.float64 else torch.float32
-        self.code = _lib.dtype_code(torch.empty(0, dtype=self.dtype))
-        outer = nx * 100.0
-        n_classes = int(round(np.log(outer / 200.0) / np.log(2.0))) + 1
-        self.key = sim.class_key(np.random.SeedSequence(seed).spawn(n_classes)[-1])
+        self.code = _lib.STEAM_F64 if self.np_t == np.float64 else _lib.STEAM_F32
+        self.setup = member_setup(self.shape, seed, alpha, c1, H, Hz, self.np_t)
         self.kernel = sim._turbulon_envelope(1, 0.5, 0.5, 0.5, dtype=np.float64)
-        self.alpha = float(alpha)
-        pcs = c1 / n_per_dyad ** (1.0 / alpha)
-        self.pcs = float(self.np_t(pcs))
-        self.shift = float(self.np_t(sim.levy_log_mean(alpha) * pcs ** alpha))
-        self.n_zero = int(round(2 * min_distance_to_ground))
-        self.factor, self.fill = self._world_ledger()
+        rc = ResidentClass(self.setup, self.dtype)
+        f = dict(dtype=self.dtype, device='cuda')
+        h = torch.zeros(self.shape, **f)
+        q = torch.zeros(self.shape, **f)
+        F = torch.ones(self.shape, **f)
+        diag = {k: torch.empty(self.shape, **f) for k in ("T", "qv", "qc", "qi", "p")}
+        rc.step(h, q, F, diagnostics=diag)
+        self.ledger = rc.class_ledger()   # raises if a persistent phase gave up
+        self.block = rc.ledger.clone()    # the world ledger, device
+        self.cells = rc.cells
+        self.fields = ({'h': h, 'qt': q, 'flux': F, 'qc': diag['qc'], 'qi': diag['qi']}
+                       if keep_fields else None)
+        del rc, diag
+        torch.cuda.empty_cache()
 
-    def region(self, origin, box):
-        r = _lib.Region()
-        for a in range(3):
-            r.shape[a] = int(box[a])
-            r.origin[a] = int(origin[a])
-            r.world[a] = int(self.shape[a])
-            r.sparsity[a] = 1
-            r.key[a] = int(self.key[a]) & 0xFFFFFFFF
-        return r
+    def world_field(self, name='flux'):
+        """A field of the world's own step (device; ``keep_fields`` only)."""
+        if self.fields is None:
+            raise RuntimeError("TileWorld: built without keep_fields")
+        return self.fields[name]
 
-    def advance(self, F, product, origin, box, sums, zero_bottom, zero_top, ws, stream):
-        """F = max(F + T * (eps F), 0) on a box at a world origin (enqueued)."""
-        lib = self.lib
-        nx, ny, nz = box
-        region = self.region(origin, box)
-        _lib.check(lib.steam_flux_noise_async(
-            self.code, ctypes.byref(region), self.alpha, self.pcs, self.shift, self.n_zero,
-            int(zero_bottom), int(zero_top), _lib.ptr(F), _lib.ptr(product), None,
-            _lib.ptr(sums), _lib.ptr(ws), ws.numel(), stream))
-        plan = _utils.plan_convolution(self.kernel, box, self.np_t)
-        _utils.run_plan_async(plan, product, F, None, _lib.STEAM_EPI_FLUX, None,
-                              ctypes.c_void_p(sums.data_ptr() + 24), ws, stream)
-
-    def workspace_bytes(self, box):
-        lib = self.lib
-        plan = _utils.plan_convolution(self.kernel, box, self.np_t)
-        return max(lib.steam_flux_noise_workspace_bytes(),
-                   _utils.plan_workspace_bytes(plan, self.code, box))
-
-    def _world_ledger(self):
-        """The restore factor realized over the whole world (one advance)."""
-        torch = _lib.require_cuda("TileWorld")
-        F = torch.ones(self.shape, dtype=self.dtype, device='cuda')
-        product = torch.empty_like(F)
-        sums = torch.zeros(8, dtype=torch.float64, device='cuda')
-        ledger = torch.zeros(10, dtype=torch.float64, device='cuda')
-        ws = torch.empty(self.workspace_bytes(self.shape), dtype=torch.uint8, device='cuda')
-        stream = _lib.stream()
-        self.advance(F, product, (0, 0, 0), self.shape, sums, True, True, ws, stream)
-        cells = float(F.numel())
-        _lib.check(self.lib.steam_flux_finish_async(
-            self.code, F.numel(), _lib.ptr(F), _lib.ptr(sums),
-            ctypes.c_void_p(sums.data_ptr() + 24), cells, _lib.ptr(ledger), stream))
-        led = ledger.cpu().numpy()
-        self.world_ledger = led
-        self._world_F = F  # kept only while the caller asks for it (world_field)
-        return float(led[8]), int(led[9])
-
-    def world_field(self):
-        """The whole-world advanced flux of the ledger measurement (device)."""
-        return self._world_F
-
-    def drop_world_field(self):
-        self._world_F = None
-
-    def box_depth(self, n):
-        """Most levels a tile box of an n-cube spans (halo, plus the zeroed
-        bottom/top bands pulled in whole)."""
-        return min(self.shape[2], n + 2 * HALO + 2 * self.n_zero)
+    def drop_world_fields(self):
+        self.fields = None
 
     def tile_box(self, origin, n):
-        """(box origin, box shape, z offset of the tile in the box, zero flags)."""
+        """(box origin, box shape, the tile's first level) of a tile: the
+        tile plus HALO in x and y (wrapping in the world), and the levels
+        from the ground to at least HALO above the tile.  The box's level
+        count is a multiple of 4 exactly when the world's is: the kernels
+        pick their vectorised forms by that, and the box must run the same
+        arithmetic as the world to reproduce its bits."""
         x0, y0, z0 = (int(v) for v in origin)
-        nz = self.shape[2]
-        if not (0 <= z0 and z0 + n <= nz):
+        nx, ny, nz = self.shape
+        if not (n >= 1 and 0 <= z0 and z0 + n <= nz):
             raise ValueError(f"tile z range [{z0}, {z0 + n}) outside [0, {nz})")
-        bz0 = max(0, z0 - HALO)
-        if bz0 < self.n_zero:  # the zeroed bottom levels sit at the box bottom
-            bz0 = 0
-        bz1 = min(nz, z0 + n + HALO)
-        if bz1 > nz - self.n_zero:
-            bz1 = nz
-        return ((x0 - HALO) % self.shape[0], (y0 - HALO) % self.shape[1], bz0), \
-            (n + 2 * HALO, n + 2 * HALO, bz1 - bz0), z0 - bz0, bz0 == 0, bz1 == nz
+        bz = min(nz, z0 + n + HALO)
+        if nz % 4 == 0:
+            bz = min(nz, (bz + 3) // 4 * 4)
+        elif bz % 4 == 0 and bz < nz:
+            bz += 1
+        return ((x0 - HALO) % nx, (y0 - HALO) % ny, 0), (n + 2 * HALO, n + 2 * HALO, bz), z0
+
+    def box_setup(self, box_shape):
+        """The class set-up of a box of ``box_shape`` that starts at the
+        ground: the world's per-level vectors for its levels (its origin is
+        set per request)."""
+        s = self.setup
+        nzb = int(box_shape[2])
+        return s._replace(
+            shape=tuple(int(v) for v in box_shape), z=s.z[:nzb], h_mean=s.h_mean[:nzb],
+            qt_mean=s.qt_mean[:nzb], C_h=s.C_h[:nzb], C_qt=s.C_qt[:nzb], b_h=s.b_h[:nzb],
+            b_qt=s.b_qt[:nzb], aspect=s.aspect[:nzb],
+            region=sim.NoiseRegion(s.region.key, (0, 0, 0), self.shape),
+            plan=_utils.plan_convolution(self.kernel, box_shape, self.np_t),
+            zero_bottom=True, zero_top=nzb == self.shape[2], window=None, deficit=None)
+
+    def box_bytes(self, n):
+        """Device bytes one request of an n-cube may hold: its box's state
+        (3), work (3) and diagnostic (5) fields over full columns, and the
+        tile's five fields."""
+        elem = 8 if self.np_t == np.float64 else 4
+        return elem * (11 * (n + 2 * HALO) ** 2 * self.shape[2] + 5 * n ** 3)
 
 
 class _Slot:
+    """A CUDA stream with buffers for the largest box and tile."""
+
     def __init__(self, world, max_n, torch):
         self.stream = torch.cuda.Stream()
-        nbox = max_n + 2 * HALO
-        zbox = world.box_depth(max_n)
-        cap = nbox * nbox * zbox
-        self.F = torch.empty(cap, dtype=world.dtype, device='cuda')
-        self.product = torch.empty(cap, dtype=world.dtype, device='cuda')
-        self.sums = torch.zeros(8, dtype=torch.float64, device='cuda')
-        ws = max(world.workspace_bytes((nbox, nbox, zbox)), 1)
-        self.ws = torch.empty(ws, dtype=torch.uint8, device='cuda')
-        # the tile's cells, contiguous, then page-locked: both sized once here so
-        # serving allocates nothing (a first allocation on a stream blocks the
-        # host loop for tens of ms)
-        self.out = torch.empty(max_n ** 3, dtype=world.dtype, device='cuda')
-        self.host = torch.empty(max_n ** 3, dtype=world.dtype, pin_memory=True)
+        nb = max_n + 2 * HALO
+        cap = nb * nb * world.shape[2]
+        f = dict(dtype=world.dtype, device='cuda')
+        self.buf = {k: torch.empty(cap, **f)
+                    for k in ('h', 'qt', 'F', 'product', 'W', 'inc', 'T', 'qv', 'qc', 'qi', 'p')}
+        self.out = torch.empty(5 * max_n ** 3, **f)
+        self.host = torch.empty(5 * max_n ** 3, dtype=world.dtype, pin_memory=True)
         self.event = torch.cuda.Event()
         self.request = None
+        self.classes = {}  # box shape -> (ResidentClass, ReplayBlock)
+
+    def views(self, box):
+        cnt = box[0] * box[1] * box[2]
+        return {k: v[:cnt].view(box) for k, v in self.buf.items()}
 
 
 class TileServer:
@@ -169,30 +162,7 @@ class TileServer:
         self.in_flight_bytes = 0
 
     def request_bytes(self, n):
-        nbox = n + 2 * HALO
-        elem = 8 if self.world.np_t == np.float64 else 4
-        return 2 * elem * nbox * nbox * self.world.box_depth(n) + elem * n ** 3
-
-    def _launch(self, slot, req):
-        import torch
-        w = self.world
-        origin, n = req['origin'], req['n']
-        borig, box, zoff, zb, zt = w.tile_box(origin, n)
-        cnt = box[0] * box[1] * box[2]
-        F = slot.F[:cnt].view(box)
-        product = slot.product[:cnt].view(box)
-        with torch.cuda.stream(slot.stream):
-            stream = _lib.stream()
-            _lib.check(w.lib.steam_scale(w.code, cnt, _lib.ptr(F), 1.0, 1, stream))
-            w.advance(F, product, borig, box, slot.sums, zb, zt, slot.ws, stream)
-            # the world restore on the tile's cells only, into the contiguous buffer
-            out = slot.out[:n ** 3]
-            _lib.check(w.lib.steam_tile_extract(
-                w.code, box[0], box[1], box[2], _lib.ptr(F), HALO, HALO, zoff, n, n, n,
-                w.factor, w.fill, _lib.ptr(out), stream))
-            slot.host[:n ** 3].copy_(out, non_blocking=True)
-            slot.event.record(slot.stream)
-        slot.request = req
+        return self.world.box_bytes(int(n))
 
     def check_request(self, req):
         """Refuse a request this server cannot hold, before it takes a slot."""
@@ -201,21 +171,83 @@ class TileServer:
             raise ValueError(f"tile size {n} outside [1, {self.max_n}] (the server's max_n)")
         self.world.tile_box(req['origin'], n)  # raises ValueError on a bad z range
 
+    def _class_for(self, slot, box):
+        hit = slot.classes.get(box)
+        if hit is None:
+            import torch
+            from .resident import ResidentClass
+            w = self.world
+            with torch.cuda.stream(slot.stream):
+                rc = ResidentClass(w.box_setup(box), w.dtype)
+                rep = rc.replay_block(w.block, w.cells, w.shape[2])
+                _lib.WORKSPACE.get(rc.workspace_bytes())  # the slot stream's scratch
+            slot.stream.synchronize()
+            hit = (rc, rep)
+            slot.classes[box] = hit
+        return hit
+
+    def prepare(self, requests):
+        """Build, on every slot, the box classes (their per-level vectors,
+        convolution plans and replay blocks) the requests will need, so that
+        serving allocates nothing."""
+        boxes = {self.world.tile_box(r['origin'], int(r['n']))[1] for r in requests}
+        for slot in self.slots:
+            for box in boxes:
+                self._class_for(slot, box)
+
+    def _launch(self, slot, req):
+        import torch
+        w = self.world
+        origin, n = req['origin'], int(req['n'])
+        borig, box, z0 = w.tile_box(origin, n)
+        rc, rep = self._class_for(slot, box)
+        v = slot.views(box)
+        cnt = box[0] * box[1] * box[2]
+        lib, code = w.lib, w.code
+        with torch.cuda.stream(slot.stream):
+            stream = _lib.stream()
+            # the world's rest state on the box
+            _lib.check(lib.steam_scale(code, cnt, _lib.ptr(v['h']), 0.0, 1, stream))
+            _lib.check(lib.steam_scale(code, cnt, _lib.ptr(v['qt']), 0.0, 1, stream))
+            _lib.check(lib.steam_scale(code, cnt, _lib.ptr(v['F']), 1.0, 1, stream))
+            rc.set_origin(borig, w.shape)
+            diag = {k: v[k] for k in ("T", "qv", "qc", "qi", "p")}
+            rc.step(v['h'], v['qt'], v['F'], diagnostics=diag, replay=rep,
+                    work=(v['product'], v['W'], v['inc']), copy_ledger=False)
+            n3 = n ** 3
+            for i, key in enumerate(('h', 'qt', 'F', 'qc', 'qi')):
+                _lib.check(lib.steam_tile_extract(
+                    code, box[0], box[1], box[2], _lib.ptr(v[key]), HALO, HALO, z0, n, n, n,
+                    1.0, 0, _lib.ptr(slot.out[i * n3:(i + 1) * n3]), stream))
+            slot.host[:5 * n3].copy_(slot.out[:5 * n3], non_blocking=True)
+            slot.event.record(slot.stream)
+        slot.request = req
+
+    def _fields(self, slot, n):
+        n3 = n ** 3
+        flat = slot.host[:5 * n3].numpy()
+        return {name: flat[i * n3:(i + 1) * n3].reshape(n, n, n).copy()
+                for i, name in enumerate(FIELDS)}
+
     def tile(self, origin, n):
-        """One tile, alone (synchronous); returns a host array."""
+        """One tile, alone (synchronous); returns {field: host array}."""
         slot = self.slots[0]
         req = {'origin': origin, 'n': int(n)}
         self.check_request(req)
+        self.prepare([req])
         self._launch(slot, req)
         slot.event.synchronize()
         slot.request = None
-        return slot.host[:n ** 3].view(n, n, n).numpy().copy()
+        return self._fields(slot, int(n))
 
     def serve(self, requests, keep=False):
         """Serve ``requests`` (dicts with 'arrival' seconds, 'origin', 'n'),
         admitting each at its arrival time as slots and budget allow.
         Returns the requests with 'start', 'done', 'latency' (seconds) and,
-        with ``keep``, 'tile' (host array)."""
+        with ``keep``, 'tile' ({field: host array})."""
+        for req in requests:
+            self.check_request(req)
+        self.prepare(requests)
         # the host loop is the server's critical path: no collection pauses
         # while requests are in flight
         gc_was = gc.isenabled()
@@ -227,8 +259,6 @@ class TileServer:
                 gc.enable()
 
     def _serve(self, requests, keep):
-        for req in requests:
-            self.check_request(req)
         pending = deque(sorted(requests, key=lambda r: r['arrival']))
         free = list(self.slots)
         busy = []
@@ -260,8 +290,7 @@ class TileServer:
                     req['done'] = time.perf_counter() - t0
                     req['latency'] = req['done'] - req['arrival']
                     if keep:
-                        n = req['n']
-                        req['tile'] = slot.host[:n ** 3].view(n, n, n).numpy().copy()
+                        req['tile'] = self._fields(slot, int(req['n']))
                     self.in_flight_bytes -= req['bytes']
                     slot.request = None
                     busy.remove(slot)

@@ -466,17 +466,31 @@ def _advective_weight(field_3d, dx, dy, z_coords, aspect_z):
 # ---------------------------------------------------------------------------
 
 def bounded_add_device(pert_t, mean_1d, inc_t, phi_min, phi_max, window=None,
-                       n_rescale=10, record_applied=False):
+                       n_rescale=10, record_applied=False, ledger=None):
+    """The bounded add on device tensors; with ``ledger`` (a recorded
+    BoundedAddLedger) the apply-only replay, which reduces nothing and
+    returns that ledger."""
     lib = _lib.load()
     nx, ny, nz = (int(n) for n in pert_t.shape)
-    ws = _lib.WORKSPACE.get(lib.steam_bounded_add_workspace_bytes(nz, int(n_rescale)))
-    led = _lib.dout(5 * nz)
+    if ledger is not None:
+        R = ledger.n_rescale
+        if ledger.a0.shape[0] != nz:
+            raise ValueError(f"bounded-add ledger has {ledger.a0.shape[0]} levels for {nz}")
+        ws = _lib.WORKSPACE.get(lib.steam_bounded_add_replay_workspace_bytes(nz, R))
+        _lib.check(lib.steam_bounded_add_replay(
+            _lib.dtype_code(pert_t), nx, ny, nz, _lib.ptr(pert_t), _lib.dvec(mean_1d),
+            _lib.ptr(inc_t), float(phi_min), float(phi_max), R, int(bool(record_applied)),
+            _lib.dvec(ledger.to_device()), _lib.ptr(ws), ws.numel(), _lib.stream()))
+        return ledger
+    R = int(n_rescale)
+    ws = _lib.WORKSPACE.get(lib.steam_bounded_add_workspace_bytes(nz, R))
+    width = lib.steam_bounded_add_ledger_doubles(R)
+    led = _lib.dout(width * nz)
     _lib.check(lib.steam_bounded_add(
         _lib.dtype_code(pert_t), nx, ny, nz, _lib.ptr(pert_t), _lib.dvec(mean_1d),
         _lib.ptr(inc_t), float(phi_min), float(phi_max), _lib.window_arg(window),
-        int(n_rescale), int(bool(record_applied)), led, _lib.ptr(ws), ws.numel(),
-        _lib.stream()))
-    return BoundedAddLedger.from_device(np.ctypeslib.as_array(led)[:5 * nz])
+        R, int(bool(record_applied)), led, _lib.ptr(ws), ws.numel(), _lib.stream()))
+    return BoundedAddLedger.from_device(np.ctypeslib.as_array(led)[:width * nz], R)
 
 
 def _bounded_amplitude_add(perturbation_field, mean_1d, increment, phi_min, phi_max,
@@ -484,17 +498,15 @@ def _bounded_amplitude_add(perturbation_field, mean_1d, increment, phi_min, phi_
                            ledger=None):
     """Add a class increment under the three deposit conditions
     (steam/simulate.py:3114-3283).  Mutates ``perturbation_field`` (and
-    ``increment`` with record_applied).  Apply-only replay (``ledger``) is not
-    offered by the device solve, which records a0/mu rather than the full
-    rescale sequence."""
+    ``increment`` with record_applied).  With ``ledger`` (a BoundedAddLedger a
+    device solve recorded) the recorded per-level sequence is applied with no
+    reduction (the apply-only replay, steam/simulate.py:3196-3213) and the
+    same ledger is returned."""
     check_device(device, "_bounded_amplitude_add")
-    if ledger is not None:
-        raise NotImplementedError("_bounded_amplitude_add: ledger replay is not implemented "
-                                  "on the device path")
     p_t, p_host = to_device(perturbation_field)
     i_t, i_host = to_device(increment, dtype=p_t.dtype, copy=not record_applied)
     out = bounded_add_device(p_t, mean_1d, i_t, phi_min, phi_max, window, n_rescale,
-                             record_applied)
+                             record_applied, ledger=ledger)
     if p_host is not None:
         to_host(p_t, out=perturbation_field)
     if record_applied and i_host is not None:
@@ -502,10 +514,20 @@ def _bounded_amplitude_add(perturbation_field, mean_1d, increment, phi_min, phi_
     return out
 
 
-def project_device(pert_t, mean_1d, phi_min, phi_max, window=None):
+def project_device(pert_t, mean_1d, phi_min, phi_max, window=None, ledger=None):
+    """The per-level mean-preserving projection on a device tensor; with
+    ``ledger`` (a recorded ProjectionLedger) the apply-only replay."""
     lib = _lib.load()
     nx, ny, nz = (int(n) for n in pert_t.shape)
     ws = _lib.WORKSPACE.get(lib.steam_bounded_add_workspace_bytes(nz, 1))
+    if ledger is not None:
+        if np.asarray(ledger.mu).shape != (nz,):
+            raise ValueError(f"projection ledger has {np.size(ledger.mu)} levels for {nz}")
+        _lib.check(lib.steam_project_bounds_replay(
+            _lib.dtype_code(pert_t), nx, ny, nz, _lib.ptr(pert_t), _lib.dvec(mean_1d),
+            float(phi_min), float(phi_max), _lib.dvec(ledger.mu), _lib.ptr(ws), ws.numel(),
+            _lib.stream()))
+        return ledger
     mu = _lib.dout(nz)
     _lib.check(lib.steam_project_bounds(
         _lib.dtype_code(pert_t), nx, ny, nz, _lib.ptr(pert_t), _lib.dvec(mean_1d),
@@ -517,13 +539,11 @@ def project_device(pert_t, mean_1d, phi_min, phi_max, window=None):
 def _project_onto_bounds(perturbation_field, mean_1d, phi_min, phi_max, window=None,
                          device='cuda', ledger=None):
     """Mean-preserving projection onto [phi_min, phi_max] per level
-    (steam/simulate.py:3417-3489)."""
+    (steam/simulate.py:3417-3489); with ``ledger`` the recorded shifts are
+    applied with no reduction (the replay branch)."""
     check_device(device, "_project_onto_bounds")
-    if ledger is not None:
-        raise NotImplementedError("_project_onto_bounds: ledger replay is not implemented "
-                                  "on the device path")
     t, host = to_device(perturbation_field)
-    out = project_device(t, mean_1d, phi_min, phi_max, window)
+    out = project_device(t, mean_1d, phi_min, phi_max, window, ledger=ledger)
     if host is not None:
         to_host(t, out=perturbation_field)
     return out
@@ -548,9 +568,11 @@ def _level_sums(t, window=None):
     return np.ctypeslib.as_array(out)[:4 * nz].reshape(nz, 4).copy()
 
 
-def compose_output_device(state_t, deficit_t, mean_1d, phi_min, phi_max, window=None):
+def compose_output_device(state_t, deficit_t, mean_1d, phi_min, phi_max, window=None,
+                          ledger=None):
     """state + deficit + mean, projected, clamped (steam/simulate.py:3558-3599).
-    Consumes ``deficit_t`` (it becomes the output)."""
+    Consumes ``deficit_t`` (it becomes the output).  ``ledger``: a recorded
+    ProjectionLedger to replay instead of solving the projection."""
     torch = _lib.require_cuda("_compose_output")
     np_t = np.float64 if state_t.dtype == torch.float64 else np.float32
     projection = None
@@ -559,7 +581,8 @@ def compose_output_device(state_t, deficit_t, mean_1d, phi_min, phi_max, window=
         out = state_t.clone()
     else:
         _accumulate(deficit_t, state_t, None, ones)
-        projection = project_device(deficit_t, mean_1d, phi_min, phi_max, window)
+        projection = project_device(deficit_t, mean_1d, phi_min, phi_max, window,
+                                    ledger=ledger)
         out = deficit_t
     nx, ny, nz = (int(n) for n in out.shape)
     mean = np.asarray(mean_1d, dtype=np_t).astype(np.float64)
@@ -574,26 +597,34 @@ def _compose_output(state, deficit, mean_1d, phi_min, phi_max, window=None,
     check_device(device, "_compose_output")
     s_t, s_host = to_device(state)
     d_t = None if deficit is None else to_device(deficit, dtype=s_t.dtype, copy=True)[0]
-    out, proj = compose_output_device(s_t, d_t, mean_1d, phi_min, phi_max, window)
+    out, proj = compose_output_device(s_t, d_t, mean_1d, phi_min, phi_max, window,
+                                      ledger=ledger)
     return (to_host(out) if s_host is not None else out), proj
 
 
-def compose_flux_output_device(state_t, deficit_t, window=None):
+def compose_flux_output_device(state_t, deficit_t, window=None, ledger=None):
     """Flux state + deficit, clip at 0, volume-mean restore
-    (steam/simulate.py:3602-3649).  Consumes ``deficit_t``."""
+    (steam/simulate.py:3602-3649).  Consumes ``deficit_t``.  ``ledger``: a
+    recorded FluxOutputLedger whose means are applied instead of measured."""
     torch = _lib.require_cuda("_compose_flux_output")
     if deficit_t is None:
         return state_t, None
     lib = _lib.load()
     np_t = np.float64 if state_t.dtype == torch.float64 else np.float32
-    nz = state_t.shape[2]
-    ent = _level_sums(state_t, window)
-    entering = MeanReduction(float(ent[:, 0].sum()), int(ent[:, 3].sum()))
-    _accumulate(deficit_t, state_t, None, np.ones(nz))
-    deficit_t.clamp_(min=0)
-    rea = _level_sums(deficit_t, window)
-    realized = MeanReduction(float(rea[:, 0].sum()), int(rea[:, 3].sum()))
+    nx, ny, nz = (int(n) for n in state_t.shape)
     code = _lib.dtype_code(deficit_t)
+    if ledger is None:
+        ent = _level_sums(state_t, window)
+        entering = MeanReduction(float(ent[:, 0].sum()), int(ent[:, 3].sum()))
+    _accumulate(deficit_t, state_t, None, np.ones(nz))
+    _lib.check(lib.steam_add_levels_clamp(code, nx, ny, nz, _lib.ptr(deficit_t),
+                                          _lib.dvec(np.zeros(nz)), 0.0, float(np.inf),
+                                          _lib.stream()))
+    if ledger is None:
+        rea = _level_sums(deficit_t, window)
+        realized = MeanReduction(float(rea[:, 0].sum()), int(rea[:, 3].sum()))
+    else:
+        entering, realized = ledger.entering, ledger.realized
     if realized.mean > 0:
         _lib.check(lib.steam_scale(code, deficit_t.numel(), _lib.ptr(deficit_t),
                                    float(np_t(entering.mean / realized.mean)), 0, _lib.stream()))
@@ -606,7 +637,7 @@ def compose_flux_output_device(state_t, deficit_t, window=None):
 def _compose_flux_output(state, deficit, window=None, ledger=None):
     s_t, s_host = to_device(state)
     d_t = None if deficit is None else to_device(deficit, dtype=s_t.dtype, copy=True)[0]
-    out, led = compose_flux_output_device(s_t, d_t, window)
+    out, led = compose_flux_output_device(s_t, d_t, window, ledger=ledger)
     if s_host is not None:
         return to_host(out), led
     return out, led
@@ -712,7 +743,8 @@ def run_class(hp, qp, F, dh, dq, dF, cs, cl, increment_dir=None, index=0, reside
         # the applied increment is only needed for a deficit or a record
         record = (dfield is not None and cs.deficit is not None) or increment_dir is not None
         cl.bounded_add[name] = bounded_add_device(pert, mean_1d, inc, lo, hi, cs.window,
-                                                  record_applied=record)
+                                                  record_applied=record,
+                                                  ledger=cl.bounded_add.get(name))
         if dfield is not None and cs.deficit is not None:
             _accumulate(dfield, inc, None, cs.deficit)
         if increment_dir is not None:
@@ -1066,9 +1098,12 @@ def simulate(h_profile, qt_profile, nx, ny, dx, dy, outer_scale, spheroscale,
     z_final = final_grid['z'].astype(np.float32)
     h_mean_final = np.interp(z_final, z_profile, h_profile).astype(np.float32)
     qt_mean_final = np.interp(z_final, z_profile, qt_profile).astype(np.float32)
-    h_3d, proj_h = compose_output_device(h_pert, deficit_h, h_mean_final, h_min, h_max)
-    qt_3d, proj_qt = compose_output_device(qt_pert, deficit_qt, qt_mean_final, qt_min, qt_max)
-    flux_3d, run_ledger.flux_output = compose_flux_output_device(flux_field, deficit_flux)
+    h_3d, proj_h = compose_output_device(h_pert, deficit_h, h_mean_final, h_min, h_max,
+                                         ledger=run_ledger.projection.get('h'))
+    qt_3d, proj_qt = compose_output_device(qt_pert, deficit_qt, qt_mean_final, qt_min, qt_max,
+                                           ledger=run_ledger.projection.get('qt'))
+    flux_3d, run_ledger.flux_output = compose_flux_output_device(
+        flux_field, deficit_flux, ledger=run_ledger.flux_output)
     if proj_h is not None:
         run_ledger.projection['h'] = proj_h
     if proj_qt is not None:
