@@ -114,8 +114,10 @@ int steam_flux_noise(int dtype, const steam_region_t* region, double alpha,
  * Epilogues: STEAM_EPI_STORE writes out; STEAM_EPI_FLUX treats `out` as the
  * flux F and applies F = max(F + conv, 0) (steam/simulate.py:2192-2203),
  * writing to sums_out (HOST, 3 doubles) { sum(F) over window, window cells,
- * count of F+conv < 0 over the whole array }. */
-enum { STEAM_EPI_STORE = 0, STEAM_EPI_FLUX = 1 };
+ * count of F+conv < 0 over the whole array }; STEAM_EPI_FLUX_INNER is the
+ * same with the clip count over the window alone (a tile's own columns:
+ * steam/streaming.py:1234). */
+enum { STEAM_EPI_STORE = 0, STEAM_EPI_FLUX = 1, STEAM_EPI_FLUX_INNER = 2 };
 typedef struct {
   int32_t kz, ky, kx;
   int32_t cz, cy, cx;
@@ -226,6 +228,21 @@ int steam_add_levels_clamp(int dtype, int64_t nx, int64_t ny, int64_t nz, void* 
  * streamed output writes (steam/streaming.py:1462-1692), on the device. */
 int steam_slab_zmajor(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* field,
                       int64_t z0, int64_t dz, void* out, steam_stream_t stream);
+
+/* ---- out-of-core transfers (steam/streaming.py:1139-1280 tile passes) -------
+ * steam_box_h2d: the box of bx x by columns at (x0, y0) of a HOST field
+ * (nx, ny, nz), wrapping in x and y, levels [z0, z0 + bz), into a contiguous
+ * DEVICE box (bx, by, bz).  steam_box_d2h: the window (ox, oy, oz) + (bx, by,
+ * bz) of a DEVICE box (bx_full, by_full, bz_full) into the HOST field at
+ * (x0, y0, z0), wrapping.  Asynchronous on the stream (page-locked host
+ * memory for overlap); elem_bytes 4 or 8. */
+int steam_box_h2d(int32_t elem_bytes, const void* host, int64_t nx, int64_t ny, int64_t nz,
+                  int64_t x0, int64_t y0, int64_t z0, int64_t bx, int64_t by, int64_t bz,
+                  void* dev, steam_stream_t stream);
+int steam_box_d2h(int32_t elem_bytes, const void* dev, int64_t bx_full, int64_t by_full,
+                  int64_t bz_full, int64_t ox, int64_t oy, int64_t oz, int64_t bx, int64_t by,
+                  int64_t bz, void* host, int64_t nx, int64_t ny, int64_t nz, int64_t x0,
+                  int64_t y0, int64_t z0, steam_stream_t stream);
 
 /* ---- level-weighted accumulate ------------------------------------------
  * acc += coef[z] * (a - b), or coef[z] * a when b is NULL: the compensation

@@ -19,6 +19,7 @@ STEAM_F32 = 0
 STEAM_F64 = 1
 STEAM_EPI_STORE = 0
 STEAM_EPI_FLUX = 1
+STEAM_EPI_FLUX_INNER = 2
 
 c_i32 = ctypes.c_int32
 c_i64 = ctypes.c_int64
@@ -98,6 +99,11 @@ _SIGNATURES = {
                                               c_dbl, c_dbl, c_vp]),
     "steam_slab_zmajor": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i64, c_i64,
                                          c_vp, c_vp]),
+    "steam_box_h2d": (ctypes.c_int, [c_i32, c_vp, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64,
+                                     c_i64, c_i64, c_i64, c_vp, c_vp]),
+    "steam_box_d2h": (ctypes.c_int, [c_i32, c_vp, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64,
+                                     c_i64, c_i64, c_i64, c_vp, c_i64, c_i64, c_i64, c_i64,
+                                     c_i64, c_i64, c_vp]),
     "steam_level_sums_workspace_bytes": (c_size, [c_i64]),
     "steam_level_sums": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                         ctypes.POINTER(Window), c_dp, c_vp, c_size, c_vp]),

@@ -2,6 +2,8 @@
 // elementwise helpers shared by the entry points.
 #include "common.cuh"
 
+#include <algorithm>
+
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -371,5 +373,101 @@ extern "C" int steam_slab_zmajor(int dtype, int64_t nx, int64_t ny, int64_t nz,
   else
     return fail(STEAM_ERR_ARG, "steam_slab_zmajor: bad dtype");
   STEAM_LAUNCH_CHECK("steam_slab_zmajor");
+  return STEAM_OK;
+}
+
+// ---- wrapped boxes of columns between a host field and a device box --------------
+// A box of bx x by columns starting at (x0, y0) of an (nx, ny, nz) field,
+// wrapping in x and y, levels [z0, z0 + bz): up to four 3D copies (one per
+// wrapped part), each a pitched copy of whole column runs.
+static int box_copy(size_t elem, void* host, int64_t nx, int64_t ny, int64_t nz, int64_t x0,
+                    int64_t y0, int64_t z0, int64_t bx, int64_t by, int64_t bz, void* dev,
+                    int to_device, cudaStream_t s) {
+  const char* who = to_device ? "steam_box_h2d" : "steam_box_d2h";
+  STEAM_REQUIRE(nx > 0 && ny > 0 && nz > 0 && bx >= 0 && by >= 0 && bz >= 0,
+                std::string(who) + ": bad extent");
+  STEAM_REQUIRE(bx <= nx && by <= ny && z0 >= 0 && z0 + bz <= nz,
+                std::string(who) + ": box larger than the field");
+  STEAM_REQUIRE(x0 >= 0 && x0 < nx && y0 >= 0 && y0 < ny, std::string(who) + ": origin outside");
+  if (bx * by * bz == 0) return STEAM_OK;
+  STEAM_REQUIRE(host && dev, std::string(who) + ": null pointer");
+  for (int64_t xa = 0; xa < bx;) {
+    const int64_t hx = (x0 + xa) % nx;
+    const int64_t nxp = std::min(bx - xa, nx - hx);
+    for (int64_t ya = 0; ya < by;) {
+      const int64_t hy = (y0 + ya) % ny;
+      const int64_t nyp = std::min(by - ya, ny - hy);
+      cudaMemcpy3DParms p = {};
+      cudaPitchedPtr hp = make_cudaPitchedPtr(host, (size_t)nz * elem, (size_t)nz, (size_t)ny);
+      cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)bz * elem, (size_t)bz, (size_t)by);
+      const cudaPos hpos = make_cudaPos((size_t)z0 * elem, (size_t)hy, (size_t)hx);
+      const cudaPos dpos = make_cudaPos(0, (size_t)ya, (size_t)xa);
+      p.extent = make_cudaExtent((size_t)bz * elem, (size_t)nyp, (size_t)nxp);
+      if (to_device) {
+        p.srcPtr = hp;
+        p.srcPos = hpos;
+        p.dstPtr = dp;
+        p.dstPos = dpos;
+        p.kind = cudaMemcpyHostToDevice;
+      } else {
+        p.srcPtr = dp;
+        p.srcPos = dpos;
+        p.dstPtr = hp;
+        p.dstPos = hpos;
+        p.kind = cudaMemcpyDeviceToHost;
+      }
+      STEAM_CUDA(cudaMemcpy3DAsync(&p, s));
+      ya += nyp;
+    }
+    xa += nxp;
+  }
+  return STEAM_OK;
+}
+
+extern "C" int steam_box_h2d(int32_t elem_bytes, const void* host, int64_t nx, int64_t ny,
+                             int64_t nz, int64_t x0, int64_t y0, int64_t z0, int64_t bx,
+                             int64_t by, int64_t bz, void* dev, steam_stream_t stream) {
+  STEAM_REQUIRE(elem_bytes == 4 || elem_bytes == 8, "steam_box_h2d: element size 4 or 8");
+  return box_copy((size_t)elem_bytes, const_cast<void*>(host), nx, ny, nz, x0, y0, z0, bx, by,
+                  bz, dev, 1, (cudaStream_t)stream);
+}
+
+extern "C" int steam_box_d2h(int32_t elem_bytes, const void* dev, int64_t bx_full,
+                             int64_t by_full, int64_t bz_full, int64_t ox, int64_t oy,
+                             int64_t oz, int64_t bx, int64_t by, int64_t bz, void* host,
+                             int64_t nx, int64_t ny, int64_t nz, int64_t x0, int64_t y0,
+                             int64_t z0, steam_stream_t stream) {
+  STEAM_REQUIRE(elem_bytes == 4 || elem_bytes == 8, "steam_box_d2h: element size 4 or 8");
+  STEAM_REQUIRE(ox >= 0 && oy >= 0 && oz >= 0 && ox + bx <= bx_full && oy + by <= by_full &&
+                    oz + bz <= bz_full,
+                "steam_box_d2h: window outside the device box");
+  if (bx * by * bz == 0) return STEAM_OK;
+  STEAM_REQUIRE(dev && host, "steam_box_d2h: null pointer");
+  // the window of the device box as its own pitched array: start pointer at
+  // (ox, oy, oz), pitches of the full box
+  const size_t e = (size_t)elem_bytes;
+  cudaStream_t s = (cudaStream_t)stream;
+  STEAM_REQUIRE(bx <= nx && by <= ny && z0 >= 0 && z0 + bz <= nz,
+                "steam_box_d2h: box larger than the field");
+  STEAM_REQUIRE(x0 >= 0 && x0 < nx && y0 >= 0 && y0 < ny, "steam_box_d2h: origin outside");
+  for (int64_t xa = 0; xa < bx;) {
+    const int64_t hx = (x0 + xa) % nx;
+    const int64_t nxp = std::min(bx - xa, nx - hx);
+    for (int64_t ya = 0; ya < by;) {
+      const int64_t hy = (y0 + ya) % ny;
+      const int64_t nyp = std::min(by - ya, ny - hy);
+      cudaMemcpy3DParms p = {};
+      p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(dev), (size_t)bz_full * e,
+                                     (size_t)bz_full, (size_t)by_full);
+      p.srcPos = make_cudaPos((size_t)oz * e, (size_t)(oy + ya), (size_t)(ox + xa));
+      p.dstPtr = make_cudaPitchedPtr(host, (size_t)nz * e, (size_t)nz, (size_t)ny);
+      p.dstPos = make_cudaPos((size_t)z0 * e, (size_t)hy, (size_t)hx);
+      p.extent = make_cudaExtent((size_t)bz * e, (size_t)nyp, (size_t)nxp);
+      p.kind = cudaMemcpyDeviceToHost;
+      STEAM_CUDA(cudaMemcpy3DAsync(&p, s));
+      ya += nyp;
+    }
+    xa += nxp;
+  }
   return STEAM_OK;
 }

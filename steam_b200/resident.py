@@ -40,7 +40,7 @@ class ResidentClass:
     ``setup`` is a ``simulate.ClassSetup``; its convolution plan may be of
     any kind (separable, FFT or direct)."""
 
-    def __init__(self, setup, dtype=None):
+    def __init__(self, setup, dtype=None, autotune=True):
         torch = _lib.require_cuda("resident class step")
         from . import simulate as sim
         self.lib = _lib.load()
@@ -100,7 +100,7 @@ class ResidentClass:
         self.cells = float(cols * nz)
         from . import utils as _utils
         _utils.prepare_plan(setup.plan, dev, self.dtype)
-        if nx * ny * nz >= (1 << 28) and setup.plan.kind == 'separable':
+        if autotune and nx * ny * nz >= (1 << 28) and setup.plan.kind == 'separable':
             # a field this large amortises timing its convolution's tile
             # lengths once (the tile never changes a result)
             from .ensemble import autotune_conv

@@ -71,7 +71,7 @@ class ConvPlan:
     z_taps: object = None
     y_taps: object = None
     x_taps: object = None
-    kernel: object = None          # the unfolded kernel (host float64), fft / direct
+    kernel: object = None          # the unfolded kernel (host float64)
     centre: tuple = (0, 0)         # (cx, cy) for the unfolded kernel, fft / direct
     device_data: dict = None       # per (device, dtype): kernel / spectrum tensors
     error: float = 0.0             # relative Frobenius error of the factorisation
@@ -228,6 +228,7 @@ def plan_convolution(kernel, field_shape, dtype=np.float32, tol=None):
     # filter (pair), which the FFT convolution beats
     if sep is not None and (_fused_separable(sep) or not fft_ok):
         plan = sep
+        plan.kernel = k64
     else:
         plan = ConvPlan(kind='fft' if fft_ok else 'direct', shape=k64.shape, kernel=k64,
                         centre=(effective_centre(k64.shape[0], nx),
@@ -341,7 +342,7 @@ def run_plan(plan, field_t, out_t, pre_div=None, pre_mul=None,
                 code, nx, ny, nz, _lib.ptr(data[0]), kx, ky, kz, cx, cy, _lib.ptr(field_t), pd,
                 pm, _lib.ptr(out_t), epilogue, win, sums, _lib.ptr(ws), ws.numel(),
                 _lib.stream()))
-    if epilogue == _lib.STEAM_EPI_FLUX:
+    if epilogue != _lib.STEAM_EPI_STORE:
         return (sums[0], sums[1], sums[2])
     return None
 
