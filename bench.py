@@ -74,6 +74,11 @@ def parse(argv=None):
                     help="Poisson arrival rates (requests/s) of the serving episode")
     ap.add_argument("--ensemble-members", type=int, default=256,
                     help="members of the batched-ensemble episode (0: skip)")
+    ap.add_argument("--streamed-steps", type=int, default=1,
+                    help="out-of-core class steps of the workload with its fields in "
+                         "page-locked host memory (0: skip)")
+    ap.add_argument("--streamed-tile", type=int, default=512,
+                    help="column tile of the out-of-core step (plus a 7-cell halo)")
     return ap.parse_args(argv)
 
 
@@ -384,6 +389,11 @@ def slowest_rank_ms(ms, world, device):
     return float(t.item())
 
 
+def replicas_mvox(nvox, ms, world):
+    """Whole-job Mvoxels/s of one workload per rank in ``ms``."""
+    return world * nvox / (ms / 1e3) / 1e6
+
+
 def replica_throughput(nvox, steps, ms, world):
     """Whole-job Mvoxels/s: every rank processed ``steps`` workloads of ``nvox``
     voxels; ``ms`` is the slowest rank's time."""
@@ -637,6 +647,44 @@ def main(argv=None):
         del ens, members
         torch.cuda.empty_cache()
 
+    # out-of-core: the same class step with h', qt', F in page-locked host
+    # memory, column tiles (+ halo) and level slabs streamed through the
+    # device, transfers overlapped with compute on three streams
+    streamed = None
+    if args.streamed_steps > 0:
+        from steam_b200.outofcore import host_scratch, streamed_class_step
+        torch.cuda.empty_cache()
+        scratch = host_scratch(shape, np_t)
+        host = {}
+        for k, t in (('h', h0), ('qt', q0), ('F', F0)):
+            host[k] = torch.empty(shape, dtype=tdt, pin_memory=True)
+            host[k].copy_(t)
+        outs = {k: torch.empty(shape, dtype=tdt, pin_memory=True).numpy() for k in ('qc', 'qi')}
+        keep = {k: v.clone() for k, v in host.items()}
+        del h0, q0, F0, hp, qp, F
+        torch.cuda.empty_cache()
+        tile = (args.streamed_tile, args.streamed_tile)
+        times = []
+        for _ in range(args.streamed_steps):
+            for k in host:
+                host[k].copy_(keep[k])
+            torch.cuda.synchronize()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record()
+            streamed_class_step(host['h'].numpy(), host['qt'].numpy(), host['F'].numpy(), setup,
+                                tile=tile, slab_levels=32, out=outs, scratch=scratch)
+            s1.record()
+            torch.cuda.synchronize()
+            times.append(s0.elapsed_time(s1))
+        ms = slowest_rank_ms(min(times), world, "cuda")
+        streamed = {"mvoxels_per_s": replicas_mvox(nvox, ms, world), "ms_per_step": ms,
+                    "tile": list(tile), "halo": 7, "slab_levels": 32,
+                    "note": "fields in page-locked host memory; per class step: flux "
+                            "measure, pattern measure, two second convolutions, bounded "
+                            "adds on level slabs, restore + thermodynamics"}
+        del host, keep, outs, scratch
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(tuple(args.cpu_sample))
@@ -649,7 +697,7 @@ def main(argv=None):
             "dtype": args.dtype, "data": "synthetic (seeded state and noise)",
             "config": config_dict(shape, world, args.shape),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "error": error,
-            "serving": serving,
+            "streamed": streamed, "serving": serving,
             "ensemble": ensemble,
             "gpu_launches": int(launches), "clocks": clk,
         }

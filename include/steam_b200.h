@@ -114,10 +114,12 @@ int steam_flux_noise(int dtype, const steam_region_t* region, double alpha,
  * Epilogues: STEAM_EPI_STORE writes out; STEAM_EPI_FLUX treats `out` as the
  * flux F and applies F = max(F + conv, 0) (steam/simulate.py:2192-2203),
  * writing to sums_out (HOST, 3 doubles) { sum(F) over window, window cells,
- * count of F+conv < 0 over the whole array }; STEAM_EPI_FLUX_INNER is the
- * same with the clip count over the window alone (a tile's own columns:
- * steam/streaming.py:1234). */
-enum { STEAM_EPI_STORE = 0, STEAM_EPI_FLUX = 1, STEAM_EPI_FLUX_INNER = 2 };
+ * count of F+conv < 0 over the whole array }.  STEAM_EPI_STORE_WIDE stores
+ * like STEAM_EPI_STORE with the flux convolution's float64 accumulation (the
+ * fused separable form; the FFT form computes in float32 and the direct sum
+ * in float64 either way): the tiled flux advance stores its convolution and
+ * applies the epilogue per tile (steam_flux_clip_async). */
+enum { STEAM_EPI_STORE = 0, STEAM_EPI_FLUX = 1, STEAM_EPI_STORE_WIDE = 2 };
 typedef struct {
   int32_t kz, ky, kx;
   int32_t cz, cy, cx;
@@ -228,6 +230,17 @@ int steam_add_levels_clamp(int dtype, int64_t nx, int64_t ny, int64_t nz, void* 
  * streamed output writes (steam/streaming.py:1462-1692), on the device. */
 int steam_slab_zmajor(int dtype, int64_t nx, int64_t ny, int64_t nz, const void* field,
                       int64_t z0, int64_t dz, void* out, steam_stream_t stream);
+
+/* ---- the flux epilogue on its own, over a tile's columns --------------------
+ * F = max(F + conv, 0) with sums_dev (DEVICE, 2 doubles) = { sum F over the
+ * window, count of F + conv < 0 over the window }: the tiled driver's
+ * per-tile measure of the realized flux and the clip count of the tile's own
+ * columns (steam/streaming.py:1225-1236), for a convolution run with
+ * STEAM_EPI_STORE on the tile's box. */
+int steam_flux_clip_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* flux,
+                          const void* conv, const steam_window_t* window, double* sums_dev,
+                          void* workspace, size_t workspace_bytes, steam_stream_t stream);
+size_t steam_flux_clip_workspace_bytes(int64_t nx, int64_t ny, int64_t nz);
 
 /* ---- out-of-core transfers (steam/streaming.py:1139-1280 tile passes) -------
  * steam_box_h2d: the box of bx x by columns at (x0, y0) of a HOST field

@@ -19,7 +19,7 @@ STEAM_F32 = 0
 STEAM_F64 = 1
 STEAM_EPI_STORE = 0
 STEAM_EPI_FLUX = 1
-STEAM_EPI_FLUX_INNER = 2
+STEAM_EPI_STORE_WIDE = 2
 
 c_i32 = ctypes.c_int32
 c_i64 = ctypes.c_int64
@@ -99,6 +99,10 @@ _SIGNATURES = {
                                               c_dbl, c_dbl, c_vp]),
     "steam_slab_zmajor": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_i64, c_i64,
                                          c_vp, c_vp]),
+    "steam_flux_clip_workspace_bytes": (c_size, [c_i64, c_i64, c_i64]),
+    "steam_flux_clip_async": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp, c_vp,
+                                             ctypes.POINTER(Window), c_vp, c_vp, c_size,
+                                             c_vp]),
     "steam_box_h2d": (ctypes.c_int, [c_i32, c_vp, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64,
                                      c_i64, c_i64, c_i64, c_vp, c_vp]),
     "steam_box_d2h": (ctypes.c_int, [c_i32, c_vp, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64,

@@ -376,6 +376,41 @@ extern "C" int steam_slab_zmajor(int dtype, int64_t nx, int64_t ny, int64_t nz,
   return STEAM_OK;
 }
 
+// ---- the flux epilogue on its own -------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) flux_clip_kernel(int64_t nx, int64_t ny, int64_t nz,
+                                                        T* __restrict__ f,
+                                                        const T* __restrict__ conv,
+                                                        int64_t wx0, int64_t wx1, int64_t wy0,
+                                                        int64_t wy1,
+                                                        double* __restrict__ partials) {
+  __shared__ double scratch[32];
+  const int64_t n = nx * ny * nz;
+  double s_f = 0.0, s_clip = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = i / nz;
+    const int64_t y = col % ny, x = col / ny;
+    const bool inw = x >= wx0 && x < wx1 && y >= wy0 && y < wy1;
+    // F + conv rounded once to the storage dtype, as the fused epilogues do
+    T v = (T)((double)f[i] + (double)conv[i]);
+    if (v < (T)0) {
+      if (inw) s_clip += 1.0;
+      v = (T)0;
+    }
+    f[i] = v;
+    if (inw) s_f += (double)v;
+  }
+  const double t0 = block_sum(s_f, scratch);
+  const double t1 = block_sum(s_clip, scratch);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = t0;
+    partials[gridDim.x + blockIdx.x] = t1;
+  }
+}
+
+static int flux_clip_grid(int64_t n) { return stride_grid(n, 256, 4); }
+
 // ---- wrapped boxes of columns between a host field and a device box --------------
 // A box of bx x by columns starting at (x0, y0) of an (nx, ny, nz) field,
 // wrapping in x and y, levels [z0, z0 + bz): up to four 3D copies (one per
@@ -470,4 +505,44 @@ extern "C" int steam_box_d2h(int32_t elem_bytes, const void* dev, int64_t bx_ful
     xa += nxp;
   }
   return STEAM_OK;
+}
+
+extern "C" size_t steam_flux_clip_workspace_bytes(int64_t nx, int64_t ny, int64_t nz) {
+  return carve_bytes((size_t)2 * flux_clip_grid(nx * ny * nz), sizeof(double));
+}
+
+extern "C" int steam_flux_clip_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* flux,
+                                     const void* conv, const steam_window_t* window,
+                                     double* sums_dev, void* workspace, size_t workspace_bytes,
+                                     steam_stream_t stream) {
+  STEAM_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "steam_flux_clip_async: negative extent");
+  STEAM_REQUIRE(sums_dev, "steam_flux_clip_async: null sums_dev");
+  if (window)
+    STEAM_REQUIRE(window->x0 >= 0 && window->x1 <= nx && window->x0 <= window->x1 &&
+                      window->y0 >= 0 && window->y1 <= ny && window->y0 <= window->y1,
+                  "steam_flux_clip_async: window outside the array");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n = nx * ny * nz;
+  if (n == 0) {
+    STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
+    return STEAM_OK;
+  }
+  STEAM_REQUIRE(flux && conv, "steam_flux_clip_async: null field");
+  const int grid = flux_clip_grid(n);
+  Carver c(workspace, workspace_bytes);
+  double* partials = c.take<double>((size_t)2 * grid);
+  if (!partials) return fail(STEAM_ERR_WORKSPACE, "steam_flux_clip_async: workspace too small");
+  const int64_t wx0 = window ? window->x0 : 0, wx1 = window ? window->x1 : nx;
+  const int64_t wy0 = window ? window->y0 : 0, wy1 = window ? window->y1 : ny;
+  if (dtype == STEAM_F32)
+    flux_clip_kernel<float><<<grid, 256, 0, s>>>(nx, ny, nz, (float*)flux, (const float*)conv,
+                                                 wx0, wx1, wy0, wy1, partials);
+  else if (dtype == STEAM_F64)
+    flux_clip_kernel<double><<<grid, 256, 0, s>>>(nx, ny, nz, (double*)flux,
+                                                  (const double*)conv, wx0, wx1, wy0, wy1,
+                                                  partials);
+  else
+    return fail(STEAM_ERR_ARG, "steam_flux_clip_async: bad dtype");
+  STEAM_LAUNCH_CHECK("steam_flux_clip_async");
+  return reduce_partials(partials, grid, 2, sums_dev, s);
 }

@@ -225,23 +225,23 @@ __global__ void __launch_bounds__(256) xpass_kernel(
         for (int j = 0; j < kx; ++j) acc += tp[j] * col[-j * kTE];
       }
       const int64_t o = x * pe + e0 + ee;
-      if (epi.mode != STEAM_EPI_STORE) {
+      if (epi.mode == STEAM_EPI_FLUX) {
         // F + conv rounded once to the storage dtype
         T f = (T)((double)out[o] + acc);
-        const int64_t y = (e0 + ee) / nz;
-        const bool inw = x >= epi.wx0 && x < epi.wx1 && y >= epi.wy0 && y < epi.wy1;
         if (f < (T)0) {
-          if (epi.mode == STEAM_EPI_FLUX || inw) s_clip += 1.0;
+          s_clip += 1.0;
           f = (T)0;
         }
         out[o] = f;
-        if (inw) s_f += (double)f;
+        int64_t y = (e0 + ee) / nz;
+        if (x >= epi.wx0 && x < epi.wx1 && y >= epi.wy0 && y < epi.wy1)
+          s_f += (double)f;
       } else {
         out[o] = (T)acc;
       }
     }
   }
-  if (epi.mode != STEAM_EPI_STORE) {
+  if (epi.mode == STEAM_EPI_FLUX) {
     double t0 = block_sum(s_f, scratch);
     double t1 = block_sum(s_clip, scratch);
     if (threadIdx.x == 0) {
@@ -447,9 +447,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
   commit_loads(s_in0);
   __syncthreads();
   if (count > 1) issue_loads(s_in0 + R * C);
-  const bool flux_epi = epi.mode != STEAM_EPI_STORE;
-  // the clip count over every cell (STEAM_EPI_FLUX) or the window's alone
-  const bool clip_all = epi.mode == STEAM_EPI_FLUX;
+  const bool flux_epi = epi.mode == STEAM_EPI_FLUX;
   const int count_i = (int)count;
   int rph = 0;  // ring phase: k mod K
   for (int k = 0; k < count_i; ++k) {
@@ -593,7 +591,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
           T f1 = add_rn(fprev1, (T)acc[es][1]);
           if (ok0) {
             if (f0 < (T)0) {
-              if (clip_all || (in_wx && iny0)) s_clip += 1.0;
+              s_clip += 1.0;
               f0 = (T)0;
             }
             outp[o0] = f0;
@@ -601,7 +599,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
           }
           if (ok1) {
             if (f1 < (T)0) {
-              if (clip_all || (in_wx && iny1)) s_clip += 1.0;
+              s_clip += 1.0;
               f1 = (T)0;
             }
             outp[o1] = f1;
@@ -634,7 +632,7 @@ __global__ void __launch_bounds__(kFThreads, (sizeof(A) == 4 ? (K <= 13 ? 3 : 2)
 #undef STEAM_RING_CASE
     rph = rph + 1 == K ? 0 : rph + 1;
   }
-  if (epi.mode != STEAM_EPI_STORE) {
+  if (epi.mode == STEAM_EPI_FLUX) {
     double t0 = block_sum(s_f, scratch);
     double t1 = block_sum(s_clip, scratch);
     if (threadIdx.x == 0) {
@@ -847,7 +845,7 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
                                          partials, s)
                : launch_fused<T, T>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi, partials, s);
   if (rc) return rc;
-  if (epilogue != STEAM_EPI_STORE) {
+  if (epilogue == STEAM_EPI_FLUX) {
     int rc = reduce_partials(partials, (int)grid, 2, totals, s);
     if (rc) return rc;
     if (totals_dev) return STEAM_OK;
@@ -957,7 +955,7 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                                            epi, partials);
     STEAM_LAUNCH_CHECK("conv x-pass");
   }
-  if (epilogue != STEAM_EPI_STORE) {
+  if (epilogue == STEAM_EPI_FLUX) {
     rc = reduce_partials(partials, xgrid, 2, totals, s);
     if (rc) return rc;
     if (totals_dev) return STEAM_OK;
@@ -1012,9 +1010,9 @@ extern "C" int steam_conv_separable(
   STEAM_REQUIRE(spec && z_taps && y_taps && x_taps,
                 "steam_conv_separable: null spec or taps");
   STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || epilogue == STEAM_EPI_FLUX ||
-                    epilogue == STEAM_EPI_FLUX_INNER,
+                    epilogue == STEAM_EPI_STORE_WIDE,
                 "steam_conv_separable: unknown epilogue");
-  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || sums_out,
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_out,
                 "steam_conv_separable: flux epilogue needs sums_out");
   if (window) {
     STEAM_REQUIRE(window->x0 >= 0 && window->x1 <= nx &&
@@ -1023,7 +1021,7 @@ extern "C" int steam_conv_separable(
                   "steam_conv_separable: window outside the array");
   }
   if (nx * ny * nz == 0) {
-    if (epilogue != STEAM_EPI_STORE) {
+    if (epilogue == STEAM_EPI_FLUX) {
       sums_out[0] = 0.0;
       sums_out[1] = 0.0;
       sums_out[2] = 0.0;
@@ -1054,9 +1052,9 @@ extern "C" int steam_conv_separable_async(
   STEAM_REQUIRE(spec && z_taps && y_taps && x_taps,
                 "steam_conv_separable_async: null spec or taps");
   STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || epilogue == STEAM_EPI_FLUX ||
-                    epilogue == STEAM_EPI_FLUX_INNER,
+                    epilogue == STEAM_EPI_STORE_WIDE,
                 "steam_conv_separable_async: unknown epilogue");
-  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || sums_dev,
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_dev,
                 "steam_conv_separable_async: flux epilogue needs sums_dev");
   if (window) {
     STEAM_REQUIRE(window->x0 >= 0 && window->x1 <= nx &&
@@ -1066,7 +1064,7 @@ extern "C" int steam_conv_separable_async(
   }
   cudaStream_t s = (cudaStream_t)stream;
   if (nx * ny * nz == 0) {
-    if (epilogue != STEAM_EPI_STORE) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
+    if (epilogue == STEAM_EPI_FLUX) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
     return STEAM_OK;
   }
   STEAM_REQUIRE(in && out, "steam_conv_separable_async: null field pointer");

@@ -294,14 +294,14 @@ fft_conv_kernel(const float* __restrict__ in, float* __restrict__ out,
                                      col ? v[m0 + 2].y : v[m0 + 2].x,
                                      col ? v[m0 + 3].y : v[m0 + 3].x);
               float4* dst = reinterpret_cast<float4*>(o + z);
-              if (g.mode != STEAM_EPI_STORE) {
+              if (g.mode == STEAM_EPI_FLUX) {
                 const float4 f = *dst;
                 float r[4] = {(float)((double)f.x + (double)c.x), (float)((double)f.y + (double)c.y),
                               (float)((double)f.z + (double)c.z), (float)((double)f.w + (double)c.w)};
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                   if (r[q] < 0.f) {
-                    if (g.mode == STEAM_EPI_FLUX || inwin) s_clip += 1.0;
+                    s_clip += 1.0;
                     r[q] = 0.f;
                   }
                   if (inwin) s_f += (double)r[q];
@@ -317,10 +317,10 @@ fft_conv_kernel(const float* __restrict__ in, float* __restrict__ out,
               const int z = Z0 + m - (g.kz - 1);
               if (z >= g.nz || m - (g.kz - 1) >= g.bz) continue;
               float c = col ? v[m].y : v[m].x;
-              if (g.mode != STEAM_EPI_STORE) {
+              if (g.mode == STEAM_EPI_FLUX) {
                 c = (float)((double)o[z] + (double)c);
                 if (c < 0.f) {
-                  if (g.mode == STEAM_EPI_FLUX || inwin) s_clip += 1.0;
+                  s_clip += 1.0;
                   c = 0.f;
                 }
                 if (inwin) s_f += (double)c;
@@ -333,7 +333,7 @@ fft_conv_kernel(const float* __restrict__ in, float* __restrict__ out,
     }
     __syncthreads();
   }
-  if (g.mode != STEAM_EPI_STORE) {
+  if (g.mode == STEAM_EPI_FLUX) {
     const double t0 = block_sum(s_f, scratch);
     const double t1 = block_sum(s_clip, scratch);
     if (t == 0) {
@@ -424,20 +424,19 @@ direct_conv_kernel(const T* __restrict__ in, int64_t nx, int64_t ny, int nz,
         }
       }
     }
-    if (mode != STEAM_EPI_STORE) {
+    if (mode == STEAM_EPI_FLUX) {
       T f = (T)((double)out[i] + acc);
-      const bool inw = x >= wx0 && x < wx1 && y >= wy0 && y < wy1;
       if (f < (T)0) {
-        if (mode == STEAM_EPI_FLUX || inw) s_clip += 1.0;
+        s_clip += 1.0;
         f = (T)0;
       }
       out[i] = f;
-      if (inw) s_f += (double)f;
+      if (x >= wx0 && x < wx1 && y >= wy0 && y < wy1) s_f += (double)f;
     } else {
       out[i] = (T)acc;
     }
   }
-  if (mode != STEAM_EPI_STORE) {
+  if (mode == STEAM_EPI_FLUX) {
     const double t0 = block_sum(s_f, scratch);
     const double t1 = block_sum(s_clip, scratch);
     if (threadIdx.x == 0) {
@@ -494,7 +493,7 @@ int check_common(const char* fn, int64_t nx, int64_t ny, int64_t nz, int kx, int
   STEAM_REQUIRE(kx >= 1 && ky >= 1 && kz >= 1, f + ": kernel extents must be >= 1");
   STEAM_REQUIRE(cx >= 0 && cx < kx && cy >= 0 && cy < ky, f + ": centre outside the kernel");
   STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || epilogue == STEAM_EPI_FLUX ||
-                    epilogue == STEAM_EPI_FLUX_INNER,
+                    epilogue == STEAM_EPI_STORE_WIDE,
                 f + ": unknown epilogue");
   STEAM_REQUIRE(nz < ((int64_t)1 << 31), f + ": nz above 2^31");
   if (w)
@@ -568,7 +567,7 @@ int run_fft(int64_t nx, int64_t ny, int64_t nz, int kx, int ky, int kz, int cx, 
   fft_conv_kernel<<<grid, kFftThreads, kFftSmem, s>>>(
       (const float*)in, (float*)out, pre, (const float2*)spectrum, g, partials);
   STEAM_LAUNCH_CHECK("steam_conv_fft");
-  if (epilogue != STEAM_EPI_STORE)
+  if (epilogue == STEAM_EPI_FLUX)
     return finish_sums(partials, grid, sums_dev ? sums_dev : totals, sums_out,
                        win_cells(w, nx, ny) * nz, s);
   return STEAM_OK;
@@ -602,7 +601,7 @@ int run_direct(int64_t nx, int64_t ny, int64_t nz, const void* kernel, int kx, i
       use_pre ? pre : nullptr, epilogue, w ? w->x0 : 0, w ? w->x1 : nx, w ? w->y0 : 0,
       w ? w->y1 : ny, (T*)out, partials);
   STEAM_LAUNCH_CHECK("steam_conv_direct");
-  if (epilogue != STEAM_EPI_STORE)
+  if (epilogue == STEAM_EPI_FLUX)
     return finish_sums(partials, grid, sums_dev ? sums_dev : totals, sums_out,
                        win_cells(w, nx, ny) * nz, s);
   return STEAM_OK;
@@ -655,9 +654,9 @@ extern "C" int steam_conv_fft(int64_t nx, int64_t ny, int64_t nz, int32_t kx, in
                               steam_stream_t stream) {
   int rc = check_common("steam_conv_fft", nx, ny, nz, kx, ky, kz, cx, cy, epilogue, window);
   if (rc) return rc;
-  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || sums_out, "steam_conv_fft: flux epilogue needs sums_out");
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_out, "steam_conv_fft: flux epilogue needs sums_out");
   if (nx * ny * nz == 0) {
-    if (epilogue != STEAM_EPI_STORE) sums_out[0] = sums_out[1] = sums_out[2] = 0.0;
+    if (epilogue == STEAM_EPI_FLUX) sums_out[0] = sums_out[1] = sums_out[2] = 0.0;
     return STEAM_OK;
   }
   return run_fft(nx, ny, nz, kx, ky, kz, cx, cy, spectrum_dev, in, nullptr, pre_div, pre_mul,
@@ -674,11 +673,11 @@ extern "C" int steam_conv_fft_async(int64_t nx, int64_t ny, int64_t nz, int32_t 
                                     steam_stream_t stream) {
   int rc = check_common("steam_conv_fft_async", nx, ny, nz, kx, ky, kz, cx, cy, epilogue, window);
   if (rc) return rc;
-  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || sums_dev,
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_dev,
                 "steam_conv_fft_async: flux epilogue needs sums_dev");
   cudaStream_t s = (cudaStream_t)stream;
   if (nx * ny * nz == 0) {
-    if (epilogue != STEAM_EPI_STORE) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
+    if (epilogue == STEAM_EPI_FLUX) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
     return STEAM_OK;
   }
   return run_fft(nx, ny, nz, kx, ky, kz, cx, cy, spectrum_dev, in, (const float*)pre_dev,
@@ -699,10 +698,10 @@ extern "C" int steam_conv_direct(int dtype, int64_t nx, int64_t ny, int64_t nz,
                                  steam_stream_t stream) {
   int rc = check_common("steam_conv_direct", nx, ny, nz, kx, ky, kz, cx, cy, epilogue, window);
   if (rc) return rc;
-  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || sums_out,
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_out,
                 "steam_conv_direct: flux epilogue needs sums_out");
   if (nx * ny * nz == 0) {
-    if (epilogue != STEAM_EPI_STORE) sums_out[0] = sums_out[1] = sums_out[2] = 0.0;
+    if (epilogue == STEAM_EPI_FLUX) sums_out[0] = sums_out[1] = sums_out[2] = 0.0;
     return STEAM_OK;
   }
   cudaStream_t s = (cudaStream_t)stream;
@@ -727,11 +726,11 @@ extern "C" int steam_conv_direct_async(int dtype, int64_t nx, int64_t ny, int64_
   int rc = check_common("steam_conv_direct_async", nx, ny, nz, kx, ky, kz, cx, cy, epilogue,
                         window);
   if (rc) return rc;
-  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || sums_dev,
+  STEAM_REQUIRE(epilogue != STEAM_EPI_FLUX || sums_dev,
                 "steam_conv_direct_async: flux epilogue needs sums_dev");
   cudaStream_t s = (cudaStream_t)stream;
   if (nx * ny * nz == 0) {
-    if (epilogue != STEAM_EPI_STORE) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
+    if (epilogue == STEAM_EPI_FLUX) STEAM_CUDA(cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), s));
     return STEAM_OK;
   }
   if (dtype == STEAM_F32)

@@ -92,13 +92,25 @@ class _Pipe:
         self.freed = [None, None]
 
 
+def host_scratch(shape, dtype):
+    """The page-locked host arrays a streamed class step of ``shape`` works
+    in (the new flux and both increments), for reuse across calls."""
+    import torch
+    tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+    return {k: torch.empty(tuple(shape), dtype=tdt, pin_memory=True).numpy()
+            for k in ('F_new', 'h', 'qt')}
+
+
 def streamed_class_step(h, qt, flux, setup, tile=(256, 256), slab_levels=32,
-                        diagnostics=('qc', 'qi'), out=None, surface_pressure=101325.0):
+                        diagnostics=('qc', 'qi'), out=None, surface_pressure=101325.0,
+                        scratch=None):
     """One class step (flux advance, both scalar branches, thermodynamics) on
     HOST arrays h', qt', F of ``setup.shape`` (updated in place), with at
     most a tile of columns plus its halo, or a slab of levels, on the device
-    at a time.  Page-locked arrays let every copy run asynchronously.
-    Returns ({diagnostic: host array}, ClassLedger)."""
+    at a time.  Page-locked arrays let every copy run asynchronously;
+    ``scratch`` (see ``host_scratch``) holds the step's own host arrays,
+    allocated page-locked per call otherwise.  Returns ({diagnostic: host
+    array}, ClassLedger)."""
     torch = _lib.require_cuda("streamed_class_step")
     from .resident import N_RESCALE, ResidentClass
     lib = _lib.load()
@@ -190,7 +202,9 @@ def streamed_class_step(h, qt, flux, setup, tile=(256, 256), slab_levels=32,
         return ctypes.c_void_p(t.data_ptr() + 8 * int(n))
 
     # ---- pass 1: flux measure ------------------------------------------------
-    F_new = np.empty_like(flux)
+    if scratch is None:
+        scratch = host_scratch((nx, ny, nz), np_t)
+    F_new = scratch['F_new']
 
     def p1_up(b, item):
         upload_box(b, item, ('F',))
@@ -198,8 +212,15 @@ def streamed_class_step(h, qt, flux, setup, tile=(256, 256), slab_levels=32,
     def p1_comp(b, item):
         shape, _ = box(item)
         noise(b, item, off(sums[b], 0))
-        _utils.run_plan_async(plan(shape), view(b, 'P', shape), view(b, 'F', shape), None,
-                              _lib.STEAM_EPI_FLUX_INNER, window(item), off(sums[b], 3))
+        # the convolution stored, then the flux epilogue with the clip
+        # counted over the tile's own columns
+        _utils.run_plan_async(plan(shape), view(b, 'P', shape), view(b, 'W', shape), None,
+                              _lib.STEAM_EPI_STORE_WIDE, None, None)
+        ws = _lib.WORKSPACE.get(lib.steam_flux_clip_workspace_bytes(*shape))
+        _lib.check(lib.steam_flux_clip_async(code, *shape, _lib.ptr(view(b, 'F', shape)),
+                                             _lib.ptr(view(b, 'W', shape)),
+                                             _lib.window_arg(window(item)), off(sums[b], 3),
+                                             _lib.ptr(ws), ws.numel(), _lib.stream()))
 
     def p1_down(b, item):
         shape, _ = box(item)
@@ -263,7 +284,7 @@ def streamed_class_step(h, qt, flux, setup, tile=(256, 256), slab_levels=32,
     cl.pattern['qt'] = PatternLedger(ps_q[:nz].copy(), ps_q[nz:].astype(np.int64))
 
     # ---- pass 3: second convolutions ------------------------------------------
-    inc = {'h': np.empty_like(h), 'qt': np.empty_like(qt)}
+    inc = {'h': scratch['h'], 'qt': scratch['qt']}
     for name in ('h', 'qt'):
         def p3_up(b, item, name=name):
             upload_box(b, item, ('F', name))

@@ -342,7 +342,7 @@ def run_plan(plan, field_t, out_t, pre_div=None, pre_mul=None,
                 code, nx, ny, nz, _lib.ptr(data[0]), kx, ky, kz, cx, cy, _lib.ptr(field_t), pd,
                 pm, _lib.ptr(out_t), epilogue, win, sums, _lib.ptr(ws), ws.numel(),
                 _lib.stream()))
-    if epilogue != _lib.STEAM_EPI_STORE:
+    if epilogue == _lib.STEAM_EPI_FLUX:
         return (sums[0], sums[1], sums[2])
     return None
 
