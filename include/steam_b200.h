@@ -138,14 +138,31 @@ int steam_conv_separable(int dtype, int64_t nx, int64_t ny, int64_t nz,
                          const steam_window_t* window, double* sums_out,
                          void* workspace, size_t workspace_bytes,
                          steam_stream_t stream);
-/* Tuning of the fused separable kernel, which has no counterpart in the
+/* Tuning of the fused separable kernels, which have no counterpart in the
  * reference (its FFT block length is fixed, steam/utils.py:341): x planes
  * per CTA for fields of shape (nx, ny, nz), chosen by the host autotuner
- * (steam_b200/ensemble.py); 0 restores the default (256).  The chunk changes
- * which CTA computes an output, never the order of its sums, so results are
- * identical for every chunk.  The workspace query already covers any chunk. */
+ * (steam_b200/ensemble.py); 0 restores the default (256 for the scalar fused
+ * kernel; for the packed float32 kernel the chunk that fills whole waves of
+ * CTAs).  The chunk changes which CTA computes an output, never the order of
+ * its sums, so results are identical for every chunk.  The workspace query
+ * already covers any chunk. */
 int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t chunk);
 int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz);
+
+/* Float32 flux convolutions (STEAM_EPI_FLUX on float32 fields) run on the
+ * packed float32 kernel by default (wide = 0); wide = 1 runs them with
+ * float64 taps and accumulators instead.  Process-wide. */
+int steam_conv_set_flux_wide(int32_t wide);
+
+/* The packed kernel's slab copies complete on mbarriers whose waits are
+ * bounded: a block that waits past the limit waits (bounded again) for its
+ * copies in flight, counts itself here and leaves without finishing its
+ * tile.  Reads the count of such blocks since the last call into *count and
+ * resets it (synchronises the current device). */
+int steam_take_wait_errors(int32_t* count);
+
+/* Launches of the packed float32 kernel so far in this process. */
+int64_t steam_conv_packed_launches(void);
 
 /* ---- a9/a10 for kernels without a separable form -----------------------
  * The Morlet turbulon (steam/turbulons.py:40-48) and any kernel whose Tucker

@@ -7,8 +7,10 @@
 //   y-pass: v_p = u_c (*)_y Y_b     (TY x TZ tiles of one x-plane)
 //   x-pass: out = sum_a (sum_p mix_ap v_p) (*)_x X_a, with the epilogue.
 #include "common.cuh"
+#include "conv.cuh"
 #include <type_traits>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -17,48 +19,6 @@
 #include <vector>
 
 namespace steam {
-
-constexpr int kMaxTaps = 1536;
-constexpr int kMaxZ = 8;
-constexpr int kMaxPairs = 16;
-constexpr int kMaxX = 4;
-
-// Taps, mixing weights and every accumulator are float64 for both storage
-// dtypes: the turbulon kernel's terms cancel (it has zero sum), and float32
-// taps with float32 sums put ~1e-5 relative error into the log of a flux
-// advanced next to its clip.  Fields and intermediates stay in the storage
-// dtype.
-template <typename T>
-struct SepParams {
-  int kz, ky, kx, cz, cy, cx;
-  int nzf, nyf, nxf, npairs;
-  int pair_z[kMaxPairs];
-  int pair_y[kMaxPairs];
-  double mix[kMaxX * kMaxPairs];
-  double taps[kMaxTaps];  // z taps, then y taps, then x taps
-  __host__ __device__ const double* ztap(int f) const { return taps + f * kz; }
-  __host__ __device__ const double* ytap(int f) const {
-    return taps + nzf * kz + f * ky;
-  }
-  __host__ __device__ const double* xtap(int f) const {
-    return taps + nzf * kz + nyf * ky + f * kx;
-  }
-};
-
-__device__ __forceinline__ int64_t wrapi(int64_t v, int64_t n) {
-  int64_t r = v % n;
-  return r < 0 ? r + n : r;
-}
-
-// The input scaling of the second convolution, f' = f / mean(z) * C_k(z)
-// (steam/simulate.py:1989-1992), as ONE multiply by C_k / mean formed in
-// float64 and rounded to the field's type: within a unit in the last place
-// of the two separately rounded operations, and a multiply instead of a
-// division on every staged element.
-template <typename T>
-__device__ __forceinline__ T pre_scale(T div, T mul) {
-  return (T)((double)mul / (double)div);
-}
 
 // ---- z-pass -------------------------------------------------------------
 // Block = CB consecutive columns (contiguous in memory), staged with zero
@@ -165,11 +125,6 @@ __global__ void __launch_bounds__(256) ypass_kernel(
 // ---- x-pass -------------------------------------------------------------
 constexpr int kTX = 16;
 constexpr int kTE = 128;
-
-struct XEpi {
-  int mode;
-  int64_t wx0, wx1, wy0, wy1;
-};
 
 template <typename T>
 __global__ void __launch_bounds__(256) xpass_kernel(
@@ -670,6 +625,17 @@ static int fused_chunk(int64_t nx, int64_t ny, int64_t nz) {
   return it == g_chunk.end() ? kFChunk : it->second;
 }
 
+// the autotuner's chunk for the shape, 0 when it has set none
+int chunk_override(int64_t nx, int64_t ny, int64_t nz) {
+  std::lock_guard<std::mutex> lock(g_chunk_mu);
+  auto it = g_chunk.find(std::make_tuple(nx, ny, nz));
+  return it == g_chunk.end() ? 0 : it->second;
+}
+
+// float32 flux convolutions with float64 accumulation (the scalar fused
+// kernel) instead of the packed float32 kernel: steam_conv_set_flux_wide
+static std::atomic<int> g_flux_wide{0};
+
 static int64_t fused_grid(int64_t nx, int64_t ny, int64_t nz, int chunk) {
   const int64_t nzt = (nz + kFZ - 1) / kFZ, nyt = (ny + kFY - 1) / kFY;
   const int64_t nxc = (nx + chunk - 1) / chunk;
@@ -806,11 +772,12 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
                      const double* pre_mul, const T* pre_dev, void* out_v, int epilogue,
                      const steam_window_t* win, double* sums_out, double* totals_dev,
                      void* ws, size_t ws_bytes, cudaStream_t s) {
-  const int64_t grid = fused_grid(nx, ny, nz, fused_chunk(nx, ny, nz));
+  int64_t grid = fused_grid(nx, ny, nz, fused_chunk(nx, ny, nz));
   Carver c(ws, ws_bytes);
   const bool use_pre = pre_div != nullptr || pre_mul != nullptr || pre_dev != nullptr;
   T* pre = c.take<T>((size_t)2 * nz);
-  double* partials = c.take<double>((size_t)grid * 2);
+  // room for either kernel's partial sums (the packed grid is at most this)
+  double* partials = c.take<double>((size_t)fused_grid(nx, ny, nz, kFChunkMin) * 2);
   double* totals = c.take<double>(2);
   if (!pre || !partials || !totals)
     return fail(STEAM_ERR_WORKSPACE, "steam_conv_separable: workspace too small");
@@ -840,10 +807,23 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
   epi.wx1 = win ? win->x1 : nx;
   epi.wy0 = win ? win->y0 : 0;
   epi.wy1 = win ? win->y1 : ny;
-  int rc = epilogue != STEAM_EPI_STORE
-               ? launch_fused<T, double>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi,
-                                         partials, s)
-               : launch_fused<T, T>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi, partials, s);
+  int rc;
+  bool packed = false;
+  if constexpr (sizeof(T) == 4) {
+    packed = (epilogue == STEAM_EPI_STORE || (epilogue == STEAM_EPI_FLUX && !g_flux_wide.load())) &&
+             packed_supported(p, nx, ny, nz, in_v, out_v, epilogue);
+  }
+  if (packed) {
+    grid = packed_grid(nx, ny, nz);
+    rc = packed_launch(reinterpret_cast<const SepParams<float>&>(p), nx, ny, nz,
+                       (const float*)in_v, (float*)out_v, use_pre ? (const float*)pre : nullptr,
+                       epilogue, epi, partials, s);
+  } else {
+    rc = epilogue != STEAM_EPI_STORE
+             ? launch_fused<T, double>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi,
+                                       partials, s)
+             : launch_fused<T, T>(p, grid, (const T*)in_v, (T*)out_v, pre, g, epi, partials, s);
+  }
   if (rc) return rc;
   if (epilogue == STEAM_EPI_FLUX) {
     int rc = reduce_partials(partials, (int)grid, 2, totals, s);
@@ -1077,6 +1057,12 @@ extern "C" int steam_conv_separable_async(
                                  nullptr, (const double*)pre_dev, out, epilogue, window,
                                  nullptr, sums_dev, workspace, workspace_bytes, s);
   return fail(STEAM_ERR_ARG, "steam_conv_separable_async: bad dtype");
+}
+
+extern "C" int steam_conv_set_flux_wide(int32_t wide) {
+  STEAM_REQUIRE(wide == 0 || wide == 1, "steam_conv_set_flux_wide: wide must be 0 or 1");
+  g_flux_wide.store(wide);
+  return STEAM_OK;
 }
 
 extern "C" int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t chunk) {
