@@ -517,6 +517,40 @@ int steam_bounded_add_replay_async(int dtype, int64_t nx, int64_t ny, int64_t nz
  * reference, whose bounded add has no device-side wait. */
 int steam_set_barrier_spin_limit(int64_t polls);
 
+/* Grouped bounded adds (no counterpart in the reference, which runs one
+ * field at a time): n independent fields' steam_bounded_add_async solves
+ * (record_applied = 0) as one launch per stage -- the first and apply sweeps
+ * over a flat grid, each persistent phase as one cooperative launch whose
+ * blocks split into per-field teams with their own grid barriers.  Each
+ * field's block counts follow from its own shape, so a field's result does
+ * not depend on the others in the group (it differs from the single call's
+ * in the last bits of its sums: another block partition).  Every field:
+ * nz % 4 == 0 (4 .. 1024), 16-byte aligned pert and increment.
+ *
+ * prepare (synchronous, outside stream capture) lays the group's state out
+ * in `workspace` (DEVICE, steam_bounded_add_group_workspace_bytes) and
+ * records it under that address; async enqueues the solves (capturable,
+ * repeatable: the same fields each time); release forgets the group.
+ * ledger: DEVICE, nz * (7 + 2 n_rescale) doubles per field (the record of
+ * steam_bounded_add_async), or NULL. */
+typedef struct {
+  int64_t nx, ny, nz;
+  void* pert;            /* DEVICE (nx, ny, nz), updated in place */
+  void* increment;       /* DEVICE (nx, ny, nz), consumed */
+  const double* mean;    /* DEVICE, nz */
+  double phi_min, phi_max;
+  int32_t has_window;    /* 0: the whole array */
+  steam_window_t window;
+  double* ledger;
+} steam_ba_problem_t;
+size_t steam_bounded_add_group_workspace_bytes(int dtype, int32_t n,
+                                               const steam_ba_problem_t* problems,
+                                               int32_t n_rescale);
+int steam_bounded_add_group_prepare(int dtype, int32_t n, const steam_ba_problem_t* problems,
+                                    int32_t n_rescale, void* workspace, size_t workspace_bytes);
+int steam_bounded_add_group_async(void* workspace, steam_stream_t stream);
+int steam_bounded_add_group_release(void* workspace);
+
 int steam_bounded_add_async(int dtype, int64_t nx, int64_t ny, int64_t nz, void* pert,
                             const double* mean_dev, void* increment, double phi_min,
                             double phi_max, const steam_window_t* window, int32_t n_rescale,

@@ -42,6 +42,14 @@ class Window(ctypes.Structure):
     _fields_ = [("x0", c_i64), ("x1", c_i64), ("y0", c_i64), ("y1", c_i64)]
 
 
+class BAProblem(ctypes.Structure):
+    """steam_ba_problem_t: one field of a grouped bounded add."""
+    _fields_ = [("nx", c_i64), ("ny", c_i64), ("nz", c_i64), ("pert", ctypes.c_void_p),
+                ("increment", ctypes.c_void_p), ("mean", ctypes.c_void_p),
+                ("phi_min", ctypes.c_double), ("phi_max", ctypes.c_double),
+                ("has_window", c_i32), ("window", Window), ("ledger", ctypes.c_void_p)]
+
+
 class SepConv(ctypes.Structure):
     """steam_sepconv_t"""
     _fields_ = [("kz", c_i32), ("ky", c_i32), ("kx", c_i32),
@@ -127,6 +135,14 @@ _SIGNATURES = {
                                          c_vp, c_dbl, c_dbl, ctypes.POINTER(Window), c_i32,
                                          c_i32, c_dp, c_vp, c_size, c_vp]),
     "steam_set_barrier_spin_limit": (ctypes.c_int, [c_i64]),
+    "steam_bounded_add_group_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int, c_i32,
+                                                                 ctypes.POINTER(BAProblem),
+                                                                 c_i32]),
+    "steam_bounded_add_group_prepare": (ctypes.c_int, [ctypes.c_int, c_i32,
+                                                       ctypes.POINTER(BAProblem), c_i32, c_vp,
+                                                       ctypes.c_size_t]),
+    "steam_bounded_add_group_async": (ctypes.c_int, [c_vp, c_vp]),
+    "steam_bounded_add_group_release": (ctypes.c_int, [c_vp]),
     "steam_bounded_add_ledger_doubles": (c_size, [c_i32]),
     "steam_project_bounds_replay": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                                    c_dp, c_dbl, c_dbl, c_dp, c_vp, c_size,

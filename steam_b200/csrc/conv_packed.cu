@@ -420,35 +420,25 @@ bool even_about_centre(const double* t) {
   return true;
 }
 
-int resident_ctas() {
-  static std::atomic<int> cached{0};
-  int v = cached.load();
-  if (v) return v;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm, packed_conv_kernel<false, true, false>, kPThreads, kPSmem) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  v = per_sm * sm_count();
-  cached.store(v);
-  return v;
-}
-
 // x planes per CTA: the autotuner's choice for the shape, else the chunk
-// that minimises (waves of CTAs) x (planes per CTA, halo included)
+// that minimises the busiest SM's work.  Two CTAs fit an SM (registers and
+// shared memory) and share its issue slots, so an SM's time is the planes of
+// all CTAs it runs, halo included; a CTA alone on its SM runs at about 0.7 of
+// the pair's throughput (its barrier stalls are not covered).
 int64_t packed_chunk(int64_t nx, int64_t ny, int64_t nz) {
   const int over = chunk_override(nx, ny, nz);
   if (over > 0) return over;
   const int64_t tiles = ((nz + kPZ - 1) / kPZ) * ((ny + kPY - 1) / kPY);
-  const int64_t slots = resident_ctas();
-  int64_t best = nx, best_cost = -1;
+  const int64_t sms = sm_count();
+  int64_t best = nx;
+  double best_cost = -1.0;
   for (int64_t n = 1; n <= nx; ++n) {
     const int64_t chunk = (nx + n - 1) / n;
     if (chunk < kPChunkMin && n > 1) break;
-    const int64_t nchunks = (nx + chunk - 1) / chunk;
-    const int64_t waves = (tiles * nchunks + slots - 1) / slots;
-    const int64_t cost = waves * (chunk + kPK - 1);
-    if (best_cost < 0 || cost < best_cost) {
+    const int64_t ctas = tiles * ((nx + chunk - 1) / chunk);
+    const int64_t per_sm = (ctas + sms - 1) / sms;
+    const double cost = (double)(per_sm * (chunk + kPK - 1)) / (per_sm == 1 ? 0.7 : 1.0);
+    if (best_cost < 0.0 || cost < best_cost) {
       best_cost = cost;
       best = chunk;
     }
@@ -481,11 +471,13 @@ bool packed_supported(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t
     if (!even_about_centre(p.ztap(f))) return false;
   for (int f = 0; f < p.nyf; ++f)
     if (!even_about_centre(p.ytap(f))) return false;
-  if (nz % 4 != 0 || nz < kPC || ny % 2 != 0 || ny < 2 || nx < 1) return false;
+  // (a field thinner than the staged slab takes the same copies: the parts
+  // past its extent arrive as zeros)
+  if (nz % 4 != 0 || nz < 4 || ny % 2 != 0 || ny < 2 || nx < 1) return false;
   if (nx > INT32_MAX || ny > INT32_MAX || ny * nz > ((int64_t)1 << 31)) return false;
   if (((uintptr_t)in % 16) != 0 || ((uintptr_t)out % 16) != 0) return false;
-  if (!encode_fn()) return false;
-  return true;
+  CUtensorMap probe;
+  return encode_map(&probe, (const float*)in, nx, ny, nz, 2);
 }
 
 int64_t packed_grid(int64_t nx, int64_t ny, int64_t nz) {

@@ -13,6 +13,10 @@
 #include <cmath>
 #include <limits>
 #include <vector>
+#include <algorithm>
+#include <array>
+#include <mutex>
+#include <map>
 
 namespace steam {
 
@@ -623,12 +627,16 @@ __device__ __forceinline__ V ldc(const V* p) {
   return *p;
 }
 
+// vb / nvb: this block's index among the blocks that share the sweep of this
+// field, and their count (blockIdx.x / gridDim.x for a launch of its own; a
+// block's range within a grouped launch over several fields)
 template <typename T, int MODE, bool COH>
 __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__ pert,
                                              int record, int64_t nx, int64_t ny, int nz,
                                              const Win& w, const BAChain<T>& c,
                                              double* __restrict__ partials,
-                                             unsigned char* ba_smem, double* red) {
+                                             unsigned char* ba_smem, double* red, int vb,
+                                             int nvb) {
   // per level: fold step (dm, sc), final clip (dm), tentative step (dm),
   // mean, mu, candidates; flags as 0/1 in T
   T* s_fdm = reinterpret_cast<T*>(ba_smem);
@@ -735,7 +743,7 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   // stay pending: no later step joins them, and the apply sweep applies
   // them): it reads and writes nothing for them
   const bool work = active && !(MODE == BA_STATS && (on & 0xf00u) == 0u);
-  if ((MODE == BA_STATS || MODE == BA_MU) && blockIdx.x == 0)
+  if ((MODE == BA_STATS || MODE == BA_MU) && vb == 0)
     for (int g = threadIdx.x; g < nz / 4; g += blockDim.x)
       c.grp[g] = MODE == BA_STATS && (s_ton[4 * g] != (T)0 || s_ton[4 * g + 1] != (T)0 ||
                                        s_ton[4 * g + 2] != (T)0 || s_ton[4 * g + 3] != (T)0);
@@ -823,9 +831,9 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     }
   };
   if (active && MODE == BA_APPLY) {
-    const int64_t step = (int64_t)gridDim.x * cpi;
+    const int64_t step = (int64_t)nvb * cpi;
     ColWalk cw;
-    cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
+    cw.init((int64_t)vb * cpi + cofs, step, ny);
     // two columns in flight per thread
     constexpr int U = 2;
     while (cw.col + (U - 1) * step < ncol) {
@@ -855,9 +863,9 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     // ring by cp.async while it works on the current column, so the loads in
     // flight do not depend on registers (a thread reads back only what it
     // copied itself: no block barrier)
-    const int64_t step = (int64_t)gridDim.x * cpi;
+    const int64_t step = (int64_t)nvb * cpi;
     ColWalk cw, front;
-    cw.init((int64_t)blockIdx.x * cpi + cofs, step, ny);
+    cw.init((int64_t)vb * cpi + cofs, step, ny);
     front = cw;
     T* ring = reinterpret_cast<T*>(ba_smem + ba_fold_param_bytes<T>(nz));
     auto slot = [&](int s, int f) { return ring + ((size_t)(s * 2 + f) * kLvThreads + t) * 4; };
@@ -885,7 +893,7 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   }
   if (MODE == BA_APPLY) return;
   // deterministic reduction: per level, the cpi column slots in order
-  const int nb = gridDim.x;
+  const int nb = nvb;
   // partial rows: stats {sum d, sum |d|}; shift {mean_k, count_k} per candidate
   // (dealt over the groups in the loop: slot [cofs][gi][l], and 0 for the
   // levels of groups out of it, whose sums are not read)
@@ -906,7 +914,7 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
       const int col = compact ? (gix[z >> 2] >= 0 ? 4 * gix[z >> 2] + (z & 3) : -1) : z;
       if (col >= 0)
         for (int cc = 0; cc < cpi; ++cc) sacc += red[cc * rw + col];
-      partials[((size_t)q * nz + z) * nb + blockIdx.x] = sacc;
+      partials[((size_t)q * nz + z) * nb + vb] = sacc;
     }
   }
 }
@@ -921,7 +929,8 @@ __global__ void __launch_bounds__(kLvThreads, 4)
   if (c.run && *c.run == 0) return;
   __shared__ double red[4 * kLvThreads];
   extern __shared__ unsigned char ba_smem[];
-  ba_fold_body<T, MODE, false>(d0, pert, record, nx, ny, nz, w, c, partials, ba_smem, red);
+  ba_fold_body<T, MODE, false>(d0, pert, record, nx, ny, nz, w, c, partials, ba_smem, red,
+                               blockIdx.x, gridDim.x);
 }
 
 template <typename T>
@@ -1174,7 +1183,7 @@ __host__ __device__ inline int ba_flag_count(int R) {
 
 // chain reset and the mean profile, in the working dtype
 template <typename T>
-__global__ void ba_init_kernel(BAState<T> st, const double* __restrict__ mean_1d) {
+__device__ __forceinline__ void ba_init_body(const BAState<T>& st, const double* __restrict__ mean_1d) {
   const int nz = st.nz, R = st.R;
   for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
     st.nsteps[z] = 0;
@@ -1205,6 +1214,11 @@ __global__ void ba_init_kernel(BAState<T> st, const double* __restrict__ mean_1d
   }
 }
 
+template <typename T>
+__global__ void ba_init_kernel(BAState<T> st, const double* __restrict__ mean_1d) {
+  ba_init_body(st, mean_1d);
+}
+
 // reduce_partials_kernel that does nothing when its sweep did not run
 __global__ void reduce_partials_if_kernel(const double* __restrict__ partials, int nblocks,
                                           double* __restrict__ out, const int* __restrict__ run) {
@@ -1220,7 +1234,7 @@ __global__ void reduce_partials_if_kernel(const double* __restrict__ partials, i
 // Leaves the demean/clip/rescale loop: the final demean is the level's
 // current mean, and its shift solve starts from a bracket symmetric about 0.
 template <typename T>
-__device__ void ba_leave_loop(BAState<T>& st, int z) {
+__device__ void ba_leave_loop(const BAState<T>& st, int z) {
   st.still[z] = 0;
   st.final_d[z] = st.cur_mean[z];
   st.has_final[z] = 1;
@@ -1229,7 +1243,7 @@ __device__ void ba_leave_loop(BAState<T>& st, int z) {
 
 // Prepares rescale step k for a level still in the loop.
 template <typename T>
-__device__ void ba_prepare_step(BAState<T>& st, int z, int k, int* next_flag) {
+__device__ void ba_prepare_step(const BAState<T>& st, int z, int k, int* next_flag) {
   st.demean[z * st.R + k] = (T)st.cur_mean[z];
   st.scale[z * st.R + k] = (T)1;
   st.nsteps[z] = k + 1;
@@ -1239,7 +1253,7 @@ __device__ void ba_prepare_step(BAState<T>& st, int z, int k, int* next_flag) {
 
 // After a write-back sweep: every final part of the chain is now stored.
 template <typename T>
-__device__ void ba_note_stored(BAState<T>& st, int z) {
+__device__ void ba_note_stored(const BAState<T>& st, int z) {
   // only a statistics sweep that processed the level's group stores its
   // pending steps; a shift sweep stores nothing (the apply sweep applies
   // whatever is still pending)
@@ -1249,13 +1263,13 @@ __device__ void ba_note_stored(BAState<T>& st, int z) {
 }
 
 template <typename T>
-__device__ void ba_count_sweep(BAState<T>& st) {
+__device__ void ba_count_sweep(const BAState<T>& st) {
   if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
 }
 
 // After the first stats sweep: a0 = mean|d| and the entering mean.
 template <typename T>
-__global__ void ba_a0_kernel(BAState<T> st, const double* __restrict__ tot) {
+__device__ __forceinline__ void ba_a0_body(const BAState<T>& st, const double* __restrict__ tot) {
   const int nz = st.nz;
   ba_count_sweep(st);
   for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
@@ -1277,9 +1291,14 @@ __global__ void ba_a0_kernel(BAState<T> st, const double* __restrict__ tot) {
   }
 }
 
+template <typename T>
+__global__ void ba_a0_kernel(BAState<T> st, const double* __restrict__ tot) {
+  ba_a0_body(st, tot);
+}
+
 // After rescale sweep k.
 template <typename T, bool COH = false>
-__device__ void ba_loop_level(BAState<T>& st, const double* tot, int k, int z) {
+__device__ void ba_loop_level(const BAState<T>& st, const double* tot, int k, int z) {
   const int nz = st.nz;
   ba_note_stored(st, z);
   if (!st.still[z]) return;
@@ -1315,7 +1334,7 @@ __global__ void ba_loop_kernel(BAState<T> st, const double* __restrict__ tot, in
 // After the loop: every active level starts its shift solve.  Its first
 // candidate is mu = 0, whose mean is the post-clip level mean.
 template <typename T>
-__global__ void ba_mu_init_kernel(BAState<T> st) {
+__device__ __forceinline__ void ba_mu_init_body(const BAState<T>& st) {
   const int nz = st.nz;
   for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += gridDim.x * blockDim.x) {
     if (!st.active[z]) continue;
@@ -1330,9 +1349,14 @@ __global__ void ba_mu_init_kernel(BAState<T> st) {
   }
 }
 
+template <typename T>
+__global__ void ba_mu_init_kernel(BAState<T> st) {
+  ba_mu_init_body(st);
+}
+
 // After mu sweep it.
 template <typename T, bool COH = false>
-__device__ void ba_mu_level(BAState<T>& st, const double* tot, int it, int z) {
+__device__ void ba_mu_level(const BAState<T>& st, const double* tot, int it, int z) {
   const int nz = st.nz;
   ba_note_stored(st, z);
   if (!st.need[z]) return;
@@ -1381,7 +1405,8 @@ __global__ void ba_mu_kernel(BAState<T> st, const double* __restrict__ tot, int 
 constexpr long long kBarSpinLimit = 1ll << 26;  // ~ seconds with the back-off below
 std::atomic<long long> g_bar_spin_limit{kBarSpinLimit};
 
-__device__ bool grid_barrier(unsigned* bar, long long spin_limit) {
+// `nblocks` blocks meet at `bar` (the blocks of one field's phase)
+__device__ bool grid_barrier(unsigned* bar, long long spin_limit, unsigned nblocks) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1391,7 +1416,7 @@ __device__ bool grid_barrier(unsigned* bar, long long spin_limit) {
     const unsigned g = *vgen;
     __threadfence();
     const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-    if (arrived == gridDim.x) {
+    if (arrived == nblocks) {
       atomicExch(bar, 0u);
       __threadfence();
       atomicAdd(bar + 1, 1u);
@@ -1412,6 +1437,43 @@ __device__ bool grid_barrier(unsigned* bar, long long spin_limit) {
   return ok_s != 0;
 }
 
+// One field's persistent phase on blocks vb = 0 .. nvb - 1 of the launch.
+template <typename T, int MODE>
+__device__ __forceinline__ void ba_phase_body(T* __restrict__ d0, T* __restrict__ pert,
+                                              int64_t nx, int64_t ny, int nz, const Win& w,
+                                              BAChain<T> c, const BAState<T>& st,
+                                              double* __restrict__ partials,
+                                              double* __restrict__ totals, int flag_base,
+                                              int n_iter, unsigned char* ba_smem, double* red,
+                                              int vb, int nvb) {
+  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
+  const int nb = nvb;
+  c.run = nullptr;
+  for (int it = 0; it < n_iter; ++it) {
+    // read after a barrier: every block sees the same flag
+    if (__ldcg(st.flags + flag_base + it) == 0) break;
+    ba_fold_body<T, MODE, true>(d0, pert, 0, nx, ny, nz, w, c, partials, ba_smem, red, vb,
+                                nvb);
+    if (!grid_barrier(st.bar, st.spin_limit, nvb)) return;
+    // totals[r] = the r-th row of block partials, summed in a fixed order
+    for (int r = vb; r < Q * nz; r += nb) {
+      double acc = 0.0;
+      for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += __ldcg(partials + (size_t)r * nb + i);
+      const double sum = block_sum(acc, red);
+      if (threadIdx.x == 0) totals[r] = sum;
+    }
+    if (!grid_barrier(st.bar, st.spin_limit, nvb)) return;
+    if (vb == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
+    for (int z = vb * blockDim.x + threadIdx.x; z < nz; z += nb * blockDim.x) {
+      if (MODE == BA_MU)
+        ba_mu_level<T, true>(st, totals, it, z);
+      else
+        ba_loop_level<T, true>(st, totals, it, z);
+    }
+    if (!grid_barrier(st.bar, st.spin_limit, nvb)) return;
+  }
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_kernel(
     T* __restrict__ d0, T* __restrict__ pert, int64_t nx, int64_t ny, int nz, Win w,
@@ -1419,36 +1481,13 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_
     int flag_base, int n_iter) {
   __shared__ double red[4 * kLvThreads];
   extern __shared__ unsigned char ba_smem[];
-  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
-  const int nb = gridDim.x;
-  c.run = nullptr;
-  for (int it = 0; it < n_iter; ++it) {
-    // read after a barrier: every block sees the same flag
-    if (__ldcg(st.flags + flag_base + it) == 0) break;
-    ba_fold_body<T, MODE, true>(d0, pert, 0, nx, ny, nz, w, c, partials, ba_smem, red);
-    if (!grid_barrier(st.bar, st.spin_limit)) return;
-    // totals[r] = the r-th row of block partials, summed in a fixed order
-    for (int r = blockIdx.x; r < Q * nz; r += nb) {
-      double acc = 0.0;
-      for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += __ldcg(partials + (size_t)r * nb + i);
-      const double sum = block_sum(acc, red);
-      if (threadIdx.x == 0) totals[r] = sum;
-    }
-    if (!grid_barrier(st.bar, st.spin_limit)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
-    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < nz; z += nb * blockDim.x) {
-      if (MODE == BA_MU)
-        ba_mu_level<T, true>(st, totals, it, z);
-      else
-        ba_loop_level<T, true>(st, totals, it, z);
-    }
-    if (!grid_barrier(st.bar, st.spin_limit)) return;
-  }
+  ba_phase_body<T, MODE>(d0, pert, nx, ny, nz, w, c, st, partials, totals, flag_base, n_iter,
+                         ba_smem, red, blockIdx.x, gridDim.x);
 }
 
 // Fixes mu for the levels that needed a shift and writes the ledger.
 template <typename T>
-__global__ void ba_finish_kernel(BAState<T> st) {
+__device__ __forceinline__ void ba_finish_body(const BAState<T>& st) {
   const int nz = st.nz;
   // + the apply sweep; -1 when a persistent phase's grid barrier gave up
   const int sweeps = st.bar[2] ? -1 : st.flags[ba_flag_count<T>(st.R) - 1] + 1;
@@ -1477,6 +1516,11 @@ __global__ void ba_finish_kernel(BAState<T> st) {
   }
 }
 
+template <typename T>
+__global__ void ba_finish_kernel(BAState<T> st) {
+  ba_finish_body(st);
+}
+
 static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
   return carve_bytes((size_t)3 * nz, sizeof(int)) +                       // nsteps, has_final, has_mu
          carve_bytes((size_t)nz * (2 * (size_t)R + 4 + kMuCand), elem) +   // chain values
@@ -1489,6 +1533,73 @@ static size_t ba_state_bytes(int64_t nz, int R, size_t elem) {
          carve_bytes((size_t)nz, sizeof(double)) +                          // mean upload
          carve_bytes((size_t)nz / 4 + 1, sizeof(int)) +                     // grp
          (size_t)32 * 256;  // the 256-byte alignment of every separate carve
+}
+
+// The solve's per-level state, carved from a workspace (the ledger too when
+// `own_ledger`); false when it does not fit.
+template <typename T>
+static bool carve_ba_state(Carver& c, int64_t nz, int R, bool own_ledger, BAState<T>& st) {
+  st.nsteps = c.take<int>(nz);
+  st.has_final = c.take<int>(nz);
+  st.has_mu = c.take<int>(nz);
+  st.demean = c.take<T>((size_t)nz * (R > 0 ? R : 1));
+  st.scale = c.take<T>((size_t)nz * (R > 0 ? R : 1));
+  st.final_dm = c.take<T>(nz);
+  st.mu = c.take<T>(nz);
+  st.mean = c.take<T>(nz);
+  st.cand = c.take<T>((size_t)nz * kMuCand);
+  st.a0 = c.take<double>(nz);
+  st.cur_mean = c.take<double>(nz);
+  st.final_d = c.take<double>(nz);
+  st.active = c.take<int>(nz);
+  st.still = c.take<int>(nz);
+  st.n_loop = c.take<int>(nz);
+  st.need = c.take<int>(nz);
+  st.applied = c.take<int>(nz);
+  st.fin_stored = c.take<int>(nz);
+  st.grp = c.take<int>(nz / 4 + 1);
+  st.solver = c.take<MuSolver<T>>(nz);
+  st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
+  st.bar = c.take<unsigned>(4);
+  st.ledger = own_ledger ? c.take<double>((size_t)ba_ledger_width(R) * nz) : nullptr;
+  return st.nsteps && st.has_final && st.has_mu && st.demean && st.scale && st.final_dm &&
+         st.mu && st.mean && st.cand && st.a0 && st.cur_mean && st.final_d && st.active &&
+         st.still && st.n_loop && st.need && st.applied && st.fin_stored && st.grp &&
+         st.solver && st.flags && st.bar && (st.ledger || !own_ledger);
+}
+
+template <typename T>
+static void set_ba_scalars(BAState<T>& st, int64_t nz, int R, const Win& w, double phi_min,
+                           double phi_max) {
+  st.R = R;
+  st.nz = (int)nz;
+  st.spin_limit = g_bar_spin_limit.load();
+  st.N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
+  st.width = phi_max - phi_min;
+  st.tol_rel = sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49);
+}
+
+template <typename T>
+static BAChain<T> ba_chain(const BAState<T>& st, int R, double phi_min, double phi_max) {
+  BAChain<T> ch;
+  ch.nsteps = st.nsteps;
+  ch.demean = st.demean;
+  ch.scale = st.scale;
+  ch.has_final = st.has_final;
+  ch.final_dm = st.final_dm;
+  ch.has_mu = st.has_mu;
+  ch.mu = st.mu;
+  ch.cand = st.cand;
+  ch.mean = st.mean;
+  ch.run = nullptr;
+  ch.applied = st.applied;
+  ch.fin_stored = st.fin_stored;
+  ch.still = st.still;
+  ch.grp = st.grp;
+  ch.R = R;
+  ch.lo = (T)phi_min;
+  ch.hi = (T)phi_max;
+  return ch;
 }
 
 // Enqueues the whole bounded add on stream s: no host synchronisation and no
@@ -1514,41 +1625,9 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   double* partials = c.take<double>((size_t)grid * Qmax * nz);
   double* totals = c.take<double>((size_t)Qmax * nz);
   BAState<T> st;
-  st.nsteps = c.take<int>(nz);
-  st.has_final = c.take<int>(nz);
-  st.has_mu = c.take<int>(nz);
-  st.demean = c.take<T>((size_t)nz * (R > 0 ? R : 1));
-  st.scale = c.take<T>((size_t)nz * (R > 0 ? R : 1));
-  st.final_dm = c.take<T>(nz);
-  st.mu = c.take<T>(nz);
-  st.mean = c.take<T>(nz);
-  st.cand = c.take<T>((size_t)nz * kMuCand);
-  st.a0 = c.take<double>(nz);
-  st.cur_mean = c.take<double>(nz);
-  st.final_d = c.take<double>(nz);
-  st.active = c.take<int>(nz);
-  st.still = c.take<int>(nz);
-  st.n_loop = c.take<int>(nz);
-  st.need = c.take<int>(nz);
-  st.applied = c.take<int>(nz);
-  st.fin_stored = c.take<int>(nz);
-  st.grp = c.take<int>(nz / 4 + 1);
-  st.solver = c.take<MuSolver<T>>(nz);
-  st.flags = c.take<int>((size_t)ba_flag_count<T>(R));
-  st.bar = c.take<unsigned>(4);
-  st.ledger = c.take<double>((size_t)ba_ledger_width(R) * nz);
-  if (!partials || !totals || !st.nsteps || !st.has_final || !st.has_mu || !st.demean ||
-      !st.scale || !st.final_dm || !st.mu || !st.mean || !st.cand || !st.a0 || !st.cur_mean ||
-      !st.final_d || !st.active || !st.still || !st.n_loop || !st.need || !st.applied ||
-      !st.fin_stored || !st.grp || !st.solver ||
-      !st.flags || !st.bar || !st.ledger)
+  if (!partials || !totals || !carve_ba_state<T>(c, nz, R, true, st))
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add: workspace too small");
-  st.R = R;
-  st.nz = (int)nz;
-  st.spin_limit = g_bar_spin_limit.load();
-  st.N = (double)((w.x1 - w.x0) * (w.y1 - w.y0));
-  st.width = phi_max - phi_min;
-  st.tol_rel = sizeof(T) == 4 ? ldexp(1.0, -20) : ldexp(1.0, -49);
+  set_ba_scalars(st, nz, R, w, phi_min, phi_max);
   *ledger_dev = st.ledger;
 
   const bool vec4 = nz % 4 == 0 && nz <= 4 * kLvThreads &&
@@ -1582,23 +1661,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
     STEAM_CUDA(cudaFuncSetAttribute(ba_sweep_kernel<T, BA_APPLY, kLvMaxJ>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ba_sm));
   }
-  BAChain<T> ch;
-  ch.nsteps = st.nsteps;
-  ch.demean = st.demean;
-  ch.scale = st.scale;
-  ch.has_final = st.has_final;
-  ch.final_dm = st.final_dm;
-  ch.has_mu = st.has_mu;
-  ch.mu = st.mu;
-  ch.cand = st.cand;
-  ch.mean = st.mean;
-  ch.applied = st.applied;
-  ch.fin_stored = st.fin_stored;
-  ch.still = st.still;
-  ch.grp = st.grp;
-  ch.R = R;
-  ch.lo = (T)phi_min;
-  ch.hi = (T)phi_max;
+  BAChain<T> ch = ba_chain(st, R, phi_min, phi_max);
   const int lv_blocks = (int)((nz + 255) / 256);
 
   auto sweep = [&](int mode, const int* run, T* out, int rec) -> int {
@@ -1719,6 +1782,289 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
   STEAM_LAUNCH_CHECK("bounded_add finish");
   // apply (always runs)
   if ((rc = sweep(BA_APPLY, nullptr, inc, record))) return rc;
+  return STEAM_OK;
+}
+
+// ---- grouped bounded adds: many fields, one launch per stage ------------------
+// An ensemble's members each run a bounded add on fields of their own shape.
+// Launched one by one, each solve pays its launch and grid-barrier latency on
+// its own; here all of them share one launch per stage: the first sweep and
+// the apply sweep over a flat grid in which every field owns a contiguous
+// range of blocks, the small per-level kernels over a (levels, fields) grid,
+// and each persistent phase as ONE cooperative launch whose blocks split into
+// per-field teams, each with its own grid barrier (a team waits only for its
+// own field's blocks).  Each field's block counts follow from its own shape
+// alone, so its sums -- and its result -- do not depend on the other fields.
+// Only the vectorised layout (nz % 4 == 0, 16-byte aligned fields) is
+// grouped.
+constexpr int kGroupFoldGroups = 64;     // column groups per block, first/apply sweeps
+constexpr int kGroupPhaseGroups = 2048;  // column groups per block, persistent phases
+
+template <typename T>
+struct BAGroupRec {
+  BAState<T> st;
+  BAChain<T> ch;
+  T* pert;
+  T* inc;
+  double* partials;
+  double* totals;
+  const double* mean;
+  Win w;
+  int64_t nx, ny;
+  int nz;
+  int fold_nb;  // blocks of the first and apply sweeps
+  int ph_nb;    // blocks of each persistent phase
+};
+
+// the field that owns block b of a grouped launch: start[p] <= b < start[p + 1]
+__device__ __forceinline__ int group_owner(const int* __restrict__ start, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T>
+__global__ void bag_init_kernel(const BAGroupRec<T>* __restrict__ recs) {
+  const BAGroupRec<T>& r = recs[blockIdx.y];
+  ba_init_body(r.st, r.mean);
+}
+
+template <typename T>
+__global__ void bag_a0_kernel(const BAGroupRec<T>* __restrict__ recs) {
+  const BAGroupRec<T>& r = recs[blockIdx.y];
+  ba_a0_body(r.st, r.totals);
+}
+
+template <typename T>
+__global__ void bag_mu_init_kernel(const BAGroupRec<T>* __restrict__ recs) {
+  ba_mu_init_body(recs[blockIdx.y].st);
+}
+
+template <typename T>
+__global__ void bag_finish_kernel(const BAGroupRec<T>* __restrict__ recs) {
+  ba_finish_body(recs[blockIdx.y].st);
+}
+
+// totals[row] of the first sweep, rows 2 nz of each field (y: the field)
+template <typename T>
+__global__ void bag_reduce_kernel(const BAGroupRec<T>* __restrict__ recs) {
+  __shared__ double scratch[32];
+  const BAGroupRec<T>& r = recs[blockIdx.y];
+  const int nb = r.fold_nb;
+  for (int row = blockIdx.x; row < 2 * r.nz; row += gridDim.x) {
+    const double* src = r.partials + (size_t)row * nb;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += src[i];
+    const double sum = block_sum(acc, scratch);
+    if (threadIdx.x == 0) r.totals[row] = sum;
+  }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, 4)
+    bag_fold_kernel(const BAGroupRec<T>* __restrict__ recs, const int* __restrict__ start,
+                    int n) {
+  __shared__ double red[4 * kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  const int p = group_owner(start, n, blockIdx.x);
+  const BAGroupRec<T>& r = recs[p];
+  ba_fold_body<T, MODE, false>(r.inc, r.pert, 0, r.nx, r.ny, r.nz, r.w, r.ch, r.partials,
+                               ba_smem, red, blockIdx.x - __ldg(start + p), r.fold_nb);
+}
+
+// one cooperative launch of a phase over fields p0 .. p0 + n - 1; start[i]:
+// the first block of field p0 + i
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3))
+    bag_phase_kernel(const BAGroupRec<T>* __restrict__ recs, const int* __restrict__ start,
+                     int p0, int n, int flag_base, int n_iter) {
+  __shared__ double red[4 * kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  const int i = group_owner(start, n, blockIdx.x);
+  const BAGroupRec<T>& r = recs[p0 + i];
+  ba_phase_body<T, MODE>(r.inc, r.pert, r.nx, r.ny, r.nz, r.w, r.ch, r.st, r.partials,
+                         r.totals, flag_base, n_iter, ba_smem, red,
+                         blockIdx.x - __ldg(start + i), r.ph_nb);
+}
+
+struct BAGroupPlan {
+  int dtype = 0, n = 0, R = 0;
+  int nz_max = 0;
+  int fold_blocks = 0;            // total blocks of the flat sweeps
+  size_t sm_sums = 0, sm_apply = 0;
+  void* recs = nullptr;           // device BAGroupRec<T>[n]
+  int* fold_start = nullptr;      // device [n]
+  int* ph_start = nullptr;        // device [n]: first block within the field's batch
+  std::vector<std::array<int, 3>> batches;  // {first field, fields, blocks}
+};
+static std::mutex g_group_mu;
+static std::map<void*, BAGroupPlan> g_groups;
+
+static size_t group_state_bytes(const steam_ba_problem_t& q, int R, size_t elem) {
+  // state, partials of either sweep kind, totals
+  const int64_t nz = q.nz;
+  const int64_t ncol = q.nx * q.ny;
+  const int64_t cpb = nz > 0 ? kLvThreads / (nz / 4) : 1;
+  const int64_t groups = (ncol + cpb - 1) / cpb;
+  const int64_t nb = std::max<int64_t>(
+      std::max<int64_t>((groups + kGroupFoldGroups - 1) / kGroupFoldGroups, 1),
+      std::max<int64_t>((groups + kGroupPhaseGroups - 1) / kGroupPhaseGroups, 1));
+  return ba_state_bytes(nz, R, elem) +
+         carve_bytes((size_t)nb * 2 * kMuCand * nz, sizeof(double)) +
+         carve_bytes((size_t)2 * kMuCand * nz, sizeof(double)) + 512;
+}
+
+template <typename T>
+static size_t group_bytes(int n, const steam_ba_problem_t* q, int R) {
+  size_t b = carve_bytes((size_t)n, sizeof(BAGroupRec<T>)) + 2 * carve_bytes((size_t)n, sizeof(int));
+  for (int i = 0; i < n; ++i) b += group_state_bytes(q[i], R, sizeof(T));
+  return b + 4096;
+}
+
+template <typename T>
+static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, size_t ws_bytes,
+                         int dtype) {
+  Carver c(ws, ws_bytes);
+  BAGroupPlan plan;
+  plan.dtype = dtype;
+  plan.n = n;
+  plan.R = R;
+  plan.recs = c.take<BAGroupRec<T>>((size_t)n);
+  plan.fold_start = c.take<int>((size_t)n);
+  plan.ph_start = c.take<int>((size_t)n);
+  if (!plan.recs || !plan.fold_start || !plan.ph_start)
+    return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
+  std::vector<BAGroupRec<T>> recs((size_t)n);
+  std::vector<int> fold_start((size_t)n), ph_start((size_t)n), ph_nb((size_t)n);
+  int fold_total = 0;
+  for (int i = 0; i < n; ++i) {
+    const steam_ba_problem_t& p = q[i];
+    const int64_t nz = p.nz, ncol = p.nx * p.ny;
+    const steam_window_t* win = p.has_window ? &p.window : nullptr;
+    BAGroupRec<T>& r = recs[(size_t)i];
+    r.w = make_win(win, p.nx, p.ny);
+    if (!carve_ba_state<T>(c, nz, R, p.ledger == nullptr, r.st))
+      return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
+    if (p.ledger) r.st.ledger = p.ledger;
+    set_ba_scalars(r.st, nz, R, r.w, p.phi_min, p.phi_max);
+    r.ch = ba_chain(r.st, R, p.phi_min, p.phi_max);
+    const int64_t cpb = kLvThreads / (nz / 4);
+    const int64_t groups = (ncol + cpb - 1) / cpb;
+    r.fold_nb = (int)std::max<int64_t>((groups + kGroupFoldGroups - 1) / kGroupFoldGroups, 1);
+    r.ph_nb = (int)std::max<int64_t>((groups + kGroupPhaseGroups - 1) / kGroupPhaseGroups, 1);
+    const int nbmax = std::max(r.fold_nb, r.ph_nb);
+    r.partials = c.take<double>((size_t)nbmax * 2 * kMuCand * nz);
+    r.totals = c.take<double>((size_t)2 * kMuCand * nz);
+    if (!r.partials || !r.totals)
+      return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
+    r.st.wb = 1;
+    r.pert = (T*)p.pert;
+    r.inc = (T*)p.increment;
+    r.mean = p.mean;
+    r.nx = p.nx;
+    r.ny = p.ny;
+    r.nz = (int)nz;
+    fold_start[(size_t)i] = fold_total;
+    fold_total += r.fold_nb;
+    ph_nb[(size_t)i] = r.ph_nb;
+    plan.nz_max = std::max(plan.nz_max, (int)nz);
+  }
+  plan.fold_blocks = fold_total;
+  plan.sm_sums = ba_fold_smem_bytes<T>(plan.nz_max);
+  plan.sm_apply = ba_fold_param_bytes<T>(plan.nz_max);
+  // co-resident capacity of the cooperative phases (the smaller of the two)
+  int cap = 0;
+  for (int mode = 0; mode < 2; ++mode) {
+    auto kern = mode ? bag_phase_kernel<T, BA_MU> : bag_phase_kernel<T, BA_STATS>;
+    STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)plan.sm_sums));
+    int per_sm = 0;
+    STEAM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLvThreads,
+                                                             plan.sm_sums));
+    STEAM_REQUIRE(per_sm >= 1, "steam_bounded_add_group_prepare: a phase does not fit an SM");
+    const int c_m = per_sm * sm_count();
+    cap = cap == 0 ? c_m : std::min(cap, c_m);
+  }
+  // teams in batches that fit the co-resident capacity (a field's team is
+  // never split; a team larger than the capacity is cut to it)
+  int b0 = 0, bn = 0, bblocks = 0;
+  for (int i = 0; i < n; ++i) {
+    int nb = std::min(ph_nb[(size_t)i], cap);
+    if (nb != ph_nb[(size_t)i]) {
+      recs[(size_t)i].ph_nb = nb;
+      ph_nb[(size_t)i] = nb;
+    }
+    if (bblocks + nb > cap) {
+      plan.batches.push_back({b0, bn, bblocks});
+      b0 = i;
+      bn = 0;
+      bblocks = 0;
+    }
+    ph_start[(size_t)i] = bblocks;
+    bblocks += nb;
+    ++bn;
+  }
+  if (bn > 0) plan.batches.push_back({b0, bn, bblocks});
+  STEAM_CUDA(cudaMemcpy(plan.recs, recs.data(), sizeof(BAGroupRec<T>) * (size_t)n,
+                        cudaMemcpyHostToDevice));
+  STEAM_CUDA(cudaMemcpy(plan.fold_start, fold_start.data(), sizeof(int) * (size_t)n,
+                        cudaMemcpyHostToDevice));
+  STEAM_CUDA(cudaMemcpy(plan.ph_start, ph_start.data(), sizeof(int) * (size_t)n,
+                        cudaMemcpyHostToDevice));
+  STEAM_CUDA(cudaFuncSetAttribute(bag_fold_kernel<T, BA_SUMS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)plan.sm_sums));
+  STEAM_CUDA(cudaFuncSetAttribute(bag_fold_kernel<T, BA_APPLY>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)plan.sm_apply));
+  std::lock_guard<std::mutex> lock(g_group_mu);
+  g_groups[ws] = plan;
+  return STEAM_OK;
+}
+
+template <typename T>
+static int group_enqueue(const BAGroupPlan& plan, cudaStream_t s) {
+  const auto* recs = (const BAGroupRec<T>*)plan.recs;
+  const int n = plan.n, R = plan.R;
+  const dim3 lv((unsigned)((plan.nz_max + 255) / 256), (unsigned)n);
+  bag_init_kernel<T><<<lv, 256, 0, s>>>(recs);
+  STEAM_LAUNCH_CHECK("bounded_add group init");
+  bag_fold_kernel<T, BA_SUMS><<<plan.fold_blocks, kLvThreads, plan.sm_sums, s>>>(
+      recs, plan.fold_start, n);
+  STEAM_LAUNCH_CHECK("bounded_add group sweep");
+  bag_reduce_kernel<T><<<dim3((unsigned)std::min(2 * plan.nz_max, 512), (unsigned)n), 256, 0,
+                         s>>>(recs);
+  STEAM_LAUNCH_CHECK("bounded_add group reduce");
+  bag_a0_kernel<T><<<lv, 256, 0, s>>>(recs);
+  STEAM_LAUNCH_CHECK("bounded_add group a0");
+  auto phase = [&](int mode, int flag_base, int n_iter) -> int {
+    auto kern = mode == BA_MU ? bag_phase_kernel<T, BA_MU> : bag_phase_kernel<T, BA_STATS>;
+    for (const auto& b : plan.batches) {
+      int p0 = b[0], nb = b[1];
+      const int* start = plan.ph_start + p0;
+      void* args[] = {(void*)&recs, (void*)&start, &p0, &nb, &flag_base, &n_iter};
+      STEAM_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)b[2]),
+                                             dim3(kLvThreads), args, plan.sm_sums, s));
+      count_launch();
+    }
+    return STEAM_OK;
+  };
+  int rc;
+  if (R > 0 && (rc = phase(BA_STATS, 1, R))) return rc;
+  bag_mu_init_kernel<T><<<lv, 256, 0, s>>>(recs);
+  STEAM_LAUNCH_CHECK("bounded_add group mu init");
+  if ((rc = phase(BA_MU, 1 + R, kMuMaxSweeps))) return rc;
+  bag_finish_kernel<T><<<lv, 256, 0, s>>>(recs);
+  STEAM_LAUNCH_CHECK("bounded_add group finish");
+  bag_fold_kernel<T, BA_APPLY><<<plan.fold_blocks, kLvThreads, plan.sm_apply, s>>>(
+      recs, plan.fold_start, n);
+  STEAM_LAUNCH_CHECK("bounded_add group apply");
   return STEAM_OK;
 }
 
@@ -2417,6 +2763,74 @@ extern "C" int steam_bounded_add_async(int dtype, int64_t nx, int64_t ny, int64_
                                      record_applied, nullptr, ledger_dev, workspace,
                                      workspace_bytes, s);
   return fail(STEAM_ERR_ARG, "steam_bounded_add_async: bad dtype");
+}
+
+static int group_check(int dtype, int32_t n, const steam_ba_problem_t* q, int32_t R) {
+  STEAM_REQUIRE(dtype == STEAM_F32 || dtype == STEAM_F64,
+                "steam_bounded_add_group: bad dtype");
+  STEAM_REQUIRE(n >= 1 && q != nullptr, "steam_bounded_add_group: no fields");
+  STEAM_REQUIRE(R >= 0 && R <= 64, "steam_bounded_add_group: n_rescale out of range");
+  const size_t elem = dtype == STEAM_F64 ? 8 : 4;
+  for (int i = 0; i < n; ++i) {
+    const steam_ba_problem_t& p = q[i];
+    const std::string who = "steam_bounded_add_group: field " + std::to_string(i);
+    STEAM_REQUIRE(p.nx >= 1 && p.ny >= 1 && p.nz >= 4, who + ": empty or thinner than 4 levels");
+    STEAM_REQUIRE(p.nz % 4 == 0 && p.nz <= 4 * kLvThreads,
+                  who + ": nz must be a multiple of 4, at most 1024");
+    STEAM_REQUIRE(p.pert && p.increment && p.mean, who + ": null pointer");
+    STEAM_REQUIRE((uintptr_t)p.pert % 16 == 0 && (uintptr_t)p.increment % 16 == 0,
+                  who + ": fields must be 16-byte aligned");
+    STEAM_REQUIRE(p.phi_max > p.phi_min, who + ": phi_max must exceed phi_min");
+    STEAM_REQUIRE((elem == 4 ? ba_fold_smem_bytes<float>(p.nz) : ba_fold_smem_bytes<double>(p.nz)) <=
+                      200 * 1024,
+                  who + ": nz too large");
+    if (p.has_window) {
+      int rc = check_win(&p.window, p.nx, p.ny, who.c_str());
+      if (rc) return rc;
+      STEAM_REQUIRE(p.window.x1 > p.window.x0 && p.window.y1 > p.window.y0,
+                    who + ": empty window");
+    }
+  }
+  return STEAM_OK;
+}
+
+extern "C" size_t steam_bounded_add_group_workspace_bytes(int dtype, int32_t n,
+                                                          const steam_ba_problem_t* problems,
+                                                          int32_t n_rescale) {
+  if (n < 1 || !problems) return 0;
+  return dtype == STEAM_F64 ? group_bytes<double>(n, problems, n_rescale)
+                            : group_bytes<float>(n, problems, n_rescale);
+}
+
+extern "C" int steam_bounded_add_group_prepare(int dtype, int32_t n,
+                                               const steam_ba_problem_t* problems,
+                                               int32_t n_rescale, void* workspace,
+                                               size_t workspace_bytes) {
+  int rc = group_check(dtype, n, problems, n_rescale);
+  if (rc) return rc;
+  STEAM_REQUIRE(workspace != nullptr, "steam_bounded_add_group_prepare: null workspace");
+  if (dtype == STEAM_F32)
+    return group_prepare<float>(n, problems, n_rescale, workspace, workspace_bytes, dtype);
+  return group_prepare<double>(n, problems, n_rescale, workspace, workspace_bytes, dtype);
+}
+
+extern "C" int steam_bounded_add_group_async(void* workspace, steam_stream_t stream) {
+  BAGroupPlan plan;
+  {
+    std::lock_guard<std::mutex> lock(g_group_mu);
+    auto it = g_groups.find(workspace);
+    STEAM_REQUIRE(it != g_groups.end(),
+                  "steam_bounded_add_group_async: workspace holds no prepared group");
+    plan = it->second;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  return plan.dtype == STEAM_F32 ? group_enqueue<float>(plan, s) : group_enqueue<double>(plan, s);
+}
+
+extern "C" int steam_bounded_add_group_release(void* workspace) {
+  std::lock_guard<std::mutex> lock(g_group_mu);
+  g_groups.erase(workspace);
+  return STEAM_OK;
 }
 
 extern "C" int steam_project_bounds(int dtype, int64_t nx, int64_t ny,

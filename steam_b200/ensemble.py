@@ -4,11 +4,14 @@ A member is one class step of its own world (its shape, seed, alpha, C1, H,
 Hz): the finest class of a root run over the member's domain, run by a
 ``ResidentClass`` on device fields.  ``Ensemble`` spreads the members over a
 few CUDA streams and captures one step of all of them into a single CUDA
-graph: a replay then issues every member's 32 library launches (noise, the
-three convolutions, patterns, the bounded adds' sweeps and persistent solve
-phases, thermodynamics) with one launch call, and members of uneven sizes fill
-the GPU side by side (a bounded add's persistent phase is sized by its
-member's work, so a small member's phase leaves most SMs to the others).
+graph: a replay then issues the whole step with one launch call.  The step
+runs stage by stage: every member's flux advance and h increment (its
+streaming kernels, spread over the streams), then ONE grouped bounded add of
+h over all members (``steam_bounded_add_group_async``: one launch per stage of
+the solve, each persistent phase a single cooperative launch whose blocks
+split into per-member teams with their own grid barriers), every member's qt
+increment, one grouped bounded add of qt, and every member's thermodynamics.
+Members of uneven sizes fill the GPU side by side.
 
 ``autotune_conv`` is the tile-shape autotuner: for a field shape it times the
 fused convolution at a few x-chunk lengths (planes per CTA; short chunks give
@@ -26,6 +29,7 @@ import numpy as np
 from . import _lib
 from . import simulate as sim
 from . import utils as _utils
+from . import resident as _resident
 from .resident import ResidentClass
 
 CHUNKS = (16, 32, 64, 128, 256, 384, 512)
@@ -132,6 +136,16 @@ class Member:
     def step(self):
         self.rc.step(self.h, self.q, self.F, diagnostics=self.diag)
 
+    def buffers(self):
+        """The member's work fields for a stage-by-stage step: the product,
+        the pattern, and one increment per scalar (both bounded adds of the
+        ensemble run after all members' increments are in)."""
+        import torch
+        product, W, inc_h = self.rc._work(self.F)
+        if getattr(self, 'inc_qt', None) is None:
+            self.inc_qt = torch.empty_like(inc_h)
+        return product, W, inc_h, self.inc_qt
+
 
 class Ensemble:
     """Members spread over ``n_streams`` streams; one step of all of them
@@ -139,9 +153,11 @@ class Ensemble:
     starts from the members' initial state (the reset copies are part of it),
     so every step does the same work."""
 
-    def __init__(self, members, n_streams=4, tune=True):
+    def __init__(self, members, n_streams=4, tune=True, grouped=True):
         torch = _lib.require_cuda("Ensemble")
         self.members = list(members)
+        self.grouped = False
+        self.groups = {}
         self.streams = [torch.cuda.Stream() for _ in range(max(1, int(n_streams)))]
         # largest members first, dealt round-robin, so the streams carry
         # similar work
@@ -160,6 +176,91 @@ class Ensemble:
         # and its stream's workspace before anything is captured
         self.step_eager()
         torch.cuda.synchronize()
+        if grouped:
+            self.groups = self._prepare_groups()
+            self.grouped = bool(self.groups)
+            if self.grouped:
+                self.step_eager()
+                torch.cuda.synchronize()
+
+    def _prepare_groups(self):
+        """One grouped bounded add per scalar over every member (members
+        whose layout the grouped solve does not take -- nz % 4 != 0 or
+        unaligned fields -- keep the per-member path for the whole step)."""
+        import torch
+        lib = _lib.load()
+        groups = {}
+        if any(m.rc.code != self.members[0].rc.code or m.voxels == 0 or
+               m.params['shape'][2] % 4 for m in self.members):
+            return {}
+        code = self.members[0].rc.code
+        for name in ('h', 'qt'):
+            probs = []
+            for m in self.members:
+                _, _, inc_h, inc_qt = m.buffers()
+                pert, inc = (m.h, inc_h) if name == 'h' else (m.q, inc_qt)
+                probs.append(m.rc.bounded_add_problem(name, pert, inc))
+            arr = (_lib.BAProblem * len(probs))(*probs)
+            nbytes = lib.steam_bounded_add_group_workspace_bytes(code, len(probs), arr,
+                                                                 _resident.N_RESCALE)
+            ws = torch.empty(int(nbytes), dtype=torch.uint8, device='cuda')
+            _lib.check(lib.steam_bounded_add_group_prepare(
+                code, len(probs), arr, _resident.N_RESCALE, _lib.ptr(ws), int(nbytes)))
+            groups[name] = (ws, arr)
+        return groups
+
+    def release(self):
+        """Forget the grouped solves' device state (the graph too)."""
+        lib = _lib.load()
+        for ws, _ in self.groups.values():
+            lib.steam_bounded_add_group_release(_lib.ptr(ws))
+        self.groups = {}
+        self.grouped = False
+        self.graph = None
+
+    def _fan(self, fn):
+        """fn(member) for every member on the members' streams, joined back
+        to the current stream."""
+        import torch
+        main = torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(main)
+        for s, lane in zip(self.streams, self.lanes):
+            with torch.cuda.stream(s):
+                for m in lane:
+                    fn(m)
+        for s in self.streams:
+            main.wait_stream(s)
+
+    def _issue_grouped(self):
+        """One ensemble step stage by stage: every member's flux advance and
+        h increment (over the streams), ONE grouped bounded add of h over all
+        members, every member's qt increment, one grouped bounded add of qt,
+        every member's thermodynamics."""
+        lib = _lib.load()
+
+        def first(m):
+            m.reset()
+            product, W, inc_h, _ = m.buffers()
+            m.rc.enqueue_flux(m.F, product)
+            m.rc.enqueue_increment('h', m.h, product, W, inc_h)
+
+        def second(m):
+            product, W, _, inc_qt = m.buffers()
+            m.rc.enqueue_increment('qt', m.q, product, W, inc_qt)
+
+        def third(m):
+            m.rc.enqueue_thermo(m.h, m.q, m.diag)
+            m.rc.ledger_host.copy_(m.rc.ledger, non_blocking=True)
+            m.rc.ledger_ready.record()
+
+        self._fan(first)
+        _lib.check(lib.steam_bounded_add_group_async(_lib.ptr(self.groups['h'][0]),
+                                                     _lib.stream()))
+        self._fan(second)
+        _lib.check(lib.steam_bounded_add_group_async(_lib.ptr(self.groups['qt'][0]),
+                                                     _lib.stream()))
+        self._fan(third)
 
     @property
     def voxels(self):
@@ -167,6 +268,9 @@ class Ensemble:
 
     def _issue(self):
         import torch
+        if self.grouped:
+            self._issue_grouped()
+            return
         main = torch.cuda.current_stream()
         for s in self.streams:
             s.wait_stream(main)

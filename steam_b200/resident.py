@@ -178,81 +178,138 @@ class ResidentClass:
         stencil).  ``work``: three field-shaped tensors (the product, the
         pattern and the increment) to use instead of this class's own."""
         import torch
-        lib, cs, code = self.lib, self.setup, self.code
-        nx, ny, nz = self.shape
         for t in (hp, qp, F):
             if tuple(t.shape) != self.shape or t.dtype != self.dtype or not t.is_contiguous():
                 raise ValueError("resident class step: fields must be contiguous "
                                  f"{self.shape} {self.dtype} CUDA tensors")
         product, W, inc = self._work(F) if work is None else work
-        stream = _lib.stream()
-        win = _lib.window_arg(cs.window)
-        L = self.ledger
-        plan = cs.plan
-        ws = _lib.WORKSPACE.get(self.workspace_bytes())
-        src = L if replay is None else replay.block
-        cells = self.cells if replay is None else replay.cells
-        wsp, wsn = _lib.ptr(ws), ws.numel()
-        # flux advance
-        _lib.check(lib.steam_flux_noise_async(
-            code, ctypes.byref(self.region), self.alpha, self.pcs, self.shift, int(cs.n_zero),
-            int(bool(cs.zero_bottom)), int(bool(cs.zero_top)), _lib.ptr(F), _lib.ptr(product),
-            win, _off(L, self.o_ns), wsp, wsn, stream))
-        _utils.run_plan_async(plan, product, F, None, _lib.STEAM_EPI_FLUX, cs.window,
-                              _off(L, self.o_cs), ws, stream)
-        _lib.check(lib.steam_flux_finish_async(
-            code, F.numel(), _lib.ptr(F), _off(src, self.o_ns), _off(src, self.o_cs), cells,
-            _off(L, self.o_fl), stream))
+        self.enqueue_flux(F, product, replay)
         if done is not None:
             done['F'] = torch.cuda.Event()
             done['F'].record()
         # the two scalars
-        h_min, h_max, qt_min, qt_max = cs.bounds
-        for name, pert, lo, hi in (('h', hp, h_min, h_max), ('qt', qp, qt_min, qt_max)):
+        for name, pert in (('h', hp), ('qt', qp)):
             if ready is not None and name in ready:
                 torch.cuda.current_stream().wait_event(ready[name])
-            ps = _off(L, self.o_ps[name])
-            _lib.check(lib.steam_scalar_pattern_async(
-                code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.vecs[name]), _lib.ptr(product),
-                _off(L, self.o_fl + 7), float(cs.dx), float(cs.dy), _lib.dvec(self.z), 1,
-                float(lo), float(hi), _lib.ptr(W), win, ps, wsp, wsn, stream))
-            _lib.check(lib.steam_pattern_norm_async(
-                code, nz, _off(src, self.o_ps[name]), _lib.ptr(self.mul[name]),
-                _lib.ptr(self.pre[name]), stream))
-            _utils.run_plan_async(plan, W, inc, self.pre[name], _lib.STEAM_EPI_STORE,
-                                  cs.window, None, ws, stream)
-            if replay is None:
-                _lib.check(lib.steam_bounded_add_async(
-                    code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
-                    float(lo), float(hi), win, N_RESCALE, 0, _off(L, self.o_ba[name]), wsp,
-                    wsn, stream))
-            else:
-                _lib.check(lib.steam_bounded_add_replay_async(
-                    code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
-                    float(lo), float(hi), N_RESCALE, 0, _off(replay.block, self.o_ba[name]),
-                    wsp, wsn, stream))
+            self.enqueue_increment(name, pert, product, W, inc, replay)
+            self.enqueue_bounded_add(name, pert, inc, replay)
             if done is not None:
                 done[name] = torch.cuda.Event()
                 done[name].record()
         if diagnostics is not None:
-            d = diagnostics
             for ev in before_thermo:
                 torch.cuda.current_stream().wait_event(ev)
-            _lib.check(lib.steam_thermo_async(
-                code, nx, ny, nz, _lib.ptr(hp), _lib.ptr(qp), _lib.ptr(self.prof), 1,
-                _lib.dvec(self.bounds), float(surface_pressure), None, _lib.ptr(d["T"]),
-                _lib.ptr(d["qv"]), _lib.ptr(d["qc"]), _lib.ptr(d["qi"]), _lib.ptr(d["p"]),
-                stream))
+            self.enqueue_thermo(hp, qp, diagnostics, surface_pressure)
             if done is not None:
                 done['diag'] = torch.cuda.Event()
                 done['diag'].record()
         if copy_ledger:
-            self.ledger_host.copy_(L, non_blocking=True)
+            self.ledger_host.copy_(self.ledger, non_blocking=True)
             self.ledger_ready.record()
         elif done is not None:
             done['end'] = torch.cuda.Event()
             done['end'].record()
         return self
+
+    # ---- the step's stages, each enqueued on the current stream -------------
+    # (``step`` runs them in order; a batched ensemble interleaves them across
+    # its members and runs the bounded adds of all members as one group)
+
+    def _ws(self):
+        ws = _lib.WORKSPACE.get(self.workspace_bytes())
+        return ws, _lib.ptr(ws), ws.numel()
+
+    def enqueue_flux(self, F, product, replay=None):
+        """Flux advance: noise x F into ``product``, the flux convolution
+        with its clip and window sum, the restore to the entering mean."""
+        lib, cs, code = self.lib, self.setup, self.code
+        stream = _lib.stream()
+        L = self.ledger
+        src = L if replay is None else replay.block
+        cells = self.cells if replay is None else replay.cells
+        ws, wsp, wsn = self._ws()
+        _lib.check(lib.steam_flux_noise_async(
+            code, ctypes.byref(self.region), self.alpha, self.pcs, self.shift, int(cs.n_zero),
+            int(bool(cs.zero_bottom)), int(bool(cs.zero_top)), _lib.ptr(F), _lib.ptr(product),
+            _lib.window_arg(cs.window), _off(L, self.o_ns), wsp, wsn, stream))
+        _utils.run_plan_async(cs.plan, product, F, None, _lib.STEAM_EPI_FLUX, cs.window,
+                              _off(L, self.o_cs), ws, stream)
+        _lib.check(lib.steam_flux_finish_async(
+            code, F.numel(), _lib.ptr(F), _off(src, self.o_ns), _off(src, self.o_cs), cells,
+            _off(L, self.o_fl), stream))
+
+    def enqueue_increment(self, name, pert, product, W, inc, replay=None):
+        """Scalar ``name``'s pattern into ``W``, its per-level normalisation
+        and the second convolution into ``inc``."""
+        lib, cs, code = self.lib, self.setup, self.code
+        nx, ny, nz = self.shape
+        stream = _lib.stream()
+        L = self.ledger
+        src = L if replay is None else replay.block
+        ws, wsp, wsn = self._ws()
+        lo, hi = self._bounds(name)
+        _lib.check(lib.steam_scalar_pattern_async(
+            code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.vecs[name]), _lib.ptr(product),
+            _off(L, self.o_fl + 7), float(cs.dx), float(cs.dy), _lib.dvec(self.z), 1,
+            float(lo), float(hi), _lib.ptr(W), _lib.window_arg(cs.window),
+            _off(L, self.o_ps[name]), wsp, wsn, stream))
+        _lib.check(lib.steam_pattern_norm_async(
+            code, nz, _off(src, self.o_ps[name]), _lib.ptr(self.mul[name]),
+            _lib.ptr(self.pre[name]), stream))
+        _utils.run_plan_async(cs.plan, W, inc, self.pre[name], _lib.STEAM_EPI_STORE,
+                              cs.window, None, ws, stream)
+
+    def enqueue_bounded_add(self, name, pert, inc, replay=None):
+        """Scalar ``name``'s bounded amplitude-preserving add of ``inc``
+        (solved, or replayed from ``replay``'s chain)."""
+        lib, cs, code = self.lib, self.setup, self.code
+        nx, ny, nz = self.shape
+        stream = _lib.stream()
+        ws, wsp, wsn = self._ws()
+        lo, hi = self._bounds(name)
+        if replay is None:
+            _lib.check(lib.steam_bounded_add_async(
+                code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
+                float(lo), float(hi), _lib.window_arg(cs.window), N_RESCALE, 0,
+                _off(self.ledger, self.o_ba[name]), wsp, wsn, stream))
+        else:
+            _lib.check(lib.steam_bounded_add_replay_async(
+                code, nx, ny, nz, _lib.ptr(pert), _lib.ptr(self.mean[name]), _lib.ptr(inc),
+                float(lo), float(hi), N_RESCALE, 0, _off(replay.block, self.o_ba[name]),
+                wsp, wsn, stream))
+
+    def bounded_add_problem(self, name, pert, inc):
+        """Scalar ``name``'s bounded add as one field of a grouped solve
+        (``steam_ba_problem_t``); its record goes to this class's ledger."""
+        nx, ny, nz = self.shape
+        lo, hi = self._bounds(name)
+        p = _lib.BAProblem()
+        p.nx, p.ny, p.nz = nx, ny, nz
+        p.pert = pert.data_ptr()
+        p.increment = inc.data_ptr()
+        p.mean = self.mean[name].data_ptr()
+        p.phi_min, p.phi_max = float(lo), float(hi)
+        w = self.setup.window
+        p.has_window = 0 if w is None else 1
+        if w is not None:
+            p.window = _lib.Window(*[int(v) for v in w])
+        p.ledger = self.ledger.data_ptr() + 8 * int(self.o_ba[name])
+        return p
+
+    def enqueue_thermo(self, hp, qp, diagnostics, surface_pressure=101325.0):
+        """Composition with the mean profiles, the bounds and the
+        thermodynamic map into ``diagnostics`` (T, qv, qc, qi, p)."""
+        nx, ny, nz = self.shape
+        d = diagnostics
+        _lib.check(self.lib.steam_thermo_async(
+            self.code, nx, ny, nz, _lib.ptr(hp), _lib.ptr(qp), _lib.ptr(self.prof), 1,
+            _lib.dvec(self.bounds), float(surface_pressure), None, _lib.ptr(d["T"]),
+            _lib.ptr(d["qv"]), _lib.ptr(d["qc"]), _lib.ptr(d["qi"]), _lib.ptr(d["p"]),
+            _lib.stream()))
+
+    def _bounds(self, name):
+        h_min, h_max, qt_min, qt_max = self.setup.bounds
+        return (h_min, h_max) if name == 'h' else (qt_min, qt_max)
 
     def host_step(self, h, qt, flux, diagnostics=('qc', 'qi'), out=None,
                   surface_pressure=101325.0, wait=True):

@@ -92,7 +92,8 @@ class TileWorld:
         from the ground to at least HALO above the tile.  The box's level
         count is a multiple of 4 exactly when the world's is: the kernels
         pick their vectorised forms by that, and the box must run the same
-        arithmetic as the world to reproduce its bits."""
+        arithmetic as the world to reproduce its bits; so does the parity of
+        its row count."""
         x0, y0, z0 = (int(v) for v in origin)
         nx, ny, nz = self.shape
         if not (n >= 1 and 0 <= z0 and z0 + n <= nz):
@@ -102,7 +103,12 @@ class TileWorld:
             bz = min(nz, (bz + 3) // 4 * 4)
         elif bz % 4 == 0 and bz < nz:
             bz += 1
-        return ((x0 - HALO) % nx, (y0 - HALO) % ny, 0), (n + 2 * HALO, n + 2 * HALO, bz), z0
+        # the box's row count has the world's parity (the packed convolution
+        # takes even row counts only), one spare row past the halo if needed
+        by = n + 2 * HALO
+        if by % 2 != ny % 2:
+            by += 1
+        return ((x0 - HALO) % nx, (y0 - HALO) % ny, 0), (n + 2 * HALO, by, bz), z0
 
     def box_setup(self, box_shape):
         """The class set-up of a box of ``box_shape`` that starts at the
@@ -123,7 +129,7 @@ class TileWorld:
         (3), work (3) and diagnostic (5) fields over full columns, and the
         tile's five fields."""
         elem = 8 if self.np_t == np.float64 else 4
-        return elem * (11 * (n + 2 * HALO) ** 2 * self.shape[2] + 5 * n ** 3)
+        return elem * (11 * (n + 2 * HALO) * (n + 2 * HALO + 1) * self.shape[2] + 5 * n ** 3)
 
 
 class _Slot:
@@ -132,7 +138,7 @@ class _Slot:
     def __init__(self, world, max_n, torch):
         self.stream = torch.cuda.Stream()
         nb = max_n + 2 * HALO
-        cap = nb * nb * world.shape[2]
+        cap = nb * (nb + 1) * world.shape[2]
         f = dict(dtype=world.dtype, device='cuda')
         self.buf = {k: torch.empty(cap, **f)
                     for k in ('h', 'qt', 'F', 'product', 'W', 'inc', 'T', 'qv', 'qc', 'qi', 'p')}

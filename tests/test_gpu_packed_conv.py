@@ -4,7 +4,8 @@ The separable 13-tap turbulon filters on float32 fields run on the packed
 kernel (tensor-copied slabs, f32x2 arithmetic): against the FP64 oracle
 (steam/utils.py:293-427 semantics: x/y circular, z linear) on shapes with
 interior tiles only, rows that wrap (edge tiles), fields narrower in y than a
-tile's staged rows, partial y and z tiles and x chunks that wrap; with the
+tile's staged rows or thinner in z than its staged columns, partial y and z
+tiles and x chunks that wrap; with the
 input scaling prologue and the flux epilogue; against the scalar fused kernel
 with float64 accumulation; bit for bit across x chunks; and with no slab wait
 given up.
@@ -25,7 +26,8 @@ pytestmark = pytest.mark.gpu
 
 BAR = 5e-7
 K64 = O.turbulon_envelope(1, 0.5, 0.5, 0.5, shape='mexican_hat', dtype=np.float64)
-SHAPES = [(64, 64, 64), (40, 70, 52), (20, 40, 48), (33, 96, 96), (128, 128, 64)]
+SHAPES = [(64, 64, 64), (40, 70, 52), (20, 40, 48), (33, 96, 96), (128, 128, 64),
+          (16, 30, 16), (14, 22, 8)]
 
 
 def rel_l2(a, b):
