@@ -516,9 +516,11 @@ def main(argv=None):
     # of each entry's kernels in an ncu capture at 512x512x256 FP32, per voxel;
     # the kernels stream their fields once, so the traffic scales with voxels
     # (the convolution figure is the mean of its flux launch and two scalar ones)
-    dram_per_voxel = {"steam_conv_separable_async": 9.24, "steam_thermo_async": 29.77,
+    # (the bounded add's figure sums its first sweep, two persistent phases and
+    # apply sweep: the solve streams d and the perturbation about 5 times)
+    dram_per_voxel = {"steam_conv_separable_async": 9.19, "steam_thermo_async": 29.77,
                       "steam_flux_noise_async": 7.45, "steam_scalar_pattern_async": 14.96,
-                      "steam_flux_finish_async": 7.13}
+                      "steam_flux_finish_async": 7.13, "steam_bounded_add_async": 32.58}
     traffic = (dram_per_voxel[name] * nvox if args.dtype == "f32" and name in dram_per_voxel
                else None)
     # the instruction-issue roofline beside it: warp instructions per voxel of
@@ -526,9 +528,9 @@ def main(argv=None):
     # smsp__inst_executed.sum / voxels; the convolution figure is the mean of
     # its flux launch and two scalar ones) against 4 warp instructions per
     # cycle per SM at the SM clock sampled during the timed region
-    inst_per_voxel = {"steam_conv_separable_async": 7.801, "steam_thermo_async": 8.480,
+    inst_per_voxel = {"steam_conv_separable_async": 3.617, "steam_thermo_async": 8.480,
                       "steam_flux_noise_async": 7.781, "steam_scalar_pattern_async": 2.497,
-                      "steam_flux_finish_async": 0.107}
+                      "steam_flux_finish_async": 0.107, "steam_bounded_add_async": 5.87}
     issue = None
     if args.dtype == "f32" and name in inst_per_voxel:
         sms = torch.cuda.get_device_properties(local).multi_processor_count
@@ -547,8 +549,12 @@ def main(argv=None):
                 "peak_source": "measured" if peaks else "fallback",
                 # the convolutions, noise and thermodynamics issue hundreds of
                 # instructions per voxel: their limiter is instruction issue
-                # (ncu issue-active 55-76 %), not DRAM, hence the low fraction
-                "limiter": "instruction issue (FP32/FP64 pipes), not DRAM",
+                # (ncu issue-active 55-76 %), not DRAM, hence the low fraction;
+                # the bounded add's solve sweeps its fields several times
+                "limiter": ("the solve's repeated sweeps (DRAM traffic about 2.7x the "
+                            "algorithmic bytes) and its grid barriers"
+                            if name == "steam_bounded_add_async" else
+                            "instruction issue (FP32/FP64 pipes), not DRAM"),
                 "issue": issue,
                 "bounded_add_sweeps": ba_sweeps,
                 "breakdown_ms_per_step": {k: round(v[0] / max(args.steps, 1), 3)
@@ -639,12 +645,27 @@ def main(argv=None):
         graph = ens.throughput(steps=3, graph=True)
         ens.check()
         ensemble = {"members": len(members), "voxels": ens.voxels,
-                    "eager_fp32": eager, "graph_fp32": graph,
-                    "plain_fp64_stagewise": plain_fp64_throughput(members, steps=1)}
-        ensemble["graph_fp32_over_plain_fp64"] = (
-            ensemble["graph_fp32"]["mvoxels_per_s"]
-            / ensemble["plain_fp64_stagewise"]["mvoxels_per_s"])
+                    "grouped_bounded_adds": ens.grouped,
+                    "eager_fp32": eager, "graph_fp32": graph}
+        ens.release()
         del ens, members
+        torch.cuda.empty_cache()
+        # the same members in float64: the resident graph (precision apart
+        # from API) and the plain stage-by-stage drop-in (API apart)
+        members = config_members(args.ensemble_members, dtype=np.float64)
+        ens = Ensemble(members, n_streams=4, tune=False)
+        ensemble["graph_fp64"] = ens.throughput(steps=2, graph=True)
+        ens.check()
+        ens.release()
+        del ens
+        torch.cuda.empty_cache()
+        ensemble["plain_fp64_stagewise"] = plain_fp64_throughput(members, steps=1)
+        r = {k: ensemble[k]["mvoxels_per_s"] for k in ("graph_fp32", "graph_fp64",
+                                                       "plain_fp64_stagewise")}
+        ensemble["graph_fp32_over_plain_fp64"] = r["graph_fp32"] / r["plain_fp64_stagewise"]
+        ensemble["graph_fp64_over_plain_fp64"] = r["graph_fp64"] / r["plain_fp64_stagewise"]
+        ensemble["graph_fp32_over_graph_fp64"] = r["graph_fp32"] / r["graph_fp64"]
+        del members
         torch.cuda.empty_cache()
 
     # out-of-core: the same class step with h', qt', F in page-locked host

@@ -521,10 +521,10 @@ int steam_set_barrier_spin_limit(int64_t polls);
  * field at a time): n independent fields' steam_bounded_add_async solves
  * (record_applied = 0) as one launch per stage -- the first and apply sweeps
  * over a flat grid, each persistent phase as one cooperative launch whose
- * blocks split into per-field teams with their own grid barriers.  Each
- * field's block counts follow from its own shape, so a field's result does
- * not depend on the others in the group (it differs from the single call's
- * in the last bits of its sums: another block partition).  Every field:
+ * blocks split into per-field teams with their own grid barriers, a team's
+ * size the field's share of the co-resident capacity.  A field's result is
+ * the single call's to rounding (another block partition of its sums); the
+ * same group gives the same bits every time.  Every field:
  * nz % 4 == 0 (4 .. 1024), 16-byte aligned pert and increment.
  *
  * prepare (synchronous, outside stream capture) lays the group's state out

@@ -1793,12 +1793,13 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
 // range of blocks, the small per-level kernels over a (levels, fields) grid,
 // and each persistent phase as ONE cooperative launch whose blocks split into
 // per-field teams, each with its own grid barrier (a team waits only for its
-// own field's blocks).  Each field's block counts follow from its own shape
-// alone, so its sums -- and its result -- do not depend on the other fields.
-// Only the vectorised layout (nz % 4 == 0, 16-byte aligned fields) is
-// grouped.
+// own field's blocks).  A team's size is its field's share of the co-resident
+// capacity (in proportion to its column groups), so every team sweeps about
+// the same bytes per block and the phase ends when they all do; a field's
+// sums therefore depend on the group it is solved in (the same group gives
+// the same bits every time).  Only the vectorised layout (nz % 4 == 0,
+// 16-byte aligned fields) is grouped.
 constexpr int kGroupFoldGroups = 64;     // column groups per block, first/apply sweeps
-constexpr int kGroupPhaseGroups = 2048;  // column groups per block, persistent phases
 
 template <typename T>
 struct BAGroupRec {
@@ -1906,15 +1907,24 @@ struct BAGroupPlan {
 static std::mutex g_group_mu;
 static std::map<void*, BAGroupPlan> g_groups;
 
+// blocks whose partial sums a field's buffers hold: its first sweep's, and
+// the most a phase team can get (a share of the co-resident capacity, at most
+// one block per kPhaseMinGroups column groups)
+static int64_t group_partial_blocks(int64_t groups) {
+  const int64_t fold = std::max<int64_t>((groups + kGroupFoldGroups - 1) / kGroupFoldGroups, 1);
+  const int64_t team = std::min<int64_t>(
+      std::max<int64_t>((groups + kPhaseMinGroups - 1) / kPhaseMinGroups, 1),
+      (int64_t)4 * sm_count());
+  return std::max(fold, team);
+}
+
 static size_t group_state_bytes(const steam_ba_problem_t& q, int R, size_t elem) {
   // state, partials of either sweep kind, totals
   const int64_t nz = q.nz;
   const int64_t ncol = q.nx * q.ny;
   const int64_t cpb = nz > 0 ? kLvThreads / (nz / 4) : 1;
   const int64_t groups = (ncol + cpb - 1) / cpb;
-  const int64_t nb = std::max<int64_t>(
-      std::max<int64_t>((groups + kGroupFoldGroups - 1) / kGroupFoldGroups, 1),
-      std::max<int64_t>((groups + kGroupPhaseGroups - 1) / kGroupPhaseGroups, 1));
+  const int64_t nb = group_partial_blocks(groups);
   return ba_state_bytes(nz, R, elem) +
          carve_bytes((size_t)nb * 2 * kMuCand * nz, sizeof(double)) +
          carve_bytes((size_t)2 * kMuCand * nz, sizeof(double)) + 512;
@@ -1940,42 +1950,12 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
   plan.ph_start = c.take<int>((size_t)n);
   if (!plan.recs || !plan.fold_start || !plan.ph_start)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
-  std::vector<BAGroupRec<T>> recs((size_t)n);
-  std::vector<int> fold_start((size_t)n), ph_start((size_t)n), ph_nb((size_t)n);
-  int fold_total = 0;
+  std::vector<int64_t> groups((size_t)n);
   for (int i = 0; i < n; ++i) {
-    const steam_ba_problem_t& p = q[i];
-    const int64_t nz = p.nz, ncol = p.nx * p.ny;
-    const steam_window_t* win = p.has_window ? &p.window : nullptr;
-    BAGroupRec<T>& r = recs[(size_t)i];
-    r.w = make_win(win, p.nx, p.ny);
-    if (!carve_ba_state<T>(c, nz, R, p.ledger == nullptr, r.st))
-      return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
-    if (p.ledger) r.st.ledger = p.ledger;
-    set_ba_scalars(r.st, nz, R, r.w, p.phi_min, p.phi_max);
-    r.ch = ba_chain(r.st, R, p.phi_min, p.phi_max);
-    const int64_t cpb = kLvThreads / (nz / 4);
-    const int64_t groups = (ncol + cpb - 1) / cpb;
-    r.fold_nb = (int)std::max<int64_t>((groups + kGroupFoldGroups - 1) / kGroupFoldGroups, 1);
-    r.ph_nb = (int)std::max<int64_t>((groups + kGroupPhaseGroups - 1) / kGroupPhaseGroups, 1);
-    const int nbmax = std::max(r.fold_nb, r.ph_nb);
-    r.partials = c.take<double>((size_t)nbmax * 2 * kMuCand * nz);
-    r.totals = c.take<double>((size_t)2 * kMuCand * nz);
-    if (!r.partials || !r.totals)
-      return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
-    r.st.wb = 1;
-    r.pert = (T*)p.pert;
-    r.inc = (T*)p.increment;
-    r.mean = p.mean;
-    r.nx = p.nx;
-    r.ny = p.ny;
-    r.nz = (int)nz;
-    fold_start[(size_t)i] = fold_total;
-    fold_total += r.fold_nb;
-    ph_nb[(size_t)i] = r.ph_nb;
-    plan.nz_max = std::max(plan.nz_max, (int)nz);
+    const int64_t cpb = kLvThreads / (q[i].nz / 4);
+    groups[(size_t)i] = (q[i].nx * q[i].ny + cpb - 1) / cpb;
+    plan.nz_max = std::max(plan.nz_max, (int)q[i].nz);
   }
-  plan.fold_blocks = fold_total;
   plan.sm_sums = ba_fold_smem_bytes<T>(plan.nz_max);
   plan.sm_apply = ba_fold_param_bytes<T>(plan.nz_max);
   // co-resident capacity of the cooperative phases (the smaller of the two)
@@ -1991,26 +1971,88 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
     const int c_m = per_sm * sm_count();
     cap = cap == 0 ? c_m : std::min(cap, c_m);
   }
-  // teams in batches that fit the co-resident capacity (a field's team is
-  // never split; a team larger than the capacity is cut to it)
-  int b0 = 0, bn = 0, bblocks = 0;
-  for (int i = 0; i < n; ++i) {
-    int nb = std::min(ph_nb[(size_t)i], cap);
-    if (nb != ph_nb[(size_t)i]) {
-      recs[(size_t)i].ph_nb = nb;
-      ph_nb[(size_t)i] = nb;
-    }
-    if (bblocks + nb > cap) {
-      plan.batches.push_back({b0, bn, bblocks});
-      b0 = i;
-      bn = 0;
-      bblocks = 0;
-    }
-    ph_start[(size_t)i] = bblocks;
-    bblocks += nb;
-    ++bn;
+  // Batches of fields for the phases: as few as leave at least half of each
+  // batch's slots to deal out beyond one block per field; the fields dealt
+  // largest first to the batch with the least work so far.  Within a batch a
+  // field's team is one block plus its share of the spare slots in
+  // proportion to its column groups (at most one block per kPhaseMinGroups
+  // groups), so every team sweeps about the same bytes per block.
+  const int B = std::max(1, (2 * n + cap - 1) / cap);
+  std::vector<int> idx((size_t)n);
+  for (int i = 0; i < n; ++i) idx[(size_t)i] = i;
+  std::stable_sort(idx.begin(), idx.end(),
+                   [&](int a, int b) { return groups[(size_t)a] > groups[(size_t)b]; });
+  std::vector<std::vector<int>> members((size_t)B);
+  std::vector<int64_t> load((size_t)B, 0);
+  for (int i : idx) {
+    int best = -1;
+    for (int b = 0; b < B; ++b)
+      if ((int)members[(size_t)b].size() < cap &&
+          (best < 0 || load[(size_t)b] < load[(size_t)best]))
+        best = b;
+    STEAM_REQUIRE(best >= 0, "steam_bounded_add_group_prepare: too many fields");
+    members[(size_t)best].push_back(i);
+    load[(size_t)best] += groups[(size_t)i];
   }
-  if (bn > 0) plan.batches.push_back({b0, bn, bblocks});
+  std::vector<int> order, team((size_t)n);
+  for (int b = 0; b < B; ++b) {
+    auto& m = members[(size_t)b];
+    std::sort(m.begin(), m.end());
+    const int64_t spare = cap - (int64_t)m.size();
+    for (int i : m) {
+      const int64_t g = groups[(size_t)i];
+      const int64_t share = 1 + (int64_t)((double)spare * (double)g /
+                                          (double)std::max<int64_t>(load[(size_t)b], 1));
+      const int64_t useful = std::max<int64_t>((g + kPhaseMinGroups - 1) / kPhaseMinGroups, 1);
+      team[(size_t)i] = (int)std::min(std::min(share, useful), group_partial_blocks(g));
+      order.push_back(i);
+    }
+  }
+  // the fields' records in batch order
+  std::vector<BAGroupRec<T>> recs((size_t)n);
+  std::vector<int> fold_start((size_t)n), ph_start((size_t)n);
+  int fold_total = 0;
+  for (int k = 0; k < n; ++k) {
+    const int i = order[(size_t)k];
+    const steam_ba_problem_t& p = q[i];
+    const int64_t nz = p.nz;
+    const steam_window_t* win = p.has_window ? &p.window : nullptr;
+    BAGroupRec<T>& r = recs[(size_t)k];
+    r.w = make_win(win, p.nx, p.ny);
+    if (!carve_ba_state<T>(c, nz, R, p.ledger == nullptr, r.st))
+      return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
+    if (p.ledger) r.st.ledger = p.ledger;
+    set_ba_scalars(r.st, nz, R, r.w, p.phi_min, p.phi_max);
+    r.ch = ba_chain(r.st, R, p.phi_min, p.phi_max);
+    const int64_t g = groups[(size_t)i];
+    r.fold_nb = (int)std::max<int64_t>((g + kGroupFoldGroups - 1) / kGroupFoldGroups, 1);
+    r.ph_nb = team[(size_t)i];
+    r.partials = c.take<double>((size_t)group_partial_blocks(g) * 2 * kMuCand * nz);
+    r.totals = c.take<double>((size_t)2 * kMuCand * nz);
+    if (!r.partials || !r.totals)
+      return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
+    r.st.wb = 1;
+    r.pert = (T*)p.pert;
+    r.inc = (T*)p.increment;
+    r.mean = p.mean;
+    r.nx = p.nx;
+    r.ny = p.ny;
+    r.nz = (int)nz;
+    fold_start[(size_t)k] = fold_total;
+    fold_total += r.fold_nb;
+  }
+  plan.fold_blocks = fold_total;
+  int k0 = 0;
+  for (int b = 0; b < B; ++b) {
+    const int nb = (int)members[(size_t)b].size();
+    int blocks = 0;
+    for (int k = k0; k < k0 + nb; ++k) {
+      ph_start[(size_t)k] = blocks;
+      blocks += recs[(size_t)k].ph_nb;
+    }
+    if (nb > 0) plan.batches.push_back({k0, nb, blocks});
+    k0 += nb;
+  }
   STEAM_CUDA(cudaMemcpy(plan.recs, recs.data(), sizeof(BAGroupRec<T>) * (size_t)n,
                         cudaMemcpyHostToDevice));
   STEAM_CUDA(cudaMemcpy(plan.fold_start, fold_start.data(), sizeof(int) * (size_t)n,

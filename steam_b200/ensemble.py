@@ -384,3 +384,29 @@ def plain_fp64_throughput(members, steps=1):
     e1.synchronize()
     ms = e0.elapsed_time(e1)
     return {"mvoxels_per_s": voxels * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps}
+
+
+def main(argv=None):
+    """``python -m steam_b200.ensemble --members N --steps K``: build the
+    configuration's members (``config_members``), an ``Ensemble`` over four
+    streams (no autotuning), run K eager steps and print the device time."""
+    import argparse
+    import torch
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--f64", action="store_true")
+    args = ap.parse_args(argv)
+    members = config_members(args.members, dtype=np.float64 if args.f64 else np.float32)
+    ens = Ensemble(members, n_streams=args.streams, tune=False)
+    res = ens.throughput(steps=args.steps, graph=False)
+    ens.check()
+    print({"members": len(members), "voxels": ens.voxels, "grouped": ens.grouped, **res})
+    ens.release()
+    torch.cuda.synchronize()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -3,10 +3,10 @@
 Several fields of different shapes, windows and bounds solved as one group
 (``steam_bounded_add_group_*``: one launch per stage, per-field teams in the
 persistent phases) against the oracle's bounded add of each field
-(steam/simulate.py:3114-3283) and against the single-field call; a field's
-result does not depend on which other fields share its group; repeats are
-bit-identical; the ledger records match the single call's; and the grouped
-ensemble step agrees with the per-member one.
+(steam/simulate.py:3114-3283), against the single-field call and against
+the same field solved alone (team sizes, hence block partials, depend on the
+group); repeats of a group are bit-identical; the ledger records match the
+single call's; and the grouped ensemble step agrees with the per-member one.
 
 Bars: float32, a cell within twice the shift's stopping tolerance a0 2^-20
 (the device stops once the root is bracketed that narrowly; the oracle's
@@ -112,16 +112,18 @@ def test_group_against_oracle(dtype):
         lib.steam_bounded_add_group_release(_lib.ptr(ws))
 
 
-def test_group_matches_single_calls_and_is_composition_free():
+def test_group_matches_single_calls_and_alone():
     import torch
     from steam_b200 import simulate as sim
     dtype = np.float32
     fields, ws, lib = _run_group(dtype, CASES, torch)
     alone, ws1, _ = _run_group(dtype, CASES[2:3], torch)
     try:
-        # field 2 alone and in the group: the same bits
-        assert _same_bits(alone[0][0], fields[2][0])
-        assert _same_bits(alone[0][3], fields[2][3])
+        # field 2 alone and in the group (other team sizes, so other block
+        # partials): the same solve to rounding
+        a0 = alone[0][3].cpu().numpy().reshape(CASES[2][0][2], -1)[:, 0]
+        np.testing.assert_allclose(alone[0][0].cpu().numpy(), fields[2][0].cpu().numpy(),
+                                   rtol=0, atol=_f32_bar(a0, 0.0, 0.03))
         for (shape, seed, lo, hi, win), (p, d, m, led, pert, mean, inc) in zip(CASES, fields):
             p_s = pert.astype(dtype)
             rec = sim._bounded_amplitude_add(p_s, mean.astype(dtype), inc.astype(dtype), lo, hi,
