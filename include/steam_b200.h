@@ -148,6 +148,13 @@ int steam_conv_separable(int dtype, int64_t nx, int64_t ny, int64_t nz,
  * already covers any chunk. */
 int steam_conv_set_xchunk(int64_t nx, int64_t ny, int64_t nz, int32_t chunk);
 int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz);
+/* The packed float32 kernel's CTA tile height for fields of shape (nx, ny,
+ * nz): 32 rows (256 threads, two CTAs per SM) or 64 rows (512 threads, one
+ * per SM, 1.19 instead of 1.375 staged rows per output row); 0 restores 32.
+ * Every output voxel's arithmetic is the same at either height, so results
+ * are identical. */
+int steam_conv_set_tile_rows(int64_t nx, int64_t ny, int64_t nz, int32_t rows);
+int steam_conv_get_tile_rows(int64_t nx, int64_t ny, int64_t nz);
 
 /* Float32 flux convolutions (STEAM_EPI_FLUX on float32 fields) run on the
  * packed float32 kernel by default (wide = 0); wide = 1 runs them with

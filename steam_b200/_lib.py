@@ -79,6 +79,8 @@ _SIGNATURES = {
                                             c_vp]),
     "steam_conv_set_xchunk": (ctypes.c_int, [c_i64, c_i64, c_i64, c_i32]),
     "steam_conv_get_xchunk": (ctypes.c_int, [c_i64, c_i64, c_i64]),
+    "steam_conv_set_tile_rows": (ctypes.c_int, [c_i64, c_i64, c_i64, c_i32]),
+    "steam_conv_get_tile_rows": (ctypes.c_int, [c_i64, c_i64, c_i64]),
     "steam_conv_set_flux_wide": (ctypes.c_int, [c_i32]),
     "steam_take_wait_errors": (ctypes.c_int, [ctypes.POINTER(c_i32)]),
     "steam_conv_packed_launches": (c_i64, []),

@@ -25,7 +25,9 @@
 #include <cuda.h>
 
 #include <atomic>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 #include "conv.cuh"
 
@@ -37,27 +39,35 @@ namespace {
 
 constexpr int kPK = 13;              // taps per axis
 constexpr int kPH = (kPK - 1) / 2;   // the filters' centre (half width)
-constexpr int kPY = 32;              // output rows per tile
 constexpr int kPZ = 32;              // output columns per tile
-constexpr int kPR = kPY + kPK - 1;   // staged rows
 constexpr int kPLead = 8;            // staged columns before the tile
 constexpr int kPC = kPZ + 2 * kPLead;  // staged columns (z0 - 8 .. z0 + 39)
-constexpr int kPThreads = 256;
 constexpr int kPStages = 4;          // slab buffers
-constexpr int kPSlab = kPR * kPC;    // floats per slab buffer
-constexpr int kPU = kPR * kPZ;       // floats per z-filter output plane
-constexpr int kPTasks = kPR * (kPZ / 8);  // z-filter tasks (8 columns each)
 constexpr int kPChunkMin = 16;
 // polls of a slab's mbarrier before a block gives up (a tensor copy lands in
 // microseconds; this is seconds)
 constexpr long long kTmaWaitLimit = 1ll << 24;
 
-static_assert(kPR % 2 == 0, "edge tiles copy the slab in row pairs");
-static_assert(kPTasks <= kPThreads, "one z-filter task per thread");
-static_assert((kPSlab * 4) % 128 == 0, "slab buffers stay 128-byte aligned");
-
-constexpr size_t kPSmem = sizeof(float) * ((size_t)kPStages * kPSlab + 4 * kPU + kPC) +
-                          sizeof(uint64_t) * kPStages;
+// A tile of TY output rows (32 or 64) x kPZ columns: TY / 2 x 16 threads, each
+// owning 2 rows x 2 columns; TY + 12 staged rows.  The arithmetic of an output
+// voxel is the same for every tile height, so the height (chosen per shape by
+// the autotuner) never changes a result.
+template <int TY>
+struct PTile {
+  static constexpr int Y = TY;
+  static constexpr int R = TY + kPK - 1;        // staged rows
+  static constexpr int Threads = TY * 8;
+  static constexpr int Slab = R * kPC;          // floats per slab buffer
+  static constexpr int U = R * kPZ;             // floats per z-filter output plane
+  static constexpr int Tasks = R * (kPZ / 8);   // z-filter tasks (8 columns each)
+  static constexpr int MinBlocks = TY == 32 ? 2 : 1;
+  static constexpr size_t Smem =
+      sizeof(float) * ((size_t)kPStages * Slab + 4 * (size_t)U + kPC) +
+      sizeof(uint64_t) * kPStages;
+  static_assert(R % 2 == 0, "edge tiles copy the slab in row pairs");
+  static_assert(Tasks <= Threads, "one z-filter task per thread");
+  static_assert((Slab * 4) % 128 == 0, "slab buffers stay 128-byte aligned");
+};
 
 // Filters as {t, t} pairs (kernel-parameter constants): z and y filters by
 // distance from the centre (tap kPH + d, d = 0..6), x filters by tap index,
@@ -130,7 +140,7 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 // z filters of one staged row, output columns 8q .. 8q + 7 of the tile.
 // Window element e is staged column 8q + 2 + e; output column 8q + o has its
 // centre at e = o + 6.
-template <bool PRE>
+template <bool PRE, int U>
 __device__ __forceinline__ void z_task(const float* __restrict__ sl, float* __restrict__ su,
                                        const float* __restrict__ s_pre,
                                        const PackedTaps& tp, int task) {
@@ -164,19 +174,22 @@ __device__ __forceinline__ void z_task(const float* __restrict__ sl, float* __re
     u1[o] = a1;
   }
   float* d0 = su + r * kPZ + 8 * q;
-  float* d1 = d0 + kPU;
+  float* d1 = d0 + U;
   *reinterpret_cast<float4*>(d0) = make_float4(u0[0].x, u0[0].y, u0[1].x, u0[1].y);
   *reinterpret_cast<float4*>(d0 + 4) = make_float4(u0[2].x, u0[2].y, u0[3].x, u0[3].y);
   *reinterpret_cast<float4*>(d1) = make_float4(u1[0].x, u1[0].y, u1[1].x, u1[1].y);
   *reinterpret_cast<float4*>(d1 + 4) = make_float4(u1[2].x, u1[2].y, u1[3].x, u1[3].y);
 }
 
-template <bool PRE, bool P3, bool FLUX>
-__global__ void __launch_bounds__(kPThreads, 2) packed_conv_kernel(
+template <int TY, bool PRE, bool P3, bool FLUX>
+__global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) packed_conv_kernel(
     const __grid_constant__ CUtensorMap tm_box, const __grid_constant__ CUtensorMap tm_pair,
     float* __restrict__ out, const float* __restrict__ pre,
     const __grid_constant__ PackedTaps tp, PackedGeom g, XEpi epi,
     double* __restrict__ partials) {
+  using Tl = PTile<TY>;
+  constexpr int kPY = Tl::Y, kPR = Tl::R, kPThreads = Tl::Threads, kPSlab = Tl::Slab,
+                kPU = Tl::U, kPTasks = Tl::Tasks;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ double scratch[32];
   float* slab = reinterpret_cast<float*>(smem_raw);
@@ -257,7 +270,7 @@ __global__ void __launch_bounds__(kPThreads, 2) packed_conv_kernel(
       fprev1 = *reinterpret_cast<const float2*>(outp + o0 + g.nz);
     }
     float* su = su0 + (k & 1) * 2 * kPU;
-    if (t < kPTasks) z_task<PRE>(slab + b * kPSlab, su, s_pre, tp, t);
+    if (t < kPTasks) z_task<PRE, kPU>(slab + b * kPSlab, su, s_pre, tp, t);
     // one barrier per plane: the z filters of plane k are in su[k & 1] and
     // every read of slab buffer b is done; a block whose copy never landed
     // leaves together
@@ -421,14 +434,27 @@ bool even_about_centre(const double* t) {
 }
 
 // x planes per CTA: the autotuner's choice for the shape, else the chunk
-// that minimises the busiest SM's work.  Two CTAs fit an SM (registers and
-// shared memory) and share its issue slots, so an SM's time is the planes of
-// all CTAs it runs, halo included; a CTA alone on its SM runs at about 0.7 of
-// the pair's throughput (its barrier stalls are not covered).
+// that minimises the busiest SM's work.  Two 32-row CTAs fit an SM (registers
+// and shared memory) and share its issue slots, so an SM's time is the planes
+// of all CTAs it runs, halo included, plus about one CTA's worth for the
+// uneven finish; a CTA alone on its SM runs at about 0.7 of the pair's
+// throughput (its barrier stalls are not covered).
+// output rows per tile for fields of a shape: the autotuner's choice
+// (steam_conv_set_tile_rows), 32 otherwise
+std::mutex g_rows_mu;
+std::map<std::tuple<int64_t, int64_t, int64_t>, int> g_rows;
+
+int packed_rows(int64_t nx, int64_t ny, int64_t nz) {
+  std::lock_guard<std::mutex> lock(g_rows_mu);
+  auto it = g_rows.find(std::make_tuple(nx, ny, nz));
+  return it == g_rows.end() ? 32 : it->second;
+}
+
 int64_t packed_chunk(int64_t nx, int64_t ny, int64_t nz) {
   const int over = chunk_override(nx, ny, nz);
   if (over > 0) return over;
-  const int64_t tiles = ((nz + kPZ - 1) / kPZ) * ((ny + kPY - 1) / kPY);
+  const int rows = packed_rows(nx, ny, nz);
+  const int64_t tiles = ((nz + kPZ - 1) / kPZ) * ((ny + rows - 1) / rows);
   const int64_t sms = sm_count();
   int64_t best = nx;
   double best_cost = -1.0;
@@ -437,7 +463,11 @@ int64_t packed_chunk(int64_t nx, int64_t ny, int64_t nz) {
     if (chunk < kPChunkMin && n > 1) break;
     const int64_t ctas = tiles * ((nx + chunk - 1) / chunk);
     const int64_t per_sm = (ctas + sms - 1) / sms;
-    const double cost = (double)(per_sm * (chunk + kPK - 1)) / (per_sm == 1 ? 0.7 : 1.0);
+    // (one more CTA's planes for the spread of CTA times under the hardware's
+    // dynamic dispatch; a 64-row CTA has the SM to itself: no pair to cover
+    // its stalls)
+    const double cost =
+        (double)((per_sm + 1) * (chunk + kPK - 1)) / (per_sm == 1 && rows == 32 ? 0.7 : 1.0);
     if (best_cost < 0.0 || cost < best_cost) {
       best_cost = cost;
       best = chunk;
@@ -446,16 +476,33 @@ int64_t packed_chunk(int64_t nx, int64_t ny, int64_t nz) {
   return best < kPChunkMin && nx >= kPChunkMin ? kPChunkMin : best;
 }
 
-template <bool PRE, bool P3, bool FLUX>
+template <int TY, bool PRE, bool P3, bool FLUX>
 cudaError_t launch_v(const CUtensorMap& box, const CUtensorMap& pair, float* out,
                      const float* pre, const PackedTaps& tp, const PackedGeom& g,
                      const XEpi& epi, double* partials, int64_t grid, cudaStream_t s) {
-  auto kern = packed_conv_kernel<PRE, P3, FLUX>;
+  using Tl = PTile<TY>;
+  auto kern = packed_conv_kernel<TY, PRE, P3, FLUX>;
   cudaError_t e =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmem);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tl::Smem);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)grid, kPThreads, kPSmem, s>>>(box, pair, out, pre, tp, g, epi, partials);
+  kern<<<(unsigned)grid, Tl::Threads, Tl::Smem, s>>>(box, pair, out, pre, tp, g, epi, partials);
   return cudaGetLastError();
+}
+
+template <int TY>
+cudaError_t launch_rows(int v, const CUtensorMap& box, const CUtensorMap& pair, float* out,
+                        const float* pre, const PackedTaps& tp, const PackedGeom& g,
+                        const XEpi& epi, double* partials, int64_t grid, cudaStream_t s) {
+  switch (v) {
+    case 0: return launch_v<TY, false, false, false>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    case 1: return launch_v<TY, false, false, true>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    case 2: return launch_v<TY, false, true, false>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    case 3: return launch_v<TY, false, true, true>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    case 4: return launch_v<TY, true, false, false>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    case 5: return launch_v<TY, true, false, true>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    case 6: return launch_v<TY, true, true, false>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+    default: return launch_v<TY, true, true, true>(box, pair, out, pre, tp, g, epi, partials, grid, s);
+  }
 }
 
 }  // namespace
@@ -482,12 +529,15 @@ bool packed_supported(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t
 
 int64_t packed_grid(int64_t nx, int64_t ny, int64_t nz) {
   const int64_t chunk = packed_chunk(nx, ny, nz);
-  return ((nz + kPZ - 1) / kPZ) * ((ny + kPY - 1) / kPY) * ((nx + chunk - 1) / chunk);
+  const int rows = packed_rows(nx, ny, nz);
+  return ((nz + kPZ - 1) / kPZ) * ((ny + rows - 1) / rows) * ((nx + chunk - 1) / chunk);
 }
 
 int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
                   const float* in, float* out, const float* pre, int epilogue,
                   const XEpi& epi, double* partials, cudaStream_t s) {
+  const int rows = packed_rows(nx, ny, nz);
+  const int kPR = rows + kPK - 1;
   CUtensorMap box, pair;
   if (!encode_map(&pair, in, nx, ny, nz, 2))
     return fail(STEAM_ERR_CUDA, "steam_conv_separable: tensor map encoding failed");
@@ -527,23 +577,14 @@ int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
   g.ny = ny;
   g.nz = (int)nz;
   g.nzt = (int)((nz + kPZ - 1) / kPZ);
-  g.nyt = (int)((ny + kPY - 1) / kPY);
+  g.nyt = (int)((ny + rows - 1) / rows);
   g.chunk = packed_chunk(nx, ny, nz);
   const int64_t grid = (int64_t)g.nzt * g.nyt * ((nx + g.chunk - 1) / g.chunk);
   STEAM_REQUIRE(grid < ((int64_t)1 << 31), "steam_conv_separable: grid too large");
   const int v = (pre != nullptr ? 4 : 0) | (p3 ? 2 : 0) | (epilogue == STEAM_EPI_FLUX ? 1 : 0);
-  cudaError_t e;
-#define STEAM_PV(n, a, b, c) \
-  case n:                    \
-    e = launch_v<a, b, c>(box, pair, out, pre, tp, g, epi, partials, grid, s); \
-    break;
-  switch (v) {
-    STEAM_PV(0, false, false, false) STEAM_PV(1, false, false, true)
-    STEAM_PV(2, false, true, false) STEAM_PV(3, false, true, true)
-    STEAM_PV(4, true, false, false) STEAM_PV(5, true, false, true)
-    STEAM_PV(6, true, true, false) default: STEAM_PV(7, true, true, true)
-  }
-#undef STEAM_PV
+  cudaError_t e = rows == 64
+                      ? launch_rows<64>(v, box, pair, out, pre, tp, g, epi, partials, grid, s)
+                      : launch_rows<32>(v, box, pair, out, pre, tp, g, epi, partials, grid, s);
   count_launch();
   if (e != cudaSuccess)
     return fail(STEAM_ERR_CUDA, std::string("conv packed launch: ") + cudaGetErrorString(e));
@@ -554,6 +595,22 @@ int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
 }  // namespace steam
 
 extern "C" int64_t steam_conv_packed_launches(void) { return steam::g_packed_launches.load(); }
+
+extern "C" int steam_conv_set_tile_rows(int64_t nx, int64_t ny, int64_t nz, int32_t rows) {
+  STEAM_REQUIRE(nx >= 1 && ny >= 1 && nz >= 1, "steam_conv_set_tile_rows: empty shape");
+  STEAM_REQUIRE(rows == 0 || rows == 32 || rows == 64,
+                "steam_conv_set_tile_rows: rows must be 0 (default), 32 or 64");
+  std::lock_guard<std::mutex> lock(steam::g_rows_mu);
+  if (rows == 0)
+    steam::g_rows.erase(std::make_tuple(nx, ny, nz));
+  else
+    steam::g_rows[std::make_tuple(nx, ny, nz)] = rows;
+  return STEAM_OK;
+}
+
+extern "C" int steam_conv_get_tile_rows(int64_t nx, int64_t ny, int64_t nz) {
+  return steam::packed_rows(nx, ny, nz);
+}
 
 extern "C" int steam_take_wait_errors(int32_t* count) {
   if (!count) return steam::fail(STEAM_ERR_ARG, "steam_take_wait_errors: count is null");

@@ -14,9 +14,10 @@ increment, one grouped bounded add of qt, and every member's thermodynamics.
 Members of uneven sizes fill the GPU side by side.
 
 ``autotune_conv`` is the tile-shape autotuner: for a field shape it times the
-fused convolution at a few x-chunk lengths (planes per CTA; short chunks give
-small members enough CTAs, long ones amortise the halo) and installs the
-fastest for that shape.  The chunk never changes the result.
+fused convolution over its CTA tile heights (32 or 64 rows for the packed
+float32 kernel) and x-chunk lengths (planes per CTA; short chunks give small
+members enough CTAs, long ones amortise the halo) and installs the fastest
+for that shape.  Neither changes the result.
 """
 
 from __future__ import annotations
@@ -72,8 +73,11 @@ def member_setup(shape, seed, alpha=1.8, c1=0.1, H=1.0 / 3.0, Hz=5.0 / 9.0,
 
 
 def autotune_conv(setup, dtype, chunks=CHUNKS, repeats=3):
-    """Time the fused convolution of ``setup``'s kernel on its shape at each
-    x-chunk, install the fastest; returns {chunk: ms}."""
+    """Time the fused convolution of ``setup``'s kernel on its shape over its
+    CTA tile shapes -- for float32 fields the packed kernel's tile height (32
+    or 64 rows) -- and x-chunk lengths (0: the kernel's own wave model), and
+    install the fastest pair; returns {(rows, chunk): ms}.  Neither changes a
+    result."""
     torch = _lib.require_cuda("autotune_conv")
     lib = _lib.load()
     shape = tuple(int(n) for n in setup.shape)
@@ -85,20 +89,25 @@ def autotune_conv(setup, dtype, chunks=CHUNKS, repeats=3):
         return {}
     f = torch.randn(shape, dtype=dtype, device='cuda')
     out = torch.empty_like(f)
+    rows_set = (32, 64) if dtype == torch.float32 else (32,)
     times = {}
-    for c in chunks:
-        if c > 2 * shape[0] and c != chunks[0]:
-            continue
-        _lib.check(lib.steam_conv_set_xchunk(*shape, int(c)))
-        _utils.run_plan(plan, f, out)  # warm
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(repeats):
-            _utils.run_plan(plan, f, out)
-        e1.record()
-        e1.synchronize()
-        times[c] = e0.elapsed_time(e1) / repeats
-    best = min(times, key=times.get)
+    for rows in rows_set:
+        _lib.check(lib.steam_conv_set_tile_rows(*shape, int(rows)))
+        for c in (0,) + tuple(chunks):
+            if c > 2 * shape[0]:
+                continue
+            _lib.check(lib.steam_conv_set_xchunk(*shape, int(c)))
+            _utils.run_plan(plan, f, out)  # warm
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(repeats):
+                _utils.run_plan(plan, f, out)
+            e1.record()
+            e1.synchronize()
+            times[(rows, c)] = e0.elapsed_time(e1) / repeats
+    rows, best = min(times, key=times.get)
+    _lib.check(lib.steam_conv_set_tile_rows(*shape, int(rows)))
     _lib.check(lib.steam_conv_set_xchunk(*shape, int(best)))
     _TUNED[key] = times
     return times

@@ -187,3 +187,35 @@ def test_packed_chunks_are_bit_identical(U):
     for o in outs[1:]:
         assert torch.equal(o, outs[0])
     assert _wait_errors(lib) == 0
+
+
+@pytest.mark.parametrize("shape", [(40, 70, 52), (33, 96, 96), (24, 130, 64)])
+def test_packed_tile_heights_are_bit_identical(U, shape):
+    """The 64-row tile (512 threads) against the 32-row tile: the same bits,
+    and the oracle's result; the autotuner's setting is per shape."""
+    import torch
+    lib = _lib.load()
+    rng = np.random.default_rng(len(shape) + shape[1])
+    f = torch.as_tensor(rng.standard_normal(shape).astype(np.float32), device='cuda')
+    F = torch.as_tensor((1.0 + 0.1 * rng.random(shape)).astype(np.float32), device='cuda')
+    plan = U.plan_convolution(K64, shape, np.float32)
+    outs, fluxes = [], []
+    try:
+        for rows in (32, 64):
+            _lib.check(lib.steam_conv_set_tile_rows(*shape, rows))
+            assert lib.steam_conv_get_tile_rows(*shape) == rows
+            o = torch.empty_like(f)
+            U.run_plan(plan, f, o)
+            outs.append(o)
+            fl = F.clone()
+            U.run_plan(plan, 0.3 * f, fl, epilogue=_lib.STEAM_EPI_FLUX)
+            fluxes.append(fl)
+    finally:
+        _lib.check(lib.steam_conv_set_tile_rows(*shape, 0))
+    assert lib.steam_conv_get_tile_rows(*shape) == 32
+    assert torch.equal(outs[0], outs[1])
+    assert torch.equal(fluxes[0], fluxes[1])
+    want = O.convolve(f.cpu().numpy().astype(np.float64), K64)
+    assert rel_l2(outs[1].cpu().numpy(), want) < BAR
+    assert lib.steam_conv_set_tile_rows(*shape, 48) != 0
+    assert _wait_errors(lib) == 0
