@@ -156,6 +156,35 @@ int steam_conv_get_xchunk(int64_t nx, int64_t ny, int64_t nz);
 int steam_conv_set_tile_rows(int64_t nx, int64_t ny, int64_t nz, int32_t rows);
 int steam_conv_get_tile_rows(int64_t nx, int64_t ny, int64_t nz);
 
+/* Grouped convolutions (no counterpart in the reference): n float32 fields
+ * convolved with the same separable filters (a spec steam_conv_separable
+ * runs on the packed kernel) as ONE launch, every field its own range of
+ * blocks.  A field's blocks and x chunk are those of a launch of its own, so
+ * its output and its flux sums are the same bits.  Every field: the packed
+ * kernel's layout (nz % 4 == 0, ny even, 16-byte aligned in and out), nx, ny
+ * >= 13, 32-row tiles; all fields or none take the input scaling.
+ * prepare (synchronous, outside stream capture) lays the group out in
+ * `workspace` (DEVICE, steam_conv_group_workspace_bytes) and records it under
+ * that address; async enqueues the convolutions (capturable, repeatable on
+ * the same buffers); release forgets the group.  sums: DEVICE, 2 doubles per
+ * field for STEAM_EPI_FLUX ({sum F over the window, clip count}), or NULL. */
+typedef struct {
+  int64_t nx, ny, nz;
+  const void* in;        /* DEVICE float32 (nx, ny, nz) */
+  void* out;             /* DEVICE float32 (nx, ny, nz); F for STEAM_EPI_FLUX */
+  const void* pre;       /* DEVICE float32 [2][nz] {div, mul}, or NULL */
+  int32_t has_window;    /* 0: the whole array */
+  steam_window_t window;
+  double* sums;
+} steam_conv_problem_t;
+size_t steam_conv_group_workspace_bytes(int32_t n, const steam_conv_problem_t* problems);
+int steam_conv_group_prepare(const steam_sepconv_t* spec, const double* z_taps,
+                             const double* y_taps, const double* x_taps, int32_t n,
+                             const steam_conv_problem_t* problems, int32_t epilogue,
+                             void* workspace, size_t workspace_bytes);
+int steam_conv_group_async(void* workspace, steam_stream_t stream);
+int steam_conv_group_release(void* workspace);
+
 /* Float32 flux convolutions (STEAM_EPI_FLUX on float32 fields) run on the
  * packed float32 kernel by default (wide = 0); wide = 1 runs them with
  * float64 taps and accumulators instead.  Process-wide. */

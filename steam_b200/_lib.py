@@ -50,6 +50,13 @@ class BAProblem(ctypes.Structure):
                 ("has_window", c_i32), ("window", Window), ("ledger", ctypes.c_void_p)]
 
 
+class ConvProblem(ctypes.Structure):
+    """steam_conv_problem_t: one field of a grouped convolution."""
+    _fields_ = [("nx", c_i64), ("ny", c_i64), ("nz", c_i64), ("in_", ctypes.c_void_p),
+                ("out", ctypes.c_void_p), ("pre", ctypes.c_void_p), ("has_window", c_i32),
+                ("window", Window), ("sums", ctypes.c_void_p)]
+
+
 class SepConv(ctypes.Structure):
     """steam_sepconv_t"""
     _fields_ = [("kz", c_i32), ("ky", c_i32), ("kx", c_i32),
@@ -82,6 +89,12 @@ _SIGNATURES = {
     "steam_conv_set_tile_rows": (ctypes.c_int, [c_i64, c_i64, c_i64, c_i32]),
     "steam_conv_get_tile_rows": (ctypes.c_int, [c_i64, c_i64, c_i64]),
     "steam_conv_set_flux_wide": (ctypes.c_int, [c_i32]),
+    "steam_conv_group_workspace_bytes": (ctypes.c_size_t, [c_i32, ctypes.POINTER(ConvProblem)]),
+    "steam_conv_group_prepare": (ctypes.c_int, [ctypes.POINTER(SepConv), c_dp, c_dp, c_dp,
+                                                c_i32, ctypes.POINTER(ConvProblem), c_i32,
+                                                c_vp, ctypes.c_size_t]),
+    "steam_conv_group_async": (ctypes.c_int, [c_vp, c_vp]),
+    "steam_conv_group_release": (ctypes.c_int, [c_vp]),
     "steam_take_wait_errors": (ctypes.c_int, [ctypes.POINTER(c_i32)]),
     "steam_conv_packed_launches": (c_i64, []),
     "steam_conv_fft_spectrum_bytes": (c_size, []),

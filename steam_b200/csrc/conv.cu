@@ -1059,6 +1059,33 @@ extern "C" int steam_conv_separable_async(
   return fail(STEAM_ERR_ARG, "steam_conv_separable_async: bad dtype");
 }
 
+extern "C" size_t steam_conv_group_workspace_bytes(int32_t n,
+                                                 const steam_conv_problem_t* problems) {
+  if (n < 1 || !problems) return 0;
+  return packed_group_bytes(n, problems);
+}
+
+extern "C" int steam_conv_group_prepare(const steam_sepconv_t* spec, const double* z_taps,
+                                        const double* y_taps, const double* x_taps, int32_t n,
+                                        const steam_conv_problem_t* problems, int32_t epilogue,
+                                        void* workspace, size_t workspace_bytes) {
+  STEAM_REQUIRE(spec && z_taps && y_taps && x_taps, "steam_conv_group_prepare: null filters");
+  STEAM_REQUIRE(n >= 1 && problems, "steam_conv_group_prepare: no fields");
+  STEAM_REQUIRE(workspace, "steam_conv_group_prepare: null workspace");
+  std::unique_ptr<SepParams<float>> p(new SepParams<float>());
+  int rc = fill_params<float>(spec, z_taps, y_taps, x_taps, *p);
+  if (rc) return rc;
+  return packed_group_prepare(*p, n, problems, epilogue, workspace, workspace_bytes);
+}
+
+extern "C" int steam_conv_group_async(void* workspace, steam_stream_t stream) {
+  return packed_group_enqueue(workspace, (cudaStream_t)stream);
+}
+
+extern "C" int steam_conv_group_release(void* workspace) {
+  return packed_group_release(workspace);
+}
+
 extern "C" int steam_conv_set_flux_wide(int32_t wide) {
   STEAM_REQUIRE(wide == 0 || wide == 1, "steam_conv_set_flux_wide: wide must be 0 or 1");
   g_flux_wide.store(wide);

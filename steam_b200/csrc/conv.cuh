@@ -68,4 +68,12 @@ int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
                   const float* in, float* out, const float* pre, int epilogue,
                   const XEpi& epi, double* partials, cudaStream_t s);
 
+// Grouped launches of the packed kernel over many fields with the same
+// filters (steam_conv_group_*).
+size_t packed_group_bytes(int n, const steam_conv_problem_t* q);
+int packed_group_prepare(const SepParams<float>& p, int n, const steam_conv_problem_t* q,
+                         int epilogue, void* ws, size_t ws_bytes);
+int packed_group_enqueue(void* ws, cudaStream_t s);
+int packed_group_release(void* ws);
+
 }  // namespace steam

@@ -28,6 +28,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 #include "conv.cuh"
 
@@ -181,12 +182,13 @@ __device__ __forceinline__ void z_task(const float* __restrict__ sl, float* __re
   *reinterpret_cast<float4*>(d1 + 4) = make_float4(u1[2].x, u1[2].y, u1[3].x, u1[3].y);
 }
 
+// One field's convolution on blocks vb = 0 .. nvb - 1 (the block index and
+// count of a launch of its own, or a range of a grouped launch).
 template <int TY, bool PRE, bool P3, bool FLUX>
-__global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) packed_conv_kernel(
-    const __grid_constant__ CUtensorMap tm_box, const __grid_constant__ CUtensorMap tm_pair,
-    float* __restrict__ out, const float* __restrict__ pre,
-    const __grid_constant__ PackedTaps tp, PackedGeom g, XEpi epi,
-    double* __restrict__ partials) {
+__device__ __forceinline__ void packed_conv_body(
+    const CUtensorMap* tm_box, const CUtensorMap* tm_pair, float* __restrict__ out,
+    const float* __restrict__ pre, const PackedTaps& tp, const PackedGeom& g, const XEpi& epi,
+    double* __restrict__ partials, int vb, int nvb) {
   using Tl = PTile<TY>;
   constexpr int kPY = Tl::Y, kPR = Tl::R, kPThreads = Tl::Threads, kPSlab = Tl::Slab,
                 kPU = Tl::U, kPTasks = Tl::Tasks;
@@ -197,9 +199,9 @@ __global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) pack
   float* s_pre = su0 + 4 * kPU;           // [kPC]
   uint64_t* bars = reinterpret_cast<uint64_t*>(s_pre + kPC);
   const int t = threadIdx.x, lane = t & 31;
-  const int zt_i = blockIdx.x % g.nzt;
-  const int yt_i = (blockIdx.x / g.nzt) % g.nyt;
-  const int64_t xc = blockIdx.x / ((int64_t)g.nzt * g.nyt);
+  const int zt_i = vb % g.nzt;
+  const int yt_i = (vb / g.nzt) % g.nyt;
+  const int64_t xc = vb / ((int64_t)g.nzt * g.nyt);
   const int z0 = zt_i * kPZ;
   const int64_t y0 = (int64_t)yt_i * kPY;
   const int64_t xb = xc * g.chunk;
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) pack
     if (interior) {
       if (lane == 0) {
         mbar_expect_tx(bar, kPSlab * 4);
-        tma_load_3d(dst, &tm_box, zc, (int)(y0 - kPH), (int)xi, bar);
+        tma_load_3d(dst, tm_box, zc, (int)(y0 - kPH), (int)xi, bar);
       }
     } else {
       if (lane == 0) mbar_expect_tx(bar, kPSlab * 4);
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) pack
       for (int pr = lane; pr < kPR / 2; pr += 32) {
         int64_t yy = (y0 - kPH + 2 * pr) % g.ny;
         if (yy < 0) yy += g.ny;
-        tma_load_3d(dst + pr * 2 * kPC * 4, &tm_pair, zc, (int)yy, (int)xi, bar);
+        tma_load_3d(dst + pr * 2 * kPC * 4, tm_pair, zc, (int)yy, (int)xi, bar);
       }
     }
   };
@@ -384,9 +386,68 @@ __global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) pack
     const double t0 = block_sum(s_f, scratch);
     const double t1 = block_sum(s_clip, scratch);
     if (t == 0) {
-      partials[blockIdx.x] = t0;
-      partials[gridDim.x + blockIdx.x] = t1;
+      partials[vb] = t0;
+      partials[nvb + vb] = t1;
     }
+  }
+}
+
+template <int TY, bool PRE, bool P3, bool FLUX>
+__global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) packed_conv_kernel(
+    const __grid_constant__ CUtensorMap tm_box, const __grid_constant__ CUtensorMap tm_pair,
+    float* __restrict__ out, const float* __restrict__ pre,
+    const __grid_constant__ PackedTaps tp, PackedGeom g, XEpi epi,
+    double* __restrict__ partials) {
+  packed_conv_body<TY, PRE, P3, FLUX>(&tm_box, &tm_pair, out, pre, tp, g, epi, partials,
+                                      blockIdx.x, gridDim.x);
+}
+
+// ---- grouped form: many fields with the same filters, one launch ---------
+// A member: its tensor maps (device memory, 64-byte aligned), geometry,
+// epilogue window and partial sums, and its range of the launch's blocks.
+// Its blocks and chunk are those of a launch of its own, so its outputs and
+// sums are the same bits.
+struct alignas(64) PackedMember {
+  CUtensorMap box;
+  CUtensorMap pair;
+  float* out;
+  const float* pre;
+  double* partials;  // [2][nblocks] for the flux epilogue
+  double* sums;      // the member's flux totals (device, 2 doubles) or null
+  PackedGeom g;
+  XEpi epi;
+  int block0, nblocks;
+};
+
+template <int TY, bool PRE, bool P3, bool FLUX>
+__global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) packed_group_kernel(
+    const PackedMember* __restrict__ mem, const int* __restrict__ start, int n,
+    const __grid_constant__ PackedTaps tp) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= (int)blockIdx.x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const PackedMember& m = mem[lo];
+  const PackedGeom g = m.g;
+  const XEpi epi = m.epi;
+  packed_conv_body<TY, PRE, P3, FLUX>(&m.box, &m.pair, m.out, m.pre, tp, g, epi, m.partials,
+                                      (int)blockIdx.x - m.block0, m.nblocks);
+}
+
+// the members' flux totals {sum F over the window, clip count}, one block each
+__global__ void packed_group_sums_kernel(const PackedMember* __restrict__ mem) {
+  __shared__ double scratch[32];
+  const PackedMember& m = mem[blockIdx.x];
+  if (!m.sums) return;
+  for (int q = 0; q < 2; ++q) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < m.nblocks; i += blockDim.x) acc += m.partials[q * m.nblocks + i];
+    const double sum = block_sum(acc, scratch);
+    if (threadIdx.x == 0) m.sums[q] = sum;
   }
 }
 
@@ -505,6 +566,36 @@ cudaError_t launch_rows(int v, const CUtensorMap& box, const CUtensorMap& pair, 
   }
 }
 
+PackedTaps make_taps(const SepParams<float>& p, bool* p3_out) {
+  PackedTaps tp;
+  bool p3 = true;
+  for (int d = 0; d <= kPH; ++d) {
+    for (int f = 0; f < 2; ++f) {
+      const float zv = f < p.nzf ? (float)p.ztap(f)[kPH + d] : 0.f;
+      const float yv = f < p.nyf ? (float)p.ytap(f)[kPH + d] : 0.f;
+      tp.z[f][d] = make_float2(zv, zv);
+      tp.y[f][d] = make_float2(yv, yv);
+    }
+  }
+  for (int i = 0; i < kPK; ++i)
+    for (int f = 0; f < 2; ++f) {
+      const float xv = f < p.nxf ? (float)p.xtap(f)[i] : 0.f;
+      tp.x[f][i] = make_float2(xv, xv);
+    }
+  for (int a = 0; a < 2; ++a)
+    for (int cb = 0; cb < 4; ++cb) {
+      const int c = cb / 2, b = cb % 2;
+      double v = 0.0;
+      for (int q = 0; q < p.npairs; ++q)
+        if (a < p.nxf && p.pair_z[q] == c && p.pair_y[q] == b) v += p.mix[a * p.npairs + q];
+      tp.mix[a][cb] = make_float2((float)v, (float)v);
+      if (cb == 3 && (float)v != 0.f) p3 = false;
+    }
+  tp.cx = p.cx;
+  *p3_out = p3;
+  return tp;
+}
+
 }  // namespace
 
 bool packed_supported(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
@@ -547,31 +638,8 @@ int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
   } else {
     box = pair;  // every tile wraps in y: only the row-pair copies run
   }
-  PackedTaps tp;
-  for (int d = 0; d <= kPH; ++d) {
-    for (int f = 0; f < 2; ++f) {
-      const float zv = f < p.nzf ? (float)p.ztap(f)[kPH + d] : 0.f;
-      const float yv = f < p.nyf ? (float)p.ytap(f)[kPH + d] : 0.f;
-      tp.z[f][d] = make_float2(zv, zv);
-      tp.y[f][d] = make_float2(yv, yv);
-    }
-  }
-  for (int i = 0; i < kPK; ++i)
-    for (int f = 0; f < 2; ++f) {
-      const float xv = f < p.nxf ? (float)p.xtap(f)[i] : 0.f;
-      tp.x[f][i] = make_float2(xv, xv);
-    }
   bool p3 = true;
-  for (int a = 0; a < 2; ++a)
-    for (int cb = 0; cb < 4; ++cb) {
-      const int c = cb / 2, b = cb % 2;
-      double v = 0.0;
-      for (int q = 0; q < p.npairs; ++q)
-        if (a < p.nxf && p.pair_z[q] == c && p.pair_y[q] == b) v += p.mix[a * p.npairs + q];
-      tp.mix[a][cb] = make_float2((float)v, (float)v);
-      if (cb == 3 && (float)v != 0.f) p3 = false;
-    }
-  tp.cx = p.cx;
+  const PackedTaps tp = make_taps(p, &p3);
   PackedGeom g;
   g.nx = nx;
   g.ny = ny;
@@ -589,6 +657,158 @@ int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
   if (e != cudaSuccess)
     return fail(STEAM_ERR_CUDA, std::string("conv packed launch: ") + cudaGetErrorString(e));
   g_packed_launches.fetch_add(1);
+  return STEAM_OK;
+}
+
+// ---- grouped launches -------------------------------------------------------
+struct PackedGroupPlan {
+  int n = 0, total = 0, variant = 0;
+  PackedTaps tp;
+  PackedMember* mem = nullptr;
+  int* start = nullptr;
+};
+static std::mutex g_pgroup_mu;
+static std::map<void*, PackedGroupPlan> g_pgroups;
+
+static int64_t group_member_blocks(int64_t nx, int64_t ny, int64_t nz) {
+  const int64_t chunk = packed_chunk(nx, ny, nz);
+  return ((nz + kPZ - 1) / kPZ) * ((ny + 32 - 1) / 32) * ((nx + chunk - 1) / chunk);
+}
+
+size_t packed_group_bytes(int n, const steam_conv_problem_t* q) {
+  size_t b = carve_bytes((size_t)n, sizeof(PackedMember)) + carve_bytes((size_t)n, sizeof(int));
+  for (int i = 0; i < n; ++i)
+    b += carve_bytes((size_t)2 * group_member_blocks(q[i].nx, q[i].ny, q[i].nz), sizeof(double));
+  return b + 4096;
+}
+
+int packed_group_prepare(const SepParams<float>& p, int n, const steam_conv_problem_t* q,
+                         int epilogue, void* ws, size_t ws_bytes) {
+  STEAM_REQUIRE(epilogue == STEAM_EPI_STORE || epilogue == STEAM_EPI_FLUX,
+                "steam_conv_group_prepare: epilogue must be STORE or FLUX");
+  STEAM_REQUIRE(p.cx == kPH, "steam_conv_group_prepare: the x filter's centre must be 6");
+  const bool pre = q[0].pre != nullptr;
+  for (int i = 0; i < n; ++i) {
+    const steam_conv_problem_t& m = q[i];
+    const std::string who = "steam_conv_group_prepare: field " + std::to_string(i);
+    STEAM_REQUIRE((m.pre != nullptr) == pre, who + ": every field or none takes the scaling");
+    STEAM_REQUIRE(m.nx >= kPK && m.ny >= kPK, who + ": narrower than the filters");
+    STEAM_REQUIRE(packed_rows(m.nx, m.ny, m.nz) == 32, who + ": tuned to 64-row tiles");
+    STEAM_REQUIRE(packed_supported(p, m.nx, m.ny, m.nz, m.in, m.out, epilogue),
+                  who + ": not a packed-kernel layout (float32, nz % 4 == 0, ny even, "
+                        "16-byte aligned)");
+    if (m.has_window) {
+      STEAM_REQUIRE(m.window.x0 >= 0 && m.window.x1 <= m.nx && m.window.x0 < m.window.x1 &&
+                        m.window.y0 >= 0 && m.window.y1 <= m.ny && m.window.y0 < m.window.y1,
+                    who + ": window outside the array");
+    }
+  }
+  Carver c(ws, ws_bytes);
+  PackedGroupPlan plan;
+  plan.n = n;
+  plan.mem = c.take<PackedMember>((size_t)n);
+  plan.start = c.take<int>((size_t)n);
+  if (!plan.mem || !plan.start)
+    return fail(STEAM_ERR_WORKSPACE, "steam_conv_group_prepare: workspace too small");
+  std::vector<PackedMember> mem((size_t)n);
+  std::vector<int> start((size_t)n);
+  int64_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    const steam_conv_problem_t& m = q[i];
+    PackedMember& r = mem[(size_t)i];
+    if (!encode_map(&r.pair, (const float*)m.in, m.nx, m.ny, m.nz, 2))
+      return fail(STEAM_ERR_CUDA, "steam_conv_group_prepare: tensor map encoding failed");
+    if (m.ny >= 32 + kPK - 1) {
+      if (!encode_map(&r.box, (const float*)m.in, m.nx, m.ny, m.nz, 32 + kPK - 1))
+        return fail(STEAM_ERR_CUDA, "steam_conv_group_prepare: tensor map encoding failed");
+    } else {
+      r.box = r.pair;
+    }
+    r.out = (float*)m.out;
+    r.pre = (const float*)m.pre;
+    r.g.nx = m.nx;
+    r.g.ny = m.ny;
+    r.g.nz = (int)m.nz;
+    r.g.nzt = (int)((m.nz + kPZ - 1) / kPZ);
+    r.g.nyt = (int)((m.ny + 31) / 32);
+    r.g.chunk = packed_chunk(m.nx, m.ny, m.nz);
+    r.epi.mode = epilogue;
+    r.epi.wx0 = m.has_window ? m.window.x0 : 0;
+    r.epi.wx1 = m.has_window ? m.window.x1 : m.nx;
+    r.epi.wy0 = m.has_window ? m.window.y0 : 0;
+    r.epi.wy1 = m.has_window ? m.window.y1 : m.ny;
+    const int64_t nb = (int64_t)r.g.nzt * r.g.nyt * ((m.nx + r.g.chunk - 1) / r.g.chunk);
+    r.partials = c.take<double>((size_t)2 * nb);
+    if (!r.partials)
+      return fail(STEAM_ERR_WORKSPACE, "steam_conv_group_prepare: workspace too small");
+    r.sums = epilogue == STEAM_EPI_FLUX ? m.sums : nullptr;
+    r.block0 = (int)total;
+    r.nblocks = (int)nb;
+    start[(size_t)i] = (int)total;
+    total += nb;
+    STEAM_REQUIRE(total < ((int64_t)1 << 31), "steam_conv_group_prepare: grid too large");
+  }
+  bool p3 = true;
+  plan.tp = make_taps(p, &p3);
+  plan.total = (int)total;
+  plan.variant = (pre ? 4 : 0) | (p3 ? 2 : 0) | (epilogue == STEAM_EPI_FLUX ? 1 : 0);
+  STEAM_CUDA(cudaMemcpy(plan.mem, mem.data(), sizeof(PackedMember) * (size_t)n,
+                        cudaMemcpyHostToDevice));
+  STEAM_CUDA(cudaMemcpy(plan.start, start.data(), sizeof(int) * (size_t)n,
+                        cudaMemcpyHostToDevice));
+  std::lock_guard<std::mutex> lock(g_pgroup_mu);
+  g_pgroups[ws] = plan;
+  return STEAM_OK;
+}
+
+namespace {
+template <bool PRE, bool P3, bool FLUX>
+cudaError_t group_launch_v(const PackedGroupPlan& plan, cudaStream_t s) {
+  using Tl = PTile<32>;
+  auto kern = packed_group_kernel<32, PRE, P3, FLUX>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tl::Smem);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)plan.total, Tl::Threads, Tl::Smem, s>>>(plan.mem, plan.start, plan.n,
+                                                           plan.tp);
+  return cudaGetLastError();
+}
+}  // namespace
+
+int packed_group_enqueue(void* ws, cudaStream_t s) {
+  PackedGroupPlan plan;
+  {
+    std::lock_guard<std::mutex> lock(g_pgroup_mu);
+    auto it = g_pgroups.find(ws);
+    STEAM_REQUIRE(it != g_pgroups.end(),
+                  "steam_conv_group_async: workspace holds no prepared group");
+    plan = it->second;
+  }
+  cudaError_t e;
+  switch (plan.variant) {
+    case 0: e = group_launch_v<false, false, false>(plan, s); break;
+    case 1: e = group_launch_v<false, false, true>(plan, s); break;
+    case 2: e = group_launch_v<false, true, false>(plan, s); break;
+    case 3: e = group_launch_v<false, true, true>(plan, s); break;
+    case 4: e = group_launch_v<true, false, false>(plan, s); break;
+    case 5: e = group_launch_v<true, false, true>(plan, s); break;
+    case 6: e = group_launch_v<true, true, false>(plan, s); break;
+    default: e = group_launch_v<true, true, true>(plan, s); break;
+  }
+  count_launch();
+  if (e != cudaSuccess)
+    return fail(STEAM_ERR_CUDA, std::string("conv group launch: ") + cudaGetErrorString(e));
+  g_packed_launches.fetch_add(1);
+  if (plan.variant & 1) {
+    packed_group_sums_kernel<<<plan.n, 256, 0, s>>>(plan.mem);
+    STEAM_LAUNCH_CHECK("conv group sums");
+  }
+  return STEAM_OK;
+}
+
+int packed_group_release(void* ws) {
+  std::lock_guard<std::mutex> lock(g_pgroup_mu);
+  g_pgroups.erase(ws);
   return STEAM_OK;
 }
 

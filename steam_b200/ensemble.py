@@ -5,13 +5,16 @@ Hz): the finest class of a root run over the member's domain, run by a
 ``ResidentClass`` on device fields.  ``Ensemble`` spreads the members over a
 few CUDA streams and captures one step of all of them into a single CUDA
 graph: a replay then issues the whole step with one launch call.  The step
-runs stage by stage: every member's flux advance and h increment (its
-streaming kernels, spread over the streams), then ONE grouped bounded add of
-h over all members (``steam_bounded_add_group_async``: one launch per stage of
-the solve, each persistent phase a single cooperative launch whose blocks
-split into per-member teams with their own grid barriers), every member's qt
-increment, one grouped bounded add of qt, and every member's thermodynamics.
-Members of uneven sizes fill the GPU side by side.
+runs stage by stage: every member's flux noise (spread over the streams),
+ONE grouped flux convolution over all members (``steam_conv_group_async``:
+every member its own block range of one packed-kernel launch, the same bits
+as its own launch), every member's flux restore and h pattern, one grouped h
+convolution, ONE grouped bounded add of h (``steam_bounded_add_group_async``:
+one launch per stage of the solve, each persistent phase a cooperative launch
+whose blocks split into per-member teams with their own grid barriers) on a
+side stream beside every member's qt pattern and the grouped qt convolution,
+one grouped bounded add of qt, and every member's thermodynamics.  Members of
+uneven sizes fill the GPU side by side.
 
 ``autotune_conv`` is the tile-shape autotuner: for a field shape it times the
 fused convolution over its CTA tile heights (32 or 64 rows for the packed
@@ -185,12 +188,54 @@ class Ensemble:
         # and its stream's workspace before anything is captured
         self.step_eager()
         torch.cuda.synchronize()
+        self.conv_groups = {}
+        self.side_stream = torch.cuda.Stream()
         if grouped:
             self.groups = self._prepare_groups()
             self.grouped = bool(self.groups)
             if self.grouped:
+                self.conv_groups = self._prepare_conv_groups()
                 self.step_eager()
                 torch.cuda.synchronize()
+
+    def _prepare_conv_groups(self):
+        """One grouped launch per convolution stage (flux, h, qt) over every
+        member, when all members share the filters and the packed kernel
+        takes their layout; otherwise the members' convolutions stay
+        per-member launches."""
+        import torch
+        lib = _lib.load()
+        plan0 = self.members[0].setup.plan
+        if plan0.kind != 'separable' or self.members[0].rc.code != _lib.STEAM_F32:
+            return {}
+        k0 = np.asarray(plan0.kernel)
+        for m in self.members:
+            pl = m.setup.plan
+            if pl.kind != 'separable' or not np.array_equal(np.asarray(pl.kernel), k0):
+                return {}
+        groups = {}
+        for stage in ('flux', 'h', 'qt'):
+            probs = []
+            for m in self.members:
+                product, W, inc_h, inc_qt = m.buffers()
+                if stage == 'flux':
+                    probs.append(m.rc.conv_problem(product, m.F, flux=True))
+                else:
+                    inc = inc_h if stage == 'h' else inc_qt
+                    probs.append(m.rc.conv_problem(W, inc, pre=m.rc.pre[stage]))
+            arr = (_lib.ConvProblem * len(probs))(*probs)
+            nbytes = lib.steam_conv_group_workspace_bytes(len(probs), arr)
+            ws = torch.empty(int(nbytes), dtype=torch.uint8, device='cuda')
+            epi = _lib.STEAM_EPI_FLUX if stage == 'flux' else _lib.STEAM_EPI_STORE
+            rc = lib.steam_conv_group_prepare(
+                ctypes.byref(plan0.spec), plan0.z_taps, plan0.y_taps, plan0.x_taps, len(probs),
+                arr, epi, _lib.ptr(ws), int(nbytes))
+            if rc != 0:
+                for w, _ in groups.values():
+                    lib.steam_conv_group_release(_lib.ptr(w))
+                return {}
+            groups[stage] = (ws, arr)
+        return groups
 
     def _prepare_groups(self):
         """One grouped bounded add per scalar over every member (members
@@ -223,7 +268,10 @@ class Ensemble:
         lib = _lib.load()
         for ws, _ in self.groups.values():
             lib.steam_bounded_add_group_release(_lib.ptr(ws))
+        for ws, _ in getattr(self, 'conv_groups', {}).values():
+            lib.steam_conv_group_release(_lib.ptr(ws))
         self.groups = {}
+        self.conv_groups = {}
         self.grouped = False
         self.graph = None
 
@@ -242,33 +290,75 @@ class Ensemble:
             main.wait_stream(s)
 
     def _issue_grouped(self):
-        """One ensemble step stage by stage: every member's flux advance and
-        h increment (over the streams), ONE grouped bounded add of h over all
-        members, every member's qt increment, one grouped bounded add of qt,
-        every member's thermodynamics."""
+        """One ensemble step stage by stage: every member's flux noise (over
+        the streams), ONE grouped flux convolution, every member's flux
+        restore and h pattern, one grouped h convolution, ONE grouped bounded
+        add of h over all members (on a side stream, beside the next two
+        stages), every member's qt pattern, one grouped qt convolution, one
+        grouped bounded add of qt, every member's thermodynamics.  (Without conv groups each member runs its own
+        convolutions inside the fanned stages.)"""
         lib = _lib.load()
+        cg = self.conv_groups
 
-        def first(m):
-            m.reset()
-            product, W, inc_h, _ = m.buffers()
-            m.rc.enqueue_flux(m.F, product)
-            m.rc.enqueue_increment('h', m.h, product, W, inc_h)
+        def conv(stage):
+            _lib.check(lib.steam_conv_group_async(_lib.ptr(cg[stage][0]), _lib.stream()))
 
-        def second(m):
-            product, W, _, inc_qt = m.buffers()
-            m.rc.enqueue_increment('qt', m.q, product, W, inc_qt)
+        def ba(name):
+            _lib.check(lib.steam_bounded_add_group_async(_lib.ptr(self.groups[name][0]),
+                                                         _lib.stream()))
+
+        if cg:
+            def noise(m):
+                m.reset()
+                product, _, _, _ = m.buffers()
+                m.rc.enqueue_noise(m.F, product)
+
+            def finish_h(m):
+                product, W, _, _ = m.buffers()
+                m.rc.enqueue_flux_finish(m.F)
+                m.rc.enqueue_pattern('h', m.h, product, W)
+
+            def pattern_q(m):
+                product, W, _, _ = m.buffers()
+                m.rc.enqueue_pattern('qt', m.q, product, W)
+
+            import torch
+            main = torch.cuda.current_stream()
+            self._fan(noise)
+            conv('flux')
+            self._fan(finish_h)
+            conv('h')
+            # h's bounded add on a side stream while the qt patterns and the
+            # qt convolution run (they read qt', the product and W, never h')
+            side = self.side_stream
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                ba('h')
+            self._fan(pattern_q)
+            conv('qt')
+            ba('qt')
+            main.wait_stream(side)
+        else:
+            def first(m):
+                m.reset()
+                product, W, inc_h, _ = m.buffers()
+                m.rc.enqueue_flux(m.F, product)
+                m.rc.enqueue_increment('h', m.h, product, W, inc_h)
+
+            def second(m):
+                product, W, _, inc_qt = m.buffers()
+                m.rc.enqueue_increment('qt', m.q, product, W, inc_qt)
+
+            self._fan(first)
+            ba('h')
+            self._fan(second)
+            ba('qt')
 
         def third(m):
             m.rc.enqueue_thermo(m.h, m.q, m.diag)
             m.rc.ledger_host.copy_(m.rc.ledger, non_blocking=True)
             m.rc.ledger_ready.record()
 
-        self._fan(first)
-        _lib.check(lib.steam_bounded_add_group_async(_lib.ptr(self.groups['h'][0]),
-                                                     _lib.stream()))
-        self._fan(second)
-        _lib.check(lib.steam_bounded_add_group_async(_lib.ptr(self.groups['qt'][0]),
-                                                     _lib.stream()))
         self._fan(third)
 
     @property

@@ -222,25 +222,43 @@ class ResidentClass:
     def enqueue_flux(self, F, product, replay=None):
         """Flux advance: noise x F into ``product``, the flux convolution
         with its clip and window sum, the restore to the entering mean."""
+        cs = self.setup
+        ws, _, _ = self._ws()
+        self.enqueue_noise(F, product)
+        _utils.run_plan_async(cs.plan, product, F, None, _lib.STEAM_EPI_FLUX, cs.window,
+                              _off(self.ledger, self.o_cs), ws, _lib.stream())
+        self.enqueue_flux_finish(F, replay)
+
+    def enqueue_noise(self, F, product):
+        """The flux noise: product = eps F and the entering sums."""
         lib, cs, code = self.lib, self.setup, self.code
-        stream = _lib.stream()
-        L = self.ledger
-        src = L if replay is None else replay.block
-        cells = self.cells if replay is None else replay.cells
         ws, wsp, wsn = self._ws()
         _lib.check(lib.steam_flux_noise_async(
             code, ctypes.byref(self.region), self.alpha, self.pcs, self.shift, int(cs.n_zero),
             int(bool(cs.zero_bottom)), int(bool(cs.zero_top)), _lib.ptr(F), _lib.ptr(product),
-            _lib.window_arg(cs.window), _off(L, self.o_ns), wsp, wsn, stream))
-        _utils.run_plan_async(cs.plan, product, F, None, _lib.STEAM_EPI_FLUX, cs.window,
-                              _off(L, self.o_cs), ws, stream)
-        _lib.check(lib.steam_flux_finish_async(
-            code, F.numel(), _lib.ptr(F), _off(src, self.o_ns), _off(src, self.o_cs), cells,
-            _off(L, self.o_fl), stream))
+            _lib.window_arg(cs.window), _off(self.ledger, self.o_ns), wsp, wsn, _lib.stream()))
+
+    def enqueue_flux_finish(self, F, replay=None):
+        """The restore of F to its entering mean (after the flux convolution)."""
+        L = self.ledger
+        src = L if replay is None else replay.block
+        cells = self.cells if replay is None else replay.cells
+        _lib.check(self.lib.steam_flux_finish_async(
+            self.code, F.numel(), _lib.ptr(F), _off(src, self.o_ns), _off(src, self.o_cs),
+            cells, _off(L, self.o_fl), _lib.stream()))
 
     def enqueue_increment(self, name, pert, product, W, inc, replay=None):
         """Scalar ``name``'s pattern into ``W``, its per-level normalisation
         and the second convolution into ``inc``."""
+        cs = self.setup
+        ws, _, _ = self._ws()
+        self.enqueue_pattern(name, pert, product, W, replay)
+        _utils.run_plan_async(cs.plan, W, inc, self.pre[name], _lib.STEAM_EPI_STORE,
+                              cs.window, None, ws, _lib.stream())
+
+    def enqueue_pattern(self, name, pert, product, W, replay=None):
+        """Scalar ``name``'s pattern into ``W`` and its per-level
+        normalisation (the second convolution's input scaling)."""
         lib, cs, code = self.lib, self.setup, self.code
         nx, ny, nz = self.shape
         stream = _lib.stream()
@@ -256,8 +274,23 @@ class ResidentClass:
         _lib.check(lib.steam_pattern_norm_async(
             code, nz, _off(src, self.o_ps[name]), _lib.ptr(self.mul[name]),
             _lib.ptr(self.pre[name]), stream))
-        _utils.run_plan_async(cs.plan, W, inc, self.pre[name], _lib.STEAM_EPI_STORE,
-                              cs.window, None, ws, stream)
+
+    def conv_problem(self, src, out, pre=None, flux=False):
+        """A convolution of this class as one field of a grouped launch
+        (``steam_conv_problem_t``): the flux convolution (``flux``: its sums
+        go to this class's ledger) or a second convolution with ``pre``."""
+        nx, ny, nz = self.shape
+        p = _lib.ConvProblem()
+        p.nx, p.ny, p.nz = nx, ny, nz
+        p.in_ = src.data_ptr()
+        p.out = out.data_ptr()
+        p.pre = None if pre is None else pre.data_ptr()
+        w = self.setup.window
+        p.has_window = 0 if w is None else 1
+        if w is not None:
+            p.window = _lib.Window(*[int(v) for v in w])
+        p.sums = self.ledger.data_ptr() + 8 * int(self.o_cs) if flux else None
+        return p
 
     def enqueue_bounded_add(self, name, pert, inc, replay=None):
         """Scalar ``name``'s bounded amplitude-preserving add of ``inc``
