@@ -632,14 +632,14 @@ def main(argv=None):
         del srv, tw
 
     # batched ensemble: members of uneven sizes (64^3 .. 256x256x128, log-uniform)
-    # and parameters, over four streams, eagerly and from one captured CUDA
+    # and parameters, over eight streams, eagerly and from one captured CUDA
     # graph; beside it the plain FP64 drop-in (stage by stage, float64) on the
     # same members
     ensemble = None
     if args.ensemble_members > 0:
         from steam_b200.ensemble import Ensemble, config_members, plain_fp64_throughput
         members = config_members(args.ensemble_members)
-        ens = Ensemble(members, n_streams=4)
+        ens = Ensemble(members, n_streams=8)
         eager = ens.throughput(steps=3, graph=False)
         ens.check()
         graph = ens.throughput(steps=3, graph=True)
@@ -653,7 +653,7 @@ def main(argv=None):
         # the same members in float64: the resident graph (precision apart
         # from API) and the plain stage-by-stage drop-in (API apart)
         members = config_members(args.ensemble_members, dtype=np.float64)
-        ens = Ensemble(members, n_streams=4, tune=False)
+        ens = Ensemble(members, n_streams=8, tune=False)
         ensemble["graph_fp64"] = ens.throughput(steps=2, graph=True)
         ens.check()
         ens.release()

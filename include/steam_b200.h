@@ -159,8 +159,11 @@ int steam_conv_get_tile_rows(int64_t nx, int64_t ny, int64_t nz);
 /* Grouped convolutions (no counterpart in the reference): n float32 fields
  * convolved with the same separable filters (a spec steam_conv_separable
  * runs on the packed kernel) as ONE launch, every field its own range of
- * blocks.  A field's blocks and x chunk are those of a launch of its own, so
- * its output and its flux sums are the same bits.  Every field: the packed
+ * blocks.  A field's output is the same bits as a launch of its own.  When
+ * the group's tiles give every SM at least 4 CTAs, each field's CTAs take its
+ * whole x extent (no repeated halo planes) and its flux sums equal its own
+ * launch's to rounding; otherwise each keeps its own launch's x chunk and its
+ * sums are the same bits too.  Every field: the packed
  * kernel's layout (nz % 4 == 0, ny even, 16-byte aligned in and out), nx, ny
  * >= 13, 32-row tiles; all fields or none take the input scaling.
  * prepare (synchronous, outside stream capture) lays the group out in

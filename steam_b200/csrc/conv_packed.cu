@@ -405,8 +405,9 @@ __global__ void __launch_bounds__(PTile<TY>::Threads, PTile<TY>::MinBlocks) pack
 // ---- grouped form: many fields with the same filters, one launch ---------
 // A member: its tensor maps (device memory, 64-byte aligned), geometry,
 // epilogue window and partial sums, and its range of the launch's blocks.
-// Its blocks and chunk are those of a launch of its own, so its outputs and
-// sums are the same bits.
+// Its outputs are the same bits as a launch of its own (a voxel's arithmetic
+// does not depend on the tiling); its flux sums too when it keeps its own
+// chunk, and to rounding when the group gives it whole-x CTAs.
 struct alignas(64) PackedMember {
   CUtensorMap box;
   CUtensorMap pair;
@@ -670,15 +671,35 @@ struct PackedGroupPlan {
 static std::mutex g_pgroup_mu;
 static std::map<void*, PackedGroupPlan> g_pgroups;
 
-static int64_t group_member_blocks(int64_t nx, int64_t ny, int64_t nz) {
-  const int64_t chunk = packed_chunk(nx, ny, nz);
-  return ((nz + kPZ - 1) / kPZ) * ((ny + 32 - 1) / 32) * ((nx + chunk - 1) / chunk);
+// A member's x chunk in a group: its whole x extent when the group's tiles
+// alone give every SM at least kGroupTilesPerSm CTAs (the other members fill
+// the GPU, so a member needs no short chunks of its own, and whole-x CTAs
+// carry no repeated 12-plane halo), its own launch's chunk otherwise.
+constexpr int kGroupTilesPerSm = 4;
+
+static int64_t member_tiles(int64_t ny, int64_t nz) {
+  return ((nz + kPZ - 1) / kPZ) * ((ny + 32 - 1) / 32);
+}
+
+static bool group_whole_x(int n, const steam_conv_problem_t* q) {
+  int64_t tiles = 0;
+  for (int i = 0; i < n; ++i) tiles += member_tiles(q[i].ny, q[i].nz);
+  return tiles >= (int64_t)kGroupTilesPerSm * sm_count();
+}
+
+static int64_t group_member_chunk(const steam_conv_problem_t& m, bool whole_x) {
+  return whole_x ? m.nx : packed_chunk(m.nx, m.ny, m.nz);
 }
 
 size_t packed_group_bytes(int n, const steam_conv_problem_t* q) {
   size_t b = carve_bytes((size_t)n, sizeof(PackedMember)) + carve_bytes((size_t)n, sizeof(int));
-  for (int i = 0; i < n; ++i)
-    b += carve_bytes((size_t)2 * group_member_blocks(q[i].nx, q[i].ny, q[i].nz), sizeof(double));
+  const bool whole_x = group_whole_x(n, q);
+  for (int i = 0; i < n; ++i) {
+    const int64_t chunk = group_member_chunk(q[i], whole_x);
+    b += carve_bytes((size_t)2 * member_tiles(q[i].ny, q[i].nz) *
+                         ((q[i].nx + chunk - 1) / chunk),
+                     sizeof(double));
+  }
   return b + 4096;
 }
 
@@ -712,6 +733,7 @@ int packed_group_prepare(const SepParams<float>& p, int n, const steam_conv_prob
     return fail(STEAM_ERR_WORKSPACE, "steam_conv_group_prepare: workspace too small");
   std::vector<PackedMember> mem((size_t)n);
   std::vector<int> start((size_t)n);
+  const bool whole_x = group_whole_x(n, q);
   int64_t total = 0;
   for (int i = 0; i < n; ++i) {
     const steam_conv_problem_t& m = q[i];
@@ -731,7 +753,7 @@ int packed_group_prepare(const SepParams<float>& p, int n, const steam_conv_prob
     r.g.nz = (int)m.nz;
     r.g.nzt = (int)((m.nz + kPZ - 1) / kPZ);
     r.g.nyt = (int)((m.ny + 31) / 32);
-    r.g.chunk = packed_chunk(m.nx, m.ny, m.nz);
+    r.g.chunk = group_member_chunk(m, whole_x);
     r.epi.mode = epilogue;
     r.epi.wx0 = m.has_window ? m.window.x0 : 0;
     r.epi.wx1 = m.has_window ? m.window.x1 : m.nx;

@@ -1,11 +1,12 @@
 """Grouped packed convolutions (needs a B200).
 
 Fields of different shapes convolved with the same turbulon filters as one
-launch (``steam_conv_group_*``): each field's output -- and, with the flux
-epilogue, its window sum and clip count -- is the same bits as its own
-launch of the packed kernel (its blocks and x chunk are the same); the
-grouped ensemble step with its convolutions grouped equals the one with
-per-member convolutions bit for bit.
+launch (``steam_conv_group_*``): each field's output is the same bits as its
+own launch of the packed kernel, and with the flux epilogue its window sum
+and clip count are the same bits (a small group: each field keeps its own x
+chunk); the ensemble step with its convolutions grouped (a large group: each
+member's CTAs take its whole x extent) equals the one with per-member
+convolutions to rounding.
 """
 
 import numpy as np
@@ -114,7 +115,7 @@ def test_group_rejects_other_layouts():
     assert rc != 0 and b"layout" in lib.steam_last_error()
 
 
-def test_ensemble_with_grouped_convolutions_equals_per_member_convolutions():
+def test_ensemble_with_grouped_convolutions_against_per_member_convolutions():
     import torch
     from steam_b200.ensemble import Ensemble, Member
     shapes = [(64, 64, 64), (80, 80, 64), (48, 48, 48), (96, 64, 32)]
@@ -132,5 +133,52 @@ def test_ensemble_with_grouped_convolutions_equals_per_member_convolutions():
     torch.cuda.synchronize()
     for m, ref in zip(members, a):
         for x, y in zip((m.h, m.q, m.F, m.diag['qc']), ref):
-            assert torch.equal(x, y)
+            rel = float(torch.linalg.vector_norm((x - y).double()) /
+                        max(float(torch.linalg.vector_norm(y.double())), 1e-30))
+            assert rel < 1e-6, rel
     ens.release()
+
+
+def test_large_group_whole_x_chunks():
+    """A group whose tiles fill every SM (each member's CTAs then take its
+    whole x extent): outputs the same bits as own launches, flux sums equal
+    to rounding, clip counts equal."""
+    import ctypes
+    import torch
+    from steam_b200 import utils as U
+    lib = _lib.load()
+    shape = (24, 256, 256)  # 64 tiles each: 10 members fill 148 SMs x 4
+    plan = U.plan_convolution(K64, shape, np.float32)
+    rng = np.random.default_rng(8)
+    fields, probs = [], []
+    for i in range(10):
+        src = torch.as_tensor((0.5 * rng.standard_normal(shape)).astype(np.float32), device='cuda')
+        F = torch.as_tensor((1.0 + 0.1 * rng.random(shape)).astype(np.float32), device='cuda')
+        sums = torch.zeros(2, dtype=torch.float64, device='cuda')
+        p = _lib.ConvProblem()
+        p.nx, p.ny, p.nz = shape
+        p.in_, p.out, p.pre = src.data_ptr(), F.data_ptr(), None
+        p.has_window = 0
+        p.sums = sums.data_ptr()
+        probs.append(p)
+        fields.append((src, F.clone(), F, sums))
+    arr = (_lib.ConvProblem * len(probs))(*probs)
+    nbytes = lib.steam_conv_group_workspace_bytes(len(probs), arr)
+    ws = torch.empty(int(nbytes), dtype=torch.uint8, device='cuda')
+    _lib.check(lib.steam_conv_group_prepare(ctypes.byref(plan.spec), plan.z_taps, plan.y_taps,
+                                            plan.x_taps, len(probs), arr, _lib.STEAM_EPI_FLUX,
+                                            _lib.ptr(ws), int(nbytes)))
+    try:
+        _lib.check(lib.steam_conv_group_async(_lib.ptr(ws), _lib.stream()))
+        torch.cuda.synchronize()
+        for src, F0, F, sums in fields:
+            own = F0.clone()
+            own_sums = torch.zeros(2, dtype=torch.float64, device='cuda')
+            U.run_plan_async(plan, src, own, None, _lib.STEAM_EPI_FLUX, None,
+                             ctypes.c_void_p(own_sums.data_ptr()))
+            torch.cuda.synchronize()
+            assert torch.equal(own, F)
+            assert float(sums[1]) == float(own_sums[1]) and float(sums[1]) > 0
+            assert float(sums[0]) == pytest.approx(float(own_sums[0]), rel=1e-13)
+    finally:
+        lib.steam_conv_group_release(_lib.ptr(ws))
