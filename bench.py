@@ -541,6 +541,17 @@ def main(argv=None):
             issue = {"achieved": ach, "peak": pk, "unit": "G warp instructions/s",
                      "frac": ach / pk, "inst_per_voxel": inst_per_voxel[name],
                      "sm_mhz": mhz, "sms": sms}
+    # the autotuner's choice for the convolution at this shape (CTA tile
+    # height x x chunk, timed once at set-up; 0 = the kernel's wave model)
+    conv_tuning = None
+    from steam_b200 import ensemble as _ens
+    tuned = _ens._TUNED.get((tuple(shape), tdt))
+    if tuned:
+        best = min(tuned, key=tuned.get)
+        conv_tuning = {"rows": int(best[0]), "chunk": int(best[1]),
+                       "ms": round(tuned[best], 3),
+                       "model_chunk_ms": round(tuned.get((32, 0), float("nan")), 3),
+                       "candidates": len(tuned)}
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic / 1e9 if traffic is not None else None,
@@ -557,6 +568,7 @@ def main(argv=None):
                             "instruction issue (FP32/FP64 pipes), not DRAM"),
                 "issue": issue,
                 "bounded_add_sweeps": ba_sweeps,
+                "conv_tuning": conv_tuning,
                 "breakdown_ms_per_step": {k: round(v[0] / max(args.steps, 1), 3)
                                           for k, v in sorted(calls.items(),
                                                              key=lambda kv: -kv[1][0])}}
