@@ -11,11 +11,8 @@ constexpr int kMaxZ = 8;
 constexpr int kMaxPairs = 16;
 constexpr int kMaxX = 4;
 
-// Taps, mixing weights and every accumulator are float64 for both storage
-// dtypes: the turbulon kernel's terms cancel (it has zero sum), and float32
-// taps with float32 sums put ~1e-5 relative error into the log of a flux
-// advanced next to its clip.  Fields and intermediates stay in the storage
-// dtype.
+// The filters of a separable convolution as the host factored them, in
+// float64 (each kernel rounds them to its arithmetic type).
 template <typename T>
 struct SepParams {
   int kz, ky, kx, cz, cy, cx;
