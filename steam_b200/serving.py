@@ -337,9 +337,16 @@ def poisson_trace(world, rate, n_requests, seed=4, sizes=(32, 64, 128, 256),
 
 
 def latency_summary(done):
+    """p50/p99 latency (arrival to host), overall and per size, and the tile
+    voxels served per second; ``offered_voxels_per_s``, the tile voxels the
+    arrivals asked for per second, beside it: when it exceeds the served
+    rate the device is saturated and the queue sets the latency."""
     lat = np.array([r['latency'] for r in done])
     vox = sum(r['n'] ** 3 for r in done)
     span = max(r['done'] for r in done) - min(r['arrival'] for r in done)
+    arrivals = sorted(r['arrival'] for r in done)
+    a_span = arrivals[-1] - arrivals[0]
+    offered = vox / a_span if a_span > 0 else None
     by = {}
     for n in sorted({r['n'] for r in done}):
         ln = np.array([r['latency'] for r in done if r['n'] == n])
@@ -347,4 +354,5 @@ def latency_summary(done):
                        "p99_ms": float(np.percentile(ln, 99) * 1e3)}
     return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "voxels_per_s": vox / span if span > 0 else None, "by_size": by}
+            "voxels_per_s": vox / span if span > 0 else None,
+            "offered_voxels_per_s": offered, "by_size": by}
