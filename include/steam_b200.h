@@ -199,6 +199,12 @@ int steam_conv_set_flux_wide(int32_t wide);
  * tile.  Reads the count of such blocks since the last call into *count and
  * resets it (synchronises the current device). */
 int steam_take_wait_errors(int32_t* count);
+/* The packed kernel's slab-wait limit in polls (0: the default, seconds of
+ * waiting) and a test hook: withhold = 1 issues no slab copy at all, so that
+ * every wait runs out with nothing in flight -- the blocks give up and count
+ * themselves -- without any fault.  Read when a launch is enqueued (a group:
+ * when it is prepared); 0, 0 restores the defaults. */
+int steam_set_copy_wait(int64_t polls, int32_t withhold);
 
 /* Launches of the packed float32 kernel so far in this process. */
 int64_t steam_conv_packed_launches(void);

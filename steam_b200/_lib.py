@@ -96,6 +96,7 @@ _SIGNATURES = {
     "steam_conv_group_async": (ctypes.c_int, [c_vp, c_vp]),
     "steam_conv_group_release": (ctypes.c_int, [c_vp]),
     "steam_take_wait_errors": (ctypes.c_int, [ctypes.POINTER(c_i32)]),
+    "steam_set_copy_wait": (ctypes.c_int, [c_i64, c_i32]),
     "steam_conv_packed_launches": (c_i64, []),
     "steam_conv_fft_spectrum_bytes": (c_size, []),
     "steam_conv_fft_spectrum": (ctypes.c_int, [c_vp, c_i32, c_i32, c_i32, c_vp, c_vp]),

@@ -85,7 +85,14 @@ struct PackedGeom {
   int64_t nx, ny;
   int nz, nzt, nyt;
   int64_t chunk;
+  long long wait_limit;  // polls of a slab's mbarrier before the block gives up
+  int withhold;          // test hook: no slab copy is issued, so every wait runs out
 };
+
+// steam_set_copy_wait: the wait limit (default kTmaWaitLimit) and the test
+// hook (default off), read when a launch is enqueued or a group prepared
+std::atomic<long long> g_copy_wait_limit{kTmaWaitLimit};
+std::atomic<int> g_copy_withhold{0};
 
 __device__ unsigned g_tma_wait_errors;
 std::atomic<long long> g_packed_launches{0};
@@ -118,9 +125,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
-// waits for the phase of `parity` to complete, at most kTmaWaitLimit polls
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < kTmaWaitLimit; ++i)
+// waits for the phase of `parity` to complete, at most `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -220,6 +227,7 @@ __device__ __forceinline__ void packed_conv_body(
   __syncthreads();
   // warp 0 stages input plane k into buffer k % kPStages
   auto issue = [&](int k) {
+    if (g.withhold) return;  // test hook: nothing in flight, every wait runs out
     const int b = k % kPStages;
     const uint32_t bar = smem_u32(bars + b);
     const uint32_t dst = smem_u32(slab + b * kPSlab);
@@ -262,7 +270,8 @@ __device__ __forceinline__ void packed_conv_body(
   bool gave_up = false;
   for (; k < count; ++k) {
     const int b = k % kPStages;
-    const bool landed = mbar_wait(smem_u32(bars + b), (uint32_t)((k / kPStages) & 1));
+    const bool landed =
+        mbar_wait(smem_u32(bars + b), (uint32_t)((k / kPStages) & 1), g.wait_limit);
     const int j = k - (kPK - 1);  // the output plane this iteration completes
     const int64_t x = xb + j;
     float* outp = out + (j >= 0 ? x : 0) * plane_elems;
@@ -376,7 +385,8 @@ __device__ __forceinline__ void packed_conv_body(
     if (t == 0) {
       const int last = (k + kPStages) < count ? (k + kPStages) : count;
       for (int kk = k; kk < last; ++kk)
-        (void)mbar_wait(smem_u32(bars + kk % kPStages), (uint32_t)((kk / kPStages) & 1));
+        (void)mbar_wait(smem_u32(bars + kk % kPStages), (uint32_t)((kk / kPStages) & 1),
+                        g.wait_limit);
       atomicAdd(&g_tma_wait_errors, 1u);
     }
     __syncthreads();
@@ -648,6 +658,8 @@ int packed_launch(const SepParams<float>& p, int64_t nx, int64_t ny, int64_t nz,
   g.nzt = (int)((nz + kPZ - 1) / kPZ);
   g.nyt = (int)((ny + rows - 1) / rows);
   g.chunk = packed_chunk(nx, ny, nz);
+  g.wait_limit = g_copy_wait_limit.load();
+  g.withhold = g_copy_withhold.load();
   const int64_t grid = (int64_t)g.nzt * g.nyt * ((nx + g.chunk - 1) / g.chunk);
   STEAM_REQUIRE(grid < ((int64_t)1 << 31), "steam_conv_separable: grid too large");
   const int v = (pre != nullptr ? 4 : 0) | (p3 ? 2 : 0) | (epilogue == STEAM_EPI_FLUX ? 1 : 0);
@@ -754,6 +766,8 @@ int packed_group_prepare(const SepParams<float>& p, int n, const steam_conv_prob
     r.g.nzt = (int)((m.nz + kPZ - 1) / kPZ);
     r.g.nyt = (int)((m.ny + 31) / 32);
     r.g.chunk = group_member_chunk(m, whole_x);
+    r.g.wait_limit = g_copy_wait_limit.load();
+    r.g.withhold = g_copy_withhold.load();
     r.epi.mode = epilogue;
     r.epi.wx0 = m.has_window ? m.window.x0 : 0;
     r.epi.wx1 = m.has_window ? m.window.x1 : m.nx;
@@ -852,6 +866,14 @@ extern "C" int steam_conv_set_tile_rows(int64_t nx, int64_t ny, int64_t nz, int3
 
 extern "C" int steam_conv_get_tile_rows(int64_t nx, int64_t ny, int64_t nz) {
   return steam::packed_rows(nx, ny, nz);
+}
+
+extern "C" int steam_set_copy_wait(int64_t polls, int32_t withhold) {
+  if (polls < 0 || (withhold != 0 && withhold != 1))
+    return steam::fail(STEAM_ERR_ARG, "steam_set_copy_wait: polls >= 0, withhold 0 or 1");
+  steam::g_copy_wait_limit.store(polls == 0 ? steam::kTmaWaitLimit : (long long)polls);
+  steam::g_copy_withhold.store(withhold);
+  return STEAM_OK;
 }
 
 extern "C" int steam_take_wait_errors(int32_t* count) {

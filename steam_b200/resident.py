@@ -448,6 +448,11 @@ class ResidentClass:
         device itself and passes False."""
         if wait:
             self.ledger_ready.synchronize()
+        n = ctypes.c_int32(0)
+        _lib.check(self.lib.steam_take_wait_errors(ctypes.byref(n)))
+        if n.value:
+            raise RuntimeError(f"resident class step: {n.value} convolution blocks gave up "
+                               "waiting for their slab copies; the step's fields are invalid")
         return self.parse_ledger(self.ledger_host.numpy().copy(), cl)
 
     def parse_ledger(self, v, cl=None):
