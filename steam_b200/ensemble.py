@@ -263,10 +263,20 @@ class Ensemble:
             groups[name] = (ws, arr)
         return groups
 
+    def __del__(self):
+        # the library keys a prepared group by its workspace's address: forget
+        # it before the workspace memory can be reused
+        try:
+            self.release()
+        except Exception:
+            pass
+
     def release(self):
         """Forget the grouped solves' device state (the graph too)."""
+        if not getattr(self, 'groups', None) and not getattr(self, 'conv_groups', None):
+            return
         lib = _lib.load()
-        for ws, _ in self.groups.values():
+        for ws, _ in getattr(self, 'groups', {}).values():
             lib.steam_bounded_add_group_release(_lib.ptr(ws))
         for ws, _ in getattr(self, 'conv_groups', {}).values():
             lib.steam_conv_group_release(_lib.ptr(ws))
