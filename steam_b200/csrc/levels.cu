@@ -1814,7 +1814,8 @@ struct BAGroupRec {
   int64_t nx, ny;
   int nz;
   int fold_nb;  // blocks of the first and apply sweeps
-  int ph_nb;    // blocks of each persistent phase
+  int ph_nb;    // blocks of the rescale-loop phase
+  int mu_nb;    // blocks of the shift-solve phase
 };
 
 // the field that owns block b of a grouped launch: start[p] <= b < start[p + 1]
@@ -1891,7 +1892,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3))
   const BAGroupRec<T>& r = recs[p0 + i];
   ba_phase_body<T, MODE>(r.inc, r.pert, r.nx, r.ny, r.nz, r.w, r.ch, r.st, r.partials,
                          r.totals, flag_base, n_iter, ba_smem, red,
-                         blockIdx.x - __ldg(start + i), r.ph_nb);
+                         blockIdx.x - __ldg(start + i), MODE == BA_MU ? r.mu_nb : r.ph_nb);
 }
 
 struct BAGroupPlan {
@@ -1901,8 +1902,10 @@ struct BAGroupPlan {
   size_t sm_sums = 0, sm_apply = 0;
   void* recs = nullptr;           // device BAGroupRec<T>[n]
   int* fold_start = nullptr;      // device [n]
-  int* ph_start = nullptr;        // device [n]: first block within the field's batch
-  std::vector<std::array<int, 3>> batches;  // {first field, fields, blocks}
+  int* ph_start = nullptr;        // device [n]: first block within the field's rescale batch
+  int* mu_start = nullptr;        // device [n]: the same for the shift batches
+  std::vector<std::array<int, 3>> batches;     // rescale phase: {first field, fields, blocks}
+  std::vector<std::array<int, 3>> mu_batches;  // shift phase
 };
 static std::mutex g_group_mu;
 static std::map<void*, BAGroupPlan> g_groups;
@@ -1932,7 +1935,7 @@ static size_t group_state_bytes(const steam_ba_problem_t& q, int R, size_t elem)
 
 template <typename T>
 static size_t group_bytes(int n, const steam_ba_problem_t* q, int R) {
-  size_t b = carve_bytes((size_t)n, sizeof(BAGroupRec<T>)) + 2 * carve_bytes((size_t)n, sizeof(int));
+  size_t b = carve_bytes((size_t)n, sizeof(BAGroupRec<T>)) + 3 * carve_bytes((size_t)n, sizeof(int));
   for (int i = 0; i < n; ++i) b += group_state_bytes(q[i], R, sizeof(T));
   return b + 4096;
 }
@@ -1948,7 +1951,8 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
   plan.recs = c.take<BAGroupRec<T>>((size_t)n);
   plan.fold_start = c.take<int>((size_t)n);
   plan.ph_start = c.take<int>((size_t)n);
-  if (!plan.recs || !plan.fold_start || !plan.ph_start)
+  plan.mu_start = c.take<int>((size_t)n);
+  if (!plan.recs || !plan.fold_start || !plan.ph_start || !plan.mu_start)
     return fail(STEAM_ERR_WORKSPACE, "steam_bounded_add_group_prepare: workspace too small");
   std::vector<int64_t> groups((size_t)n);
   for (int i = 0; i < n; ++i) {
@@ -1958,8 +1962,8 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
   }
   plan.sm_sums = ba_fold_smem_bytes<T>(plan.nz_max);
   plan.sm_apply = ba_fold_param_bytes<T>(plan.nz_max);
-  // co-resident capacity of the cooperative phases (the smaller of the two)
-  int cap = 0;
+  // co-resident capacity of each cooperative phase
+  int caps[2] = {0, 0};
   for (int mode = 0; mode < 2; ++mode) {
     auto kern = mode ? bag_phase_kernel<T, BA_MU> : bag_phase_kernel<T, BA_STATS>;
     STEAM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1968,52 +1972,67 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
     STEAM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLvThreads,
                                                              plan.sm_sums));
     STEAM_REQUIRE(per_sm >= 1, "steam_bounded_add_group_prepare: a phase does not fit an SM");
-    const int c_m = per_sm * sm_count();
-    cap = cap == 0 ? c_m : std::min(cap, c_m);
+    caps[mode] = per_sm * sm_count();
   }
-  // Batches of fields for the phases: as few as leave at least half of each
-  // batch's slots to deal out beyond one block per field; the fields dealt
-  // largest first to the batch with the least work so far.  Within a batch a
-  // field's team is one block plus its share of the spare slots in
-  // proportion to its column groups (at most one block per kPhaseMinGroups
-  // groups), so every team sweeps about the same bytes per block.  (One
-  // batch of the 256-member ensemble at three shift-phase blocks per SM --
-  // 347 blocks, the shift phase's accumulators spilling -- ran 16.7 ms of
-  // phases against 16.1 ms in two batches.)
-  const int B = std::max(1, (2 * n + cap - 1) / cap);
-  std::vector<int> idx((size_t)n);
-  for (int i = 0; i < n; ++i) idx[(size_t)i] = i;
-  std::stable_sort(idx.begin(), idx.end(),
-                   [&](int a, int b) { return groups[(size_t)a] > groups[(size_t)b]; });
-  std::vector<std::vector<int>> members((size_t)B);
-  std::vector<int64_t> load((size_t)B, 0);
-  for (int i : idx) {
-    int best = -1;
-    for (int b = 0; b < B; ++b)
-      if ((int)members[(size_t)b].size() < cap &&
-          (best < 0 || load[(size_t)b] < load[(size_t)best]))
-        best = b;
-    STEAM_REQUIRE(best >= 0, "steam_bounded_add_group_prepare: too many fields");
-    members[(size_t)best].push_back(i);
-    load[(size_t)best] += groups[(size_t)i];
-  }
-  std::vector<int> order, team((size_t)n);
-  for (int b = 0; b < B; ++b) {
-    auto& m = members[(size_t)b];
-    std::sort(m.begin(), m.end());
-    const int64_t spare = cap - (int64_t)m.size();
-    for (int i : m) {
-      const int64_t g = groups[(size_t)i];
-      const int64_t share = 1 + (int64_t)((double)spare * (double)g /
-                                          (double)std::max<int64_t>(load[(size_t)b], 1));
-      const int64_t useful = std::max<int64_t>((g + kPhaseMinGroups - 1) / kPhaseMinGroups, 1);
-      team[(size_t)i] = (int)std::min(std::min(share, useful), group_partial_blocks(g));
-      order.push_back(i);
+  // Batches of fields, per phase: as few as leave at least 40 % of each
+  // batch's slots to deal out beyond one block per field (a batch lasts as
+  // long as its slowest field's iterations, so fewer batches win); the
+  // fields dealt largest first to the batch with the least work so far.
+  // Within a batch a field's team is one block plus its share of the spare
+  // slots in proportion to its column groups (at most one block per
+  // kPhaseMinGroups groups), so every team sweeps about the same bytes per
+  // block.  The fields' records are laid out in the rescale phase's batch
+  // order; the shift phase's batches are lists of fields, each contiguous
+  // in that order when both phases take the same number of batches.
+  auto layout = [&](int cap, std::vector<int>& order, std::vector<int>& team,
+                    std::vector<std::vector<int>>& members) -> int {
+    const int per_batch = std::max(1, (cap * 3) / 5);
+    const int B = std::max(1, (n + per_batch - 1) / per_batch);
+    std::vector<int> idx((size_t)n);
+    for (int i = 0; i < n; ++i) idx[(size_t)i] = i;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int a, int b) { return groups[(size_t)a] > groups[(size_t)b]; });
+    members.assign((size_t)B, {});
+    std::vector<int64_t> load((size_t)B, 0);
+    for (int i : idx) {
+      int best = -1;
+      for (int b = 0; b < B; ++b)
+        if ((int)members[(size_t)b].size() < cap &&
+            (best < 0 || load[(size_t)b] < load[(size_t)best]))
+          best = b;
+      STEAM_REQUIRE(best >= 0, "steam_bounded_add_group_prepare: too many fields");
+      members[(size_t)best].push_back(i);
+      load[(size_t)best] += groups[(size_t)i];
     }
-  }
-  // the fields' records in batch order
+    team.assign((size_t)n, 1);
+    order.clear();
+    for (int b = 0; b < B; ++b) {
+      auto& m = members[(size_t)b];
+      std::sort(m.begin(), m.end());
+      const int64_t spare = cap - (int64_t)m.size();
+      for (int i : m) {
+        const int64_t g = groups[(size_t)i];
+        const int64_t share = 1 + (int64_t)((double)spare * (double)g /
+                                            (double)std::max<int64_t>(load[(size_t)b], 1));
+        const int64_t useful =
+            std::max<int64_t>((g + kPhaseMinGroups - 1) / kPhaseMinGroups, 1);
+        team[(size_t)i] = (int)std::min(std::min(share, useful), group_partial_blocks(g));
+        order.push_back(i);
+      }
+    }
+    return STEAM_OK;
+  };
+  std::vector<int> order, team, mu_order, mu_team;
+  std::vector<std::vector<int>> members, mu_members;
+  int rcl = layout(caps[0], order, team, members);
+  if (rcl) return rcl;
+  rcl = layout(caps[1], mu_order, mu_team, mu_members);
+  if (rcl) return rcl;
+  // the fields' records in the rescale phase's batch order
+  std::vector<int> pos((size_t)n);
+  for (int k = 0; k < n; ++k) pos[(size_t)order[(size_t)k]] = k;
   std::vector<BAGroupRec<T>> recs((size_t)n);
-  std::vector<int> fold_start((size_t)n), ph_start((size_t)n);
+  std::vector<int> fold_start((size_t)n), ph_start((size_t)n), mu_start((size_t)n);
   int fold_total = 0;
   for (int k = 0; k < n; ++k) {
     const int i = order[(size_t)k];
@@ -2030,6 +2049,7 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
     const int64_t g = groups[(size_t)i];
     r.fold_nb = (int)std::max<int64_t>((g + kGroupFoldGroups - 1) / kGroupFoldGroups, 1);
     r.ph_nb = team[(size_t)i];
+    r.mu_nb = mu_team[(size_t)i];
     r.partials = c.take<double>((size_t)group_partial_blocks(g) * 2 * kMuCand * nz);
     r.totals = c.take<double>((size_t)2 * kMuCand * nz);
     if (!r.partials || !r.totals)
@@ -2046,8 +2066,8 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
   }
   plan.fold_blocks = fold_total;
   int k0 = 0;
-  for (int b = 0; b < B; ++b) {
-    const int nb = (int)members[(size_t)b].size();
+  for (size_t b = 0; b < members.size(); ++b) {
+    const int nb = (int)members[b].size();
     int blocks = 0;
     for (int k = k0; k < k0 + nb; ++k) {
       ph_start[(size_t)k] = blocks;
@@ -2056,11 +2076,31 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
     if (nb > 0) plan.batches.push_back({k0, nb, blocks});
     k0 += nb;
   }
+  // the shift phase's batches must be contiguous runs of records: when its
+  // layout differs in batch count, its fields take the rescale order and are
+  // cut into runs that fit its capacity
+  k0 = 0;
+  while (k0 < n) {
+    int blocks = 0, k = k0;
+    while (k < n && blocks + recs[(size_t)k].mu_nb <= caps[1]) {
+      mu_start[(size_t)k] = blocks;
+      blocks += recs[(size_t)k].mu_nb;
+      ++k;
+    }
+    STEAM_REQUIRE(k > k0, "steam_bounded_add_group_prepare: a team exceeds the capacity");
+    plan.mu_batches.push_back({k0, k - k0, blocks});
+    k0 = k;
+  }
+  (void)mu_order;
+  (void)mu_members;
+  (void)pos;
   STEAM_CUDA(cudaMemcpy(plan.recs, recs.data(), sizeof(BAGroupRec<T>) * (size_t)n,
                         cudaMemcpyHostToDevice));
   STEAM_CUDA(cudaMemcpy(plan.fold_start, fold_start.data(), sizeof(int) * (size_t)n,
                         cudaMemcpyHostToDevice));
   STEAM_CUDA(cudaMemcpy(plan.ph_start, ph_start.data(), sizeof(int) * (size_t)n,
+                        cudaMemcpyHostToDevice));
+  STEAM_CUDA(cudaMemcpy(plan.mu_start, mu_start.data(), sizeof(int) * (size_t)n,
                         cudaMemcpyHostToDevice));
   STEAM_CUDA(cudaFuncSetAttribute(bag_fold_kernel<T, BA_SUMS>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2090,9 +2130,11 @@ static int group_enqueue(const BAGroupPlan& plan, cudaStream_t s) {
   STEAM_LAUNCH_CHECK("bounded_add group a0");
   auto phase = [&](int mode, int flag_base, int n_iter) -> int {
     auto kern = mode == BA_MU ? bag_phase_kernel<T, BA_MU> : bag_phase_kernel<T, BA_STATS>;
-    for (const auto& b : plan.batches) {
+    const auto& batches = mode == BA_MU ? plan.mu_batches : plan.batches;
+    const int* starts = mode == BA_MU ? plan.mu_start : plan.ph_start;
+    for (const auto& b : batches) {
       int p0 = b[0], nb = b[1];
-      const int* start = plan.ph_start + p0;
+      const int* start = starts + p0;
       void* args[] = {(void*)&recs, (void*)&start, &p0, &nb, &flag_base, &n_iter};
       STEAM_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)b[2]),
                                              dim3(kLvThreads), args, plan.sm_sums, s));
