@@ -74,6 +74,8 @@ def parse(argv=None):
                     help="Poisson arrival rates (requests/s) of the serving episode")
     ap.add_argument("--ensemble-members", type=int, default=256,
                     help="members of the batched-ensemble episode (0: skip)")
+    ap.add_argument("--no-k61", dest="k61", action="store_false",
+                    help="skip the 61^3-kernel convolution at 512x512x256")
     ap.add_argument("--streamed-steps", type=int, default=1,
                     help="out-of-core class steps of the workload with its fields in "
                          "page-locked host memory (0: skip)")
@@ -680,6 +682,33 @@ def main(argv=None):
         del members
         torch.cuda.empty_cache()
 
+    # the 61^3 kernel (sparsity 5: the 512x512x256 configuration's
+    # "64-voxel kernel support"): one float32 convolution at 512x512x256,
+    # which runs as the separable z/y/x passes (a 61-tap ring does not fit
+    # the fused kernels' registers)
+    k61 = None
+    if args.k61 and args.dtype == "f32":
+        from steam_b200 import simulate as _sim
+        from steam_b200 import utils as _u
+        shp = (512, 512, 256)
+        kern = _sim._turbulon_envelope(1, 0.1, 0.1, 0.1, dtype=np.float64)
+        plan = _u.plan_convolution(kern, shp, np.float32)
+        fk = torch.randn(shp, device="cuda")
+        ok = torch.empty_like(fk)
+        for _ in range(2):
+            _u.run_plan_async(plan, fk, ok)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            _u.run_plan_async(plan, fk, ok)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        k61 = {"kernel": list(kern.shape), "shape": list(shp), "plan": plan.kind,
+               "ms": round(ms, 3), "mvoxels_per_s": fk.numel() / (ms / 1e3) / 1e6}
+        del fk, ok
+        torch.cuda.empty_cache()
+
     # out-of-core: the same class step with h', qt', F in page-locked host
     # memory, column tiles (+ halo) and level slabs streamed through the
     # device, transfers overlapped with compute on three streams
@@ -732,6 +761,7 @@ def main(argv=None):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "error": error,
             "streamed": streamed, "serving": serving,
             "ensemble": ensemble,
+            "k61": k61,
             "gpu_launches": int(launches), "clocks": clk,
         }
         print(json.dumps(line), flush=True)
