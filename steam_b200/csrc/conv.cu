@@ -20,179 +20,309 @@
 
 namespace steam {
 
+// ---- the three passes: shared structure ------------------------------------
+// Each pass is a 1D correlation along one axis with every thread computing
+// kSR consecutive outputs of that axis for one lane column: the taps, reversed
+// and zero-padded to a multiple of kSU, sit in shared memory (one broadcast
+// read per tap), the inputs in a register window of kSR + kSU - 1 values that
+// slides by kSU taps per step, so a group of kSU taps costs kSU shared loads,
+// kSU tap reads and kSR * kSU fused multiply-adds.  A is the arithmetic type:
+// the field's own for a plain convolution, float64 for the flux epilogue and
+// the wide store (the fused kernels make the same choice).
+//
+// With reversed taps r[m] = t[Kp - 1 - m] (zero for Kp - 1 - m >= K) and a
+// staged line b[j] = f[j - (Kp - 1 - c)], output i of a filter with centre c
+// is sum_m r[m] * b[i + m] = sum_l t[l] * f[i + c - l].
+constexpr int kSR = 8;  // outputs per thread along the filter axis
+constexpr int kSU = 8;  // taps per window step
+
+__host__ __device__ inline int sep_padded(int k) { return (k + kSU - 1) / kSU * kSU; }
+
+template <typename A>
+__device__ __forceinline__ A fma_a(A a, A b, A c);
+template <>
+__device__ __forceinline__ float fma_a<float>(float a, float b, float c) {
+  return __fmaf_rn(a, b, c);
+}
+template <>
+__device__ __forceinline__ double fma_a<double>(double a, double b, double c) {
+  return __fma_rn(a, b, c);
+}
+
+// acc[r] = sum_m taps[m] * line[(r + m) * stride], m < kp (kp % kSU == 0).
+template <typename A>
+__device__ __forceinline__ void sep_window(const A* __restrict__ line, int stride,
+                                           const A* __restrict__ taps, int kp,
+                                           A (&acc)[kSR]) {
+  A w[kSR + kSU - 1];
+#pragma unroll
+  for (int i = 0; i < kSR - 1; ++i) w[i] = line[i * stride];
+  for (int m0 = 0; m0 < kp; m0 += kSU) {
+#pragma unroll
+    for (int u = 0; u < kSU; ++u) w[kSR - 1 + u] = line[(m0 + kSR - 1 + u) * stride];
+#pragma unroll
+    for (int u = 0; u < kSU; ++u) {
+      const A t = taps[m0 + u];
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) acc[r] = fma_a<A>(t, w[r + u], acc[r]);
+    }
+#pragma unroll
+    for (int i = 0; i < kSR - 1; ++i) w[i] = w[kSU + i];
+  }
+}
+
+// v mod n in [0, n); one compare on the common in-range index.
+__device__ __forceinline__ int64_t wrap_fast(int64_t v, int64_t n) {
+  if (v >= 0 && v < n) return v;
+  if (v < 0 && v + n >= 0) return v + n;
+  if (v >= n && v < 2 * n) return v - n;
+  return wrapi(v, n);
+}
+
+// taps_s[f * kp + m] = taps[f * k + (kp - 1 - m)], zero past the filter.
+template <typename A>
+__device__ __forceinline__ void stage_taps(A* taps_s, const double* taps, int nf, int k,
+                                           int kp) {
+  for (int i = threadIdx.x; i < nf * kp; i += blockDim.x) {
+    const int f = i / kp, l = kp - 1 - (i - f * kp);
+    taps_s[i] = l < k ? (A)taps[f * k + l] : (A)0;
+  }
+}
+
+
 // ---- z-pass -------------------------------------------------------------
-// Block = CB consecutive columns (contiguous in memory), staged with zero
-// padding: buf[j] = in[j - (kz-1-cz)].
-template <typename T, bool PRE>
-__global__ void __launch_bounds__(256) zpass_kernel(
-    const T* __restrict__ in, int64_t ncol, int nz, int cb,
-    const T* __restrict__ pre_div, const T* __restrict__ pre_mul,
-    SepParams<T> p, T* __restrict__ out, int64_t plane) {
-  extern __shared__ unsigned char smem_raw[];
-  T* buf = reinterpret_cast<T*>(smem_raw);
-  __shared__ double taps_s[kMaxZ * 256];
-  const int kz = p.kz;
-  const int len = nz + kz - 1;
-  const int padlo = kz - 1 - p.cz;
-  for (int i = threadIdx.x; i < p.nzf * kz; i += blockDim.x)
-    taps_s[i] = p.taps[i];
-  for (int64_t col0 = (int64_t)blockIdx.x * cb; col0 < ncol;
-       col0 += (int64_t)gridDim.x * cb) {
-    const int ncb = (int)((ncol - col0) < cb ? (ncol - col0) : cb);
+// Tile = 32 consecutive columns (one per lane) x a chunk of z of 8 warps x
+// SPW segments x kSR outputs; the columns are staged with their halo at an
+// odd pitch (conflict-free column reads across the lanes) and each filter's
+// outputs go back through a second buffer so that the stores run along z.
+constexpr int kZCols = 32;
+constexpr int kPassThreads = 256;
+
+template <typename A>
+constexpr int zpass_spw() { return sizeof(A) == 4 ? 4 : 2; }
+template <typename A>
+constexpr int zpass_chunk() { return (kPassThreads / 32) * kSR * zpass_spw<A>(); }
+
+template <typename A>
+static size_t zpass_smem(int nf, int kp) {
+  const int zc = zpass_chunk<A>();
+  const int ld = (zc + kp - 1) | 1;
+  return sizeof(A) * ((size_t)nf * kp + (size_t)kZCols * ld + (size_t)kZCols * (zc + 1));
+}
+
+template <typename T, typename A, bool PRE>
+__global__ void __launch_bounds__(kPassThreads) zpass_kernel(
+    const T* __restrict__ in, int64_t ncol, int nz, int kp, const T* __restrict__ pre_div,
+    const T* __restrict__ pre_mul, SepParams<T> p, T* __restrict__ out, int64_t plane) {
+  constexpr int SPW = zpass_spw<A>();
+  constexpr int ZC = zpass_chunk<A>();
+  constexpr int NW = kPassThreads / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A* taps_s = reinterpret_cast<A*>(smem_raw);
+  const int ld = (ZC + kp - 1) | 1;
+  constexpr int ldo = ZC + 1;
+  A* buf = taps_s + p.nzf * kp;
+  A* obuf = buf + kZCols * ld;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int off = kp - 1 - p.cz;
+  stage_taps<A>(taps_s, p.ztap(0), p.nzf, p.kz, kp);
+  const int64_t zchunks = (nz + ZC - 1) / ZC;
+  const int64_t ntiles = ((ncol + kZCols - 1) / kZCols) * zchunks;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t col0 = (t / zchunks) * kZCols;
+    const int z0 = (int)(t % zchunks) * ZC;
+    const int zc = (nz - z0) < ZC ? (nz - z0) : ZC;
+    const int nseg = (zc + kSR - 1) / kSR;
+    const int len = nseg * kSR + kp - 1;
+    const int ncb = (int)((ncol - col0) < kZCols ? (ncol - col0) : kZCols);
     __syncthreads();
-    for (int i = threadIdx.x; i < ncb * len; i += blockDim.x) {
-      int c = i / len, j = i - c * len;
-      int s = j - padlo;
-      T v = (T)0;
-      if (s >= 0 && s < nz) {
-        v = in[(col0 + c) * nz + s];
-        if (PRE) v = mul_rn(v, pre_scale(pre_div[s], pre_mul[s]));
+    for (int c = warp; c < kZCols; c += NW) {
+      for (int j = lane; j < len; j += 32) {
+        const int s = z0 + j - off;
+        A v = (A)0;
+        if (c < ncb && s >= 0 && s < nz) {
+          T x = in[(col0 + c) * nz + s];
+          if (PRE) x = mul_rn(x, pre_scale(pre_div[s], pre_mul[s]));
+          v = (A)x;
+        }
+        buf[c * ld + j] = v;
       }
-      buf[c * len + j] = v;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < ncb * nz; i += blockDim.x) {
-      int c = i / nz, z = i - c * nz;
-      const T* b = buf + c * len + z + kz - 1;
-      double acc[kMaxZ];
+    for (int f = 0; f < p.nzf; ++f) {
+      A acc[SPW][kSR];
 #pragma unroll
-      for (int f = 0; f < kMaxZ; ++f) acc[f] = 0.0;
-      for (int l = 0; l < kz; ++l) {
-        const double x = (double)b[-l];
+      for (int q = 0; q < SPW; ++q) {
 #pragma unroll
-        for (int f = 0; f < kMaxZ; ++f)
-          if (f < p.nzf) acc[f] += taps_s[f * kz + l] * x;
+        for (int r = 0; r < kSR; ++r) acc[q][r] = (A)0;
+        const int seg = warp + q * NW;
+        if (seg < nseg)
+          sep_window<A>(buf + lane * ld + seg * kSR, 1, taps_s + f * kp, kp, acc[q]);
       }
-      const int64_t o = (col0 + c) * nz + z;
+      __syncthreads();  // the previous filter's outputs have left obuf
 #pragma unroll
-      for (int f = 0; f < kMaxZ; ++f)
-        if (f < p.nzf) out[f * plane + o] = (T)acc[f];
+      for (int q = 0; q < SPW; ++q) {
+        const int seg = warp + q * NW;
+        if (seg < nseg) {
+#pragma unroll
+          for (int r = 0; r < kSR; ++r) obuf[lane * ldo + seg * kSR + r] = acc[q][r];
+        }
+      }
+      __syncthreads();
+      T* o = out + f * plane + col0 * nz + z0;
+      for (int c = warp; c < ncb; c += NW)
+        for (int j = lane; j < zc; j += 32) o[(int64_t)c * nz + j] = (T)obuf[c * ldo + j];
     }
   }
 }
 
 // ---- y-pass -------------------------------------------------------------
-constexpr int kTY = 16;
-constexpr int kTZ = 64;
+// Tile = one x-plane's kYT rows x 32 z (one per lane).  Each z-filtered field
+// in turn is staged with kp - 1 halo rows (wrapped: y is circular), each warp
+// owns kSR consecutive rows, and every (z filter, y filter) pair on that
+// field is one window run.
+constexpr int kYT = (kPassThreads / 32) * kSR;  // 64 rows
 
-template <typename T>
-__global__ void __launch_bounds__(256) ypass_kernel(
-    const T* __restrict__ u, int64_t nx, int64_t ny, int nz, SepParams<T> p,
+template <typename A>
+static size_t ypass_smem(int nyf, int kp) {
+  return sizeof(A) * ((size_t)nyf * kp + (size_t)(kYT + kp - 1) * 32);
+}
+
+template <typename T, typename A>
+__global__ void __launch_bounds__(kPassThreads, 3) ypass_kernel(
+    const T* __restrict__ u, int64_t nx, int64_t ny, int nz, int kp, SepParams<T> p,
     T* __restrict__ v, int64_t plane) {
-  extern __shared__ unsigned char smem_raw[];
-  T* buf = reinterpret_cast<T*>(smem_raw);  // [nzf][TY+ky-1][TZ]
-  const int ky = p.ky;
-  const int rows = kTY + ky - 1;
-  const int padlo = ky - 1 - p.cy;
-  const int64_t ytiles = (ny + kTY - 1) / kTY;
-  const int64_t ztiles = (nz + kTZ - 1) / kTZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A* taps_s = reinterpret_cast<A*>(smem_raw);
+  A* buf = taps_s + p.nyf * kp;  // [kYT + kp - 1][32]
+  const int rows = kYT + kp - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = kPassThreads / 32;
+  const int off = kp - 1 - p.cy;
+  stage_taps<A>(taps_s, p.ytap(0), p.nyf, p.ky, kp);
+  const int64_t ytiles = (ny + kYT - 1) / kYT;
+  const int64_t ztiles = (nz + 31) / 32;
   const int64_t ntiles = nx * ytiles * ztiles;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t zt = t % ztiles;
     const int64_t yt = (t / ztiles) % ytiles;
     const int64_t x = t / (ztiles * ytiles);
-    const int64_t y0 = yt * kTY;
-    const int z0 = (int)(zt * kTZ);
-    const int tz = (nz - z0) < kTZ ? (nz - z0) : kTZ;
-    __syncthreads();
-    for (int i = threadIdx.x; i < p.nzf * rows * kTZ; i += blockDim.x) {
-      int f = i / (rows * kTZ);
-      int rem = i - f * rows * kTZ;
-      int r = rem / kTZ, zz = rem - r * kTZ;
-      T val = (T)0;
-      if (zz < tz) {
-        int64_t ys = wrapi(y0 - padlo + r, ny);
-        val = u[(int64_t)f * plane + (x * ny + ys) * nz + z0 + zz];
+    const int64_t y0 = yt * kYT;
+    const int z = (int)(zt * 32) + lane;
+    const int64_t yw = y0 + warp * kSR;
+    for (int f = 0; f < p.nzf; ++f) {
+      __syncthreads();
+      const T* src = u + (int64_t)f * plane + x * ny * nz + z;
+#pragma unroll 4
+      for (int r = warp; r < rows; r += NW) {
+        const int64_t ys = wrap_fast(y0 - off + r, ny);
+        buf[r * 32 + lane] = z < nz ? (A)src[ys * nz] : (A)0;
       }
-      buf[i] = val;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kTY * kTZ; i += blockDim.x) {
-      int r = i / kTZ, zz = i - r * kTZ;
-      int64_t y = y0 + r;
-      if (y >= ny || zz >= tz) continue;
+      __syncthreads();
       for (int q = 0; q < p.npairs; ++q) {
-        const T* col = buf + (p.pair_z[q] * rows + r + ky - 1) * kTZ + zz;
-        const double* tp = p.ytap(p.pair_y[q]);
-        double acc = 0.0;
-        for (int j = 0; j < ky; ++j) acc += tp[j] * (double)col[-j * kTZ];
-        v[(int64_t)q * plane + (x * ny + y) * nz + z0 + zz] = (T)acc;
+        if (p.pair_z[q] != f) continue;
+        A acc[kSR];
+#pragma unroll
+        for (int r = 0; r < kSR; ++r) acc[r] = (A)0;
+        sep_window<A>(buf + warp * kSR * 32 + lane, 32, taps_s + p.pair_y[q] * kp, kp, acc);
+        if (z < nz) {
+          T* o = v + (int64_t)q * plane + (x * ny + yw) * nz + z;
+#pragma unroll
+          for (int r = 0; r < kSR; ++r)
+            if (yw + r < ny) o[(int64_t)r * nz] = (T)acc[r];
+        }
       }
     }
   }
 }
 
 // ---- x-pass -------------------------------------------------------------
-constexpr int kTX = 16;
-constexpr int kTE = 128;
+// Tile = kXT x-planes x 32 elements of the (y, z) plane (one per lane); each
+// staged row is the x filters' mixes of the y-filtered fields at one x
+// (wrapped: x is circular), each warp owns kSR consecutive x outputs, and the
+// epilogue follows in registers.  Tiles run x-fastest, so neighbouring tiles'
+// halo rows are read from L2.
+constexpr int kXT = (kPassThreads / 32) * kSR;  // 64 planes
 
-template <typename T>
-__global__ void __launch_bounds__(256) xpass_kernel(
-    const T* __restrict__ v, int64_t nx, int64_t ny, int nz, SepParams<T> p,
-    T* __restrict__ out, int64_t plane, XEpi epi,
-    double* __restrict__ partials) {
-  extern __shared__ unsigned char smem_raw[];
-  double* buf = reinterpret_cast<double*>(smem_raw);  // [nxf][TX+kx-1][TE]
+template <typename A>
+static size_t xpass_smem(int nxf, int kp) {
+  return sizeof(A) * ((size_t)nxf * kp + (size_t)nxf * (kXT + kp - 1) * 32);
+}
+
+static int64_t xpass_tiles(int64_t nx, int64_t ny, int64_t nz) {
+  return ((nx + kXT - 1) / kXT) * ((ny * nz + 31) / 32);
+}
+
+template <typename T, typename A>
+__global__ void __launch_bounds__(kPassThreads) xpass_kernel(
+    const T* __restrict__ v, int64_t nx, int64_t ny, int nz, int kp, SepParams<T> p,
+    T* __restrict__ out, int64_t plane, XEpi epi, double* __restrict__ partials) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double scratch[32];
-  const int kx = p.kx;
-  const int rows = kTX + kx - 1;
-  const int padlo = kx - 1 - p.cx;
+  A* taps_s = reinterpret_cast<A*>(smem_raw);
+  A* buf = taps_s + p.nxf * kp;  // [nxf][kXT + kp - 1][32]
+  const int rows = kXT + kp - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = kPassThreads / 32;
+  const int off = kp - 1 - p.cx;
+  stage_taps<A>(taps_s, p.xtap(0), p.nxf, p.kx, kp);
   const int64_t pe = ny * nz;  // elements of one x-plane
-  const int64_t etiles = (pe + kTE - 1) / kTE;
-  const int64_t xtiles = (nx + kTX - 1) / kTX;
-  const int64_t ntiles = xtiles * etiles;
+  const int64_t xtiles = (nx + kXT - 1) / kXT;
+  const int64_t ntiles = xtiles * ((pe + 31) / 32);
   double s_f = 0.0, s_clip = 0.0;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t et = t % etiles;
-    const int64_t xt = t / etiles;
-    const int64_t x0 = xt * kTX;
-    const int64_t e0 = et * kTE;
-    const int te = (pe - e0) < kTE ? (int)(pe - e0) : kTE;
+    const int64_t x0 = (t % xtiles) * kXT;
+    const int64_t e = (t / xtiles) * 32 + lane;
+    const bool live = e < pe;
     __syncthreads();
-    for (int i = threadIdx.x; i < rows * kTE; i += blockDim.x) {
-      int r = i / kTE, ee = i - r * kTE;
-      double w[kMaxX];
+#pragma unroll 2
+    for (int r = warp; r < rows; r += NW) {
+      const int64_t xs = wrap_fast(x0 - off + r, nx);
+      A w[kMaxX];
 #pragma unroll
-      for (int a = 0; a < kMaxX; ++a) w[a] = 0.0;
-      if (ee < te) {
-        int64_t xs = wrapi(x0 - padlo + r, nx);
-        const int64_t off = xs * pe + e0 + ee;
+      for (int a = 0; a < kMaxX; ++a) w[a] = (A)0;
+      if (live) {
+        const T* src = v + xs * pe + e;
         for (int q = 0; q < p.npairs; ++q) {
-          const double vq = (double)v[(int64_t)q * plane + off];
+          const A vq = (A)src[(int64_t)q * plane];
 #pragma unroll
           for (int a = 0; a < kMaxX; ++a)
-            if (a < p.nxf) w[a] += p.mix[a * p.npairs + q] * vq;
+            if (a < p.nxf) w[a] = fma_a<A>((A)p.mix[a * p.npairs + q], vq, w[a]);
         }
       }
 #pragma unroll
       for (int a = 0; a < kMaxX; ++a)
-        if (a < p.nxf) buf[(a * rows + r) * kTE + ee] = w[a];
+        if (a < p.nxf) buf[(a * rows + r) * 32 + lane] = w[a];
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kTX * kTE; i += blockDim.x) {
-      int r = i / kTE, ee = i - r * kTE;
-      int64_t x = x0 + r;
-      if (x >= nx || ee >= te) continue;
-      double acc = 0.0;
-      for (int a = 0; a < p.nxf; ++a) {
-        const double* col = buf + (a * rows + r + kx - 1) * kTE + ee;
-        const double* tp = p.xtap(a);
-        for (int j = 0; j < kx; ++j) acc += tp[j] * col[-j * kTE];
-      }
-      const int64_t o = x * pe + e0 + ee;
+    A acc[kSR];
+#pragma unroll
+    for (int r = 0; r < kSR; ++r) acc[r] = (A)0;
+    for (int a = 0; a < p.nxf; ++a)
+      sep_window<A>(buf + (a * rows + warp * kSR) * 32 + lane, 32, taps_s + a * kp, kp, acc);
+    if (!live) continue;
+    const int64_t xw = x0 + warp * kSR;
+    bool in_win = false;
+    if (epi.mode == STEAM_EPI_FLUX) {
+      const int64_t y = e / nz;
+      in_win = y >= epi.wy0 && y < epi.wy1;
+    }
+#pragma unroll
+    for (int r = 0; r < kSR; ++r) {
+      const int64_t x = xw + r;
+      if (x >= nx) break;
+      const int64_t o = x * pe + e;
       if (epi.mode == STEAM_EPI_FLUX) {
         // F + conv rounded once to the storage dtype
-        T f = (T)((double)out[o] + acc);
+        T f = (T)((double)out[o] + (double)acc[r]);
         if (f < (T)0) {
           s_clip += 1.0;
           f = (T)0;
         }
         out[o] = f;
-        int64_t y = (e0 + ee) / nz;
-        if (x >= epi.wx0 && x < epi.wx1 && y >= epi.wy0 && y < epi.wy1)
-          s_f += (double)f;
+        if (in_win && x >= epi.wx0 && x < epi.wx1) s_f += (double)f;
       } else {
-        out[o] = (T)acc;
+        out[o] = (T)acc[r];
       }
     }
   }
@@ -691,14 +821,6 @@ static int fill_params(const steam_sepconv_t* s, const double* zt,
   return STEAM_OK;
 }
 
-static int zpass_cols(int nz, int kz, size_t elem) {
-  int len = nz + kz - 1;
-  int cb = (int)((40 * 1024) / ((size_t)len * elem));
-  if (cb < 1) cb = 1;
-  if (cb > 64) cb = 64;
-  return cb;
-}
-
 static int64_t epi_cells(const steam_window_t* w, int64_t nx, int64_t ny) {
   if (!w) return nx * ny;
   return (w->x1 - w->x0) * (w->y1 - w->y0);
@@ -839,6 +961,71 @@ static int run_fused(int64_t nx, int64_t ny, int64_t nz, const SepParams<T>& p,
   return STEAM_OK;
 }
 
+// Blocks of `kern` resident per SM with `sm` bytes of dynamic shared memory
+// (at least 1, at most `cap`).
+template <typename K>
+static int pass_occupancy(K kern, size_t sm, int cap) {
+  int occ = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kPassThreads, sm) !=
+          cudaSuccess)
+    occ = 1;
+  return occ < 1 ? 1 : (occ > cap ? cap : occ);
+}
+
+// An upper bound of the x-pass grid (at most 8 blocks of 256 threads per SM):
+// the flux partial pairs it can write.
+static int xpass_grid_max(int64_t nx, int64_t ny, int64_t nz) {
+  return stride_grid(xpass_tiles(nx, ny, nz), 1, 8);
+}
+
+// The z, y and x passes in arithmetic type A: u = z filters of the input
+// (scaled by pre when given), v = the y filters of u per pair, out = the
+// mixed x filters of v with the epilogue.
+template <typename T, typename A>
+static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t nz,
+                         const T* in, const T* pre, T* u, T* v, T* out, const XEpi& epi,
+                         double* partials, int* xgrid_out, cudaStream_t s) {
+  const int64_t plane = nx * ny * nz;
+  const int kpz = sep_padded(p.kz), kpy = sep_padded(p.ky), kpx = sep_padded(p.kx);
+  const size_t smz = zpass_smem<A>(p.nzf, kpz), smy = ypass_smem<A>(p.nyf, kpy),
+               smx = xpass_smem<A>(p.nxf, kpx);
+  STEAM_REQUIRE(smz <= 200 * 1024, "steam_conv_separable: z filter too long");
+  STEAM_REQUIRE(smy <= 200 * 1024, "steam_conv_separable: y filter too long");
+  STEAM_REQUIRE(smx <= 200 * 1024, "steam_conv_separable: x filter too long");
+  {
+    const int64_t ncol = nx * ny;
+    const int64_t tiles = ((ncol + kZCols - 1) / kZCols) *
+                          ((nz + zpass_chunk<A>() - 1) / zpass_chunk<A>());
+    if (pre) {
+      auto k = zpass_kernel<T, A, true>;
+      k<<<stride_grid(tiles, 1, pass_occupancy(k, smz, 8)), kPassThreads, smz, s>>>(
+          in, ncol, (int)nz, kpz, pre, pre + nz, p, u, plane);
+    } else {
+      auto k = zpass_kernel<T, A, false>;
+      k<<<stride_grid(tiles, 1, pass_occupancy(k, smz, 8)), kPassThreads, smz, s>>>(
+          in, ncol, (int)nz, kpz, nullptr, nullptr, p, u, plane);
+    }
+    STEAM_LAUNCH_CHECK("conv z-pass");
+  }
+  {
+    const int64_t tiles = nx * ((ny + kYT - 1) / kYT) * ((nz + 31) / 32);
+    auto k = ypass_kernel<T, A>;
+    k<<<stride_grid(tiles, 1, pass_occupancy(k, smy, 8)), kPassThreads, smy, s>>>(
+        u, nx, ny, (int)nz, kpy, p, v, plane);
+    STEAM_LAUNCH_CHECK("conv y-pass");
+  }
+  {
+    auto k = xpass_kernel<T, A>;
+    const int grid = stride_grid(xpass_tiles(nx, ny, nz), 1, pass_occupancy(k, smx, 8));
+    k<<<grid, kPassThreads, smx, s>>>(v, nx, ny, (int)nz, kpx, p, out, plane, epi, partials);
+    STEAM_LAUNCH_CHECK("conv x-pass");
+    *xgrid_out = grid;
+  }
+  return STEAM_OK;
+}
+
 template <typename T>
 static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                          const steam_sepconv_t* spec, const double* zt,
@@ -863,8 +1050,7 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   T* pre = nullptr;
   const bool use_pre = pre_div != nullptr || pre_mul != nullptr || pre_dev != nullptr;
   if (use_pre) pre = c.take<T>((size_t)2 * nz);
-  int xgrid = stride_grid(((nx + kTX - 1) / kTX) * ((ny * nz + kTE - 1) / kTE), 1, 4);
-  double* partials = c.take<double>((size_t)xgrid * 2);
+  double* partials = c.take<double>((size_t)xpass_grid_max(nx, ny, nz) * 2);
   double* totals = c.take<double>(2);
   if (!u || !v || (use_pre && !pre) || !partials || !totals)
     return fail(STEAM_ERR_WORKSPACE,
@@ -884,57 +1070,20 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                                cudaMemcpyHostToDevice, s));
     STEAM_CUDA(cudaStreamSynchronize(s));
   }
-  // z-pass
-  {
-    const int64_t ncol = nx * ny;
-    int cb = zpass_cols((int)nz, p.kz, sizeof(T));
-    size_t sm = (size_t)cb * (nz + p.kz - 1) * sizeof(T);
-    int grid = stride_grid((ncol + cb - 1) / cb, 1, 4);
-    if (use_pre) {
-      STEAM_CUDA(cudaFuncSetAttribute(zpass_kernel<T, true>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sm));
-      zpass_kernel<T, true><<<grid, 256, sm, s>>>(in, ncol, (int)nz, cb, pre,
-                                                  pre + nz, p, u, plane);
-    } else {
-      STEAM_CUDA(cudaFuncSetAttribute(zpass_kernel<T, false>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sm));
-      zpass_kernel<T, false><<<grid, 256, sm, s>>>(in, ncol, (int)nz, cb,
-                                                   nullptr, nullptr, p, u,
-                                                   plane);
-    }
-    STEAM_LAUNCH_CHECK("conv z-pass");
-  }
-  // y-pass
-  {
-    size_t sm = (size_t)p.nzf * (kTY + p.ky - 1) * kTZ * sizeof(T);
-    STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: y filter too long");
-    STEAM_CUDA(cudaFuncSetAttribute(ypass_kernel<T>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sm));
-    int64_t tiles = nx * ((ny + kTY - 1) / kTY) * ((nz + kTZ - 1) / kTZ);
-    int grid = stride_grid(tiles, 1, 4);
-    ypass_kernel<T><<<grid, 256, sm, s>>>(u, nx, ny, (int)nz, p, v, plane);
-    STEAM_LAUNCH_CHECK("conv y-pass");
-  }
-  // x-pass with epilogue
-  {
-    size_t sm = (size_t)p.nxf * (kTX + p.kx - 1) * kTE * sizeof(double);
-    STEAM_REQUIRE(sm <= 200 * 1024, "steam_conv_separable: x filter too long");
-    STEAM_CUDA(cudaFuncSetAttribute(xpass_kernel<T>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sm));
-    XEpi epi;
-    epi.mode = epilogue;
-    epi.wx0 = win ? win->x0 : 0;
-    epi.wx1 = win ? win->x1 : nx;
-    epi.wy0 = win ? win->y0 : 0;
-    epi.wy1 = win ? win->y1 : ny;
-    xpass_kernel<T><<<xgrid, 256, sm, s>>>(v, nx, ny, (int)nz, p, out, plane,
-                                           epi, partials);
-    STEAM_LAUNCH_CHECK("conv x-pass");
-  }
+  XEpi epi;
+  epi.mode = epilogue;
+  epi.wx0 = win ? win->x0 : 0;
+  epi.wx1 = win ? win->x1 : nx;
+  epi.wy0 = win ? win->y0 : 0;
+  epi.wy1 = win ? win->y1 : ny;
+  int xgrid = 0;
+  // float64 arithmetic for float64 fields, the flux epilogue and the wide store
+  rc = (sizeof(T) == 8 || epilogue != STEAM_EPI_STORE)
+           ? launch_passes<T, double>(p, nx, ny, nz, in, use_pre ? pre : nullptr, u, v, out,
+                                      epi, partials, &xgrid, s)
+           : launch_passes<T, T>(p, nx, ny, nz, in, use_pre ? pre : nullptr, u, v, out, epi,
+                                 partials, &xgrid, s);
+  if (rc) return rc;
   if (epilogue == STEAM_EPI_FLUX) {
     rc = reduce_partials(partials, xgrid, 2, totals, s);
     if (rc) return rc;
@@ -959,7 +1108,7 @@ extern "C" size_t steam_conv_workspace_bytes(int dtype, int64_t nx, int64_t ny,
   if (!spec) return 0;
   size_t elem = dtype == STEAM_F64 ? 8 : 4;
   size_t plane = (size_t)(nx * ny * nz);
-  int xgrid = stride_grid(((nx + kTX - 1) / kTX) * ((ny * nz + kTE - 1) / kTE), 1, 4);
+  const int xgrid = xpass_grid_max(nx, ny, nz);
   const size_t multi = carve_bytes((size_t)spec->n_z * plane, elem) +
                       carve_bytes((size_t)spec->n_pairs * plane, elem) +
                       carve_bytes((size_t)2 * nz, elem) +
