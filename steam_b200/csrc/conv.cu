@@ -2,10 +2,11 @@
 // (the turbulon kernels are sums of a few separable terms).  Kernels without
 // such a form go to fftconv.cu.
 //
-// Three passes, each a coalesced stencil over the z-fastest layout:
-//   z-pass: u_c = f (*)_z Z_c       (columns staged in shared memory)
-//   y-pass: v_p = u_c (*)_y Y_b     (TY x TZ tiles of one x-plane)
-//   x-pass: out = sum_a (sum_p mix_ap v_p) (*)_x X_a, with the epilogue.
+// Kernels the fused forms below do not take run as three passes, each a
+// coalesced stencil over the z-fastest layout:
+//   z-pass: u_c = f (*)_z Z_c                        (32 columns per tile)
+//   y-pass: w_a = sum_p mix_ap (u_c(p) (*)_y Y_b(p))  (64 y x 32 z tiles)
+//   x-pass: out = sum_a w_a (*)_x X_a, with the epilogue (64 x x 32 tiles).
 #include "common.cuh"
 #include "conv.cuh"
 #include <type_traits>
@@ -176,77 +177,139 @@ __global__ void __launch_bounds__(kPassThreads) zpass_kernel(
   }
 }
 
+// ---- staging of the y and x passes -----------------------------------------
+// A block's work is a sequence of stages (tile, input field); the rows of
+// stage k + 1 are copied into the second of two buffers while stage k is
+// computed.  Same-type fields go by cp.async (zero-filled past the array);
+// a float32 field filtered in float64 is converted through registers.
+template <typename T, typename A>
+__device__ __forceinline__ void stage_elem(A* dst, const T* src, bool valid) {
+  if constexpr (std::is_same<T, A>::value) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(A) == 4)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src),
+                   "r"(valid ? 4 : 0)
+                   : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src),
+                   "r"(valid ? 8 : 0)
+                   : "memory");
+  } else {
+    *dst = valid ? (A)*src : (A)0;
+  }
+}
+
 // ---- y-pass -------------------------------------------------------------
-// Tile = one x-plane's kYT rows x 32 z (one per lane).  Each z-filtered field
-// in turn is staged with kp - 1 halo rows (wrapped: y is circular), each warp
-// owns kSR consecutive rows, and every (z filter, y filter) pair on that
-// field is one window run.
+// Tile = one x-plane's kYT rows x 32 z (one per lane), each warp owning kSR
+// consecutive rows.  The tile's z-filtered fields are staged in turn with
+// kp - 1 halo rows (wrapped: y is circular); every (z filter, y filter) pair
+// on a field is one window run, folded at once into the x filters' mixes
+// w_a = sum_q mix[a][q] v_q, so the pass writes nxf fields, not one per pair.
 constexpr int kYT = (kPassThreads / 32) * kSR;  // 64 rows
 
 template <typename A>
 static size_t ypass_smem(int nyf, int kp) {
-  return sizeof(A) * ((size_t)nyf * kp + (size_t)(kYT + kp - 1) * 32);
+  return sizeof(A) * ((size_t)nyf * kp + (size_t)2 * (kYT + kp - 1) * 32);
 }
 
-template <typename T, typename A>
+template <typename T, typename A, int NX>
 __global__ void __launch_bounds__(kPassThreads, 3) ypass_kernel(
     const T* __restrict__ u, int64_t nx, int64_t ny, int nz, int kp, SepParams<T> p,
-    T* __restrict__ v, int64_t plane) {
+    T* __restrict__ w, int64_t plane) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A* taps_s = reinterpret_cast<A*>(smem_raw);
-  A* buf = taps_s + p.nyf * kp;  // [kYT + kp - 1][32]
   const int rows = kYT + kp - 1;
+  A* bufs = taps_s + p.nyf * kp;  // 2 x [kYT + kp - 1][32]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = kPassThreads / 32;
   const int off = kp - 1 - p.cy;
+  const int nf = p.nzf;
   stage_taps<A>(taps_s, p.ytap(0), p.nyf, p.ky, kp);
   const int64_t ytiles = (ny + kYT - 1) / kYT;
   const int64_t ztiles = (nz + 31) / 32;
   const int64_t ntiles = nx * ytiles * ztiles;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t zt = t % ztiles;
-    const int64_t yt = (t / ztiles) % ytiles;
-    const int64_t x = t / (ztiles * ytiles);
-    const int64_t y0 = yt * kYT;
-    const int z = (int)(zt * 32) + lane;
-    const int64_t yw = y0 + warp * kSR;
-    for (int f = 0; f < p.nzf; ++f) {
-      __syncthreads();
-      const T* src = u + (int64_t)f * plane + x * ny * nz + z;
-#pragma unroll 4
-      for (int r = warp; r < rows; r += NW) {
-        const int64_t ys = wrap_fast(y0 - off + r, ny);
-        buf[r * 32 + lane] = z < nz ? (A)src[ys * nz] : (A)0;
-      }
-      __syncthreads();
-      for (int q = 0; q < p.npairs; ++q) {
-        if (p.pair_z[q] != f) continue;
-        A acc[kSR];
+  // stage k: tile blockIdx.x + (k / nf) * gridDim.x, field k % nf
+  auto issue = [&](int k) {
+    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+    if (t < ntiles) {
+      const int f = k % nf;
+      const int64_t zt = t % ztiles;
+      const int64_t yt = (t / ztiles) % ytiles;
+      const int64_t x = t / (ztiles * ytiles);
+      const int z = (int)(zt * 32) + lane;
+      const T* src = u + (int64_t)f * plane + x * ny * nz + (z < nz ? z : 0);
+      A* dst = bufs + (k & 1) * rows * 32 + lane;
+      for (int r = warp; r < rows; r += NW)
+        stage_elem<T, A>(dst + r * 32, src + wrap_fast(yt * kYT - off + r, ny) * nz, z < nz);
+    }
+    cp_async_commit();
+  };
+  A acc[NX][kSR];
+  issue(0);
+  for (int k = 0;; ++k) {
+    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+    if (t >= ntiles) break;
+    const int f = k % nf;
+    issue(k + 1);
+    cp_async_wait<1>();
+    __syncthreads();
+    if (f == 0) {
 #pragma unroll
-        for (int r = 0; r < kSR; ++r) acc[r] = (A)0;
-        sep_window<A>(buf + warp * kSR * 32 + lane, 32, taps_s + p.pair_y[q] * kp, kp, acc);
-        if (z < nz) {
-          T* o = v + (int64_t)q * plane + (x * ny + yw) * nz + z;
+      for (int a = 0; a < NX; ++a)
 #pragma unroll
-          for (int r = 0; r < kSR; ++r)
-            if (yw + r < ny) o[(int64_t)r * nz] = (T)acc[r];
+        for (int r = 0; r < kSR; ++r) acc[a][r] = (A)0;
+    }
+    const A* col = bufs + (k & 1) * rows * 32 + warp * kSR * 32 + lane;
+    for (int q = 0; q < p.npairs; ++q) {
+      if (p.pair_z[q] != f) continue;
+      A c[kSR];
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) c[r] = (A)0;
+      sep_window<A>(col, 32, taps_s + p.pair_y[q] * kp, kp, c);
+#pragma unroll
+      for (int a = 0; a < NX; ++a) {
+        if (a < p.nxf) {
+          const A m = (A)p.mix[a * p.npairs + q];
+#pragma unroll
+          for (int r = 0; r < kSR; ++r) acc[a][r] = fma_a<A>(m, c[r], acc[a][r]);
         }
       }
     }
+    if (f == nf - 1) {
+      const int64_t zt = t % ztiles;
+      const int64_t yt = (t / ztiles) % ytiles;
+      const int64_t x = t / (ztiles * ytiles);
+      const int z = (int)(zt * 32) + lane;
+      const int64_t yw = yt * kYT + warp * kSR;
+      if (z < nz) {
+#pragma unroll
+        for (int a = 0; a < NX; ++a) {
+          if (a < p.nxf) {
+            T* o = w + (int64_t)a * plane + (x * ny + yw) * nz + z;
+#pragma unroll
+            for (int r = 0; r < kSR; ++r)
+              if (yw + r < ny) o[(int64_t)r * nz] = (T)acc[a][r];
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage k's buffer is free for stage k + 2
   }
+  cp_async_wait<0>();
 }
 
 // ---- x-pass -------------------------------------------------------------
-// Tile = kXT x-planes x 32 elements of the (y, z) plane (one per lane); each
-// staged row is the x filters' mixes of the y-filtered fields at one x
-// (wrapped: x is circular), each warp owns kSR consecutive x outputs, and the
-// epilogue follows in registers.  Tiles run x-fastest, so neighbouring tiles'
-// halo rows are read from L2.
+// Tile = kXT x-planes x 32 elements of the (y, z) plane (one per lane), each
+// warp owning kSR consecutive x outputs; each x filter's mixed field is
+// staged in turn with kp - 1 halo planes (wrapped: x is circular) and its
+// window run adds into the same accumulators; the epilogue follows in
+// registers.  Tiles run x-fastest, so neighbouring tiles' halo rows come
+// from L2.
 constexpr int kXT = (kPassThreads / 32) * kSR;  // 64 planes
 
 template <typename A>
 static size_t xpass_smem(int nxf, int kp) {
-  return sizeof(A) * ((size_t)nxf * kp + (size_t)nxf * (kXT + kp - 1) * 32);
+  return sizeof(A) * ((size_t)nxf * kp + (size_t)2 * (kXT + kp - 1) * 32);
 }
 
 static int64_t xpass_tiles(int64_t nx, int64_t ny, int64_t nz) {
@@ -255,77 +318,82 @@ static int64_t xpass_tiles(int64_t nx, int64_t ny, int64_t nz) {
 
 template <typename T, typename A>
 __global__ void __launch_bounds__(kPassThreads) xpass_kernel(
-    const T* __restrict__ v, int64_t nx, int64_t ny, int nz, int kp, SepParams<T> p,
+    const T* __restrict__ w, int64_t nx, int64_t ny, int nz, int kp, SepParams<T> p,
     T* __restrict__ out, int64_t plane, XEpi epi, double* __restrict__ partials) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double scratch[32];
   A* taps_s = reinterpret_cast<A*>(smem_raw);
-  A* buf = taps_s + p.nxf * kp;  // [nxf][kXT + kp - 1][32]
   const int rows = kXT + kp - 1;
+  A* bufs = taps_s + p.nxf * kp;  // 2 x [kXT + kp - 1][32]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = kPassThreads / 32;
   const int off = kp - 1 - p.cx;
+  const int nf = p.nxf;
   stage_taps<A>(taps_s, p.xtap(0), p.nxf, p.kx, kp);
   const int64_t pe = ny * nz;  // elements of one x-plane
   const int64_t xtiles = (nx + kXT - 1) / kXT;
   const int64_t ntiles = xtiles * ((pe + 31) / 32);
+  // stage k: tile blockIdx.x + (k / nf) * gridDim.x, x filter k % nf
+  auto issue = [&](int k) {
+    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+    if (t < ntiles) {
+      const int a = k % nf;
+      const int64_t x0 = (t % xtiles) * kXT;
+      const int64_t e = (t / xtiles) * 32 + lane;
+      const T* src = w + (int64_t)a * plane + (e < pe ? e : 0);
+      A* dst = bufs + (k & 1) * rows * 32 + lane;
+      for (int r = warp; r < rows; r += NW)
+        stage_elem<T, A>(dst + r * 32, src + wrap_fast(x0 - off + r, nx) * pe, e < pe);
+    }
+    cp_async_commit();
+  };
   double s_f = 0.0, s_clip = 0.0;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t x0 = (t % xtiles) * kXT;
+  A acc[kSR];
+  issue(0);
+  for (int k = 0;; ++k) {
+    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+    if (t >= ntiles) break;
+    const int a = k % nf;
+    issue(k + 1);
+    cp_async_wait<1>();
+    __syncthreads();
+    if (a == 0) {
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) acc[r] = (A)0;
+    }
+    sep_window<A>(bufs + (k & 1) * rows * 32 + warp * kSR * 32 + lane, 32, taps_s + a * kp,
+                  kp, acc);
     const int64_t e = (t / xtiles) * 32 + lane;
-    const bool live = e < pe;
-    __syncthreads();
-#pragma unroll 2
-    for (int r = warp; r < rows; r += NW) {
-      const int64_t xs = wrap_fast(x0 - off + r, nx);
-      A w[kMaxX];
-#pragma unroll
-      for (int a = 0; a < kMaxX; ++a) w[a] = (A)0;
-      if (live) {
-        const T* src = v + xs * pe + e;
-        for (int q = 0; q < p.npairs; ++q) {
-          const A vq = (A)src[(int64_t)q * plane];
-#pragma unroll
-          for (int a = 0; a < kMaxX; ++a)
-            if (a < p.nxf) w[a] = fma_a<A>((A)p.mix[a * p.npairs + q], vq, w[a]);
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < kMaxX; ++a)
-        if (a < p.nxf) buf[(a * rows + r) * 32 + lane] = w[a];
-    }
-    __syncthreads();
-    A acc[kSR];
-#pragma unroll
-    for (int r = 0; r < kSR; ++r) acc[r] = (A)0;
-    for (int a = 0; a < p.nxf; ++a)
-      sep_window<A>(buf + (a * rows + warp * kSR) * 32 + lane, 32, taps_s + a * kp, kp, acc);
-    if (!live) continue;
-    const int64_t xw = x0 + warp * kSR;
-    bool in_win = false;
-    if (epi.mode == STEAM_EPI_FLUX) {
-      const int64_t y = e / nz;
-      in_win = y >= epi.wy0 && y < epi.wy1;
-    }
-#pragma unroll
-    for (int r = 0; r < kSR; ++r) {
-      const int64_t x = xw + r;
-      if (x >= nx) break;
-      const int64_t o = x * pe + e;
+    if (a == nf - 1 && e < pe) {
+      const int64_t xw = (t % xtiles) * kXT + warp * kSR;
+      bool in_win = false;
       if (epi.mode == STEAM_EPI_FLUX) {
-        // F + conv rounded once to the storage dtype
-        T f = (T)((double)out[o] + (double)acc[r]);
-        if (f < (T)0) {
-          s_clip += 1.0;
-          f = (T)0;
+        const int64_t y = e / nz;
+        in_win = y >= epi.wy0 && y < epi.wy1;
+      }
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) {
+        const int64_t x = xw + r;
+        if (x < nx) {
+          const int64_t o = x * pe + e;
+          if (epi.mode == STEAM_EPI_FLUX) {
+            // F + conv rounded once to the storage dtype
+            T f = (T)((double)out[o] + (double)acc[r]);
+            if (f < (T)0) {
+              s_clip += 1.0;
+              f = (T)0;
+            }
+            out[o] = f;
+            if (in_win && x >= epi.wx0 && x < epi.wx1) s_f += (double)f;
+          } else {
+            out[o] = (T)acc[r];
+          }
         }
-        out[o] = f;
-        if (in_win && x >= epi.wx0 && x < epi.wx1) s_f += (double)f;
-      } else {
-        out[o] = (T)acc[r];
       }
     }
+    __syncthreads();  // stage k's buffer is free for stage k + 2
   }
+  cp_async_wait<0>();
   if (epi.mode == STEAM_EPI_FLUX) {
     double t0 = block_sum(s_f, scratch);
     double t1 = block_sum(s_clip, scratch);
@@ -981,11 +1049,11 @@ static int xpass_grid_max(int64_t nx, int64_t ny, int64_t nz) {
 }
 
 // The z, y and x passes in arithmetic type A: u = z filters of the input
-// (scaled by pre when given), v = the y filters of u per pair, out = the
-// mixed x filters of v with the epilogue.
+// (scaled by pre when given), w = the x filters' mixes of the y-filtered
+// pairs of u, out = the x filters of w with the epilogue.
 template <typename T, typename A>
 static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t nz,
-                         const T* in, const T* pre, T* u, T* v, T* out, const XEpi& epi,
+                         const T* in, const T* pre, T* u, T* w, T* out, const XEpi& epi,
                          double* partials, int* xgrid_out, cudaStream_t s) {
   const int64_t plane = nx * ny * nz;
   const int kpz = sep_padded(p.kz), kpy = sep_padded(p.ky), kpx = sep_padded(p.kx);
@@ -1011,15 +1079,21 @@ static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t 
   }
   {
     const int64_t tiles = nx * ((ny + kYT - 1) / kYT) * ((nz + 31) / 32);
-    auto k = ypass_kernel<T, A>;
-    k<<<stride_grid(tiles, 1, pass_occupancy(k, smy, 8)), kPassThreads, smy, s>>>(
-        u, nx, ny, (int)nz, kpy, p, v, plane);
+    if (p.nxf <= 2) {
+      auto k = ypass_kernel<T, A, 2>;
+      k<<<stride_grid(tiles, 1, pass_occupancy(k, smy, 8)), kPassThreads, smy, s>>>(
+          u, nx, ny, (int)nz, kpy, p, w, plane);
+    } else {
+      auto k = ypass_kernel<T, A, kMaxX>;
+      k<<<stride_grid(tiles, 1, pass_occupancy(k, smy, 8)), kPassThreads, smy, s>>>(
+          u, nx, ny, (int)nz, kpy, p, w, plane);
+    }
     STEAM_LAUNCH_CHECK("conv y-pass");
   }
   {
     auto k = xpass_kernel<T, A>;
     const int grid = stride_grid(xpass_tiles(nx, ny, nz), 1, pass_occupancy(k, smx, 8));
-    k<<<grid, kPassThreads, smx, s>>>(v, nx, ny, (int)nz, kpx, p, out, plane, epi, partials);
+    k<<<grid, kPassThreads, smx, s>>>(w, nx, ny, (int)nz, kpx, p, out, plane, epi, partials);
     STEAM_LAUNCH_CHECK("conv x-pass");
     *xgrid_out = grid;
   }
@@ -1046,13 +1120,13 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
                         win, sums_out, totals_dev, ws, ws_bytes, s);
   Carver c(ws, ws_bytes);
   T* u = c.take<T>((size_t)p.nzf * plane);
-  T* v = c.take<T>((size_t)p.npairs * plane);
+  T* w = c.take<T>((size_t)p.nxf * plane);
   T* pre = nullptr;
   const bool use_pre = pre_div != nullptr || pre_mul != nullptr || pre_dev != nullptr;
   if (use_pre) pre = c.take<T>((size_t)2 * nz);
   double* partials = c.take<double>((size_t)xpass_grid_max(nx, ny, nz) * 2);
   double* totals = c.take<double>(2);
-  if (!u || !v || (use_pre && !pre) || !partials || !totals)
+  if (!u || !w || (use_pre && !pre) || !partials || !totals)
     return fail(STEAM_ERR_WORKSPACE,
                 "steam_conv_separable: workspace too small");
   const T* in = (const T*)in_v;
@@ -1079,9 +1153,9 @@ static int run_separable(int64_t nx, int64_t ny, int64_t nz,
   int xgrid = 0;
   // float64 arithmetic for float64 fields, the flux epilogue and the wide store
   rc = (sizeof(T) == 8 || epilogue != STEAM_EPI_STORE)
-           ? launch_passes<T, double>(p, nx, ny, nz, in, use_pre ? pre : nullptr, u, v, out,
+           ? launch_passes<T, double>(p, nx, ny, nz, in, use_pre ? pre : nullptr, u, w, out,
                                       epi, partials, &xgrid, s)
-           : launch_passes<T, T>(p, nx, ny, nz, in, use_pre ? pre : nullptr, u, v, out, epi,
+           : launch_passes<T, T>(p, nx, ny, nz, in, use_pre ? pre : nullptr, u, w, out, epi,
                                  partials, &xgrid, s);
   if (rc) return rc;
   if (epilogue == STEAM_EPI_FLUX) {
@@ -1110,7 +1184,7 @@ extern "C" size_t steam_conv_workspace_bytes(int dtype, int64_t nx, int64_t ny,
   size_t plane = (size_t)(nx * ny * nz);
   const int xgrid = xpass_grid_max(nx, ny, nz);
   const size_t multi = carve_bytes((size_t)spec->n_z * plane, elem) +
-                      carve_bytes((size_t)spec->n_pairs * plane, elem) +
+                      carve_bytes((size_t)spec->n_x * plane, elem) +
                       carve_bytes((size_t)2 * nz, elem) +
                       carve_bytes((size_t)xgrid * 2, sizeof(double)) +
                       carve_bytes(2, sizeof(double));
