@@ -50,7 +50,29 @@ __device__ __forceinline__ double fma_a<double>(double a, double b, double c) {
   return __fma_rn(a, b, c);
 }
 
-// acc[r] = sum_m taps[m] * line[(r + m) * stride], m < kp (kp % kSU == 0).
+// kSU taps from shared memory by 16-byte loads (p 16-byte aligned).
+__device__ __forceinline__ void load_taps(const float* p, float (&t)[kSU]) {
+#pragma unroll
+  for (int i = 0; i < kSU; i += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p + i);
+    t[i] = v.x;
+    t[i + 1] = v.y;
+    t[i + 2] = v.z;
+    t[i + 3] = v.w;
+  }
+}
+__device__ __forceinline__ void load_taps(const double* p, double (&t)[kSU]) {
+#pragma unroll
+  for (int i = 0; i < kSU; i += 2) {
+    const double2 v = *reinterpret_cast<const double2*>(p + i);
+    t[i] = v.x;
+    t[i + 1] = v.y;
+  }
+}
+
+// acc[r] += sum_m taps[m] * line[(r + m) * stride], m < kp (kp % kSU == 0,
+// taps 16-byte aligned).  The step loop is unrolled twice so that the
+// window's shift is a register renaming on every other step.
 template <typename A>
 __device__ __forceinline__ void sep_window(const A* __restrict__ line, int stride,
                                            const A* __restrict__ taps, int kp,
@@ -58,12 +80,15 @@ __device__ __forceinline__ void sep_window(const A* __restrict__ line, int strid
   A w[kSR + kSU - 1];
 #pragma unroll
   for (int i = 0; i < kSR - 1; ++i) w[i] = line[i * stride];
+#pragma unroll 2
   for (int m0 = 0; m0 < kp; m0 += kSU) {
 #pragma unroll
     for (int u = 0; u < kSU; ++u) w[kSR - 1 + u] = line[(m0 + kSR - 1 + u) * stride];
+    A tv[kSU];
+    load_taps(taps + m0, tv);
 #pragma unroll
     for (int u = 0; u < kSU; ++u) {
-      const A t = taps[m0 + u];
+      const A t = tv[u];
 #pragma unroll
       for (int r = 0; r < kSR; ++r) acc[r] = fma_a<A>(t, w[r + u], acc[r]);
     }
@@ -72,12 +97,20 @@ __device__ __forceinline__ void sep_window(const A* __restrict__ line, int strid
   }
 }
 
-// v mod n in [0, n); one compare on the common in-range index.
-__device__ __forceinline__ int64_t wrap_fast(int64_t v, int64_t n) {
-  if (v >= 0 && v < n) return v;
-  if (v < 0 && v + n >= 0) return v + n;
-  if (v >= n && v < 2 * n) return v - n;
-  return wrapi(v, n);
+// v mod n in [0, n) for int extents; two compares on the common index
+// within one period of the range.
+__device__ __forceinline__ int wrap32(int v, int n) {
+  if (v < 0) {
+    v += n;
+    if (v < 0) {
+      v %= n;
+      if (v < 0) v += n;
+    }
+  } else if (v >= n) {
+    v -= n;
+    if (v >= n) v %= n;
+  }
+  return v;
 }
 
 // taps_s[f * kp + m] = taps[f * k + (kp - 1 - m)], zero past the filter.
@@ -90,6 +123,25 @@ __device__ __forceinline__ void stage_taps(A* taps_s, const double* taps, int nf
   }
 }
 
+// One staged element: by cp.async when the field has the arithmetic type
+// (zero-filled when not valid; the source is then not read), converted
+// through registers otherwise.
+template <typename T, typename A>
+__device__ __forceinline__ void stage_elem(A* dst, const T* src, bool valid) {
+  if constexpr (std::is_same<T, A>::value) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(A) == 4)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src),
+                   "r"(valid ? 4 : 0)
+                   : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src),
+                   "r"(valid ? 8 : 0)
+                   : "memory");
+  } else {
+    *dst = valid ? (A)*src : (A)0;
+  }
+}
 
 // ---- z-pass -------------------------------------------------------------
 // Tile = 32 consecutive columns (one per lane) x a chunk of z of 8 warps x
@@ -138,15 +190,23 @@ __global__ void __launch_bounds__(kPassThreads) zpass_kernel(
     const int ncb = (int)((ncol - col0) < kZCols ? (ncol - col0) : kZCols);
     __syncthreads();
     for (int c = warp; c < kZCols; c += NW) {
+      const T* src = in + (col0 + (c < ncb ? c : 0)) * nz;
       for (int j = lane; j < len; j += 32) {
         const int s = z0 + j - off;
-        A v = (A)0;
-        if (c < ncb && s >= 0 && s < nz) {
-          T x = in[(col0 + c) * nz + s];
-          if (PRE) x = mul_rn(x, pre_scale(pre_div[s], pre_mul[s]));
-          v = (A)x;
+        const bool valid = c < ncb && s >= 0 && s < nz;
+        stage_elem<T, A>(buf + c * ld + j, src + (valid ? s : 0), valid);
+      }
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    if (PRE) {
+      // each thread scales the elements it staged itself (zeros stay zero)
+      for (int c = warp; c < kZCols; c += NW) {
+        for (int j = lane; j < len; j += 32) {
+          const int s = z0 + j - off;
+          if (c < ncb && s >= 0 && s < nz)
+            buf[c * ld + j] = (A)mul_rn((T)buf[c * ld + j], pre_scale(pre_div[s], pre_mul[s]));
         }
-        buf[c * ld + j] = v;
       }
     }
     __syncthreads();
@@ -177,34 +237,15 @@ __global__ void __launch_bounds__(kPassThreads) zpass_kernel(
   }
 }
 
-// ---- staging of the y and x passes -----------------------------------------
-// A block's work is a sequence of stages (tile, input field); the rows of
-// stage k + 1 are copied into the second of two buffers while stage k is
-// computed.  Same-type fields go by cp.async (zero-filled past the array);
-// a float32 field filtered in float64 is converted through registers.
-template <typename T, typename A>
-__device__ __forceinline__ void stage_elem(A* dst, const T* src, bool valid) {
-  if constexpr (std::is_same<T, A>::value) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-    if constexpr (sizeof(A) == 4)
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src),
-                   "r"(valid ? 4 : 0)
-                   : "memory");
-    else
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src),
-                   "r"(valid ? 8 : 0)
-                   : "memory");
-  } else {
-    *dst = valid ? (A)*src : (A)0;
-  }
-}
-
 // ---- y-pass -------------------------------------------------------------
 // Tile = one x-plane's kYT rows x 32 z (one per lane), each warp owning kSR
 // consecutive rows.  The tile's z-filtered fields are staged in turn with
 // kp - 1 halo rows (wrapped: y is circular); every (z filter, y filter) pair
 // on a field is one window run, folded at once into the x filters' mixes
 // w_a = sum_q mix[a][q] v_q, so the pass writes nxf fields, not one per pair.
+// A block's work is a sequence of stages (tile, input field); the rows of
+// stage k + 1 are copied into the second of two buffers while stage k is
+// computed (the x-pass runs the same way).
 constexpr int kYT = (kPassThreads / 32) * kSR;  // 64 rows
 
 template <typename A>
@@ -225,31 +266,36 @@ __global__ void __launch_bounds__(kPassThreads, 3) ypass_kernel(
   const int off = kp - 1 - p.cy;
   const int nf = p.nzf;
   stage_taps<A>(taps_s, p.ytap(0), p.nyf, p.ky, kp);
-  const int64_t ytiles = (ny + kYT - 1) / kYT;
-  const int64_t ztiles = (nz + 31) / 32;
-  const int64_t ntiles = nx * ytiles * ztiles;
+  // tile t = (x, y tile, z tile), z fastest; the host keeps every count
+  // below 2^31, so tile and row indices are 32-bit
+  const int ny32 = (int)ny;
+  const unsigned ytiles = (unsigned)((ny + kYT - 1) / kYT);
+  const unsigned ztiles = (unsigned)((nz + 31) / 32);
+  const unsigned ntiles = (unsigned)nx * ytiles * ztiles;
+  const unsigned nfu = (unsigned)nf;
   // stage k: tile blockIdx.x + (k / nf) * gridDim.x, field k % nf
-  auto issue = [&](int k) {
-    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+  auto issue = [&](unsigned k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
     if (t < ntiles) {
-      const int f = k % nf;
-      const int64_t zt = t % ztiles;
-      const int64_t yt = (t / ztiles) % ytiles;
-      const int64_t x = t / (ztiles * ytiles);
-      const int z = (int)(zt * 32) + lane;
-      const T* src = u + (int64_t)f * plane + x * ny * nz + (z < nz ? z : 0);
+      const int f = (int)(k % nfu);
+      const unsigned rest = t / ztiles;
+      const int z = (int)(t - rest * ztiles) * 32 + lane;
+      const unsigned x = rest / ytiles;
+      const int y0 = (int)(rest - x * ytiles) * kYT;
+      const T* src = u + (int64_t)f * plane + ((int64_t)x * ny) * nz + (z < nz ? z : 0);
       A* dst = bufs + (k & 1) * rows * 32 + lane;
       for (int r = warp; r < rows; r += NW)
-        stage_elem<T, A>(dst + r * 32, src + wrap_fast(yt * kYT - off + r, ny) * nz, z < nz);
+        stage_elem<T, A>(dst + r * 32, src + (int64_t)wrap32(y0 - off + r, ny32) * nz,
+                         z < nz);
     }
     cp_async_commit();
   };
   A acc[NX][kSR];
   issue(0);
-  for (int k = 0;; ++k) {
-    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+  for (unsigned k = 0;; ++k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
     if (t >= ntiles) break;
-    const int f = k % nf;
+    const int f = (int)(k % nfu);
     issue(k + 1);
     cp_async_wait<1>();
     __syncthreads();
@@ -276,16 +322,15 @@ __global__ void __launch_bounds__(kPassThreads, 3) ypass_kernel(
       }
     }
     if (f == nf - 1) {
-      const int64_t zt = t % ztiles;
-      const int64_t yt = (t / ztiles) % ytiles;
-      const int64_t x = t / (ztiles * ytiles);
-      const int z = (int)(zt * 32) + lane;
-      const int64_t yw = yt * kYT + warp * kSR;
+      const unsigned rest = t / ztiles;
+      const int z = (int)(t - rest * ztiles) * 32 + lane;
+      const unsigned x = rest / ytiles;
+      const int yw = (int)(rest - x * ytiles) * kYT + warp * kSR;
       if (z < nz) {
 #pragma unroll
         for (int a = 0; a < NX; ++a) {
           if (a < p.nxf) {
-            T* o = w + (int64_t)a * plane + (x * ny + yw) * nz + z;
+            T* o = w + (int64_t)a * plane + ((int64_t)x * ny + yw) * nz + z;
 #pragma unroll
             for (int r = 0; r < kSR; ++r)
               if (yw + r < ny) o[(int64_t)r * nz] = (T)acc[a][r];
@@ -330,30 +375,35 @@ __global__ void __launch_bounds__(kPassThreads) xpass_kernel(
   const int off = kp - 1 - p.cx;
   const int nf = p.nxf;
   stage_taps<A>(taps_s, p.xtap(0), p.nxf, p.kx, kp);
-  const int64_t pe = ny * nz;  // elements of one x-plane
-  const int64_t xtiles = (nx + kXT - 1) / kXT;
-  const int64_t ntiles = xtiles * ((pe + 31) / 32);
+  // tile t = (32-element group of the (y, z) plane, x tile), x fastest; the
+  // host keeps every count below 2^31, so tile and plane indices are 32-bit
+  const int nx32 = (int)nx;
+  const int pe = (int)(ny * nz);  // elements of one x-plane
+  const unsigned xtiles = (unsigned)((nx + kXT - 1) / kXT);
+  const unsigned ntiles = xtiles * (unsigned)((pe + 31) / 32);
+  const unsigned nfu = (unsigned)nf;
   // stage k: tile blockIdx.x + (k / nf) * gridDim.x, x filter k % nf
-  auto issue = [&](int k) {
-    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+  auto issue = [&](unsigned k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
     if (t < ntiles) {
-      const int a = k % nf;
-      const int64_t x0 = (t % xtiles) * kXT;
-      const int64_t e = (t / xtiles) * 32 + lane;
+      const int a = (int)(k % nfu);
+      const unsigned et = t / xtiles;
+      const int x0 = (int)(t - et * xtiles) * kXT;
+      const int e = (int)et * 32 + lane;
       const T* src = w + (int64_t)a * plane + (e < pe ? e : 0);
       A* dst = bufs + (k & 1) * rows * 32 + lane;
       for (int r = warp; r < rows; r += NW)
-        stage_elem<T, A>(dst + r * 32, src + wrap_fast(x0 - off + r, nx) * pe, e < pe);
+        stage_elem<T, A>(dst + r * 32, src + (int64_t)wrap32(x0 - off + r, nx32) * pe, e < pe);
     }
     cp_async_commit();
   };
   double s_f = 0.0, s_clip = 0.0;
   A acc[kSR];
   issue(0);
-  for (int k = 0;; ++k) {
-    const int64_t t = blockIdx.x + (int64_t)(k / nf) * gridDim.x;
+  for (unsigned k = 0;; ++k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
     if (t >= ntiles) break;
-    const int a = k % nf;
+    const int a = (int)(k % nfu);
     issue(k + 1);
     cp_async_wait<1>();
     __syncthreads();
@@ -363,19 +413,20 @@ __global__ void __launch_bounds__(kPassThreads) xpass_kernel(
     }
     sep_window<A>(bufs + (k & 1) * rows * 32 + warp * kSR * 32 + lane, 32, taps_s + a * kp,
                   kp, acc);
-    const int64_t e = (t / xtiles) * 32 + lane;
+    const unsigned et = t / xtiles;
+    const int e = (int)et * 32 + lane;
     if (a == nf - 1 && e < pe) {
-      const int64_t xw = (t % xtiles) * kXT + warp * kSR;
+      const int xw = (int)(t - et * xtiles) * kXT + warp * kSR;
       bool in_win = false;
       if (epi.mode == STEAM_EPI_FLUX) {
-        const int64_t y = e / nz;
+        const int y = e / nz;
         in_win = y >= epi.wy0 && y < epi.wy1;
       }
 #pragma unroll
       for (int r = 0; r < kSR; ++r) {
-        const int64_t x = xw + r;
-        if (x < nx) {
-          const int64_t o = x * pe + e;
+        const int x = xw + r;
+        if (x < nx32) {
+          const int64_t o = (int64_t)x * pe + e;
           if (epi.mode == STEAM_EPI_FLUX) {
             // F + conv rounded once to the storage dtype
             T f = (T)((double)out[o] + (double)acc[r]);
@@ -402,6 +453,265 @@ __global__ void __launch_bounds__(kPassThreads) xpass_kernel(
       partials[gridDim.x + blockIdx.x] = t1;
     }
   }
+}
+
+// ---- paired y and x passes (float32 fields, float32 arithmetic) -------------
+// The same passes with each thread owning two adjacent columns of the
+// stencil (z in the y pass, the (y, z) element in the x pass): a staged row is
+// read as one 8-byte pair per lane, and every tap is one fma.rn.f32x2 on a
+// {t, t} pair, each lane of which rounds as the scalar fma.  Tiles are
+// 64 wide; a pair whose second column is past the end is staged as zero and
+// not stored.
+
+// acc[r] += sum_m taps2[m] * line[(r + m) * stride] on pairs.
+__device__ __forceinline__ void sep_window2(const float2* __restrict__ line, int stride,
+                                            const float2* __restrict__ taps2, int kp,
+                                            float2 (&acc)[kSR]) {
+  float2 w[kSR + kSU - 1];
+#pragma unroll
+  for (int i = 0; i < kSR - 1; ++i) w[i] = line[i * stride];
+#pragma unroll 2
+  for (int m0 = 0; m0 < kp; m0 += kSU) {
+#pragma unroll
+    for (int u = 0; u < kSU; ++u) w[kSR - 1 + u] = line[(m0 + kSR - 1 + u) * stride];
+    float2 tv[kSU];
+#pragma unroll
+    for (int u = 0; u < kSU; u += 2) {
+      const float4 v = *reinterpret_cast<const float4*>(taps2 + m0 + u);
+      tv[u] = make_float2(v.x, v.y);
+      tv[u + 1] = make_float2(v.z, v.w);
+    }
+#pragma unroll
+    for (int u = 0; u < kSU; ++u) {
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) acc[r] = __ffma2_rn(tv[u], w[r + u], acc[r]);
+    }
+#pragma unroll
+    for (int i = 0; i < kSR - 1; ++i) w[i] = w[kSU + i];
+  }
+}
+
+// taps2[f * kp + m] = {t, t}, t = taps[f * k + (kp - 1 - m)], zero past the filter.
+__device__ __forceinline__ void stage_taps2(float2* taps2, const double* taps, int nf, int k,
+                                            int kp) {
+  for (int i = threadIdx.x; i < nf * kp; i += blockDim.x) {
+    const int f = i / kp, l = kp - 1 - (i - f * kp);
+    const float t = l < k ? (float)taps[f * k + l] : 0.0f;
+    taps2[i] = make_float2(t, t);
+  }
+}
+
+// Two adjacent elements src[0], src[1] into dst (8-byte aligned): one 8-byte
+// copy when both are in range and the source is 8-byte aligned, else two
+// 4-byte copies, each zero-filled when out of range.
+__device__ __forceinline__ void stage_pair(float2* dst, const float* src, int n_valid,
+                                           bool aligned) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if (aligned) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src),
+                 "r"(n_valid >= 2 ? 8 : 0)
+                 : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src),
+                 "r"(n_valid >= 1 ? 4 : 0)
+                 : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s + 4),
+                 "l"(src + (n_valid >= 2 ? 1 : 0)), "r"(n_valid >= 2 ? 4 : 0)
+                 : "memory");
+  }
+}
+
+// Stores the pair's in-range elements.
+__device__ __forceinline__ void store_pair(float* dst, float2 v, int n_valid, bool aligned) {
+  if (aligned && n_valid >= 2) {
+    *reinterpret_cast<float2*>(dst) = v;
+  } else {
+    if (n_valid >= 1) dst[0] = v.x;
+    if (n_valid >= 2) dst[1] = v.y;
+  }
+}
+
+constexpr int kPairW = 64;  // tile width in columns (32 lanes x 2)
+
+static size_t ypass2_smem(int nyf, int kp) {
+  return sizeof(float2) * ((size_t)nyf * kp + (size_t)2 * (kYT + kp - 1) * 32);
+}
+
+template <int NX>
+__global__ void __launch_bounds__(kPassThreads) ypass2_kernel(
+    const float* __restrict__ u, int64_t nx, int64_t ny, int nz, int kp, SepParams<float> p,
+    float* __restrict__ w, int64_t plane) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* taps2 = reinterpret_cast<float2*>(smem_raw);
+  const int rows = kYT + kp - 1;
+  float2* bufs = taps2 + p.nyf * kp;  // 2 x [kYT + kp - 1][32 pairs]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = kPassThreads / 32;
+  const int off = kp - 1 - p.cy;
+  const int nf = p.nzf;
+  stage_taps2(taps2, p.ytap(0), p.nyf, p.ky, kp);
+  const int ny32 = (int)ny;
+  const bool aligned = (nz & 1) == 0;
+  const unsigned ytiles = (unsigned)((ny + kYT - 1) / kYT);
+  const unsigned ztiles = (unsigned)((nz + kPairW - 1) / kPairW);
+  const unsigned ntiles = (unsigned)nx * ytiles * ztiles;
+  const unsigned nfu = (unsigned)nf;
+  auto issue = [&](unsigned k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
+    if (t < ntiles) {
+      const int f = (int)(k % nfu);
+      const unsigned rest = t / ztiles;
+      const int z = (int)(t - rest * ztiles) * kPairW + 2 * lane;
+      const unsigned x = rest / ytiles;
+      const int y0 = (int)(rest - x * ytiles) * kYT;
+      const int nv = nz - z;
+      const float* src = u + (int64_t)f * plane + ((int64_t)x * ny) * nz + (nv > 0 ? z : 0);
+      float2* dst = bufs + (k & 1) * rows * 32 + lane;
+      const int ys0 = y0 - off;
+      if (ys0 >= 0 && ys0 + rows <= ny32) {
+        const float* s = src + (int64_t)(ys0 + warp) * nz;
+        const int64_t step = (int64_t)NW * nz;
+        for (int r = warp; r < rows; r += NW, s += step) stage_pair(dst + r * 32, s, nv, aligned);
+      } else {
+        for (int r = warp; r < rows; r += NW)
+          stage_pair(dst + r * 32, src + (int64_t)wrap32(ys0 + r, ny32) * nz, nv, aligned);
+      }
+    }
+    cp_async_commit();
+  };
+  float2 acc[NX][kSR];
+  issue(0);
+  for (unsigned k = 0;; ++k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
+    if (t >= ntiles) break;
+    const int f = (int)(k % nfu);
+    issue(k + 1);
+    cp_async_wait<1>();
+    __syncthreads();
+    if (f == 0) {
+#pragma unroll
+      for (int a = 0; a < NX; ++a)
+#pragma unroll
+        for (int r = 0; r < kSR; ++r) acc[a][r] = make_float2(0.0f, 0.0f);
+    }
+    const float2* col = bufs + (k & 1) * rows * 32 + warp * kSR * 32 + lane;
+    for (int q = 0; q < p.npairs; ++q) {
+      if (p.pair_z[q] != f) continue;
+      float2 c[kSR];
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) c[r] = make_float2(0.0f, 0.0f);
+      sep_window2(col, 32, taps2 + p.pair_y[q] * kp, kp, c);
+#pragma unroll
+      for (int a = 0; a < NX; ++a) {
+        if (a < p.nxf) {
+          const float m = (float)p.mix[a * p.npairs + q];
+          const float2 m2 = make_float2(m, m);
+#pragma unroll
+          for (int r = 0; r < kSR; ++r) acc[a][r] = __ffma2_rn(m2, c[r], acc[a][r]);
+        }
+      }
+    }
+    if (f == nf - 1) {
+      const unsigned rest = t / ztiles;
+      const int z = (int)(t - rest * ztiles) * kPairW + 2 * lane;
+      const unsigned x = rest / ytiles;
+      const int yw = (int)(rest - x * ytiles) * kYT + warp * kSR;
+      const int nv = nz - z;
+      if (nv > 0) {
+#pragma unroll
+        for (int a = 0; a < NX; ++a) {
+          if (a < p.nxf) {
+            float* o = w + (int64_t)a * plane + ((int64_t)x * ny + yw) * nz + z;
+#pragma unroll
+            for (int r = 0; r < kSR; ++r)
+              if (yw + r < ny32) store_pair(o + (int64_t)r * nz, acc[a][r], nv, aligned);
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage k's buffer is free for stage k + 2
+  }
+  cp_async_wait<0>();
+}
+
+static size_t xpass2_smem(int nxf, int kp) {
+  return sizeof(float2) * ((size_t)nxf * kp + (size_t)2 * (kXT + kp - 1) * 32);
+}
+
+static int64_t xpass2_tiles(int64_t nx, int64_t ny, int64_t nz) {
+  return ((nx + kXT - 1) / kXT) * ((ny * nz + kPairW - 1) / kPairW);
+}
+
+// The plain store only (the flux epilogue and the wide store take float64
+// arithmetic); aligned_out: out is 8-byte aligned and ny * nz even.
+__global__ void __launch_bounds__(kPassThreads) xpass2_kernel(
+    const float* __restrict__ w, int64_t nx, int64_t ny, int nz, int kp, SepParams<float> p,
+    float* __restrict__ out, int64_t plane, int aligned_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* taps2 = reinterpret_cast<float2*>(smem_raw);
+  const int rows = kXT + kp - 1;
+  float2* bufs = taps2 + p.nxf * kp;  // 2 x [kXT + kp - 1][32 pairs]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = kPassThreads / 32;
+  const int off = kp - 1 - p.cx;
+  const int nf = p.nxf;
+  stage_taps2(taps2, p.xtap(0), p.nxf, p.kx, kp);
+  const int nx32 = (int)nx;
+  const int pe = (int)(ny * nz);  // elements of one x-plane
+  const bool aligned = (pe & 1) == 0;
+  const unsigned xtiles = (unsigned)((nx + kXT - 1) / kXT);
+  const unsigned ntiles = xtiles * (unsigned)((pe + kPairW - 1) / kPairW);
+  const unsigned nfu = (unsigned)nf;
+  auto issue = [&](unsigned k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
+    if (t < ntiles) {
+      const int a = (int)(k % nfu);
+      const unsigned et = t / xtiles;
+      const int x0 = (int)(t - et * xtiles) * kXT;
+      const int e = (int)et * kPairW + 2 * lane;
+      const int nv = pe - e;
+      const float* src = w + (int64_t)a * plane + (nv > 0 ? e : 0);
+      float2* dst = bufs + (k & 1) * rows * 32 + lane;
+      const int xs0 = x0 - off;
+      if (xs0 >= 0 && xs0 + rows <= nx32) {
+        const float* s = src + (int64_t)(xs0 + warp) * pe;
+        const int64_t step = (int64_t)NW * pe;
+        for (int r = warp; r < rows; r += NW, s += step) stage_pair(dst + r * 32, s, nv, aligned);
+      } else {
+        for (int r = warp; r < rows; r += NW)
+          stage_pair(dst + r * 32, src + (int64_t)wrap32(xs0 + r, nx32) * pe, nv, aligned);
+      }
+    }
+    cp_async_commit();
+  };
+  float2 acc[kSR];
+  issue(0);
+  for (unsigned k = 0;; ++k) {
+    const unsigned t = blockIdx.x + (k / nfu) * gridDim.x;
+    if (t >= ntiles) break;
+    const int a = (int)(k % nfu);
+    issue(k + 1);
+    cp_async_wait<1>();
+    __syncthreads();
+    if (a == 0) {
+#pragma unroll
+      for (int r = 0; r < kSR; ++r) acc[r] = make_float2(0.0f, 0.0f);
+    }
+    sep_window2(bufs + (k & 1) * rows * 32 + warp * kSR * 32 + lane, 32, taps2 + a * kp, kp,
+                acc);
+    const unsigned et = t / xtiles;
+    const int e = (int)et * kPairW + 2 * lane;
+    const int nv = pe - e;
+    if (a == nf - 1 && nv > 0) {
+      const int xw = (int)(t - et * xtiles) * kXT + warp * kSR;
+#pragma unroll
+      for (int r = 0; r < kSR; ++r)
+        if (xw + r < nx32)
+          store_pair(out + (int64_t)(xw + r) * pe + e, acc[r], nv, aligned_out != 0);
+    }
+    __syncthreads();  // stage k's buffer is free for stage k + 2
+  }
+  cp_async_wait<0>();
 }
 
 // ---- fused pencil convolution ----------------------------------------------
@@ -1062,6 +1372,11 @@ static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t 
   STEAM_REQUIRE(smz <= 200 * 1024, "steam_conv_separable: z filter too long");
   STEAM_REQUIRE(smy <= 200 * 1024, "steam_conv_separable: y filter too long");
   STEAM_REQUIRE(smx <= 200 * 1024, "steam_conv_separable: x filter too long");
+  // the y and x passes index tiles, rows and plane elements in 32 bits
+  const int64_t lim = (int64_t)1 << 31;
+  STEAM_REQUIRE(nx < lim && ny * nz < lim && nx * ((ny + kYT - 1) / kYT) * ((nz + 31) / 32) < lim &&
+                    xpass_tiles(nx, ny, nz) < lim,
+                "steam_conv_separable: field too large for the three-pass form");
   {
     const int64_t ncol = nx * ny;
     const int64_t tiles = ((ncol + kZCols - 1) / kZCols) *
@@ -1076,6 +1391,30 @@ static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t 
           in, ncol, (int)nz, kpz, nullptr, nullptr, p, u, plane);
     }
     STEAM_LAUNCH_CHECK("conv z-pass");
+  }
+  if constexpr (std::is_same<T, float>::value && std::is_same<A, float>::value) {
+    // plain float32 convolution: the paired y and x passes
+    const size_t smy2 = ypass2_smem(p.nyf, kpy), smx2 = xpass2_smem(p.nxf, kpx);
+    STEAM_REQUIRE(smy2 <= 200 * 1024, "steam_conv_separable: y filter too long");
+    STEAM_REQUIRE(smx2 <= 200 * 1024, "steam_conv_separable: x filter too long");
+    const int64_t ytiles = nx * ((ny + kYT - 1) / kYT) * ((nz + kPairW - 1) / kPairW);
+    if (p.nxf <= 2) {
+      auto k = ypass2_kernel<2>;
+      k<<<stride_grid(ytiles, 1, pass_occupancy(k, smy2, 8)), kPassThreads, smy2, s>>>(
+          u, nx, ny, (int)nz, kpy, p, w, plane);
+    } else {
+      auto k = ypass2_kernel<kMaxX>;
+      k<<<stride_grid(ytiles, 1, pass_occupancy(k, smy2, 8)), kPassThreads, smy2, s>>>(
+          u, nx, ny, (int)nz, kpy, p, w, plane);
+    }
+    STEAM_LAUNCH_CHECK("conv y-pass");
+    auto kx = xpass2_kernel;
+    const int grid = stride_grid(xpass2_tiles(nx, ny, nz), 1, pass_occupancy(kx, smx2, 8));
+    const int aligned_out = ((uintptr_t)out % 8 == 0 && (ny * nz) % 2 == 0) ? 1 : 0;
+    kx<<<grid, kPassThreads, smx2, s>>>(w, nx, ny, (int)nz, kpx, p, out, plane, aligned_out);
+    STEAM_LAUNCH_CHECK("conv x-pass");
+    *xgrid_out = grid;
+    return STEAM_OK;
   }
   {
     const int64_t tiles = nx * ((ny + kYT - 1) / kYT) * ((nz + 31) / 32);

@@ -6,8 +6,9 @@ run as a z pass, a y pass and an x pass through HBM, each thread computing 8
 consecutive outputs of its axis from a sliding register window.  Against the
 FP64 oracle (steam/utils.py:293-427 semantics: x/y circular, z linear) on
 interior-only shapes, partial tiles in every axis, periods shorter than the
-kernel (several wraps in x and y), z thinner than the kernel; with the input
-scaling prologue, the flux epilogue on a window and the wide store.
+kernel (several wraps in x and y), z thinner than the kernel, odd nz and
+odd y-z planes, input and output at 4-byte offsets; with the input scaling
+prologue, the flux epilogue on a window and the wide store.
 
 Bars: float64 1e-12 relative L2; float32 (float32 arithmetic in every pass)
 1e-6 relative L2 (61 taps per pass, three roundings of intermediates).
@@ -26,7 +27,7 @@ pytestmark = pytest.mark.gpu
 BAR = {np.float32: 1e-6, np.float64: 1e-12}
 K61 = O.turbulon_envelope(1, 0.1, 0.1, 0.1, shape='mexican_hat', dtype=np.float64)
 K41 = O.turbulon_envelope(1, 0.15, 0.15, 0.15, shape='mexican_hat', dtype=np.float64)
-SHAPES = [(64, 64, 64), (72, 70, 52), (33, 22, 20), (16, 12, 8), (130, 40, 100)]
+SHAPES = [(64, 64, 64), (72, 70, 52), (33, 22, 20), (16, 12, 8), (130, 40, 100), (24, 21, 13)]
 
 
 def rel_l2(a, b):
@@ -145,6 +146,25 @@ def test_wide_store_against_oracle(U):
     want = O.convolve(f.astype(np.float64), K61)
     assert rel_l2(b.cpu().numpy(), want) < 5e-7
     assert rel_l2(a.cpu().numpy(), want) < BAR[np.float32]
+
+
+@pytest.mark.parametrize("in_offset,out_offset", [(1, 0), (0, 1), (1, 1)])
+def test_unaligned_arrays(U, in_offset, out_offset):
+    """Input and output at 4-byte offsets (no 8-byte pair access there)."""
+    import torch
+    shape = (40, 34, 26)
+    n = shape[0] * shape[1] * shape[2]
+    rng = np.random.default_rng(17)
+    base_in = torch.as_tensor(rng.standard_normal(n + 1).astype(np.float32), device='cuda')
+    f = base_in[in_offset:in_offset + n].view(shape)
+    base_out = torch.zeros(n + 1, dtype=torch.float32, device='cuda')
+    out = base_out[out_offset:out_offset + n].view(shape)
+    plan = U.plan_convolution(K61, shape, np.float32)
+    U.run_plan(plan, f, out)
+    want = O.convolve(f.cpu().numpy().astype(np.float64), K61)
+    assert rel_l2(out.cpu().numpy(), want) < BAR[np.float32]
+    if out_offset:
+        assert float(base_out[0]) == 0.0
 
 
 def test_repeat_launches_are_bit_identical(U):
