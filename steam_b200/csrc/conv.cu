@@ -634,6 +634,119 @@ __global__ void __launch_bounds__(kPassThreads) ypass2_kernel(
   cp_async_wait<0>();
 }
 
+// Paired z-pass: tile = 64 consecutive columns x kZ2 z; the columns are staged
+// transposed (row j = one z level of the 64 columns, pitch 66 floats: the
+// pair reads are 8-byte aligned and conflict-free, the staging writes at most
+// two-way conflicted), so each thread's window runs down z on its two columns
+// as pairs; stages are double-buffered, one per tile, and the outputs go
+// straight to global memory (16-byte stores when nz % 4 == 0).
+constexpr int kZ2 = 128;      // z outputs per tile
+constexpr int kZ2Pitch = 66;  // floats per staged row
+
+static size_t zpass2_smem(int nzf, int kp) {
+  return sizeof(float2) * (size_t)nzf * kp +
+         sizeof(float) * (size_t)2 * (kZ2 + kp - 1) * kZ2Pitch;
+}
+
+template <bool PRE>
+__global__ void __launch_bounds__(kPassThreads) zpass2_kernel(
+    const float* __restrict__ in, int64_t ncol, int nz, int kp, const float* __restrict__ pre_div,
+    const float* __restrict__ pre_mul, SepParams<float> p, float* __restrict__ out,
+    int64_t plane) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* taps2 = reinterpret_cast<float2*>(smem_raw);
+  float* bufs = reinterpret_cast<float*>(taps2 + p.nzf * kp);  // 2 x [kZ2 + kp - 1][66]
+  const int rows = kZ2 + kp - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = kPassThreads / 32;
+  const int off = kp - 1 - p.cz;
+  stage_taps2(taps2, p.ztap(0), p.nzf, p.kz, kp);
+  const unsigned zchunks = (unsigned)((nz + kZ2 - 1) / kZ2);
+  const unsigned ntiles = (unsigned)((ncol + kPairW - 1) / kPairW) * zchunks;
+  const bool vec = (nz & 3) == 0;
+  // stage k = tile blockIdx.x + k * gridDim.x: (column block, z chunk), z fastest
+  auto issue = [&](unsigned k) {
+    const unsigned t = blockIdx.x + k * gridDim.x;
+    if (t < ntiles) {
+      const unsigned cb = t / zchunks;
+      const int z0 = (int)(t - cb * zchunks) * kZ2;
+      const int64_t col0 = (int64_t)cb * kPairW;
+      const int ncb = (int)((ncol - col0) < kPairW ? (ncol - col0) : kPairW);
+      float* buf = bufs + (k & 1) * rows * kZ2Pitch;
+      for (int c = warp; c < kPairW; c += NW) {
+        const float* src = in + (col0 + (c < ncb ? c : 0)) * nz;
+        for (int j = lane; j < rows; j += 32) {
+          const int s = z0 - off + j;
+          const bool valid = c < ncb && s >= 0 && s < nz;
+          stage_elem<float, float>(buf + j * kZ2Pitch + c, src + (valid ? s : 0), valid);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  for (unsigned k = 0;; ++k) {
+    const unsigned t = blockIdx.x + k * gridDim.x;
+    if (t >= ntiles) break;
+    issue(k + 1);
+    cp_async_wait<1>();
+    const unsigned cb = t / zchunks;
+    const int z0 = (int)(t - cb * zchunks) * kZ2;
+    const int64_t col0 = (int64_t)cb * kPairW;
+    const int ncb = (int)((ncol - col0) < kPairW ? (ncol - col0) : kPairW);
+    const int zc = (nz - z0) < kZ2 ? (nz - z0) : kZ2;
+    float* buf = bufs + (k & 1) * rows * kZ2Pitch;
+    if (PRE) {
+      // each thread scales the elements it staged itself (zeros stay zero)
+      for (int c = warp; c < ncb; c += NW) {
+        for (int j = lane; j < rows; j += 32) {
+          const int s = z0 - off + j;
+          if (s >= 0 && s < nz)
+            buf[j * kZ2Pitch + c] = mul_rn(buf[j * kZ2Pitch + c], pre_scale(pre_div[s], pre_mul[s]));
+        }
+      }
+    }
+    __syncthreads();
+    const int c = 2 * lane;
+    const int nv = ncb - c;  // columns of this thread's pair in range
+    for (int seg = warp; seg * kSR < zc; seg += NW) {
+      const float2* col = reinterpret_cast<const float2*>(buf + seg * kSR * kZ2Pitch) + lane;
+      for (int f = 0; f < p.nzf; ++f) {
+        float2 acc[kSR];
+#pragma unroll
+        for (int r = 0; r < kSR; ++r) acc[r] = make_float2(0.0f, 0.0f);
+        sep_window2(col, kZ2Pitch / 2, taps2 + f * kp, kp, acc);
+        if (nv > 0) {
+          const int zs = z0 + seg * kSR;
+          float* o0 = out + f * plane + (col0 + c) * nz + zs;
+          if (vec && zs + kSR <= nz) {
+            *reinterpret_cast<float4*>(o0) = make_float4(acc[0].x, acc[1].x, acc[2].x, acc[3].x);
+            *reinterpret_cast<float4*>(o0 + 4) =
+                make_float4(acc[4].x, acc[5].x, acc[6].x, acc[7].x);
+            if (nv > 1) {
+              *reinterpret_cast<float4*>(o0 + nz) =
+                  make_float4(acc[0].y, acc[1].y, acc[2].y, acc[3].y);
+              *reinterpret_cast<float4*>(o0 + nz + 4) =
+                  make_float4(acc[4].y, acc[5].y, acc[6].y, acc[7].y);
+            }
+          } else {
+#pragma unroll
+            for (int r = 0; r < kSR; ++r) {
+              if (zs + r < nz) {
+                o0[r] = acc[r].x;
+                if (nv > 1) o0[nz + r] = acc[r].y;
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage k's buffer is free for stage k + 2
+  }
+  cp_async_wait<0>();
+}
+
+
 static size_t xpass2_smem(int nxf, int kp) {
   return sizeof(float2) * ((size_t)nxf * kp + (size_t)2 * (kXT + kp - 1) * 32);
 }
@@ -1377,7 +1490,23 @@ static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t 
   STEAM_REQUIRE(nx < lim && ny * nz < lim && nx * ((ny + kYT - 1) / kYT) * ((nz + 31) / 32) < lim &&
                     xpass_tiles(nx, ny, nz) < lim,
                 "steam_conv_separable: field too large for the three-pass form");
-  {
+  if constexpr (std::is_same<T, float>::value && std::is_same<A, float>::value) {
+    const int64_t ncol = nx * ny;
+    const size_t smz2 = zpass2_smem(p.nzf, kpz);
+    const int64_t tiles = ((ncol + kPairW - 1) / kPairW) * ((nz + kZ2 - 1) / kZ2);
+    STEAM_REQUIRE(smz2 <= 200 * 1024, "steam_conv_separable: z filter too long");
+    STEAM_REQUIRE(tiles < lim, "steam_conv_separable: field too large for the three-pass form");
+    if (pre) {
+      auto k = zpass2_kernel<true>;
+      k<<<stride_grid(tiles, 1, pass_occupancy(k, smz2, 8)), kPassThreads, smz2, s>>>(
+          in, ncol, (int)nz, kpz, pre, pre + nz, p, u, plane);
+    } else {
+      auto k = zpass2_kernel<false>;
+      k<<<stride_grid(tiles, 1, pass_occupancy(k, smz2, 8)), kPassThreads, smz2, s>>>(
+          in, ncol, (int)nz, kpz, nullptr, nullptr, p, u, plane);
+    }
+    STEAM_LAUNCH_CHECK("conv z-pass");
+  } else {
     const int64_t ncol = nx * ny;
     const int64_t tiles = ((ncol + kZCols - 1) / kZCols) *
                           ((nz + zpass_chunk<A>() - 1) / zpass_chunk<A>());

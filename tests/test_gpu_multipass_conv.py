@@ -27,7 +27,8 @@ pytestmark = pytest.mark.gpu
 BAR = {np.float32: 1e-6, np.float64: 1e-12}
 K61 = O.turbulon_envelope(1, 0.1, 0.1, 0.1, shape='mexican_hat', dtype=np.float64)
 K41 = O.turbulon_envelope(1, 0.15, 0.15, 0.15, shape='mexican_hat', dtype=np.float64)
-SHAPES = [(64, 64, 64), (72, 70, 52), (33, 22, 20), (16, 12, 8), (130, 40, 100), (24, 21, 13)]
+SHAPES = [(64, 64, 64), (72, 70, 52), (33, 22, 20), (16, 12, 8), (130, 40, 100), (24, 21, 13),
+          (33, 21, 20)]
 
 
 def rel_l2(a, b):
