@@ -224,8 +224,9 @@ def plan_convolution(kernel, field_shape, dtype=np.float32, tol=None):
     k64 = np.ascontiguousarray(kernel, dtype=np.float64)
     fft_ok = dtype == np.float32 and max(k64.shape) <= FFT_MAX_TAPS
     # the fused separable kernel is the fastest form; a separable plan beyond
-    # it runs as three passes through HBM with one intermediate field per
-    # filter (pair), which the FFT convolution beats
+    # it runs as three passes through HBM with one intermediate field per z
+    # filter and per x filter, which the FFT convolution beats where it
+    # applies (the rank-(3, 3, 3) Morlet at 512x512x256: 1.20 against 1.60 ms)
     if sep is not None and (_fused_separable(sep) or not fft_ok):
         plan = sep
         plan.kernel = k64
