@@ -611,6 +611,36 @@ int steam_thermo_async(int dtype, int64_t nx, int64_t ny, int64_t nz, const void
                        const double* ps_field_dev, void* T, void* qv, void* qc, void* qi,
                        void* p, steam_stream_t stream);
 
+/* Grouped thermodynamics (no counterpart in the reference, which maps one
+ * field at a time): n independent fields' steam_thermo_async as ONE launch,
+ * each field's blocks a contiguous range of the grid; every field's result
+ * is the same bits as its own call.  prepare (synchronous, outside stream
+ * capture) writes the fields' descriptors and a block -> field table to
+ * `workspace` (DEVICE, steam_thermo_group_workspace_bytes) and records the
+ * group under that address; async enqueues the launch (capturable,
+ * repeatable); release forgets the group.  All fields of one group have the
+ * dtype given. */
+typedef struct {
+  int64_t nx, ny, nz;
+  const void* h;          /* DEVICE (nx, ny, nz) */
+  const void* qt;         /* DEVICE (nx, ny, nz) */
+  const double* prof;     /* DEVICE [4][nz]: as steam_thermo_async's prof_dev */
+  int32_t compose;
+  double bounds[4];       /* used when compose != 0 */
+  double surface_pressure;
+  const double* ps_field; /* DEVICE (nx, ny) or NULL */
+  void* T;                /* DEVICE outputs (nx, ny, nz) */
+  void* qv;
+  void* qc;
+  void* qi;
+  void* p;
+} steam_thermo_problem_t;
+size_t steam_thermo_group_workspace_bytes(int32_t n, const steam_thermo_problem_t* problems);
+int steam_thermo_group_prepare(int dtype, int32_t n, const steam_thermo_problem_t* problems,
+                               void* workspace, size_t workspace_bytes);
+int steam_thermo_group_async(void* workspace, steam_stream_t stream);
+int steam_thermo_group_release(void* workspace);
+
 #ifdef __cplusplus
 }
 #endif

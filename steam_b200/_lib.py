@@ -57,6 +57,15 @@ class ConvProblem(ctypes.Structure):
                 ("window", Window), ("sums", ctypes.c_void_p)]
 
 
+class ThermoProblem(ctypes.Structure):
+    """steam_thermo_problem_t: one field of a grouped thermodynamics launch."""
+    _fields_ = [("nx", c_i64), ("ny", c_i64), ("nz", c_i64), ("h", ctypes.c_void_p),
+                ("qt", ctypes.c_void_p), ("prof", ctypes.c_void_p), ("compose", c_i32),
+                ("bounds", ctypes.c_double * 4), ("surface_pressure", ctypes.c_double),
+                ("ps_field", ctypes.c_void_p), ("T", ctypes.c_void_p), ("qv", ctypes.c_void_p),
+                ("qc", ctypes.c_void_p), ("qi", ctypes.c_void_p), ("p", ctypes.c_void_p)]
+
+
 class SepConv(ctypes.Structure):
     """steam_sepconv_t"""
     _fields_ = [("kz", c_i32), ("ky", c_i32), ("kx", c_i32),
@@ -159,6 +168,11 @@ _SIGNATURES = {
                                                        ctypes.c_size_t]),
     "steam_bounded_add_group_async": (ctypes.c_int, [c_vp, c_vp]),
     "steam_bounded_add_group_release": (ctypes.c_int, [c_vp]),
+    "steam_thermo_group_workspace_bytes": (ctypes.c_size_t, [c_i32, c_vp]),
+    "steam_thermo_group_prepare": (ctypes.c_int, [ctypes.c_int, c_i32, c_vp, c_vp,
+                                                  ctypes.c_size_t]),
+    "steam_thermo_group_async": (ctypes.c_int, [c_vp, c_vp]),
+    "steam_thermo_group_release": (ctypes.c_int, [c_vp]),
     "steam_bounded_add_ledger_doubles": (c_size, [c_i32]),
     "steam_project_bounds_replay": (ctypes.c_int, [ctypes.c_int, c_i64, c_i64, c_i64, c_vp,
                                                    c_dp, c_dbl, c_dbl, c_dp, c_vp, c_size,

@@ -3,6 +3,8 @@
 #include "common.cuh"
 
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 namespace steam {
@@ -315,13 +317,15 @@ __device__ __forceinline__ double hyps_exponent(double Tl, double qvl, double gd
   return gdz / (287.04 * Tv);
 }
 
+// One block's work (block `vb` of the field's ceil(ncol / (32 kThWarps))):
+// 32 columns per warp, marched along z in chunks of kThZ levels.
 template <typename T>
-__global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
-    const T* __restrict__ h, const T* __restrict__ qt,
+__device__ __forceinline__ void thermo_body(
+    int64_t vb, const T* __restrict__ h, const T* __restrict__ qt,
     const double* __restrict__ zv, const double* __restrict__ dzv,
     const double* __restrict__ hm, const double* __restrict__ qm, int compose,
     T hlo, T hhi, T qlo, T qhi, int64_t ncol,
-    int nz, double ps, const double* __restrict__ ps_field, ThermoConst<T> k,
+    int nz, double ps, const double* __restrict__ ps_field, const ThermoConst<T>& k,
     T* __restrict__ To, T* __restrict__ qvo, T* __restrict__ qco,
     T* __restrict__ qio, T* __restrict__ po) {
   extern __shared__ unsigned char th_smem[];
@@ -335,7 +339,7 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
   // the chunk's per-level constants, per warp: g z, mean h, mean qt and the
   // hypsometric numerator (-g dz / Rd in float32, -g dz in float64)
   T* lv = base + (size_t)kThWarps * kThArrays * 32 * kThPitch + warp * 4 * kThZ;
-  const int64_t col0 = ((int64_t)blockIdx.x * kThWarps + warp) * 32;
+  const int64_t col0 = (vb * kThWarps + warp) * 32;
   if (col0 >= ncol) return;
   const int ncols = (int)((ncol - col0) < 32 ? (ncol - col0) : 32);
   const int64_t mycol = col0 + lane;
@@ -422,6 +426,52 @@ __global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
     }
     __syncwarp();
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kThWarps) thermo_kernel(
+    const T* __restrict__ h, const T* __restrict__ qt,
+    const double* __restrict__ zv, const double* __restrict__ dzv,
+    const double* __restrict__ hm, const double* __restrict__ qm, int compose,
+    T hlo, T hhi, T qlo, T qhi, int64_t ncol,
+    int nz, double ps, const double* __restrict__ ps_field, ThermoConst<T> k,
+    T* __restrict__ To, T* __restrict__ qvo, T* __restrict__ qco,
+    T* __restrict__ qio, T* __restrict__ po) {
+  thermo_body<T>(blockIdx.x, h, qt, zv, dzv, hm, qm, compose, hlo, hhi, qlo, qhi, ncol, nz, ps,
+                 ps_field, k, To, qvo, qco, qio, po);
+}
+
+// One field of a grouped thermodynamics launch (device memory): its arrays,
+// profiles (z, dz, mean h, mean qt: 4 nz), bounds and its first block.
+struct ThermoMember {
+  const void* h;
+  const void* qt;
+  const double* prof;
+  const double* ps_field;
+  void* T;
+  void* qv;
+  void* qc;
+  void* qi;
+  void* p;
+  int64_t ncol;
+  int64_t block0;
+  int32_t nz;
+  int32_t compose;
+  double bounds[4];
+  double ps;
+};
+
+// n fields in one launch: owner[b] is the field of block b.
+template <typename T>
+__global__ void __launch_bounds__(32 * kThWarps) thermo_group_kernel(
+    const ThermoMember* __restrict__ mem, const int32_t* __restrict__ owner, ThermoConst<T> k) {
+  const int64_t b = blockIdx.x;
+  const ThermoMember& m = mem[owner[b]];
+  const int nz = m.nz;
+  thermo_body<T>(b - m.block0, (const T*)m.h, (const T*)m.qt, m.prof, m.prof + nz,
+                 m.prof + 2 * nz, m.prof + 3 * nz, m.compose, (T)m.bounds[0], (T)m.bounds[1],
+                 (T)m.bounds[2], (T)m.bounds[3], m.ncol, nz, m.ps, m.ps_field, k, (T*)m.T,
+                 (T*)m.qv, (T*)m.qc, (T*)m.qi, (T*)m.p);
 }
 
 template <typename T>
@@ -554,6 +604,121 @@ extern "C" int steam_thermo_async(int dtype, int64_t nx, int64_t ny, int64_t nz,
     return fail(STEAM_ERR_ARG, "steam_thermo_async: bad dtype");
   }
   STEAM_LAUNCH_CHECK("steam_thermo_async");
+  return STEAM_OK;
+}
+
+namespace {
+struct ThermoGroupRec {
+  int dtype;
+  int n;
+  int64_t blocks;
+};
+std::mutex g_thermo_groups_mu;
+std::map<const void*, ThermoGroupRec> g_thermo_groups;
+
+size_t thermo_smem(int dtype) {
+  return ((size_t)kThWarps * kThArrays * 32 * kThPitch + kThWarps * 4 * kThZ) *
+         (dtype == STEAM_F64 ? sizeof(double) : sizeof(float));
+}
+}  // namespace
+
+// The group's workspace: the fields' descriptors, then the block -> field
+// table (one int32 per block of 128 columns).
+constexpr int64_t kThGroupMaxBlocks = (int64_t)1 << 30;
+
+static int64_t thermo_blocks(int64_t nx, int64_t ny) {
+  return (nx * ny + 32 * kThWarps - 1) / (32 * kThWarps);
+}
+
+extern "C" size_t steam_thermo_group_workspace_bytes(int32_t n,
+                                                     const steam_thermo_problem_t* problems) {
+  if (n <= 0 || !problems) return 0;
+  int64_t blocks = 0;
+  for (int i = 0; i < n; ++i)
+    if (problems[i].nx > 0 && problems[i].ny > 0) blocks += thermo_blocks(problems[i].nx, problems[i].ny);
+  return sizeof(ThermoMember) * (size_t)n + sizeof(int32_t) * (size_t)blocks;
+}
+
+extern "C" int steam_thermo_group_prepare(int dtype, int32_t n,
+                                          const steam_thermo_problem_t* problems,
+                                          void* workspace, size_t workspace_bytes) {
+  STEAM_REQUIRE(dtype == STEAM_F32 || dtype == STEAM_F64, "steam_thermo_group_prepare: bad dtype");
+  STEAM_REQUIRE(n > 0 && problems && workspace, "steam_thermo_group_prepare: empty group");
+  STEAM_REQUIRE(workspace_bytes >= steam_thermo_group_workspace_bytes(n, problems),
+                "steam_thermo_group_prepare: workspace too small");
+  std::vector<ThermoMember> mem((size_t)n);
+  int64_t blocks = 0;
+  for (int i = 0; i < n; ++i) {
+    const steam_thermo_problem_t& q = problems[i];
+    STEAM_REQUIRE(q.nx > 0 && q.ny > 0 && q.nz > 0,
+                  "steam_thermo_group_prepare: every field needs a positive extent");
+    STEAM_REQUIRE(q.nz < ((int64_t)1 << 31), "steam_thermo_group_prepare: nz too large");
+    STEAM_REQUIRE(q.h && q.qt && q.prof && q.T && q.qv && q.qc && q.qi && q.p,
+                  "steam_thermo_group_prepare: null pointer");
+    ThermoMember& m = mem[(size_t)i];
+    m.h = q.h;
+    m.qt = q.qt;
+    m.prof = q.prof;
+    m.ps_field = q.ps_field;
+    m.T = q.T;
+    m.qv = q.qv;
+    m.qc = q.qc;
+    m.qi = q.qi;
+    m.p = q.p;
+    m.ncol = q.nx * q.ny;
+    m.block0 = blocks;
+    m.nz = (int32_t)q.nz;
+    m.compose = q.compose ? 1 : 0;
+    for (int j = 0; j < 4; ++j) m.bounds[j] = q.compose ? q.bounds[j] : 0.0;
+    m.ps = q.surface_pressure;
+    blocks += thermo_blocks(q.nx, q.ny);
+  }
+  STEAM_REQUIRE(blocks <= kThGroupMaxBlocks,
+                "steam_thermo_group_prepare: group too large (2^30 blocks of 128 columns)");
+  std::vector<int32_t> owner((size_t)blocks);
+  for (int i = 0; i < n; ++i) {
+    const int64_t end = i + 1 < n ? mem[(size_t)i + 1].block0 : blocks;
+    for (int64_t b = mem[(size_t)i].block0; b < end; ++b) owner[(size_t)b] = i;
+  }
+  STEAM_CUDA(cudaMemcpy(workspace, mem.data(), sizeof(ThermoMember) * mem.size(),
+                        cudaMemcpyHostToDevice));
+  STEAM_CUDA(cudaMemcpy((char*)workspace + sizeof(ThermoMember) * mem.size(), owner.data(),
+                        sizeof(int32_t) * owner.size(), cudaMemcpyHostToDevice));
+  std::lock_guard<std::mutex> lk(g_thermo_groups_mu);
+  g_thermo_groups[workspace] = ThermoGroupRec{dtype, n, blocks};
+  return STEAM_OK;
+}
+
+extern "C" int steam_thermo_group_async(void* workspace, steam_stream_t stream) {
+  ThermoGroupRec r;
+  {
+    std::lock_guard<std::mutex> lk(g_thermo_groups_mu);
+    auto it = g_thermo_groups.find(workspace);
+    STEAM_REQUIRE(it != g_thermo_groups.end(), "steam_thermo_group_async: unknown group");
+    r = it->second;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const ThermoMember* mem = (const ThermoMember*)workspace;
+  const int32_t* owner = (const int32_t*)((const char*)workspace + sizeof(ThermoMember) * r.n);
+  const size_t sm = thermo_smem(r.dtype);
+  if (r.dtype == STEAM_F32) {
+    STEAM_CUDA(cudaFuncSetAttribute(thermo_group_kernel<float>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    thermo_group_kernel<float><<<(unsigned)r.blocks, 32 * kThWarps, sm, s>>>(
+        mem, owner, thermo_const<float>());
+  } else {
+    STEAM_CUDA(cudaFuncSetAttribute(thermo_group_kernel<double>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    thermo_group_kernel<double><<<(unsigned)r.blocks, 32 * kThWarps, sm, s>>>(
+        mem, owner, thermo_const<double>());
+  }
+  STEAM_LAUNCH_CHECK("steam_thermo_group_async");
+  return STEAM_OK;
+}
+
+extern "C" int steam_thermo_group_release(void* workspace) {
+  std::lock_guard<std::mutex> lk(g_thermo_groups_mu);
+  g_thermo_groups.erase(workspace);
   return STEAM_OK;
 }
 

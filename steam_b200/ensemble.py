@@ -189,12 +189,14 @@ class Ensemble:
         self.step_eager()
         torch.cuda.synchronize()
         self.conv_groups = {}
+        self.thermo_group = None
         self.side_stream = torch.cuda.Stream()
         if grouped:
             self.groups = self._prepare_groups()
             self.grouped = bool(self.groups)
             if self.grouped:
                 self.conv_groups = self._prepare_conv_groups()
+                self.thermo_group = self._prepare_thermo_group()
                 self.step_eager()
                 torch.cuda.synchronize()
 
@@ -237,6 +239,32 @@ class Ensemble:
             groups[stage] = (ws, arr)
         return groups
 
+    def _prepare_thermo_group(self):
+        """Every member's thermodynamics as one launch (the members' dtype is
+        common: the grouped bounded adds require it)."""
+        import torch
+        lib = _lib.load()
+        probs = []
+        for m in self.members:
+            nx, ny, nz = m.rc.shape
+            p = _lib.ThermoProblem()
+            p.nx, p.ny, p.nz = nx, ny, nz
+            p.h, p.qt, p.prof = _lib.ptr(m.h), _lib.ptr(m.q), _lib.ptr(m.rc.prof)
+            p.compose = 1
+            for j, b in enumerate(m.rc.bounds):
+                p.bounds[j] = float(b)
+            p.surface_pressure = 101325.0
+            p.ps_field = None
+            p.T, p.qv, p.qc = (_lib.ptr(m.diag[k]) for k in ("T", "qv", "qc"))
+            p.qi, p.p = _lib.ptr(m.diag["qi"]), _lib.ptr(m.diag["p"])
+            probs.append(p)
+        arr = (_lib.ThermoProblem * len(probs))(*probs)
+        nbytes = lib.steam_thermo_group_workspace_bytes(len(probs), arr)
+        ws = torch.empty(int(nbytes), dtype=torch.uint8, device='cuda')
+        _lib.check(lib.steam_thermo_group_prepare(self.members[0].rc.code, len(probs), arr,
+                                                  _lib.ptr(ws), int(nbytes)))
+        return (ws, arr)
+
     def _prepare_groups(self):
         """One grouped bounded add per scalar over every member (members
         whose layout the grouped solve does not take -- nz % 4 != 0 or
@@ -273,15 +301,19 @@ class Ensemble:
 
     def release(self):
         """Forget the grouped solves' device state (the graph too)."""
-        if not getattr(self, 'groups', None) and not getattr(self, 'conv_groups', None):
+        if (not getattr(self, 'groups', None) and not getattr(self, 'conv_groups', None) and
+                getattr(self, 'thermo_group', None) is None):
             return
         lib = _lib.load()
         for ws, _ in getattr(self, 'groups', {}).values():
             lib.steam_bounded_add_group_release(_lib.ptr(ws))
         for ws, _ in getattr(self, 'conv_groups', {}).values():
             lib.steam_conv_group_release(_lib.ptr(ws))
+        if getattr(self, 'thermo_group', None) is not None:
+            lib.steam_thermo_group_release(_lib.ptr(self.thermo_group[0]))
         self.groups = {}
         self.conv_groups = {}
+        self.thermo_group = None
         self.grouped = False
         self.graph = None
 
@@ -363,6 +395,14 @@ class Ensemble:
             ba('h')
             self._fan(second)
             ba('qt')
+
+        if self.thermo_group is not None:
+            _lib.check(lib.steam_thermo_group_async(_lib.ptr(self.thermo_group[0]),
+                                                    _lib.stream()))
+            for m in self.members:
+                m.rc.ledger_host.copy_(m.rc.ledger, non_blocking=True)
+                m.rc.ledger_ready.record()
+            return
 
         def third(m):
             m.rc.enqueue_thermo(m.h, m.q, m.diag)
