@@ -565,9 +565,11 @@ int steam_set_barrier_spin_limit(int64_t polls);
 /* Grouped bounded adds (no counterpart in the reference, which runs one
  * field at a time): n independent fields' steam_bounded_add_async solves
  * (record_applied = 0) as one launch per stage -- the first and apply sweeps
- * over a flat grid, each persistent phase as one cooperative launch whose
- * blocks split into per-field teams with their own grid barriers, a team's
- * size the field's share of the co-resident capacity.  A field's result is
+ * over a flat grid; each persistent phase's first iterations as flat
+ * launches (a sweep over the fields still in the loop, their sums, their
+ * per-level steps), the rest as one cooperative launch whose blocks split
+ * into per-field teams with their own grid barriers, a team's size the
+ * field's share of the co-resident capacity.  A field's result is
  * the single call's to rounding (another block partition of its sums); the
  * same group gives the same bits every time.  Every field:
  * nz % 4 == 0 (4 .. 1024), 16-byte aligned pert and increment.

@@ -1444,12 +1444,12 @@ __device__ __forceinline__ void ba_phase_body(T* __restrict__ d0, T* __restrict_
                                               BAChain<T> c, const BAState<T>& st,
                                               double* __restrict__ partials,
                                               double* __restrict__ totals, int flag_base,
-                                              int n_iter, unsigned char* ba_smem, double* red,
-                                              int vb, int nvb) {
+                                              int it0, int n_iter, unsigned char* ba_smem,
+                                              double* red, int vb, int nvb) {
   constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
   const int nb = nvb;
   c.run = nullptr;
-  for (int it = 0; it < n_iter; ++it) {
+  for (int it = it0; it < n_iter; ++it) {
     // read after a barrier: every block sees the same flag
     if (__ldcg(st.flags + flag_base + it) == 0) break;
     ba_fold_body<T, MODE, true>(d0, pert, 0, nx, ny, nz, w, c, partials, ba_smem, red, vb,
@@ -1481,7 +1481,7 @@ __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3)) ba_phase_
     int flag_base, int n_iter) {
   __shared__ double red[4 * kLvThreads];
   extern __shared__ unsigned char ba_smem[];
-  ba_phase_body<T, MODE>(d0, pert, nx, ny, nz, w, c, st, partials, totals, flag_base, n_iter,
+  ba_phase_body<T, MODE>(d0, pert, nx, ny, nz, w, c, st, partials, totals, flag_base, 0, n_iter,
                          ba_smem, red, blockIdx.x, gridDim.x);
 }
 
@@ -1799,7 +1799,7 @@ static int bounded_add_enqueue(int64_t nx, int64_t ny, int64_t nz, T* pert,
 // sums therefore depend on the group it is solved in (the same group gives
 // the same bits every time).  Only the vectorised layout (nz % 4 == 0,
 // 16-byte aligned fields) is grouped.
-constexpr int kGroupFoldGroups = 64;     // column groups per block, first/apply sweeps
+constexpr int kGroupFoldGroups = 64;     // column groups per block, every flat sweep
 
 template <typename T>
 struct BAGroupRec {
@@ -1880,20 +1880,80 @@ __global__ void __launch_bounds__(kLvThreads, 4)
                                ba_smem, red, blockIdx.x - __ldg(start + p), r.fold_nb);
 }
 
-// one cooperative launch of a phase over fields p0 .. p0 + n - 1; start[i]:
-// the first block of field p0 + i
+// one cooperative launch of a phase over fields p0 .. p0 + n - 1, iterations
+// it0 .. n_iter - 1; start[i]: the first block of field p0 + i
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kLvThreads, (MODE == BA_MU ? 2 : 3))
     bag_phase_kernel(const BAGroupRec<T>* __restrict__ recs, const int* __restrict__ start,
-                     int p0, int n, int flag_base, int n_iter) {
+                     int p0, int n, int flag_base, int it0, int n_iter) {
   __shared__ double red[4 * kLvThreads];
   extern __shared__ unsigned char ba_smem[];
   const int i = group_owner(start, n, blockIdx.x);
   const BAGroupRec<T>& r = recs[p0 + i];
   ba_phase_body<T, MODE>(r.inc, r.pert, r.nx, r.ny, r.nz, r.w, r.ch, r.st, r.partials,
-                         r.totals, flag_base, n_iter, ba_smem, red,
+                         r.totals, flag_base, it0, n_iter, ba_smem, red,
                          blockIdx.x - __ldg(start + i), MODE == BA_MU ? r.mu_nb : r.ph_nb);
 }
+
+// The persistent phases as flat launches, one iteration at a time: a sweep
+// over every field still in the loop (a field whose flag for this iteration
+// is 0 has left it: its blocks return at once), the fixed-order sums of each
+// field's block partials, and the per-level decision that sets the flag of
+// the next iteration.  Every field sweeps at the flat grid's full width, so
+// the fields that need more iterations do not hold the others' blocks idle.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kLvThreads, 4)
+    bag_iter_sweep_kernel(const BAGroupRec<T>* __restrict__ recs, const int* __restrict__ start,
+                          int n, int flag_base, int it) {
+  __shared__ double red[4 * kLvThreads];
+  extern __shared__ unsigned char ba_smem[];
+  const int p = group_owner(start, n, blockIdx.x);
+  const BAGroupRec<T>& r = recs[p];
+  if (r.st.flags[flag_base + it] == 0) return;
+  BAChain<T> c = r.ch;
+  c.run = nullptr;
+  ba_fold_body<T, MODE, false>(r.inc, r.pert, 0, r.nx, r.ny, r.nz, r.w, c, r.partials, ba_smem,
+                               red, blockIdx.x - __ldg(start + p), r.fold_nb);
+}
+
+template <typename T, int MODE>
+__global__ void bag_iter_rows_kernel(const BAGroupRec<T>* __restrict__ recs, int flag_base,
+                                     int it) {
+  __shared__ double scratch[32];
+  constexpr int Q = MODE == BA_MU ? 2 * kMuCand : 2;
+  const BAGroupRec<T>& r = recs[blockIdx.y];
+  if (r.st.flags[flag_base + it] == 0) return;
+  const int nb = r.fold_nb;
+  for (int row = blockIdx.x; row < Q * r.nz; row += gridDim.x) {
+    const double* src = r.partials + (size_t)row * nb;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += src[i];
+    const double sum = block_sum(acc, scratch);
+    if (threadIdx.x == 0) r.totals[row] = sum;
+  }
+}
+
+template <typename T, int MODE>
+__global__ void bag_iter_decide_kernel(const BAGroupRec<T>* __restrict__ recs, int flag_base,
+                                       int it) {
+  const BAGroupRec<T>& r = recs[blockIdx.y];
+  const BAState<T>& st = r.st;
+  if (st.flags[flag_base + it] == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st.flags[ba_flag_count<T>(st.R) - 1] += 1;
+  for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < st.nz; z += gridDim.x * blockDim.x) {
+    if (MODE == BA_MU)
+      ba_mu_level<T, false>(st, r.totals, it, z);
+    else
+      ba_loop_level<T, false>(st, r.totals, it, z);
+  }
+}
+
+// iterations of each persistent phase that a grouped solve runs as flat
+// launches before its cooperative launches take over (in the 256-member
+// ensemble every rescale loop ends within 5 iterations and every shift solve
+// within 2; a field that needs more finishes in its cooperative team)
+constexpr int kGroupFlatRescaleIters = 6;
+constexpr int kGroupFlatMuIters = 3;
 
 struct BAGroupPlan {
   int dtype = 0, n = 0, R = 0;
@@ -2108,6 +2168,12 @@ static int group_prepare(int n, const steam_ba_problem_t* q, int R, void* ws, si
   STEAM_CUDA(cudaFuncSetAttribute(bag_fold_kernel<T, BA_APPLY>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)plan.sm_apply));
+  STEAM_CUDA(cudaFuncSetAttribute(bag_iter_sweep_kernel<T, BA_STATS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)plan.sm_sums));
+  STEAM_CUDA(cudaFuncSetAttribute(bag_iter_sweep_kernel<T, BA_MU>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)plan.sm_sums));
   std::lock_guard<std::mutex> lock(g_group_mu);
   g_groups[ws] = plan;
   return STEAM_OK;
@@ -2129,13 +2195,39 @@ static int group_enqueue(const BAGroupPlan& plan, cudaStream_t s) {
   bag_a0_kernel<T><<<lv, 256, 0, s>>>(recs);
   STEAM_LAUNCH_CHECK("bounded_add group a0");
   auto phase = [&](int mode, int flag_base, int n_iter) -> int {
+    // the first iterations as flat launches over the fields still in the loop
+    // (most fields leave it within them), the rest, if any field is still in
+    // it, as cooperative launches of per-field teams that start there
+    const int n_flat = std::min(n_iter, mode == BA_MU ? kGroupFlatMuIters : kGroupFlatRescaleIters);
+    const unsigned rows = (unsigned)std::min((mode == BA_MU ? 2 * kMuCand : 2) * plan.nz_max, 16);
+    for (int it = 0; it < n_flat; ++it) {
+      if (mode == BA_MU) {
+        bag_iter_sweep_kernel<T, BA_MU><<<plan.fold_blocks, kLvThreads, plan.sm_sums, s>>>(
+            recs, plan.fold_start, n, flag_base, it);
+        STEAM_LAUNCH_CHECK("bounded_add group shift sweep");
+        bag_iter_rows_kernel<T, BA_MU><<<dim3(rows, (unsigned)n), 256, 0, s>>>(recs, flag_base, it);
+        STEAM_LAUNCH_CHECK("bounded_add group shift sums");
+        bag_iter_decide_kernel<T, BA_MU><<<lv, 256, 0, s>>>(recs, flag_base, it);
+        STEAM_LAUNCH_CHECK("bounded_add group shift step");
+      } else {
+        bag_iter_sweep_kernel<T, BA_STATS><<<plan.fold_blocks, kLvThreads, plan.sm_sums, s>>>(
+            recs, plan.fold_start, n, flag_base, it);
+        STEAM_LAUNCH_CHECK("bounded_add group rescale sweep");
+        bag_iter_rows_kernel<T, BA_STATS><<<dim3(rows, (unsigned)n), 256, 0, s>>>(recs, flag_base,
+                                                                                 it);
+        STEAM_LAUNCH_CHECK("bounded_add group rescale sums");
+        bag_iter_decide_kernel<T, BA_STATS><<<lv, 256, 0, s>>>(recs, flag_base, it);
+        STEAM_LAUNCH_CHECK("bounded_add group rescale step");
+      }
+    }
+    if (n_flat >= n_iter) return STEAM_OK;
     auto kern = mode == BA_MU ? bag_phase_kernel<T, BA_MU> : bag_phase_kernel<T, BA_STATS>;
     const auto& batches = mode == BA_MU ? plan.mu_batches : plan.batches;
     const int* starts = mode == BA_MU ? plan.mu_start : plan.ph_start;
     for (const auto& b : batches) {
-      int p0 = b[0], nb = b[1];
+      int p0 = b[0], nb = b[1], it0 = n_flat;
       const int* start = starts + p0;
-      void* args[] = {(void*)&recs, (void*)&start, &p0, &nb, &flag_base, &n_iter};
+      void* args[] = {(void*)&recs, (void*)&start, &p0, &nb, &flag_base, &it0, &n_iter};
       STEAM_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)b[2]),
                                              dim3(kLvThreads), args, plan.sm_sums, s));
       count_launch();
