@@ -8,7 +8,9 @@ FP64 oracle (steam/utils.py:293-427 semantics: x/y circular, z linear) on
 interior-only shapes, partial tiles in every axis, periods shorter than the
 kernel (several wraps in x and y), z thinner than the kernel, odd nz and
 odd y-z planes, input and output at 4-byte offsets; with the input scaling
-prologue, the flux epilogue on a window and the wide store.
+prologue, the flux epilogue on a window and the wide store; and at the
+512 x 512 x 256 configuration's full size, float32 against the float64
+device passes and linear in the input.
 
 Bars: float64 1e-12 relative L2; float32 (float32 arithmetic in every pass)
 1e-6 relative L2 (61 taps per pass, three roundings of intermediates).
@@ -178,3 +180,40 @@ def test_repeat_launches_are_bit_identical(U):
     U.run_plan(plan, f, a)
     U.run_plan(plan, f, b)
     assert torch.equal(a, b)
+
+
+def test_full_size_float32_against_float64_device():
+    """The 512 x 512 x 256 configuration's 61^3 convolution: float32 passes
+    (paired) against the float64 passes (scalar windows, held to 1e-12 of
+    the FP64 oracle above) on the same field, and linear in its input."""
+    import torch
+    shape = (512, 512, 256)
+    g = torch.Generator(device='cuda')
+    g.manual_seed(61)
+    f64 = torch.randn(shape, generator=g, device='cuda', dtype=torch.float64)
+    f32 = f64.float()
+    p32 = U_plan(shape, np.float32)
+    p64 = U_plan(shape, np.float64)
+    from steam_b200 import utils as U
+    o32 = torch.empty_like(f32)
+    o64 = torch.empty_like(f64)
+    U.run_plan(p32, f32, o32)
+    U.run_plan(p64, f32.double(), o64)
+    rel = float(torch.linalg.vector_norm(o32.double() - o64) / torch.linalg.vector_norm(o64))
+    assert rel < BAR[np.float32], rel
+    # linearity: conv(2 f + h) = 2 conv(f) + conv(h)
+    h32 = torch.randn(shape, generator=g, device='cuda', dtype=torch.float32)
+    oh = torch.empty_like(h32)
+    U.run_plan(p32, h32, oh)
+    both = torch.empty_like(h32)
+    U.run_plan(p32, 2.0 * f32 + h32, both)
+    lin = (2.0 * o32.double() + oh.double())
+    rel = float(torch.linalg.vector_norm(both.double() - lin) / torch.linalg.vector_norm(lin))
+    assert rel < 2 * BAR[np.float32], rel
+
+
+def U_plan(shape, dtype):
+    from steam_b200 import utils as U
+    plan = U.plan_convolution(K61, shape, dtype)
+    assert plan.kind == 'separable'
+    return plan
