@@ -4,9 +4,12 @@
 //
 // Kernels the fused forms below do not take run as three passes, each a
 // coalesced stencil over the z-fastest layout:
-//   z-pass: u_c = f (*)_z Z_c                        (32 columns per tile)
-//   y-pass: w_a = sum_p mix_ap (u_c(p) (*)_y Y_b(p))  (64 y x 32 z tiles)
-//   x-pass: out = sum_a w_a (*)_x X_a, with the epilogue (64 x x 32 tiles).
+//   z-pass: u_c = f (*)_z Z_c
+//   y-pass: w_a = sum_p mix_ap (u_c(p) (*)_y Y_b(p))
+//   x-pass: out = sum_a w_a (*)_x X_a, with the epilogue,
+// in float64 (or float32 with scalar windows: tiles 32 columns wide) or, for
+// a plain float32 convolution, paired (f32x2 windows on two adjacent
+// columns: tiles 64 columns wide).
 #include "common.cuh"
 #include "conv.cuh"
 #include <type_traits>
