@@ -7,9 +7,10 @@
 //   z-pass: u_c = f (*)_z Z_c
 //   y-pass: w_a = sum_p mix_ap (u_c(p) (*)_y Y_b(p))
 //   x-pass: out = sum_a w_a (*)_x X_a, with the epilogue,
-// in float64 (or float32 with scalar windows: tiles 32 columns wide) or, for
-// a plain float32 convolution, paired (f32x2 windows on two adjacent
-// columns: tiles 64 columns wide).
+// in float64 with scalar windows (tiles 32 columns wide: float64 fields, and
+// float32 fields under the flux epilogue or the wide store) or, for a plain
+// float32 convolution, paired (f32x2 windows on two adjacent columns: tiles
+// 64 columns wide).
 #include "common.cuh"
 #include "conv.cuh"
 #include <type_traits>
@@ -1546,9 +1547,7 @@ static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t 
     kx<<<grid, kPassThreads, smx2, s>>>(w, nx, ny, (int)nz, kpx, p, out, plane, aligned_out);
     STEAM_LAUNCH_CHECK("conv x-pass");
     *xgrid_out = grid;
-    return STEAM_OK;
-  }
-  {
+  } else {
     const int64_t tiles = nx * ((ny + kYT - 1) / kYT) * ((nz + 31) / 32);
     if (p.nxf <= 2) {
       auto k = ypass_kernel<T, A, 2>;
@@ -1560,11 +1559,9 @@ static int launch_passes(const SepParams<T>& p, int64_t nx, int64_t ny, int64_t 
           u, nx, ny, (int)nz, kpy, p, w, plane);
     }
     STEAM_LAUNCH_CHECK("conv y-pass");
-  }
-  {
-    auto k = xpass_kernel<T, A>;
-    const int grid = stride_grid(xpass_tiles(nx, ny, nz), 1, pass_occupancy(k, smx, 8));
-    k<<<grid, kPassThreads, smx, s>>>(w, nx, ny, (int)nz, kpx, p, out, plane, epi, partials);
+    auto kx = xpass_kernel<T, A>;
+    const int grid = stride_grid(xpass_tiles(nx, ny, nz), 1, pass_occupancy(kx, smx, 8));
+    kx<<<grid, kPassThreads, smx, s>>>(w, nx, ny, (int)nz, kpx, p, out, plane, epi, partials);
     STEAM_LAUNCH_CHECK("conv x-pass");
     *xgrid_out = grid;
   }
