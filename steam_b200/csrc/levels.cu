@@ -759,6 +759,11 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
   for (int q = 0; q < (MODE == BA_MU ? kMuCand : 1); ++q)
 #pragma unroll
     for (int l = 0; l < 4; ++l) cnt[q][l] = 0u;
+  // the shift sweep's terms common to every candidate (a cell inside the caps
+  // for all of them, or beyond one cap for all), added to each candidate's
+  // sums once, after the columns
+  double acc_all[4] = {0.0, 0.0, 0.0, 0.0};
+  unsigned cnt_all[4] = {0u, 0u, 0u, 0u};
   const int64_t ncol = nx * ny;
   auto process = [&](const ColWalk& cw, const V4<T>& dv, const V4<T>& pv) {
     const int64_t i = cw.col * nz + z4;
@@ -800,16 +805,10 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
             constexpr int KC = MODE == BA_MU ? kMuCand : 1;
             const T lo_all = sub_rn(d, s_cmax[z4 + l]), hi_all = sub_rn(d, s_cmin[z4 + l]);
             if (lo_all > clo && hi_all < chi) {
-              const double x = (double)d;
-#pragma unroll
-              for (int k = 0; k < kMuCand; ++k) {
-                acc[k][l] += x;
-                cnt[k % KC][l] += 1u;
-              }
+              acc_all[l] += (double)d;
+              cnt_all[l] += 1u;
             } else if (lo_all >= chi || hi_all <= clo) {
-              const double x = (double)(lo_all >= chi ? chi : clo);
-#pragma unroll
-              for (int k = 0; k < kMuCand; ++k) acc[k][l] += x;
+              acc_all[l] += (double)(lo_all >= chi ? chi : clo);
             } else {
 #pragma unroll
               for (int k = 0; k < kMuCand; ++k) {
@@ -892,6 +891,15 @@ __device__ __forceinline__ void ba_fold_body(T* __restrict__ d0, T* __restrict__
     cp_async_wait<0>();
   }
   if (MODE == BA_APPLY) return;
+  if constexpr (MODE == BA_MU) {
+#pragma unroll
+    for (int k = 0; k < kMuCand; ++k)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        acc[k][l] += acc_all[l];
+        cnt[k][l] += cnt_all[l];
+      }
+  }
   // deterministic reduction: per level, the cpi column slots in order
   const int nb = nvb;
   // partial rows: stats {sum d, sum |d|}; shift {mean_k, count_k} per candidate
