@@ -571,8 +571,8 @@ int steam_set_barrier_spin_limit(int64_t polls);
  * into per-field teams with their own grid barriers, a team's size the
  * field's share of the co-resident capacity.  A field's result is
  * the single call's to rounding (another block partition of its sums); the
- * same group gives the same bits every time.  Every field:
- * nz % 4 == 0 (4 .. 1024), 16-byte aligned pert and increment.
+ * same group gives the same bits every time.  At most 65535 fields; every
+ * field: nz % 4 == 0 (4 .. 1024), 16-byte aligned pert and increment.
  *
  * prepare (synchronous, outside stream capture) lays the group's state out
  * in `workspace` (DEVICE, steam_bounded_add_group_workspace_bytes) and

@@ -2956,6 +2956,8 @@ static int group_check(int dtype, int32_t n, const steam_ba_problem_t* q, int32_
   STEAM_REQUIRE(dtype == STEAM_F32 || dtype == STEAM_F64,
                 "steam_bounded_add_group: bad dtype");
   STEAM_REQUIRE(n >= 1 && q != nullptr, "steam_bounded_add_group: no fields");
+  // the per-field launches index fields by blockIdx.y
+  STEAM_REQUIRE(n <= 65535, "steam_bounded_add_group: more than 65535 fields");
   STEAM_REQUIRE(R >= 0 && R <= 64, "steam_bounded_add_group: n_rescale out of range");
   const size_t elem = dtype == STEAM_F64 ? 8 : 4;
   for (int i = 0; i < n; ++i) {
